@@ -1,0 +1,239 @@
+/* sedona_gpu.h -- C ABI of the B200 implementation of Sedona's implicit
+ * Monte Carlo transport step (packet propagation + per-zone opacity build).
+ *
+ * The boundary is the reference `transport` class (src/transport/transport.h:45-320).
+ * A host `transport` keeps owning its std::vectors; it flattens zone data to
+ * the structure-of-arrays structs below, calls these entry points, and copies
+ * results back into the same vectors it already writes out
+ * (J_nu_, zone e_abs/e_rad/f*_rad, spectrum_array flux/click, opacity tables).
+ *
+ * Conventions
+ *  - Every entry point returns 0 (SED_OK) or a positive sed_status code and
+ *    never exits the process; sed_last_error() gives the message.
+ *  - All pointers in the structs are HOST pointers unless a name ends in
+ *    `_dev`.  Nothing passed in is retained after a call returns.
+ *  - One context = one CUDA stream on one device; calls on a context are
+ *    synchronous with respect to the caller and not re-entrant.
+ *  - Arrays over (zone, frequency) are zone-major: a[zone * n_nu + bin].
+ */
+#ifndef SEDONA_GPU_H
+#define SEDONA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum sed_status {
+  SED_OK = 0,
+  SED_ERR_ARG = 1,       /* invalid argument or inconsistent sizes */
+  SED_ERR_CUDA = 2,      /* CUDA runtime error (message has the CUDA string) */
+  SED_ERR_CAPACITY = 3,  /* packet capacity (particles_max_total) exceeded */
+  SED_ERR_STATE = 4,     /* call out of order (e.g. step before set_grid) */
+  SED_ERR_LIMIT = 5,     /* a packet hit the per-packet segment limit */
+  SED_ERR_NOMEM = 6      /* device allocation failed */
+};
+
+/* Bin-edge array with the semantics of locate_array
+ * (src/utils/locate_array.h:15-217): n bins, `right[i]` is the right wall of
+ * bin i, `min` the left wall of bin 0; bins are closed on the left. */
+enum sed_locate_type { SED_LOC_FLEX = 0, SED_LOC_LIN = 1, SED_LOC_LOG = 2, SED_LOC_NONE = 3 };
+typedef struct sed_locate_grid {
+  int32_t n;
+  int32_t type;          /* enum sed_locate_type */
+  double min;
+  double del;            /* lin: bin width; log: fractional width (1+del ratio) */
+  const double* right;   /* n right walls */
+} sed_locate_grid;
+
+enum sed_grid_type { SED_GRID_1D_SPHERE = 0, SED_GRID_3D_CART = 1 };
+enum sed_precision { SED_PREC_FP64 = 0, SED_PREC_MIXED = 1 };
+
+/* Transport-step parameters: the Lua parameters transport::init reads
+ * (src/transport/transport_init.cpp:82-363) that the step depends on. */
+typedef struct sed_transport_params {
+  int32_t steady_state;          /* transport_steady_iterate > 0 */
+  int32_t radiative_eq;          /* transport_radiative_equilibrium */
+  int32_t boundary_in_reflect;   /* transport_boundary_in_reflect */
+  int32_t boundary_out_reflect;  /* transport_boundary_out_reflect */
+  int32_t store_Jnu;             /* transport_store_Jnu */
+  int32_t omit_scattering;       /* opacity_no_scattering */
+  int32_t core_fix_luminosity;   /* core_fix_luminosity */
+  int32_t tally_forces;          /* 1: tally fx/fy/fz/fr_rad as the reference does */
+  int32_t precision;             /* enum sed_precision: opacity tables FP64 or FP32 */
+  uint32_t rng_seed;             /* transport_rng_seed (Philox key) */
+  int64_t max_particles;         /* particles_max_total */
+  int64_t core_n_emit;           /* core_n_emit */
+  double core_radius;            /* core_radius */
+  double core_luminosity;        /* L_core used for this step (core_luminosity(t)) */
+  double core_temperature;       /* core_temperature */
+  double core_photon_frequency;  /* core_photon_frequency */
+  double fleck_alpha;            /* transport_fleck_alpha */
+  int32_t max_segments;          /* per-packet segment limit; 0 = default (10^7) */
+  int32_t reserved;
+  sed_locate_grid nu_grid;       /* transport_nu_grid */
+  sed_locate_grid spec_time;     /* spectrum_time_grid */
+  sed_locate_grid spec_nu;       /* spectrum_nu_grid */
+  sed_locate_grid spec_mu;       /* mu grid: init(-1, 1, spectrum_n_mu) */
+  sed_locate_grid spec_phi;      /* phi grid: init(0, 2*pi, spectrum_n_phi) */
+} sed_transport_params;
+
+/* Zone geometry and gas state (grid_general + zone, src/grid/grid_general.h:34-147,
+ * src/grid/zone.h:9-50), flattened to structure-of-arrays. */
+typedef struct sed_grid {
+  int32_t type;                  /* enum sed_grid_type */
+  int32_t n_zones;
+  int32_t homologous;            /* hydro_module == "homologous" (v = x/t) */
+  int32_t n_elems;
+  double t_now;                  /* grid time: homologous v = x / t_now */
+  /* 1D sphere: r_out[n_zones] right walls, r_min left wall of zone 0 */
+  double r_min;
+  const double* r_out;
+  const double* v_r;             /* zone outer-edge radial velocity (non-homologous only) */
+  /* 3D Cartesian: nx*ny*nz zones, index i*ny*nz + j*nz + k; each axis is a
+   * locate_array (flex when read from x_out/y_out/z_out, lin when from dr),
+   * src/grid/grid_3D_cart.cpp:120-166 */
+  int32_t nx, ny, nz;
+  sed_locate_grid x_axis, y_axis, z_axis;
+  /* per-zone state */
+  const double* vol;             /* zone volume */
+  const double* rho;
+  const double* T_gas;
+  const double* e_gas;           /* only for the Fleck factor when fleck_alpha != 0 */
+  const double* total_grey_opacity; /* zone total_grey_opacity (cm^2/g); 0 = use microphysics */
+  const double* X;               /* mass fractions [n_zones * n_elems] */
+  const int32_t* elem_Z;         /* [n_elems] */
+  const int32_t* elem_A;         /* [n_elems] */
+} sed_grid;
+
+/* Opacity switches: the opacity_* Lua parameters GasState reads
+ * (src/transport/transport_init.cpp:206-249). */
+typedef struct sed_opacity_params {
+  int32_t use_electron_scattering;
+  int32_t use_free_free;
+  int32_t use_bound_free;
+  int32_t use_line_expansion;
+  int32_t use_fuzz_expansion;
+  int32_t n_atom_zero_epsilon;
+  const int32_t* atom_zero_epsilon;  /* atomic numbers with epsilon = 0 */
+  double epsilon;                /* opacity_epsilon */
+  double maximum_opacity;        /* opacity_maximum_opacity (cm^2/g) */
+  double temp_min, temp_max;     /* limits_temp_min / limits_temp_max */
+  double line_velocity_width;    /* line_velocity_width */
+} sed_opacity_params;
+
+/* Atomic data for the elements of the grid, in elem order (LTE subset of
+ * IndividualAtomData, src/opacity/AtomicData.h:12-158, after the loader's
+ * own post-processing: extra fully-ionized stage appended, E_ion and ic set,
+ * photoionisation tables filled).  Offsets are prefix sums of length n+1. */
+typedef struct sed_atomic_data {
+  int32_t n_atoms;               /* must equal sed_grid.n_elems */
+  const int32_t* ion_off;        /* [n_atoms+1] into ion arrays */
+  const double* ion_chi;         /* ionisation energy (eV) */
+  const int32_t* lev_off;        /* [n_atoms+1] into level arrays */
+  const int32_t* lev_ion;
+  const int32_t* lev_g;
+  const int32_t* lev_ic;         /* level index (within the atom) it ionizes to, -1 none */
+  const double* lev_E;           /* excitation energy (eV) */
+  const double* lev_Eion;        /* ionisation threshold (eV) */
+  const int32_t* photo_off;      /* [total levels + 1] into photo tables */
+  const double* photo_E;         /* photoionisation table abscissae (eV) */
+  const double* photo_s;         /* cross-section (cm^2) */
+  const int32_t* line_off;       /* [n_atoms+1] level-to-level lines */
+  const int32_t* line_l;
+  const int32_t* line_u;
+  const double* line_nu;
+  const double* line_f;
+  const int32_t* fuzz_off;       /* [n_atoms+1] fuzz lines */
+  const double* fuzz_nu;
+  const double* fuzz_gf;
+  const double* fuzz_El;         /* lower-level energy (eV) */
+  const int32_t* fuzz_ion;
+} sed_atomic_data;
+
+typedef struct sed_step_stats {
+  int64_t n_packets;             /* packets propagated this step */
+  int64_t n_escaped;
+  int64_t n_absorbed;
+  int64_t n_stopped;             /* still alive at the end of the step */
+  int64_t n_segments;            /* propagate_monte_carlo loop iterations */
+  int64_t n_scatters;            /* interaction events */
+  int64_t n_limit;               /* packets stopped by the segment limit */
+  int32_t kernel_launches;       /* kernels launched by the call */
+  int32_t reserved;
+  float ms_opacity;              /* device time of the opacity build */
+  float ms_transport;            /* device time of emission + propagation */
+  float ms_total;                /* device time of the whole call */
+  float ms_propagate_kernel;     /* device time of the packet kernel alone */
+} sed_step_stats;
+
+typedef struct sed_ctx sed_ctx;
+
+/* Creates a context on `device` (-1: current device).  Replaces the
+ * allocations of transport::init (src/transport/transport_init.cpp:44-427). */
+int sed_ctx_create(const sed_transport_params* params, int device, sed_ctx** out);
+
+/* Copies zone geometry/state to the device.  Replaces grid->z[] reads on the
+ * hot path (src/grid/grid_1D_sphere.cpp:494-590, grid_3D_cart.cpp:363-469). */
+int sed_set_grid(sed_ctx* ctx, const sed_grid* grid);
+
+/* Copies atomic data and computes line bins with locate_within_bounds
+ * (AtomicData.cpp:851-852).  Replaces AtomicData/GasState::initialize. */
+int sed_set_atomic_data(sed_ctx* ctx, const sed_atomic_data* atoms);
+int sed_set_opacity_params(sed_ctx* ctx, const sed_opacity_params* op);
+
+/* Builds abs/scat opacity, emissivity CDF, n_e, Planck/Rosseland means and
+ * eps_imc for every zone.  Replaces transport::set_opacity
+ * (src/transport/transport_opacity.cpp:21-260) incl. GasState::solve_state and
+ * GasState::computeOpacity. */
+int sed_set_opacity(sed_ctx* ctx, double dt);
+
+/* Loads caller-computed tables instead of sed_set_opacity (abs, scat,
+ * emissivity CDF are [n_zones * n_nu]; eps_imc is [n_zones]; scat may be NULL
+ * when opacity_no_scattering). */
+int sed_load_opacity(sed_ctx* ctx, const double* abs, const double* scat,
+                     const double* emis_cdf, const double* eps_imc);
+
+/* Wipes tallies, emits the core packets, propagates every packet, tallies
+ * escapes and normalises J/e_abs/e_rad.  Replaces transport.cpp:46-124
+ * (wipe_radiation, emit_particles, the propagate loop, spectrum count,
+ * clean_up_particle_vector, steady-state rescale, reduce_radiation). */
+int sed_transport(sed_ctx* ctx, double dt, sed_step_stats* stats);
+
+/* sed_set_opacity followed by sed_transport: transport::step
+ * (src/transport/transport.cpp:26-140) without the temperature solve. */
+int sed_step(sed_ctx* ctx, double dt, sed_step_stats* stats);
+
+/* Results.  Sizes: spectrum n_t*n_nu*n_mu*n_phi (spectrum_array flux/click,
+ * src/transport/spectrum_array.h:28-31); J_nu n_zones*n_nu (or n_zones when
+ * store_Jnu = 0); zone arrays n_zones.  NULL pointers are skipped. */
+int sed_get_spectrum(sed_ctx* ctx, double* flux, double* click);
+int sed_get_zone_tallies(sed_ctx* ctx, double* J_nu, double* e_abs, double* e_rad,
+                         double* fx, double* fy, double* fz, double* fr);
+int sed_get_opacity(sed_ctx* ctx, double* abs, double* scat, double* emis_cdf,
+                    double* n_elec, double* eps_imc, double* planck_mean,
+                    double* rosseland_mean, double* L_thermal);
+
+/* Per-packet outcome records of the last sed_transport (replay parity):
+ * fate (ParticleFate enum, particle.h:9), final zone, number of deviates
+ * drawn after emission, and state {x,y,z,Dx,Dy,Dz,t,e,nu} (t = t_obs for
+ * escaped packets).  Recording costs memory traffic; enable it only for
+ * checks.  Arrays hold n entries. */
+int sed_record_packets(sed_ctx* ctx, int32_t enable);
+int sed_get_packet_records(sed_ctx* ctx, int64_t n, int32_t* fate, int32_t* ind,
+                           int32_t* draws, double* state9);
+
+/* Number of packets carried to the next step (time-dependent runs). */
+int64_t sed_n_particles(sed_ctx* ctx);
+const char* sed_last_error(sed_ctx* ctx);
+void sed_ctx_destroy(sed_ctx* ctx);
+
+/* Library version / build string (never NULL). */
+const char* sed_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

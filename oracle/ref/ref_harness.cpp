@@ -1,0 +1,316 @@
+// oracle/ref/ref_harness.cpp -- TEST INFRASTRUCTURE (oracle harness only).
+//
+// Drives the reference's own `transport` class (src/transport/transport.h)
+// built from its unchanged sources.  Three modes:
+//
+//   replay   one transport step that follows transport::step
+//            (src/transport/transport.cpp:26-140) call for call, except that
+//            before each packet the Philox stand-in for the GSL generator is
+//            pointed at that packet's (seed, packet id, step) stream.  The
+//            reference therefore consumes exactly the uniform deviates the
+//            CUDA packet kernel consumes, and per-packet outcomes (fate, zone,
+//            number of deviates drawn, final phase-space state) can be
+//            compared one for one.
+//   free     transport::step itself, OpenMP threads, free-running streams;
+//            prints the wall time of each step (the timed CPU baseline).
+//   opacity  transport::init + set_opacity only; dumps the opacity tables.
+//
+// Inputs: a Lua parameter file (read by the reference's ParameterReader),
+// the model file it names, and optionally a "store" file whose datasets and
+// attributes are served through the HDF5 stand-in (synthetic atomic data,
+// fuzz line lists, 3-D Cartesian models).
+//
+// Outputs: raw little-endian arrays <out>.<name>.f64 / .i32 / .i64 plus
+// <out>.meta.json describing them.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <limits>
+#include <list>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <omp.h>
+
+#include "hdf5.h"
+#include "hdf5_hl.h"
+#include "shims_control.h"
+
+#define private public
+#define protected public
+#include "transport.h"
+#include "grid_1D_sphere.h"
+#include "grid_3D_cart.h"
+#include "ParameterReader.h"
+#include "physical_constants.h"
+#undef private
+#undef protected
+
+namespace pc = physical_constants;
+
+namespace {
+
+struct Out {
+  std::string prefix;
+  std::ostringstream meta;
+  bool first = true;
+  void arr(const std::string& name, const void* p, size_t bytes, const char* ext, size_t count)
+  {
+    std::string fn = prefix + "." + name + "." + ext;
+    FILE* f = std::fopen(fn.c_str(), "wb");
+    if (!f) { std::perror(fn.c_str()); std::exit(2); }
+    if (bytes) std::fwrite(p, 1, bytes, f);
+    std::fclose(f);
+    meta << (first ? "" : ",") << "\n  \"" << name << "\": {\"file\": \"" << fn << "\", \"type\": \"" << ext
+         << "\", \"count\": " << count << "}";
+    first = false;
+  }
+  void f64(const std::string& n, const std::vector<double>& v) { arr(n, v.data(), v.size() * 8, "f64", v.size()); }
+  void i32(const std::string& n, const std::vector<int32_t>& v) { arr(n, v.data(), v.size() * 4, "i32", v.size()); }
+  void i64(const std::string& n, const std::vector<int64_t>& v) { arr(n, v.data(), v.size() * 8, "i64", v.size()); }
+  std::ostringstream scalars;
+  bool sfirst = true;
+  void scalar(const std::string& n, double v)
+  {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%.17g", v);
+    scalars << (sfirst ? "" : ", ") << "\"" << n << "\": " << buf;
+    sfirst = false;
+  }
+  void finish()
+  {
+    std::string fn = prefix + ".meta.json";
+    std::ofstream f(fn);
+    f << "{\"arrays\": {" << meta.str() << "\n},\n \"scalars\": {" << scalars.str() << "}}\n";
+  }
+};
+
+// Store file: sequence of records
+//   u8 kind (0 = f64 dataset, 1 = i32 dataset, 2 = i32 attribute)
+//   u32 n + bytes: file name;  u32 n + bytes: object path
+//   kind 2: u32 n + bytes attribute name; i32 value
+//   kind 0/1: u32 rank; u64 dims[rank]; u64 count; payload
+void load_store(const char* path)
+{
+  FILE* f = std::fopen(path, "rb");
+  if (!f) { std::perror(path); std::exit(2); }
+  auto rd = [&](void* p, size_t n) { if (std::fread(p, 1, n, f) != n) { std::fprintf(stderr, "truncated store\n"); std::exit(2); } };
+  auto rstr = [&]() { uint32_t n; rd(&n, 4); std::string s(n, '\0'); if (n) rd(&s[0], n); return s; };
+  for (;;) {
+    uint8_t kind;
+    if (std::fread(&kind, 1, 1, f) != 1) break;
+    std::string file = rstr(), obj = rstr();
+    if (kind == 2) {
+      std::string attr = rstr();
+      int32_t v; rd(&v, 4);
+      oracle_h5_put_attr_int(file.c_str(), obj.c_str(), attr.c_str(), v);
+      continue;
+    }
+    uint32_t rank; rd(&rank, 4);
+    std::vector<hsize_t> dims(rank);
+    for (uint32_t k = 0; k < rank; ++k) { uint64_t d; rd(&d, 8); dims[k] = d; }
+    uint64_t n; rd(&n, 8);
+    if (kind == 0) {
+      std::vector<double> v(n); if (n) rd(v.data(), n * 8);
+      oracle_h5_put_double(file.c_str(), obj.c_str(), v.data(), n, (int)rank, dims.data());
+    } else {
+      std::vector<int32_t> v(n); if (n) rd(v.data(), n * 4);
+      oracle_h5_put_int(file.c_str(), obj.c_str(), v.data(), n, (int)rank, dims.data());
+    }
+  }
+  std::fclose(f);
+}
+
+double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+// number of deviates emit_inner_source takes per packet (src/transport/emission.cpp:399-473)
+uint32_t core_draws_per_packet(transport& t)
+{
+  uint32_t k = (t.r_core_ == 0) ? 2 : 4;  // direction (and position on the core)
+  if (!(t.core_frequency_ > 0)) k += 2;    // frequency bin + position in bin
+  return k + 1;                            // emission time
+}
+
+void dump_tables(transport& t, Out& o)
+{
+  grid_general* g = t.grid;
+  int nz = g->n_zones, nn = t.nu_grid_.size();
+  std::vector<double> ab((size_t)nz * nn), sc((size_t)nz * nn, 0.0), em((size_t)nz * nn), j((size_t)nz * (t.store_Jnu_ ? nn : 1));
+  for (int i = 0; i < nz; ++i) {
+    for (int k = 0; k < nn; ++k) {
+      ab[(size_t)i * nn + k] = t.abs_opacity_[i][k];
+      if (!t.omit_scattering_) sc[(size_t)i * nn + k] = t.scat_opacity_[i][k];
+      em[(size_t)i * nn + k] = t.emissivity_[i].get(k);
+    }
+    for (size_t k = 0; k < t.J_nu_[i].size(); ++k) j[(size_t)i * t.J_nu_[i].size() + k] = t.J_nu_[i][k];
+  }
+  std::vector<double> ne(nz), pm(nz), rm(nz), lth(nz), epsimc(nz), eabs(nz), erad(nz), fx(nz), fy(nz), fz(nz), fr(nz), tg(nz);
+  for (int i = 0; i < nz; ++i) {
+    ne[i] = g->z[i].n_elec; pm[i] = t.planck_mean_opacity_[i]; rm[i] = t.rosseland_mean_opacity_[i];
+    lth[i] = g->z[i].L_thermal; epsimc[i] = g->z[i].eps_imc; eabs[i] = g->z[i].e_abs; erad[i] = g->z[i].e_rad;
+    fx[i] = g->z[i].fx_rad; fy[i] = g->z[i].fy_rad; fz[i] = g->z[i].fz_rad; fr[i] = g->z[i].fr_rad; tg[i] = g->z[i].T_gas;
+  }
+  std::vector<double> nu(nn), nul(nn);
+  for (int k = 0; k < nn; ++k) { nu[k] = t.nu_grid_[k]; nul[k] = t.nu_grid_.left(k); }
+  o.f64("abs", ab); o.f64("scat", sc); o.f64("emis_cdf", em); o.f64("J_nu", j);
+  o.f64("n_elec", ne); o.f64("planck_mean", pm); o.f64("rosseland_mean", rm); o.f64("L_thermal", lth);
+  o.f64("eps_imc", epsimc); o.f64("e_abs", eabs); o.f64("e_rad", erad);
+  o.f64("fx_rad", fx); o.f64("fy_rad", fy); o.f64("fz_rad", fz); o.f64("fr_rad", fr); o.f64("T_gas", tg);
+  o.f64("nu_right", nu); o.f64("nu_left", nul);
+  o.f64("spec_flux", t.optical_spectrum.flux);
+  o.f64("spec_click", t.optical_spectrum.click);
+  o.scalar("n_zones", nz); o.scalar("n_nu", nn); o.scalar("t_now", t.t_now_);
+  o.scalar("spec_n_t", t.optical_spectrum.time_grid.size());
+  o.scalar("spec_n_nu", t.optical_spectrum.wave_grid.size());
+  o.scalar("spec_n_mu", t.optical_spectrum.mu_grid.size());
+  o.scalar("spec_n_phi", t.optical_spectrum.phi_grid.size());
+}
+
+// transport::step (src/transport/transport.cpp:26-140) with per-packet
+// stream selection; returns the number of escaped packets
+int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, int threads)
+{
+  if (t.steady_state) dt = 1;
+  t.set_opacity(dt);
+  t.reduce_opacities();
+  t.reduce_Lthermal();
+  if (t.use_ddmc_) { std::fprintf(stderr, "replay: DDMC is not on the replayed path\n"); std::exit(3); }
+  t.wipe_radiation();
+
+  const size_t n_before = t.particles.size();
+  if (n_before != 0) { std::fprintf(stderr, "replay: expected an empty packet list\n"); std::exit(3); }
+  const uint32_t K = core_draws_per_packet(t);
+  oracle_rng_emission(seed, 0, step, K);
+  t.emit_particles(dt);
+  const size_t n = t.particles.size();
+  if (oracle_rng_emission_draws() != (uint64_t)K * n) {
+    std::fprintf(stderr, "replay: emission drew %llu deviates for %zu packets (expected %u each); only core emission is replayable\n",
+                 (unsigned long long)oracle_rng_emission_draws(), n, K);
+    std::exit(3);
+  }
+
+  std::vector<int32_t> fate(n), ind(n), draws(n), spec_bin(n, -1);
+  std::vector<double> st((size_t)n * 9);
+  const double T0 = now();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+  for (long i = 0; i < (long)n; ++i) {
+    particle& p = t.particles[i];
+    oracle_rng_packet(seed, (uint64_t)i, step, K);
+    p.fate = t.propagate(p, dt);
+    draws[i] = (int32_t)(oracle_rng_packet_draws() - K);
+    if (p.fate == escaped) {
+      double t_obs = p.t - p.x_dot_d() / pc::c;
+      if (p.type == photon) t.optical_spectrum.count(t_obs, p.nu, p.e, p.D);
+      p.t = t_obs;
+    }
+    fate[i] = (int32_t)p.fate; ind[i] = p.ind;
+    double* s = &st[(size_t)i * 9];
+    s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2]; s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+    s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+  }
+  const double T1 = now();
+  int n_escaped = t.clean_up_particle_vector();
+  if (t.steady_state && t.core_fix_luminosity_) {
+    double per_esc = (1.0 * n_escaped) / (1.0 * n);
+    double fac = 1.0 / per_esc;
+    t.optical_spectrum.rescale(fac);
+    for (int i = 0; i < t.grid->n_zones; ++i) {
+      t.grid->z[i].e_rad *= fac;
+      if (t.store_Jnu_)
+        for (size_t j = 0; j < (size_t)t.nu_grid_.size(); ++j) t.J_nu_[i][j] *= fac;
+    }
+  }
+  t.reduce_radiation(dt);
+  o.i32("pkt_fate", fate); o.i32("pkt_ind", ind); o.i32("pkt_draws", draws); o.f64("pkt_state", st);
+  o.scalar("n_packets", (double)n); o.scalar("n_escaped", n_escaped); o.scalar("propagate_seconds", T1 - T0);
+  o.scalar("draws_per_emitted_packet", K);
+  return n_escaped;
+}
+
+void usage()
+{
+  std::fprintf(stderr,
+               "usage: sedona_ref <replay|free|opacity> <param.lua> <out_prefix> [--store FILE] [--seed S]\n"
+               "                  [--step N] [--steps N] [--threads T] [--dt DT]\n");
+  std::exit(1);
+}
+}  // namespace
+
+int main(int argc, char** argv)
+{
+  if (argc < 4) usage();
+  std::string mode = argv[1], pfile = argv[2];
+  Out o;
+  o.prefix = argv[3];
+  uint32_t seed = 0, step = 0;
+  int steps = 1, threads = omp_get_max_threads();
+  double dt = 1.0;
+  for (int a = 4; a < argc; ++a) {
+    std::string k = argv[a];
+    if (a + 1 >= argc) usage();
+    std::string v = argv[++a];
+    if (k == "--store") load_store(v.c_str());
+    else if (k == "--seed") seed = (uint32_t)std::stoul(v);
+    else if (k == "--step") step = (uint32_t)std::stoul(v);
+    else if (k == "--steps") steps = std::stoi(v);
+    else if (k == "--threads") threads = std::stoi(v);
+    else if (k == "--dt") dt = std::stod(v);
+    else usage();
+  }
+  omp_set_num_threads(threads);
+
+  ParameterReader params(pfile, 0);
+  std::string grid_type = params.getScalar<std::string>("grid_type");
+  grid_general* grid = nullptr;
+  if (grid_type == "grid_1D_sphere") grid = new grid_1D_sphere;
+  else if (grid_type == "grid_3D_cart") grid = new grid_3D_cart;
+  else { std::fprintf(stderr, "unsupported grid_type %s\n", grid_type.c_str()); return 3; }
+  grid->init(&params);
+
+  transport t;
+  const double Ti0 = now();
+  t.init(&params, grid);
+  const double Ti1 = now();
+  o.scalar("init_seconds", Ti1 - Ti0);
+  o.scalar("threads", threads);
+
+  if (mode == "opacity") {
+    double dtt = t.steady_state ? 1.0 : dt;
+    const double T0 = now();
+    t.set_opacity(dtt);
+    const double T1 = now();
+    t.reduce_opacities();
+    o.scalar("set_opacity_seconds", T1 - T0);
+    dump_tables(t, o);
+  } else if (mode == "replay") {
+    replay_step(t, dt, seed, step, o, threads);
+    dump_tables(t, o);
+  } else if (mode == "free") {
+    oracle_rng_free_running();
+    std::vector<double> times, opac_times;
+    for (int s = 0; s < steps; ++s) {
+      const double T0 = now();
+      t.step(dt);
+      const double T1 = now();
+      times.push_back(T1 - T0);
+    }
+    // separately time the opacity build alone (set_opacity is the first phase of step)
+    const double T2 = now();
+    t.set_opacity(t.steady_state ? 1.0 : dt);
+    const double T3 = now();
+    opac_times.push_back(T3 - T2);
+    o.f64("step_seconds", times);
+    o.f64("set_opacity_seconds", opac_times);
+    dump_tables(t, o);
+  } else {
+    usage();
+  }
+  o.finish();
+  return 0;
+}

@@ -1,0 +1,1304 @@
+/* oracle/sed_oracle.c -- TEST INFRASTRUCTURE (the oracle; never shipped).
+ *
+ * Plain-C restatement of the reference's implicit Monte Carlo transport step
+ * for the functions on the GPU hot path.  Every function names the reference
+ * file:line it follows (paths relative to the reference checkout).  The
+ * arithmetic is written in the same order as the reference so that, compiled
+ * without floating-point contraction, results match the reference bit for bit
+ * up to the last-ulp behaviour of libm (log, exp, pow, sin, cos, atan2).
+ *
+ * Random numbers: the reference draws from per-thread GSL generators
+ * (src/transport/thread_RNG.cpp:91-99); here draw n of packet p comes from the
+ * Philox4x32-10 stream (seed, p, step) defined in oracle/philox.h, which the
+ * reference harness (oracle/ref) also installs in place of GSL.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "sed_oracle.h"
+#include "philox.h"
+
+/* physical constants, src/utils/physical_constants.h:9-31 (pi is 3.14159 there) */
+#define PC_PI 3.14159
+#define PC_C 2.99792458e10
+#define PC_H 6.6260755e-27
+#define PC_K 1.380658e-16
+#define PC_K_EV 8.6173324e-5
+#define PC_M_P 1.67262158e-24
+#define PC_M_E 9.10938188e-28
+#define PC_SB 5.6704e-5
+#define PC_A 7.5657e-15
+#define PC_THOMSON 0.66523e-24
+#define PC_SIGMA_TOT 0.0265400193567
+#define PC_ERGS_TO_EV 624150975230.2815
+
+enum { F_MOVING = 0, F_STOPPED = 1, F_ESCAPED = 2, F_ABSORBED = 3 };
+
+typedef struct {
+  int n, type;
+  double min, del;
+  double* x;
+} lgrid;
+
+typedef struct {
+  double x[3], D[3], t, e, nu, dvds;
+  int ind;
+  int fate;
+  uint64_t pid;
+  uint32_t n;  /* next deviate index */
+} packet;
+
+struct oracle_ctx {
+  sed_transport_params tp;
+  lgrid nu, st, sn, sm, sp;
+  /* grid */
+  int have_grid, gtype, nzones, homologous, nelem;
+  double t_grid, r_min;
+  lgrid r_out;
+  double* v_r;
+  int nx, ny, nz;
+  lgrid ax[3];
+  double *vol, *rho, *T, *e_gas, *grey, *X;
+  int *eZ, *eA;
+  /* atomic data */
+  int have_atoms;
+  int natoms;
+  int *ion_off, *lev_off, *lev_ion, *lev_g, *lev_ic, *photo_off, *line_off, *line_l, *line_u, *line_bin;
+  double *ion_chi, *lev_E, *lev_Eion, *photo_E, *photo_s, *line_nu, *line_f;
+  int *fuzz_off, *fuzz_ion, *fuzz_bin;
+  double *fuzz_nu, *fuzz_gf, *fuzz_El;
+  sed_opacity_params op;
+  int* zero_eps;
+  /* tables */
+  int have_opacity;
+  double *abs, *scat, *cdf, *eps_imc, *n_elec, *planck, *ross, *L_th;
+  double core_cdf_dummy;
+  double* core_cdf;
+  /* tallies */
+  double *J, *e_abs, *e_rad, *fx, *fy, *fz, *fr;
+  double *flux, *click;
+  int64_t nspec;
+  int64_t n_escaped_acc, n_active_acc;
+  /* records */
+  int record;
+  int64_t nrec;
+  int32_t *r_fate, *r_ind, *r_draws;
+  double* r_state;
+  uint32_t step;
+  char err[256];
+};
+
+static int fail(oracle_ctx* o, int code, const char* msg)
+{
+  snprintf(o->err, sizeof o->err, "%s", msg);
+  return code;
+}
+
+/* ---------------------------------------------------------------- locate_array */
+static void lgrid_copy(lgrid* g, const sed_locate_grid* s)
+{
+  free(g->x);
+  g->n = s->n; g->type = s->type; g->min = s->min; g->del = s->del;
+  g->x = (double*)malloc(sizeof(double) * (size_t)(s->n > 0 ? s->n : 1));
+  for (int i = 0; i < s->n; ++i) g->x[i] = s->right[i];
+}
+static double lg_left(const lgrid* g, int i) { return i == 0 ? g->min : g->x[i - 1]; } /* locate_array.h:60-62 */
+static double lg_delta(const lgrid* g, int i) { return i == 0 ? g->x[0] - g->min : g->x[i] - g->x[i - 1]; } /* :69-72 */
+static double lg_center(const lgrid* g, int i) { return i == 0 ? 0.5 * (g->min + g->x[0]) : 0.5 * (g->x[i - 1] + g->x[i]); } /* :54-57 */
+static int upper_bound_d(const double* a, int n, double v)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) { int m = lo + (hi - lo) / 2; if (a[m] <= v) lo = m + 1; else hi = m; }
+  return lo;
+}
+/* locate_array::locate, src/utils/locate_array.cpp:191-218 */
+static int lg_locate(const lgrid* g, double xv)
+{
+  if (g->n == 1) return 0;
+  if (xv >= g->x[g->n - 1]) return g->n;
+  if (xv < g->min) return 0;
+  int ind;
+  if (g->type == SED_LOC_FLEX) ind = upper_bound_d(g->x, g->n, xv);
+  else if (g->type == SED_LOC_LIN) ind = (int)floor((xv - g->min) / g->del);
+  else if (g->type == SED_LOC_LOG) ind = (int)floor(log(xv / g->min) / log(1 + g->del));
+  else ind = 0;
+  if (g->type != SED_LOC_NONE && ind != 0 && ind != g->n && (lg_left(g, ind) > xv || g->x[ind] <= xv))
+    ind = upper_bound_d(g->x, g->n, xv);
+  return ind;
+}
+/* locate_array::locate_within_bounds, locate_array.cpp:225-230 */
+static int lg_locate_wb(const lgrid* g, double xv)
+{
+  int ind = lg_locate(g, xv);
+  if (ind == g->n) return g->n - 1;
+  return ind;
+}
+/* locate_array::sample, locate_array.cpp:237-242 */
+static double lg_sample(const lgrid* g, int i, double r)
+{
+  if (g->n == 1) return 0;
+  if (i == 0) return g->min + (g->x[0] - g->min) * r;
+  return g->x[i - 1] + (g->x[i] - g->x[i - 1]) * r;
+}
+int oracle_locate(const sed_locate_grid* s, double x)
+{
+  lgrid g = {0};
+  lgrid_copy(&g, s);
+  int r = lg_locate(&g, x);
+  free(g.x);
+  return r;
+}
+
+/* cdf_array::sample, src/transport/cdf_array.h:84-89 */
+static int cdf_sample(const double* y, int n, double u)
+{
+  if (n == 1) return 0;
+  return upper_bound_d(y, n, u);
+}
+/* cdf_array::normalize, cdf_array.h:62-75 */
+static void cdf_normalize(double* y, int n)
+{
+  for (int i = 0; i < n; ++i) if (isnan(y[i])) y[i] = 0;
+  if (y[n - 1] == 0) for (int i = 0; i < n; ++i) y[i] = 1.0;
+  double N = y[n - 1];
+  for (int i = 0; i < n; ++i) y[i] /= N;
+}
+
+/* ---------------------------------------------------------------- context */
+int oracle_ctx_create(const sed_transport_params* p, oracle_ctx** out)
+{
+  if (!p || !out) return SED_ERR_ARG;
+  oracle_ctx* o = (oracle_ctx*)calloc(1, sizeof(oracle_ctx));
+  o->tp = *p;
+  lgrid_copy(&o->nu, &p->nu_grid);
+  lgrid_copy(&o->st, &p->spec_time);
+  lgrid_copy(&o->sn, &p->spec_nu);
+  lgrid_copy(&o->sm, &p->spec_mu);
+  lgrid_copy(&o->sp, &p->spec_phi);
+  o->nspec = (int64_t)o->st.n * o->sn.n * o->sm.n * o->sp.n;
+  o->flux = (double*)calloc((size_t)o->nspec, sizeof(double));
+  o->click = (double*)calloc((size_t)o->nspec, sizeof(double));
+  /* core emission spectrum, transport::setup_core_emission
+   * (src/transport/transport_init.cpp:465-556), blackbody branch */
+  int nn = o->nu.n;
+  o->core_cdf = (double*)calloc((size_t)nn, sizeof(double));
+  for (int j = 0; j < nn; ++j) {
+    double nu = lg_center(&o->nu, j), dnu = lg_delta(&o->nu, j);
+    double bb;
+    if (p->core_temperature <= 0) bb = 1;
+    else {
+      double zeta = PC_H * nu / PC_K / p->core_temperature;  /* blackbody_nu, transport_opacity.cpp:322-326 */
+      bb = 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (exp(zeta) - 1);
+    }
+    double w = bb * dnu * 1.0;  /* emissivity_weight_ = 1 (transport_init.cpp:322-332) */
+    o->core_cdf[j] = (j == 0) ? w : o->core_cdf[j - 1] + w;
+  }
+  cdf_normalize(o->core_cdf, nn);
+  *out = o;
+  return SED_OK;
+}
+
+static void free_grid(oracle_ctx* o)
+{
+  free(o->r_out.x); o->r_out.x = NULL;
+  for (int a = 0; a < 3; ++a) { free(o->ax[a].x); o->ax[a].x = NULL; }
+  free(o->v_r); free(o->vol); free(o->rho); free(o->T); free(o->e_gas); free(o->grey); free(o->X);
+  free(o->eZ); free(o->eA);
+  free(o->J); free(o->e_abs); free(o->e_rad); free(o->fx); free(o->fy); free(o->fz); free(o->fr);
+  free(o->abs); free(o->scat); free(o->cdf); free(o->eps_imc); free(o->n_elec); free(o->planck); free(o->ross); free(o->L_th);
+  o->v_r = o->vol = o->rho = o->T = o->e_gas = o->grey = o->X = NULL;
+  o->eZ = o->eA = NULL;
+}
+
+static double* dup_d(const double* s, size_t n, double fill)
+{
+  double* d = (double*)malloc(sizeof(double) * (n ? n : 1));
+  for (size_t i = 0; i < n; ++i) d[i] = s ? s[i] : fill;
+  return d;
+}
+static int* dup_i(const int32_t* s, size_t n)
+{
+  int* d = (int*)malloc(sizeof(int) * (n ? n : 1));
+  for (size_t i = 0; i < n; ++i) d[i] = s ? s[i] : 0;
+  return d;
+}
+
+int oracle_set_grid(oracle_ctx* o, const sed_grid* g)
+{
+  if (!o || !g || g->n_zones <= 0) return SED_ERR_ARG;
+  free_grid(o);
+  o->gtype = g->type;
+  o->nzones = g->n_zones;
+  o->homologous = g->homologous;
+  o->nelem = g->n_elems;
+  o->t_grid = g->t_now;
+  size_t nz = (size_t)g->n_zones;
+  if (g->type == SED_GRID_1D_SPHERE) {
+    sed_locate_grid rg = {g->n_zones, SED_LOC_FLEX, g->r_min, 0.0, g->r_out};
+    memset(&o->r_out, 0, sizeof o->r_out);
+    lgrid_copy(&o->r_out, &rg);
+    o->r_min = g->r_min;
+    o->v_r = dup_d(g->v_r, nz, 0.0);
+  } else if (g->type == SED_GRID_3D_CART) {
+    if ((int64_t)g->nx * g->ny * g->nz != g->n_zones) return fail(o, SED_ERR_ARG, "nx*ny*nz != n_zones");
+    o->nx = g->nx; o->ny = g->ny; o->nz = g->nz;
+    memset(o->ax, 0, sizeof o->ax);
+    lgrid_copy(&o->ax[0], &g->x_axis);
+    lgrid_copy(&o->ax[1], &g->y_axis);
+    lgrid_copy(&o->ax[2], &g->z_axis);
+  } else {
+    return fail(o, SED_ERR_ARG, "unsupported grid type");
+  }
+  o->vol = dup_d(g->vol, nz, 0.0);
+  o->rho = dup_d(g->rho, nz, 0.0);
+  o->T = dup_d(g->T_gas, nz, 0.0);
+  o->e_gas = dup_d(g->e_gas, nz, 0.0);
+  o->grey = dup_d(g->total_grey_opacity, nz, 0.0);
+  o->X = dup_d(g->X, nz * (size_t)(g->n_elems > 0 ? g->n_elems : 0), 0.0);
+  o->eZ = dup_i(g->elem_Z, (size_t)g->n_elems);
+  o->eA = dup_i(g->elem_A, (size_t)g->n_elems);
+  size_t nn = (size_t)o->nu.n;
+  size_t nj = o->tp.store_Jnu ? nn : 1;
+  o->J = (double*)calloc(nz * nj, sizeof(double));
+  o->e_abs = (double*)calloc(nz, sizeof(double));
+  o->e_rad = (double*)calloc(nz, sizeof(double));
+  o->fx = (double*)calloc(nz, sizeof(double));
+  o->fy = (double*)calloc(nz, sizeof(double));
+  o->fz = (double*)calloc(nz, sizeof(double));
+  o->fr = (double*)calloc(nz, sizeof(double));
+  o->abs = (double*)calloc(nz * nn, sizeof(double));
+  o->scat = (double*)calloc(nz * nn, sizeof(double));
+  o->cdf = (double*)calloc(nz * nn, sizeof(double));
+  o->eps_imc = (double*)calloc(nz, sizeof(double));
+  o->n_elec = (double*)calloc(nz, sizeof(double));
+  o->planck = (double*)calloc(nz, sizeof(double));
+  o->ross = (double*)calloc(nz, sizeof(double));
+  o->L_th = (double*)calloc(nz, sizeof(double));
+  o->have_grid = 1;
+  o->have_opacity = 0;
+  return SED_OK;
+}
+
+int oracle_set_opacity_params(oracle_ctx* o, const sed_opacity_params* op)
+{
+  if (!o || !op) return SED_ERR_ARG;
+  o->op = *op;
+  free(o->zero_eps);
+  o->zero_eps = dup_i(op->atom_zero_epsilon, (size_t)op->n_atom_zero_epsilon);
+  o->op.atom_zero_epsilon = o->zero_eps;
+  return SED_OK;
+}
+
+int oracle_set_atomic_data(oracle_ctx* o, const sed_atomic_data* a)
+{
+  if (!o || !a || a->n_atoms < 0) return SED_ERR_ARG;
+  int na = a->n_atoms;
+  o->natoms = na;
+  o->ion_off = dup_i(a->ion_off, (size_t)na + 1);
+  o->lev_off = dup_i(a->lev_off, (size_t)na + 1);
+  o->line_off = dup_i(a->line_off, (size_t)na + 1);
+  o->fuzz_off = dup_i(a->fuzz_off, (size_t)na + 1);
+  size_t ni = (size_t)o->ion_off[na], nl = (size_t)o->lev_off[na];
+  size_t nli = (size_t)o->line_off[na], nf = (size_t)o->fuzz_off[na];
+  o->ion_chi = dup_d(a->ion_chi, ni, 0.0);
+  o->lev_ion = dup_i(a->lev_ion, nl);
+  o->lev_g = dup_i(a->lev_g, nl);
+  o->lev_ic = dup_i(a->lev_ic, nl);
+  o->lev_E = dup_d(a->lev_E, nl, 0.0);
+  o->lev_Eion = dup_d(a->lev_Eion, nl, 0.0);
+  o->photo_off = dup_i(a->photo_off, nl + 1);
+  size_t np = (size_t)o->photo_off[nl];
+  o->photo_E = dup_d(a->photo_E, np, 0.0);
+  o->photo_s = dup_d(a->photo_s, np, 0.0);
+  o->line_l = dup_i(a->line_l, nli);
+  o->line_u = dup_i(a->line_u, nli);
+  o->line_nu = dup_d(a->line_nu, nli, 0.0);
+  o->line_f = dup_d(a->line_f, nli, 0.0);
+  o->line_bin = (int*)malloc(sizeof(int) * (nli ? nli : 1));
+  for (size_t i = 0; i < nli; ++i) o->line_bin[i] = lg_locate_wb(&o->nu, o->line_nu[i]); /* AtomicData.cpp:680 */
+  o->fuzz_nu = dup_d(a->fuzz_nu, nf, 0.0);
+  o->fuzz_gf = dup_d(a->fuzz_gf, nf, 0.0);
+  o->fuzz_El = dup_d(a->fuzz_El, nf, 0.0);
+  o->fuzz_ion = dup_i(a->fuzz_ion, nf);
+  o->fuzz_bin = (int*)malloc(sizeof(int) * (nf ? nf : 1));
+  for (size_t i = 0; i < nf; ++i) o->fuzz_bin[i] = lg_locate_wb(&o->nu, o->fuzz_nu[i]); /* AtomicData.cpp:851 */
+  o->have_atoms = 1;
+  return SED_OK;
+}
+
+int oracle_get_fuzz_bins(oracle_ctx* o, int32_t* bins)
+{
+  if (!o || !o->have_atoms) return SED_ERR_STATE;
+  for (int i = 0; i < o->fuzz_off[o->natoms]; ++i) bins[i] = o->fuzz_bin[i];
+  return SED_OK;
+}
+
+/* ---------------------------------------------------------------- LTE gas state */
+typedef struct {
+  double* ion_part;  /* per atom ions */
+  double* ion_frac;
+  double* lev_n;
+  double* n_dens;    /* per atom */
+  double* mass_frac;
+  double dens, temp, mu_I, n_elec, time;
+  int solve_error;
+} gas;
+
+/* AtomicSpecies::solve_lte, src/opacity/AtomicSpecies_state.cpp:56-123 */
+static void solve_lte(oracle_ctx* o, gas* g, int a, double ne)
+{
+  int i0 = o->ion_off[a], ni = o->ion_off[a + 1] - i0;
+  int l0 = o->lev_off[a], nl = o->lev_off[a + 1] - l0;
+  double T = g->temp;
+  double* part = g->ion_part + i0;
+  double* frac = g->ion_frac + i0;
+  double* lev = g->lev_n + l0;
+  for (int i = 0; i < ni; ++i) part[i] = 0;
+  for (int i = 0; i < nl; ++i) {
+    double E = o->lev_E[l0 + i];
+    int gg = o->lev_g[l0 + i];
+    int ion = o->lev_ion[l0 + i];
+    lev[i] = gg * exp(-E / PC_K_EV / T);
+    part[ion] += lev[i];
+  }
+  double lt = PC_H * PC_H / (2.0 * PC_PI * PC_M_E * PC_K * T);
+  double fac = 2 / ne / pow(lt, 1.5);
+  frac[0] = 1.;
+  double norm = 1.;
+  for (int i = 1; i < ni; ++i) {
+    double chi = o->ion_chi[i0 + i - 1];
+    double saha = exp(-1.0 * chi / PC_K_EV / T);
+    saha = saha * (part[i] / part[i - 1]) * fac;
+    frac[i] = saha * frac[i - 1];
+    if (ne < 1e-50) frac[i] = 0;
+    norm = 0;
+    for (int j = 0; j <= i; j++) norm += frac[j];
+    for (int j = 0; j <= i; j++) frac[j] = frac[j] / norm;
+  }
+  for (int i = 0; i < nl; ++i) {
+    double E = o->lev_E[l0 + i];
+    int gg = o->lev_g[l0 + i];
+    int ion = o->lev_ion[l0 + i];
+    double Z = part[ion];
+    double f = frac[ion];
+    lev[i] = f * gg * exp(-E / PC_K_EV / T) / Z;
+    if (lev[i] < 1e-30) lev[i] = 1e-30; /* min_level_pop_, AtomicSpecies_init.cpp:36 */
+  }
+}
+
+/* GasState::charge_conservation, src/opacity/GasState.cpp:242-263 */
+static double charge_conservation(oracle_ctx* o, gas* g, double ne)
+{
+  double f = 0;
+  for (int a = 0; a < o->natoms; ++a) {
+    solve_lte(o, g, a, ne);
+    int l0 = o->lev_off[a], nl = o->lev_off[a + 1] - l0;
+    double x = 0; /* AtomicSpecies::get_net_ion_fraction, AtomicSpecies.h:125-131 */
+    for (int i = 0; i < nl; ++i) x += g->lev_n[l0 + i] * o->lev_ion[l0 + i];
+    f += g->dens * g->mass_frac[a] / (o->eA[a] * PC_M_P) * x;
+  }
+  return f - ne;
+}
+
+#define SIGN(a, b) ((b) >= 0.0 ? fabs(a) : -fabs(a))
+/* GasState::ne_brent_method, src/opacity/GasState.cpp:270-337.  Also returns
+ * the last electron density the charge function was evaluated at: the atoms'
+ * populations the opacities use are those of that last evaluation. */
+static double ne_brent(oracle_ctx* o, gas* g, double x1, double x2, double tol, double* last)
+{
+  int ITMAX = 100;
+  double EPS = 3.0e-8;
+  double a = x1, b = x2, c = x2, d = 0, e = 0, min1, min2;
+  double fa = charge_conservation(o, g, a);
+  double fb = charge_conservation(o, g, b);
+  *last = b;
+  double fc, p, q, r, s, tol1, xm;
+  if ((fa > 0.0 && fb > 0.0) || (fa < 0.0 && fb < 0.0)) g->solve_error = 1;
+  fc = fb;
+  for (int iter = 1; iter <= ITMAX; iter++) {
+    if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) {
+      c = a; fc = fa; e = d = b - a;
+    }
+    if (fabs(fc) < fabs(fb)) {
+      a = b; b = c; c = a;
+      fa = fb; fb = fc; fc = fa;
+    }
+    tol1 = 2.0 * EPS * fabs(b) + 0.5 * tol;
+    xm = 0.5 * (c - b);
+    if (fabs(xm) <= tol1 || fb == 0.0) return b;
+    if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+      s = fb / fa;
+      if (a == c) {
+        p = 2.0 * xm * s;
+        q = 1.0 - s;
+      } else {
+        q = fa / fc;
+        r = fb / fc;
+        p = s * (2.0 * xm * q * (q - r) - (b - a) * (r - 1.0));
+        q = (q - 1.0) * (r - 1.0) * (s - 1.0);
+      }
+      if (p > 0.0) q = -q;
+      p = fabs(p);
+      min1 = 3.0 * xm * q - fabs(tol1 * q);
+      min2 = fabs(e * q);
+      if (2.0 * p < (min1 < min2 ? min1 : min2)) {
+        e = d;
+        d = p / q;
+      } else {
+        d = xm;
+        e = d;
+      }
+    } else {
+      d = xm;
+      e = d;
+    }
+    a = b;
+    fa = fb;
+    if (fabs(d) > tol1) b += d;
+    else b += SIGN(tol1, xm);
+    fb = charge_conservation(o, g, b);
+    *last = b;
+  }
+  g->solve_error = 2;
+  return 0.0;
+}
+
+/* AtomicSpecies::ionization_fraction, AtomicSpecies.h:118-123 (stage == index) */
+static double ion_fraction(oracle_ctx* o, gas* g, int a, int stage)
+{
+  int i0 = o->ion_off[a], ni = o->ion_off[a + 1] - i0;
+  if (stage < 0 || stage >= ni) return 0;
+  return g->ion_frac[i0 + stage];
+}
+
+/* xy_array::value_at_with_zero_edges, src/utils/xy_array.cpp:42-104 */
+static double photo_cs(oracle_ctx* o, int lev, double z)
+{
+  int p0 = o->photo_off[lev], n = o->photo_off[lev + 1] - p0;
+  const double* x = o->photo_E + p0;
+  const double* y = o->photo_s + p0;
+  if (n <= 0) return 0;
+  if (z < x[0]) return 0;
+  if (z > x[n - 1]) return 0;
+  int ind;
+  if (n == 1) ind = 0;
+  else if (z >= x[n - 1]) ind = n;
+  else if (z <= x[0]) ind = 0;
+  else {
+    int bl = 0, bu = n - 1;
+    while (bu - bl > 1) { int bm = (bu + bl) / 2; if (x[bm] <= z) bl = bm; else bu = bm; }
+    ind = bl;
+  }
+  if (n == 1) return y[0];
+  int i1, i2;
+  if (ind < n - 1) { i1 = ind; i2 = ind + 1; }
+  else { i2 = ind < n ? ind : n - 1; i1 = i2 - 1; } /* ind == n only at z == x[n-1] exactly */
+  double slope = (y[i2] - y[i1]) / (x[i2] - x[i1]);
+  return y[ind < n ? ind : n - 1] + slope * (z - x[i1]);
+}
+
+/* transport::set_opacity, src/transport/transport_opacity.cpp:21-260, for one
+ * zone: GasState::solve_state (GasState.cpp:208-233) + computeOpacity
+ * (GasState_opacities.cpp:11-136) + the emissivity CDF, cap and means. */
+static void zone_opacity(oracle_ctx* o, int iz, double dt, gas* g, double* opac, double* aopac, double* emis,
+                         double* tmp_o, double* tmp_e)
+{
+  int nn = o->nu.n;
+  double* ab = o->abs + (size_t)iz * nn;
+  double* sc = o->scat + (size_t)iz * nn;
+  double* cdf = o->cdf + (size_t)iz * nn;
+  g->dens = o->rho[iz];
+  g->temp = o->T[iz];
+  if (g->temp < o->op.temp_min) g->temp = o->op.temp_min;
+  if (g->temp > o->op.temp_max) g->temp = o->op.temp_max;
+  /* GasState::set_mass_fractions, GasState.cpp:137-156 */
+  double norm = 0.0;
+  for (int a = 0; a < o->nelem; ++a) { g->mass_frac[a] = o->X[(size_t)iz * o->nelem + a]; norm += g->mass_frac[a]; }
+  for (int a = 0; a < o->nelem; ++a) g->mass_frac[a] /= norm;
+  double inv = 0.;
+  for (int a = 0; a < o->nelem; ++a) inv += g->mass_frac[a] / o->eA[a];
+  g->mu_I = 1. / inv;
+  double grey = o->grey[iz];
+  double temp = g->temp;
+  for (int i = 0; i < nn; ++i) { ab[i] = 0; sc[i] = 0; emis[i] = 0; }
+
+  if (grey != 0) {
+    /* grey branch, GasState_opacities.cpp:29-41 */
+    double gopac = g->dens * grey;
+    for (int i = 0; i < nn; ++i) {
+      ab[i] = gopac * o->op.epsilon;
+      sc[i] = gopac * (1 - o->op.epsilon);
+      double nu = lg_center(&o->nu, i);
+      double ezeta = exp(1.0 * PC_H * nu / PC_K / temp);
+      double bb = 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (ezeta - 1);
+      emis[i] += bb * ab[i];
+    }
+  } else {
+    if (!o->have_atoms) return;
+    /* GasState::solve_state (LTE) */
+    for (int a = 0; a < o->natoms; ++a) g->n_dens[a] = g->dens * g->mass_frac[a] / (o->eA[a] * PC_M_P);
+    double max_ne = 100 * g->dens / (g->mu_I * PC_M_P);
+    double min_ne = 1e-10 * g->dens / (g->mu_I * PC_M_P);
+    g->solve_error = 0;
+    double last = 0;
+    g->n_elec = ne_brent(o, g, min_ne, max_ne, 1e-3, &last);
+    for (int a = 0; a < o->natoms; ++a) solve_lte(o, g, a, last);
+    o->n_elec[iz] = g->n_elec;
+    double ne = g->n_elec;
+
+    if (o->op.use_electron_scattering) { /* :49-58 */
+      double es = PC_THOMSON * ne;
+      for (int i = 0; i < nn; ++i) { sc[i] += es; ab[i] += 1e-20 * o->op.epsilon * es; }
+    }
+    if (o->op.use_free_free) { /* GasState::free_free_opacity, :152-183 */
+      double fac = 0;
+      for (int a = 0; a < o->natoms; ++a) {
+        int ni = o->ion_off[a + 1] - o->ion_off[a];
+        double zsq = 0;
+        for (int j = 0; j < ni; j++) zsq += ion_fraction(o, g, a, j) * j * j;
+        double n_ion = g->mass_frac[a] * g->dens / (o->eA[a] * PC_M_P);
+        fac += n_ion * zsq;
+      }
+      fac *= 3.7e8 * pow(temp, -0.5) * ne;
+      for (int i = 0; i < nn; ++i) {
+        double nu = lg_center(&o->nu, i);
+        double ezeta = exp(-1.0 * PC_H * nu / PC_K / temp);
+        double bb = 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (1.0 / ezeta - 1);
+        double op_ = fac / nu / nu / nu * (1 - ezeta);
+        ab[i] += op_;
+        emis[i] += op_ * bb;
+      }
+    }
+    if (o->op.use_bound_free) { /* GasState::bound_free_opacity :352-371 + AtomicSpecies_opacities.cpp:58-151 */
+      for (int i = 0; i < nn; ++i) { tmp_o[i] = 0; tmp_e[i] = 0; }
+      double kt_ev = PC_K_EV * temp;
+      double lam_t = sqrt(PC_H * PC_H / (2 * PC_PI * PC_M_E * PC_K * temp));
+      for (int a = 0; a < o->natoms; ++a) {
+        int l0 = o->lev_off[a], nl = o->lev_off[a + 1] - l0;
+        double nd = g->n_dens[a];
+        double* ncp = (double*)calloc((size_t)(nl ? nl : 1), sizeof(double));
+        for (int j = 0; j < nl; ++j) {
+          int ic = o->lev_ic[l0 + j];
+          if (ic == -1) continue;
+          double nc = nd * g->lev_n[l0 + ic];
+          int gl = o->lev_g[l0 + j], gc = o->lev_g[l0 + ic];
+          double gl_o_gc = (1.0 * gl) / (1.0 * gc);
+          ncp[j] = nc * gl_o_gc / 2. * lam_t * lam_t * lam_t;
+        }
+        for (int i = 0; i < nn; ++i) {
+          double nu = lg_center(&o->nu, i);
+          double E = PC_H * nu * PC_ERGS_TO_EV;
+          double emis_fac = 2. * PC_H * nu * nu * nu / PC_C / PC_C;
+          double ao = 0, ae = 0;
+          for (int j = 0; j < nl; ++j) {
+            double Eion = o->lev_Eion[l0 + j];
+            int ic = o->lev_ic[l0 + j];
+            if (ic == -1) continue;
+            if (E < Eion) continue;
+            double zeta_net = (Eion - E) / kt_ev;
+            double ezeta_net = exp(zeta_net);
+            double sigma = photo_cs(o, l0 + j, E);
+            double opac_fac = nd * g->lev_n[l0 + j] - ncp[j] * ne * ezeta_net;
+            if (opac_fac < 0) opac_fac = 0.;
+            ao += sigma * opac_fac;
+            ae += emis_fac * sigma * ncp[j] * ezeta_net;
+          }
+          tmp_o[i] += ao;
+          tmp_e[i] += ae;
+        }
+        free(ncp);
+      }
+      for (int i = 0; i < nn; ++i) { ab[i] += tmp_o[i]; emis[i] += tmp_e[i] * ne; }
+    }
+    if (o->op.use_line_expansion) { /* GasState::line_expansion_opacity :424-454 + AtomicSpecies_opacities.cpp:331-375 */
+      for (int i = 0; i < nn; ++i) { opac[i] = 0; aopac[i] = 0; }
+      for (int a = 0; a < o->natoms; ++a) {
+        double this_eps = o->op.epsilon;
+        for (int k = 0; k < o->op.n_atom_zero_epsilon; k++) if (o->zero_eps[k] == o->eZ[a]) this_eps = 0;
+        for (int i = 0; i < nn; ++i) tmp_o[i] = 0;
+        int l0 = o->lev_off[a];
+        for (int k = o->line_off[a]; k < o->line_off[a + 1]; ++k) {
+          int ll = o->line_l[k], lu = o->line_u[k];
+          double nl = g->lev_n[l0 + ll], nup = g->lev_n[l0 + lu];
+          double gl = 1.0 * o->lev_g[l0 + ll], gu = 1.0 * o->lev_g[l0 + lu];
+          if (nl < DBL_MIN) continue;
+          double nu0 = o->line_nu[k];
+          double lam = PC_C / nu0;
+          double tau = nl * g->n_dens[a] * PC_SIGMA_TOT * o->line_f[k] * g->time * lam;
+          tau = tau * (1 - nup * gl / (nl * gu));
+          if (nup * gl > nl * gu) tau = 0;
+          double etau = exp(-tau);
+          if (!isnan(etau)) tmp_o[o->line_bin[k]] += (1 - etau);
+        }
+        for (int i = 0; i < nn; ++i) {
+          tmp_o[i] = tmp_o[i] * lg_center(&o->nu, i) / lg_delta(&o->nu, i) / PC_C / g->time;
+          opac[i] += tmp_o[i];
+          aopac[i] += tmp_o[i] * this_eps;
+        }
+      }
+      for (int i = 0; i < nn; ++i) {
+        ab[i] += aopac[i];
+        sc[i] += opac[i] - aopac[i];
+        double nu = lg_center(&o->nu, i);
+        double ezeta = exp(1.0 * PC_H * nu / PC_K / temp);
+        double bb = 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (ezeta - 1);
+        emis[i] += bb * aopac[i];
+      }
+    }
+    if (o->op.use_fuzz_expansion) { /* GasState::fuzz_expansion_opacity :464-494 + AtomicSpecies_opacities.cpp:292-324 */
+      for (int i = 0; i < nn; ++i) { opac[i] = 0; aopac[i] = 0; }
+      for (int a = 0; a < o->natoms; ++a) {
+        double this_eps = o->op.epsilon;
+        for (int k = 0; k < o->op.n_atom_zero_epsilon; k++) if (o->zero_eps[k] == o->eZ[a]) this_eps = 0;
+        for (int i = 0; i < nn; ++i) tmp_o[i] = 0;
+        int i0 = o->ion_off[a];
+        for (int k = o->fuzz_off[a]; k < o->fuzz_off[a + 1]; ++k) {
+          double nu = o->fuzz_nu[k], gf = o->fuzz_gf[k], El = o->fuzz_El[k];
+          int ion = o->fuzz_ion[k];
+          double nion = g->n_dens[a] * g->ion_frac[i0 + ion];
+          double nl = nion * exp(-1.0 * El / PC_K_EV / temp) / g->ion_part[i0 + ion];
+          double lam = PC_C / nu;
+          double stim_cor = (1 - exp(-PC_H * nu / PC_K / temp));
+          double tau = PC_SIGMA_TOT * lam * nl * gf * stim_cor * g->time;
+          double etau = exp(-tau);
+          tmp_o[o->fuzz_bin[k]] += (1 - etau);
+        }
+        for (int i = 0; i < nn; ++i) {
+          tmp_o[i] = tmp_o[i] * lg_center(&o->nu, i) / lg_delta(&o->nu, i) / PC_C / g->time;
+          opac[i] += tmp_o[i];
+          aopac[i] += tmp_o[i] * this_eps;
+        }
+      }
+      for (int i = 0; i < nn; ++i) {
+        ab[i] += aopac[i];
+        sc[i] += opac[i] - aopac[i];
+        double nu = lg_center(&o->nu, i);
+        double ezeta = exp(1.0 * PC_H * nu / PC_K / temp);
+        double bb = 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (ezeta - 1);
+        emis[i] += bb * aopac[i];
+      }
+    }
+  }
+
+  /* emissivity CDF, L_thermal and the opacity cap, transport_opacity.cpp:152-179 */
+  double max_ext = o->op.maximum_opacity * o->rho[iz];
+  double L = 0;
+  if (nn == 1) {
+    double bb_int = PC_SB * pow(o->T[iz], 4) / PC_PI;
+    L += 4 * PC_PI * ab[0] * bb_int;
+    cdf[0] = 1;
+    if (o->tp.omit_scattering) sc[0] = 0;
+  } else {
+    for (int j = 0; j < nn; ++j) {
+      double ednu = emis[j] * lg_delta(&o->nu, j);
+      cdf[j] = (j == 0) ? ednu : cdf[j - 1] + ednu;
+      L += 4 * PC_PI * ednu;
+      if (o->tp.omit_scattering) sc[j] = 0;
+      if (!o->tp.omit_scattering) { if (sc[j] > max_ext) sc[j] = max_ext; }
+      if (ab[j] > max_ext) ab[j] = max_ext;
+    }
+  }
+  o->L_th[iz] = L;
+  cdf_normalize(cdf, nn);
+  /* GasState::get_planck_mean / get_rosseland_mean, GasState_opacities.cpp:564-666 */
+  if (nn == 1) {
+    o->planck[iz] = ab[0];
+    o->ross[iz] = ab[0] + sc[0];
+  } else {
+    double mean = 0, norm2 = 0, rmean = 0, rnorm = 0;
+    for (int i = 0; i < nn; ++i) {
+      double nu = lg_center(&o->nu, i);
+      double zeta = PC_H * nu / PC_K / temp;
+      double Bnu = 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (exp(zeta) - 1);
+      if (isnan(Bnu)) Bnu = 0;
+      double W = Bnu * lg_delta(&o->nu, i);
+      mean += W * (ab[i]);
+      norm2 += W;
+      double ezeta = exp(zeta);
+      double dBdT = pow(nu, 4) * ezeta / (ezeta - 1) / (ezeta - 1);
+      if (isnan(dBdT)) dBdT = 0;
+      double Wr = dBdT * lg_delta(&o->nu, i);
+      rmean += Wr / (ab[i] + sc[i]);
+      rnorm += Wr;
+    }
+    o->planck[iz] = mean / norm2;
+    o->ross[iz] = rnorm / rmean;
+  }
+  /* eps_imc, transport_opacity.cpp:231-252 */
+  if (o->tp.radiative_eq) o->eps_imc[iz] = 1.;
+  else {
+    double fleck_beta = 4.0 * PC_A * pow(o->T[iz], 4) / (o->e_gas[iz] * o->rho[iz]);
+    double tfac = PC_C * o->planck[iz] * dt;
+    double f_imc = o->tp.fleck_alpha * fleck_beta * tfac;
+    if (o->tp.fleck_alpha == 0) f_imc = 0.;
+    o->eps_imc[iz] = 1.0 / (1.0 + f_imc);
+  }
+}
+
+int oracle_set_opacity(oracle_ctx* o, double dt)
+{
+  if (!o || !o->have_grid) return SED_ERR_STATE;
+  if (o->tp.steady_state) dt = 1;
+  int nn = o->nu.n;
+  size_t ni = o->have_atoms ? (size_t)o->ion_off[o->natoms] : 1;
+  size_t nl = o->have_atoms ? (size_t)o->lev_off[o->natoms] : 1;
+  gas g;
+  memset(&g, 0, sizeof g);
+  g.ion_part = (double*)calloc(ni ? ni : 1, sizeof(double));
+  g.ion_frac = (double*)calloc(ni ? ni : 1, sizeof(double));
+  g.lev_n = (double*)calloc(nl ? nl : 1, sizeof(double));
+  g.n_dens = (double*)calloc((size_t)(o->nelem > 0 ? o->nelem : 1), sizeof(double));
+  g.mass_frac = (double*)calloc((size_t)(o->nelem > 0 ? o->nelem : 1), sizeof(double));
+  g.time = o->t_grid;
+  double* opac = (double*)calloc((size_t)nn, sizeof(double));
+  double* aopac = (double*)calloc((size_t)nn, sizeof(double));
+  double* emis = (double*)calloc((size_t)nn, sizeof(double));
+  double* t1 = (double*)calloc((size_t)nn, sizeof(double));
+  double* t2 = (double*)calloc((size_t)nn, sizeof(double));
+  for (int iz = 0; iz < o->nzones; ++iz) zone_opacity(o, iz, dt, &g, opac, aopac, emis, t1, t2);
+  free(opac); free(aopac); free(emis); free(t1); free(t2);
+  free(g.ion_part); free(g.ion_frac); free(g.lev_n); free(g.n_dens); free(g.mass_frac);
+  o->have_opacity = 1;
+  return SED_OK;
+}
+
+int oracle_load_opacity(oracle_ctx* o, const double* abs, const double* scat, const double* emis_cdf, const double* eps_imc)
+{
+  if (!o || !o->have_grid || !abs || !emis_cdf || !eps_imc) return SED_ERR_ARG;
+  size_t n = (size_t)o->nzones * o->nu.n;
+  for (size_t i = 0; i < n; ++i) {
+    o->abs[i] = abs[i];
+    o->scat[i] = scat ? scat[i] : 0.0;
+    o->cdf[i] = emis_cdf[i];
+  }
+  for (int i = 0; i < o->nzones; ++i) o->eps_imc[i] = eps_imc[i];
+  o->have_opacity = 1;
+  return SED_OK;
+}
+
+/* ---------------------------------------------------------------- geometry */
+/* grid_1D_sphere::get_zone, src/grid/grid_1D_sphere.cpp:494-505;
+ * grid_3D_cart::get_zone, src/grid/grid_3D_cart.cpp:363-390 */
+static int get_zone(const oracle_ctx* o, const double* x)
+{
+  if (o->gtype == SED_GRID_1D_SPHERE) {
+    double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    if (r < o->r_out.min) return -1;
+    if (r >= o->r_out.x[o->r_out.n - 1]) return -2;
+    return lg_locate_wb(&o->r_out, r);
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (x[a] < o->ax[a].min) return -2;
+    if (x[a] > o->ax[a].x[o->ax[a].n - 1]) return -2;
+  }
+  int i = lg_locate_wb(&o->ax[0], x[0]);
+  int j = lg_locate_wb(&o->ax[1], x[1]);
+  int k = lg_locate_wb(&o->ax[2], x[2]);
+  return i * o->ny * o->nz + j * o->nz + k;
+}
+
+/* grid_1D_sphere::get_next_zone, grid_1D_sphere.cpp:510-590;
+ * grid_3D_cart::get_next_zone, grid_3D_cart.cpp:396-469 */
+static int get_next_zone(const oracle_ctx* o, const double* x, const double* D, int i, double r_core, double* l)
+{
+  if (o->gtype == SED_GRID_1D_SPHERE) {
+    double rsq = (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    double xdotD = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]);
+    double r_o = o->r_out.x[i];
+    double l_out = -1 * xdotD + sqrt(xdotD * xdotD + r_o * r_o - rsq);
+    double r_in;
+    int ind_in;
+    if (i != 0) { r_in = o->r_out.x[i - 1]; ind_in = i - 1; }
+    else { r_in = o->r_out.min; ind_in = -1; }
+    if (r_core >= r_in) { r_in = r_core; ind_in = -1; }
+    double l_in;
+    if ((i == 0) && (r_in == 0)) l_in = -1;
+    else {
+      double rad = xdotD * xdotD + r_in * r_in - rsq;
+      if (rad < 0) l_in = -1;
+      else l_in = -1 * xdotD - sqrt(rad);
+    }
+    int ind;
+    double tiny_offset = 1 + 1e-6;
+    if ((l_out < l_in) || (l_in < 0)) {
+      ind = i + 1;
+      if (ind == o->nzones) { ind = -2; *l = l_out / tiny_offset; }
+      else *l = l_out * tiny_offset;
+    } else {
+      ind = ind_in;
+      if (ind_in == -1) *l = l_in / tiny_offset;
+      else *l = l_in * tiny_offset;
+    }
+    return ind;
+  }
+  int nyz = o->ny * o->nz;
+  int ix = i / nyz, iy = (i / o->nz) % o->ny, iz = i % o->nz;
+  int idx3[3] = {ix, iy, iz};
+  double tiny = 1e-10;
+  double len[3];
+  for (int a = 0; a < 3; ++a) {
+    const lgrid* g = &o->ax[a];
+    double dd = lg_delta(g, idx3[a]);
+    double bn = (D[a] > 0) ? g->x[idx3[a]] + dd * tiny : lg_left(g, idx3[a]) - dd * tiny;
+    len[a] = (bn - x[a]) / D[a];
+  }
+  int idx = 0, idy = 0, idz = 0;
+  if ((len[0] < len[1]) && (len[0] < len[2])) { idx = (D[0] < 0) ? -1 : 1; *l = len[0]; }
+  else if (len[1] < len[2]) { idy = (D[1] < 0) ? -1 : 1; *l = len[1]; }
+  else { idz = (D[2] < 0) ? -1 : 1; *l = len[2]; }
+  int nx_ = ix + idx, ny_ = iy + idy, nz_ = iz + idz;
+  if (nx_ < 0 || nx_ > o->nx - 1) return -2;
+  if (ny_ < 0 || ny_ > o->ny - 1) return -2;
+  if (nz_ < 0 || nz_ > o->nz - 1) return -2;
+  return nx_ * nyz + ny_ * o->nz + nz_;
+}
+
+/* get_velocity, grid_1D_sphere.cpp:707-748 / grid_3D_cart.cpp:513-521 (homologous) */
+static void get_velocity(const oracle_ctx* o, int i, const double* x, const double* D, double* v, double* dvds)
+{
+  if (o->homologous) {
+    v[0] = x[0] / o->t_grid;
+    v[1] = x[1] / o->t_grid;
+    v[2] = x[2] / o->t_grid;
+    *dvds = 1.0 / o->t_grid;
+    return;
+  }
+  if (o->gtype == SED_GRID_1D_SPHERE) {
+    double rr = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    double v_0, r_0;
+    if (i == 0) { v_0 = 0; r_0 = o->r_out.min; }
+    else { v_0 = o->v_r[i - 1]; r_0 = o->r_out.x[i - 1]; }
+    double dr = rr - r_0;
+    double dv_dr = (o->v_r[i] - v_0) / (o->r_out.x[i] - r_0);
+    double vv = v_0 + dv_dr * dr;
+    double D_dot_rhat = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]) / rr;
+    v[0] = x[0] / rr * vv;
+    v[1] = x[1] / rr * vv;
+    v[2] = x[2] / rr * vv;
+    *dvds = D_dot_rhat * D_dot_rhat * (dv_dr - vv / rr) + vv / rr;
+    if (rr == 0) { v[0] = v[1] = v[2] = 0; *dvds = dv_dr; }
+    return;
+  }
+  v[0] = v[1] = v[2] = 0; /* non-homologous 3D velocities are not on this path */
+  *dvds = 0;
+}
+
+/* transport::do_dshift, src/transport/relativity.cpp:14-43 (lab -> comoving) */
+static double dshift_lab_to_comoving(const oracle_ctx* o, packet* p)
+{
+  double v[3], dvds;
+  get_velocity(o, p->ind, p->x, p->D, v, &dvds);
+  double beta2 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / PC_C / PC_C;
+  double vdd = v[0] * p->D[0] + v[1] * p->D[1] + v[2] * p->D[2];
+  double gamma = 1.0 / sqrt(1 - beta2);
+  double dshift = gamma * (1 - vdd / PC_C);
+  p->dvds = dvds;
+  return dshift;
+}
+
+/* transport::lorentz_transform(p, tolab=1), relativity.cpp:84-127 */
+static void transform_comoving_to_lab(const oracle_ctx* o, packet* p)
+{
+  double v[3], dvds;
+  get_velocity(o, p->ind, p->x, p->D, v, &dvds);
+  v[0] *= -1; v[1] *= -1; v[2] *= -1;
+  double beta2 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / PC_C / PC_C;
+  double vdd = v[0] * p->D[0] + v[1] * p->D[1] + v[2] * p->D[2];
+  double gamma = 1.0 / sqrt(1 - beta2);
+  double dshift = gamma * (1 - vdd / PC_C);
+  p->dvds = dvds;
+  p->e *= dshift;
+  p->nu *= dshift;
+  p->D[0] = 1.0 / dshift * (p->D[0] - gamma * v[0] / PC_C * (1 - gamma * vdd / PC_C / (gamma + 1)));
+  p->D[1] = 1.0 / dshift * (p->D[1] - gamma * v[1] / PC_C * (1 - gamma * vdd / PC_C / (gamma + 1)));
+  p->D[2] = 1.0 / dshift * (p->D[2] - gamma * v[2] / PC_C * (1 - gamma * vdd / PC_C / (gamma + 1)));
+  double norm = p->D[0] * p->D[0] + p->D[1] * p->D[1] + p->D[2] * p->D[2];
+  p->D[0] /= norm;
+  p->D[1] /= norm;
+  p->D[2] /= norm;
+}
+
+static double draw(const oracle_ctx* o, packet* p)
+{
+  return oracle_packet_uniform(o->tp.rng_seed, p->pid, o->step, p->n++);
+}
+
+/* transport::isotropic_scatter, src/transport/scatter.cpp:303-351 */
+static void isotropic_scatter(const oracle_ctx* o, packet* p, int redist)
+{
+  double V[3], dvds;
+  get_velocity(o, p->ind, p->x, p->D, V, &dvds);
+  double vdotD = V[0] * p->D[0] + V[1] * p->D[1] + V[2] * p->D[2];
+  double beta2 = (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]) / PC_C / PC_C;
+  double gamma = 1.0 / sqrt(1 - beta2);
+  double dshift_in = gamma * (1 - vdotD / PC_C);
+  p->e = p->e * dshift_in;
+  p->nu = p->nu * dshift_in;
+  double mu = 1 - 2.0 * draw(o, p);
+  double phi = 2.0 * PC_PI * draw(o, p);
+  double smu = sqrt(1 - mu * mu);
+  double Dn[3] = {smu * cos(phi), smu * sin(phi), mu};
+  if (redist) { /* sample_photon_frequency, emission.cpp:27-46 */
+    int nn = o->nu.n;
+    int inu = cdf_sample(o->cdf + (size_t)p->ind * nn, nn, draw(o, p));
+    p->nu = lg_sample(&o->nu, inu, draw(o, p));
+  }
+  for (int i = 0; i < 3; i++) V[i] = -1 * V[i];
+  double vdp = (Dn[0] * V[0] + Dn[1] * V[1] + Dn[2] * V[2]);
+  double vd_out = gamma * (1 - vdp / PC_C);
+  p->D[0] = 1.0 / vd_out * (Dn[0] - gamma * V[0] / PC_C * (1 - gamma * vdp / PC_C / (gamma + 1)));
+  p->D[1] = 1.0 / vd_out * (Dn[1] - gamma * V[1] / PC_C * (1 - gamma * vdp / PC_C / (gamma + 1)));
+  p->D[2] = 1.0 / vd_out * (Dn[2] - gamma * V[2] / PC_C * (1 - gamma * vdp / PC_C / (gamma + 1)));
+  double norm = sqrt(p->D[0] * p->D[0] + p->D[1] * p->D[1] + p->D[2] * p->D[2]);
+  p->D[0] = p->D[0] / norm;
+  p->D[1] = p->D[1] / norm;
+  p->D[2] = p->D[2] / norm;
+  p->e = p->e * vd_out;
+  p->nu = p->nu * vd_out;
+}
+
+/* transport::emit_inner_source, src/transport/emission.cpp:370-485 (one packet) */
+static void emit_core_packet(const oracle_ctx* o, packet* p, double Ep, double t_now, double dt)
+{
+  double rc = o->tp.core_radius;
+  if (rc == 0) {
+    p->x[0] = p->x[1] = p->x[2] = 0;
+    double mu = 1 - 2.0 * draw(o, p);
+    double phi = 2.0 * PC_PI * draw(o, p);
+    double smu = sqrt(1 - mu * mu);
+    p->D[0] = smu * cos(phi);
+    p->D[1] = smu * sin(phi);
+    p->D[2] = mu;
+  } else {
+    double phi_core = 2 * PC_PI * draw(o, p);
+    double cosp_core = cos(phi_core);
+    double sinp_core = sin(phi_core);
+    double cost_core = 1 - 2.0 * draw(o, p);
+    double sint_core = sqrt(1 - cost_core * cost_core);
+    double a_phot = rc + rc * 1e-10;
+    p->x[0] = a_phot * sint_core * cosp_core;
+    p->x[1] = a_phot * sint_core * sinp_core;
+    p->x[2] = a_phot * cost_core;
+    double phi_loc = 2 * PC_PI * draw(o, p);
+    double cost_loc = sqrt(draw(o, p));
+    double sint_loc = sqrt(1 - cost_loc * cost_loc);
+    double D_xl = sint_loc * cos(phi_loc);
+    double D_yl = sint_loc * sin(phi_loc);
+    double D_zl = cost_loc;
+    p->D[0] = cost_core * cosp_core * D_xl - sinp_core * D_yl + sint_core * cosp_core * D_zl;
+    p->D[1] = cost_core * sinp_core * D_xl + cosp_core * D_yl + sint_core * sinp_core * D_zl;
+    p->D[2] = -sint_core * D_xl + cost_core * D_zl;
+  }
+  p->e = Ep;
+  if (o->tp.core_photon_frequency > 0) p->nu = o->tp.core_photon_frequency;
+  else {
+    int inu = cdf_sample(o->core_cdf, o->nu.n, draw(o, p));
+    p->nu = lg_sample(&o->nu, inu, draw(o, p));
+    p->e /= 1.0;  /* emissivity_weight_[inu] */
+  }
+  p->ind = get_zone(o, p->x);
+  transform_comoving_to_lab(o, p);
+  p->t = t_now + draw(o, p) * dt;
+}
+
+/* spectrum_array::count, src/transport/spectrum_array.cpp:215-246 */
+static void spectrum_count(oracle_ctx* o, double t, double w, double E, const double* D)
+{
+  double mu = D[2];
+  double phi = atan2(D[1], D[0]);
+  if (phi < 0) phi += 2. * PC_PI;
+  int t_bin = lg_locate(&o->st, t);
+  int l_bin = lg_locate(&o->sn, w);
+  int m_bin = lg_locate(&o->sm, mu);
+  int p_bin = lg_locate(&o->sp, phi);
+  if (l_bin < 0) l_bin = 0;
+  if (l_bin >= o->sn.n) l_bin = 0;
+  if ((t_bin < 0) || (l_bin < 0) || (m_bin < 0) || (p_bin < 0)) return;
+  if (t_bin >= o->st.n) return;
+  if (m_bin >= o->sm.n) return;
+  if (p_bin >= o->sp.n) return;
+  int64_t a3 = o->sp.n, a2 = (int64_t)o->sm.n * a3, a1 = (int64_t)o->sn.n * a2;
+  int64_t ind = t_bin * a1 + l_bin * a2 + m_bin * a3 + p_bin;
+  o->flux[ind] += E;
+  o->click[ind] += 1;
+}
+
+/* transport::propagate + propagate_monte_carlo, src/transport/transport.cpp:202-484 */
+static int propagate(oracle_ctx* o, packet* p, double t_now, double dt, int64_t* nseg, int64_t* nscat)
+{
+  int nn = o->nu.n;
+  int nj = o->tp.store_Jnu ? nn : 1;
+  p->ind = get_zone(o, p->x);
+  if (p->ind == -1) return F_ABSORBED;
+  if (p->ind == -2) return F_ESCAPED;
+  double tstop = t_now + dt;
+  int fate = F_MOVING;
+  int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
+  int64_t seg = 0;
+  while (fate == F_MOVING) {
+    if (seg++ >= limit) { fate = F_STOPPED; break; }
+    int iz = p->ind;
+    double d_bn = 0;
+    int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);
+    double dshift = dshift_lab_to_comoving(o, p);
+    /* transport::get_opacity, transport_opacity.cpp:268-299 */
+    double nu_cmf = p->nu * dshift;
+    int i_nu = lg_locate_wb(&o->nu, nu_cmf);
+    double a_opac = o->abs[(size_t)iz * nn + i_nu];
+    double s_opac = 0;
+    if (!o->tp.omit_scattering) s_opac = o->scat[(size_t)iz * nn + i_nu];
+    double opac = a_opac + s_opac;
+    double eps = (opac == 0) ? 0 : a_opac / opac;
+    double d_nu = lg_delta(&o->nu, i_nu) / p->nu * PC_C / p->dvds;
+    if (p->dvds == 0) d_nu = INFINITY;
+    if (d_nu < 0) d_nu = -1 * d_nu;
+    if (d_nu < d_bn) { d_bn = d_nu; new_ind = p->ind; }
+    double tot_lab = opac * dshift;
+    double tau_r = -1.0 * log(1 - draw(o, p));
+    double d_sc = tau_r / tot_lab;
+    if (tot_lab == 0) d_sc = INFINITY;
+    double d_tm = (tstop - p->t) * PC_C;
+    if (o->tp.steady_state) d_tm = INFINITY;
+    int event;
+    double this_d;
+    if ((d_sc < d_bn) && (d_sc < d_tm)) { event = 0; this_d = d_sc; }
+    else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
+    else { event = 2; this_d = d_tm; }
+    double this_E = p->e * this_d;
+    o->e_abs[iz] += this_E * dshift * (opac) * eps * dshift * o->eps_imc[iz];
+    if (o->tp.store_Jnu) o->J[(size_t)iz * nj + i_nu] += this_E;
+    else o->J[(size_t)iz * nj] += this_E;
+    if (o->tp.tally_forces) {
+      o->fx[iz] += this_E * dshift * opac * p->D[0] * dshift;
+      o->fy[iz] += this_E * dshift * opac * p->D[1] * dshift;
+      o->fz[iz] += this_E * dshift * opac * p->D[2] * dshift;
+      double rr = sqrt(p->x[0] * p->x[0] + p->x[1] * p->x[1] + p->x[2] * p->x[2]);
+      double xdotD = p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2];
+      o->fr[iz] += this_E * dshift * opac * xdotD / rr * dshift;
+    }
+    p->x[0] += this_d * p->D[0];
+    p->x[1] += this_d * p->D[1];
+    p->x[2] += this_d * p->D[2];
+    p->t = p->t + this_d / PC_C;
+    if (event == 1) {
+      if (new_ind == -1) {
+        if (o->tp.boundary_in_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
+        else { p->ind = new_ind; fate = F_ABSORBED; }
+      } else if (new_ind == -2) {
+        if (o->tp.boundary_out_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
+        else { p->ind = new_ind; fate = F_ESCAPED; }
+      } else {
+        p->ind = new_ind;
+      }
+    } else if (event == 0) {
+      /* transport::do_scatter, scatter.cpp:12-70 (photons) */
+      (*nscat)++;
+      if (draw(o, p) > eps) isotropic_scatter(o, p, 0);
+      else {
+        double z2 = draw(o, p);
+        if ((z2 > o->eps_imc[iz]) || o->tp.radiative_eq) isotropic_scatter(o, p, 1);
+        else fate = F_ABSORBED;
+      }
+    } else {
+      fate = F_STOPPED;
+    }
+  }
+  *nseg += seg;
+  return fate;
+}
+
+static uint32_t draws_per_emission(const oracle_ctx* o)
+{
+  uint32_t k = (o->tp.core_radius == 0) ? 2 : 4;
+  if (!(o->tp.core_photon_frequency > 0)) k += 2;
+  return k + 1;
+}
+
+static void wipe_tallies(oracle_ctx* o)
+{
+  size_t nz = (size_t)o->nzones;
+  size_t nj = o->tp.store_Jnu ? (size_t)o->nu.n : 1;
+  memset(o->J, 0, nz * nj * sizeof(double));
+  memset(o->e_abs, 0, nz * sizeof(double));
+  memset(o->e_rad, 0, nz * sizeof(double));
+  memset(o->fx, 0, nz * sizeof(double));
+  memset(o->fy, 0, nz * sizeof(double));
+  memset(o->fz, 0, nz * sizeof(double));
+  memset(o->fr, 0, nz * sizeof(double));
+}
+
+/* normalisation of transport::reduce_radiation, src/transport/transport_mpi.cpp:415-441,
+ * preceded by the steady-state rescale of transport.cpp:94-115 */
+static void finish_step(oracle_ctx* o, double dt, int64_t n_active, int64_t n_escaped)
+{
+  int nn = o->nu.n;
+  int nj = o->tp.store_Jnu ? nn : 1;
+  if (o->tp.steady_state && o->tp.core_fix_luminosity) {
+    double per_esc = (1.0 * n_escaped) / (1.0 * n_active);
+    double fac = 1.0 / per_esc;
+    for (int64_t i = 0; i < o->nspec; ++i) o->flux[i] *= fac;
+    for (int i = 0; i < o->nzones; ++i) {
+      o->e_rad[i] *= fac;
+      if (o->tp.store_Jnu) for (int j = 0; j < nn; ++j) o->J[(size_t)i * nj + j] *= fac;
+    }
+  }
+  for (int i = 0; i < o->nzones; ++i) {
+    double vol = o->vol[i];
+    o->e_abs[i] /= vol * dt;
+    o->fr[i] /= vol * PC_C * dt;
+    if ((nn == 1) || (!o->tp.store_Jnu)) {
+      o->e_rad[i] = o->J[(size_t)i * nj] / (vol * dt * PC_C);
+    } else {
+      double esum = 0;
+      for (int j = 0; j < nn; ++j) {
+        double d = lg_delta(&o->nu, j);
+        o->J[(size_t)i * nj + j] /= vol * dt * 4 * PC_PI * d;
+        esum += o->J[(size_t)i * nj + j] * d * 4 * PC_PI / PC_C;
+      }
+      o->e_rad[i] = esum;
+    }
+  }
+}
+
+int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t count, int finish, sed_step_stats* st)
+{
+  if (!o || !o->have_grid) return SED_ERR_STATE;
+  if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
+  if (o->tp.steady_state) dt = 1;
+  double t_now = o->t_grid;
+  int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
+  if (n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
+  if (first == 0) {
+    wipe_tallies(o);
+    memset(o->flux, 0, (size_t)o->nspec * sizeof(double));
+    memset(o->click, 0, (size_t)o->nspec * sizeof(double));
+    o->n_escaped_acc = 0;
+    o->n_active_acc = 0;
+  }
+  if (first < 0 || first + count > n_emit) return fail(o, SED_ERR_ARG, "packet range outside the emission");
+  double Ep = o->tp.core_luminosity * dt / n_emit;
+  uint32_t K = draws_per_emission(o);
+  if (o->record) {
+    free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state);
+    o->nrec = count;
+    o->r_fate = (int32_t*)calloc((size_t)count + 1, 4);
+    o->r_ind = (int32_t*)calloc((size_t)count + 1, 4);
+    o->r_draws = (int32_t*)calloc((size_t)count + 1, 4);
+    o->r_state = (double*)calloc((size_t)count * 9 + 1, 8);
+  }
+  int64_t nseg = 0, nscat = 0, nesc = 0, nabs = 0, nstop = 0;
+  for (int64_t k = 0; k < count; ++k) {
+    packet p;
+    memset(&p, 0, sizeof p);
+    p.pid = (uint64_t)(first + k);
+    p.n = 0;
+    emit_core_packet(o, &p, Ep, t_now, dt);
+    p.n = K;
+    int fate = propagate(o, &p, t_now, dt, &nseg, &nscat);
+    if (fate == F_ESCAPED) {
+      double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / PC_C;
+      spectrum_count(o, t_obs, p.nu, p.e, p.D);
+      p.t = t_obs;
+      nesc++;
+    } else if (fate == F_ABSORBED) nabs++;
+    else nstop++;
+    if (o->record) {
+      o->r_fate[k] = fate; o->r_ind[k] = p.ind; o->r_draws[k] = (int32_t)(p.n - K);
+      double* s = o->r_state + (size_t)k * 9;
+      s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2]; s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+      s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+    }
+  }
+  o->n_escaped_acc += nesc;
+  o->n_active_acc += count;
+  if (finish) finish_step(o, dt, n_emit, o->n_escaped_acc);
+  if (st) {
+    memset(st, 0, sizeof *st);
+    st->n_packets = count; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
+    st->n_segments = nseg; st->n_scatters = nscat;
+  }
+  return SED_OK;
+}
+
+int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
+{
+  if (!o) return SED_ERR_ARG;
+  return oracle_transport_range(o, dt, 0, (int64_t)(o->tp.core_n_emit / 1.0), 1, st);
+}
+
+int oracle_get_spectrum(oracle_ctx* o, double* flux, double* click)
+{
+  if (!o) return SED_ERR_ARG;
+  if (flux) memcpy(flux, o->flux, (size_t)o->nspec * sizeof(double));
+  if (click) memcpy(click, o->click, (size_t)o->nspec * sizeof(double));
+  return SED_OK;
+}
+
+int oracle_get_zone_tallies(oracle_ctx* o, double* J, double* e_abs, double* e_rad, double* fx, double* fy, double* fz, double* fr)
+{
+  if (!o || !o->have_grid) return SED_ERR_STATE;
+  size_t nz = (size_t)o->nzones, nj = o->tp.store_Jnu ? (size_t)o->nu.n : 1;
+  if (J) memcpy(J, o->J, nz * nj * sizeof(double));
+  if (e_abs) memcpy(e_abs, o->e_abs, nz * sizeof(double));
+  if (e_rad) memcpy(e_rad, o->e_rad, nz * sizeof(double));
+  if (fx) memcpy(fx, o->fx, nz * sizeof(double));
+  if (fy) memcpy(fy, o->fy, nz * sizeof(double));
+  if (fz) memcpy(fz, o->fz, nz * sizeof(double));
+  if (fr) memcpy(fr, o->fr, nz * sizeof(double));
+  return SED_OK;
+}
+
+int oracle_get_opacity(oracle_ctx* o, double* abs, double* scat, double* cdf, double* n_elec, double* eps_imc,
+                       double* planck, double* ross, double* L_th)
+{
+  if (!o || !o->have_grid) return SED_ERR_STATE;
+  size_t nz = (size_t)o->nzones, n = nz * (size_t)o->nu.n;
+  if (abs) memcpy(abs, o->abs, n * sizeof(double));
+  if (scat) memcpy(scat, o->scat, n * sizeof(double));
+  if (cdf) memcpy(cdf, o->cdf, n * sizeof(double));
+  if (n_elec) memcpy(n_elec, o->n_elec, nz * sizeof(double));
+  if (eps_imc) memcpy(eps_imc, o->eps_imc, nz * sizeof(double));
+  if (planck) memcpy(planck, o->planck, nz * sizeof(double));
+  if (ross) memcpy(ross, o->ross, nz * sizeof(double));
+  if (L_th) memcpy(L_th, o->L_th, nz * sizeof(double));
+  return SED_OK;
+}
+
+int oracle_record_packets(oracle_ctx* o, int32_t enable)
+{
+  if (!o) return SED_ERR_ARG;
+  o->record = enable;
+  return SED_OK;
+}
+
+int oracle_get_packet_records(oracle_ctx* o, int64_t n, int32_t* fate, int32_t* ind, int32_t* draws, double* state9)
+{
+  if (!o || !o->record || n > o->nrec) return SED_ERR_STATE;
+  if (fate) memcpy(fate, o->r_fate, (size_t)n * 4);
+  if (ind) memcpy(ind, o->r_ind, (size_t)n * 4);
+  if (draws) memcpy(draws, o->r_draws, (size_t)n * 4);
+  if (state9) memcpy(state9, o->r_state, (size_t)n * 9 * 8);
+  return SED_OK;
+}
+
+const char* oracle_last_error(oracle_ctx* o) { return o ? o->err : "null context"; }
+
+void oracle_ctx_destroy(oracle_ctx* o)
+{
+  if (!o) return;
+  free_grid(o);
+  free(o->nu.x); free(o->st.x); free(o->sn.x); free(o->sm.x); free(o->sp.x);
+  free(o->flux); free(o->click); free(o->core_cdf);
+  free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state);
+  if (o->have_atoms) {
+    free(o->ion_off); free(o->lev_off); free(o->lev_ion); free(o->lev_g); free(o->lev_ic); free(o->photo_off);
+    free(o->line_off); free(o->line_l); free(o->line_u); free(o->line_bin); free(o->ion_chi); free(o->lev_E);
+    free(o->lev_Eion); free(o->photo_E); free(o->photo_s); free(o->line_nu); free(o->line_f);
+    free(o->fuzz_off); free(o->fuzz_ion); free(o->fuzz_bin); free(o->fuzz_nu); free(o->fuzz_gf); free(o->fuzz_El);
+  }
+  free(o->zero_eps);
+  free(o);
+}

@@ -1,0 +1,213 @@
+"""Synthetic ejecta workloads (seeded) with the shapes of the benchmark
+configurations, plus their translation into the C ABI structs.
+
+A Workload holds Sedona parameters under their reference names (`params`),
+a zone model (`zones`) and, for microphysical opacities, an atomic model.
+Everything derived from them (bin walls, zone volumes, mass fractions) is
+computed with the reference's own formulas so the CUDA library, the oracle
+and the reference harness all see identical inputs.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Any, Optional
+
+import numpy as np
+
+from . import abi
+from .atomic import AtomicModel
+from .grids import LocGrid, PI, grid_from_spec, lin_grid, lin_grid_n, log_delta_for_bins, shell_volumes
+from .params import Params
+
+M_SUN = 1.98892e33  # physical_constants::m_sun
+
+
+@dataclass
+class ZoneModel:
+    """Zone geometry + gas state (grid_1D_sphere / grid_3D_cart + zone)."""
+    type: int
+    t_now: float
+    rho: np.ndarray
+    T: np.ndarray
+    X: np.ndarray            # [n_zones, n_elems], normalised like the model readers
+    elem_Z: np.ndarray
+    elem_A: np.ndarray
+    vol: np.ndarray
+    homologous: int = 1
+    # 1D sphere
+    r_min: float = 0.0
+    r_out: Optional[np.ndarray] = None
+    v: Optional[np.ndarray] = None
+    # 3D Cartesian
+    axes: Optional[list] = None  # [LocGrid x, y, z]
+    shape: Optional[tuple] = None
+
+    @property
+    def n_zones(self) -> int:
+        return int(self.rho.size)
+
+    @property
+    def n_elems(self) -> int:
+        return int(self.elem_Z.size)
+
+
+@dataclass
+class Workload:
+    name: str
+    params: dict[str, Any]
+    zones: ZoneModel
+    atoms: Optional[AtomicModel] = None
+    notes: dict[str, Any] = field(default_factory=dict)
+
+    # ------------------------------------------------------------ derived
+    @property
+    def P(self) -> Params:
+        return Params(self.params)
+
+    def nu_grid(self) -> LocGrid:
+        return grid_from_spec(self.P.vector("transport_nu_grid"))
+
+    def spectrum_grids(self):
+        P = self.P
+        t = P.vector("spectrum_time_grid")
+        tg = lin_grid(float(t[0]), float(t[1]), float(t[2]))          # spectrum_array.cpp:40-43
+        ng = grid_from_spec(P.vector("spectrum_nu_grid"))
+        mg = lin_grid_n(-1.0, 1.0, P.scalar("spectrum_n_mu", int))      # :66
+        pg = lin_grid_n(0.0, 2 * PI, P.scalar("spectrum_n_phi", int))   # :69
+        return tg, ng, mg, pg
+
+    @property
+    def n_packets(self) -> int:
+        return int(self.P.scalar("core_n_emit", int))
+
+    def total_grey(self) -> np.ndarray:
+        return np.full(self.zones.n_zones, float(self.P.scalar("opacity_grey_opacity")))
+
+    # ------------------------------------------------------------ C structs
+    def transport_params(self, keep: abi.Keep, precision: int = abi.PREC_FP64,
+                         n_packets: Optional[int] = None) -> abi.TransportParams:
+        P = self.P
+        tg, ng, mg, pg = self.spectrum_grids()
+        tp = abi.TransportParams()
+        tp.steady_state = int(P.scalar("transport_steady_iterate", int) > 0)
+        tp.radiative_eq = P.scalar("transport_radiative_equilibrium", int)
+        tp.boundary_in_reflect = P.scalar("transport_boundary_in_reflect", int)
+        tp.boundary_out_reflect = P.scalar("transport_boundary_out_reflect", int)
+        tp.store_Jnu = P.scalar("transport_store_Jnu", int)
+        tp.omit_scattering = P.scalar("opacity_no_scattering", int)
+        tp.core_fix_luminosity = P.scalar("core_fix_luminosity", int)
+        tp.tally_forces = 1
+        tp.precision = precision
+        tp.rng_seed = P.scalar("transport_rng_seed", int) & 0xFFFFFFFF
+        tp.max_particles = P.scalar("particles_max_total", int)
+        tp.core_n_emit = self.n_packets if n_packets is None else int(n_packets)
+        tp.core_radius = P.scalar("core_radius")
+        tp.core_luminosity = P.function("core_luminosity", self.zones.t_now)
+        tp.core_temperature = P.scalar("core_temperature")
+        tp.core_photon_frequency = P.scalar("core_photon_frequency")
+        tp.fleck_alpha = P.scalar("transport_fleck_alpha")
+        tp.max_segments = 0
+        tp.nu_grid = abi.locate_grid(keep, self.nu_grid())
+        tp.spec_time = abi.locate_grid(keep, tg)
+        tp.spec_nu = abi.locate_grid(keep, ng)
+        tp.spec_mu = abi.locate_grid(keep, mg)
+        tp.spec_phi = abi.locate_grid(keep, pg)
+        return tp
+
+    def grid_struct(self, keep: abi.Keep) -> abi.Grid:
+        z = self.zones
+        g = abi.Grid()
+        g.type = z.type
+        g.n_zones = z.n_zones
+        g.homologous = z.homologous
+        g.n_elems = z.n_elems
+        g.t_now = z.t_now
+        if z.type == abi.GRID_1D_SPHERE:
+            g.r_min = z.r_min
+            g.r_out = keep.d(z.r_out)
+            g.v_r = keep.d(z.v if z.v is not None else np.zeros(z.n_zones))
+        else:
+            g.nx, g.ny, g.nz = z.shape
+            g.x_axis = abi.locate_grid(keep, z.axes[0])
+            g.y_axis = abi.locate_grid(keep, z.axes[1])
+            g.z_axis = abi.locate_grid(keep, z.axes[2])
+        g.vol = keep.d(z.vol)
+        g.rho = keep.d(z.rho)
+        g.T_gas = keep.d(z.T)
+        g.e_gas = keep.d(np.zeros(z.n_zones))
+        g.total_grey_opacity = keep.d(self.total_grey())
+        g.X = keep.d(z.X.reshape(-1))
+        g.elem_Z = keep.i(z.elem_Z)
+        g.elem_A = keep.i(z.elem_A)
+        return g
+
+    def opacity_params(self, keep: abi.Keep) -> abi.OpacityParams:
+        P = self.P
+        op = abi.OpacityParams()
+        op.use_electron_scattering = P.scalar("opacity_electron_scattering", int)
+        op.use_free_free = P.scalar("opacity_free_free", int)
+        op.use_bound_free = P.scalar("opacity_bound_free", int)
+        op.use_line_expansion = P.scalar("opacity_line_expansion", int)
+        op.use_fuzz_expansion = P.scalar("opacity_fuzz_expansion", int)
+        ze = [int(v) for v in P.vector("opacity_atom_zero_epsilon")]
+        op.n_atom_zero_epsilon = len(ze)
+        op.atom_zero_epsilon = keep.i(np.array(ze, dtype=np.int32)) if ze else None
+        op.epsilon = P.scalar("opacity_epsilon")
+        op.maximum_opacity = P.scalar("opacity_maximum_opacity")
+        op.temp_min = P.scalar("limits_temp_min")
+        op.temp_max = P.scalar("limits_temp_max")
+        op.line_velocity_width = P.scalar("line_velocity_width")
+        return op
+
+    def atomic_struct(self, keep: abi.Keep) -> Optional[abi.AtomicData]:
+        if self.atoms is None:
+            return None
+        return self.atoms.to_struct(keep, self.nu_grid())
+
+
+# ---------------------------------------------------------------- 1D models
+def sphere_model(v_edges: np.ndarray, t_now: float, rho: np.ndarray, T: np.ndarray,
+                 X: np.ndarray, elem_Z, elem_A, r_min: float = 0.0) -> ZoneModel:
+    """A 1D_sphere "SNR" model: r_out = v t (grid_1D_sphere.cpp:318-324);
+    mass fractions normalised per zone as the reader does (:335-351)."""
+    v = np.asarray(v_edges, dtype=np.float64)
+    r_out = np.array([vi * t_now for vi in v], dtype=np.float64)
+    X = np.asarray(X, dtype=np.float64).reshape(v.size, -1)
+    Xn = np.empty_like(X)
+    for i in range(X.shape[0]):
+        norm = 0.0
+        for k in range(X.shape[1]):
+            norm += X[i, k]
+        for k in range(X.shape[1]):
+            Xn[i, k] = X[i, k] / norm
+    return ZoneModel(type=abi.GRID_1D_SPHERE, t_now=float(t_now), rho=np.asarray(rho, np.float64),
+                     T=np.asarray(T, np.float64), X=Xn,
+                     elem_Z=np.asarray(elem_Z, np.int32), elem_A=np.asarray(elem_A, np.int32),
+                     vol=shell_volumes(r_min, r_out), r_min=float(r_min), r_out=r_out, v=v)
+
+
+def lightbulb_grey(n_packets: int = 1_000_000, n_zones: int = 128, n_bins: int = 1024,
+                   radiative_eq: int = 0, seed: int = 0) -> Workload:
+    """Plain method, small: 1D homologous sphere at t = 10 d, 128 zones to
+    v_max = 1e9 cm/s, rho = 1e-13 g/cm^3, grey kappa = 0.1 cm^2/g with
+    epsilon = 0.1, central 1e4 K blackbody lightbulb, 1024 log bins
+    1e14..1e16 Hz, FP64 throughout."""
+    t = 10 * 86400.0
+    v = np.array([(i + 1) * 1e9 / n_zones for i in range(n_zones)])
+    z = sphere_model(v, t, np.full(n_zones, 1e-13), np.full(n_zones, 1e4),
+                     np.ones((n_zones, 1)), [1], [1])
+    d = log_delta_for_bins(1e14, 1e16, n_bins)
+    grid = [1e14, 1e16, d, 1]
+    params = {
+        "grid_type": "grid_1D_sphere", "hydro_module": "homologous",
+        "transport_nu_grid": grid, "spectrum_nu_grid": grid,
+        "transport_steady_iterate": 1, "transport_radiative_equilibrium": radiative_eq,
+        "opacity_grey_opacity": 0.1, "opacity_epsilon": 0.1,
+        "core_n_emit": int(n_packets), "core_radius": 0.0, "core_temperature": 1e4,
+        "core_luminosity": 1e43,
+        "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
+        "particles_max_total": max(int(1e7), int(n_packets)),
+    }
+    return Workload("lightbulb_grey_1d", params, z,
+                    notes={"log_del": d, "v_max": 1e9, "t_days": 10.0})
