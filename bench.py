@@ -1,0 +1,296 @@
+"""Benchmark: MC packets/s of one implicit Monte Carlo transport step on the
+precision configuration (1D Type Ia-like ejecta, 256 zones, 5e5 synthetic
+lines, LTE, 4096 bins, 1e7 packets; FP32 opacity tables, FP64 transport).
+
+A step is transport::step: the per-zone opacity build (LTE solve + line
+binning) followed by emission, propagation and tally normalisation of all
+packets, run through the C ABI (include/sedona_gpu.h).
+
+  value     device-resident: zone state, atomic data and tables stay in HBM;
+            timed with CUDA events on the library's stream (opacity build +
+            transport), L2 flushed between steps (256 MiB write).
+  e2e       the same step through the C ABI with host buffers: zone state
+            copied host->device (sed_set_grid), sed_step, spectrum and zone
+            tallies copied device->host, wall-clock per step.
+  --impl reference   the reference's own CPU implementation (built from the
+            reference sources into oracle/_ref/sedona_ref) on all host cores,
+            each step a bounded sample of the same workload.
+
+Multi-GPU: packets are independent, so N ranks run N independent replicas of
+the step (weak scaling); no collective is on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC packets/s at matched spectrum chi-squared (mixed/batched vs plain FP64), 1 B200"
+UNIT = "packets/s"
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, workload_fn, rank: int) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+    import run_ref
+    if not run_ref.available():
+        return {"impl": "reference", "unavailable": "reference harness oracle/_ref/sedona_ref is not built"}
+    cores = os.cpu_count() or 1
+    n_sample = args.ref_packets
+    w = workload_fn(n_sample)
+    # warm-up (untimed), then the timed steps; each step is the reference's
+    # own transport::step on a bounded packet sample
+    out = run_ref.run(w, "free", threads=cores, steps=args.warmup + args.steps, timeout=3600)
+    times = list(out["step_seconds"])[args.warmup:]
+    t_sample = sum(times) / len(times)
+    t_opac = float(out["set_opacity_seconds"][0])
+    # the opacity build is per step, propagation per packet: the reference's
+    # time for the full step is t_opac + (t_sample - t_opac) * N / n_sample
+    n_full = args.packets
+    t = t_opac + max(t_sample - t_opac, 0.0) * n_full / n_sample
+    value = n_full / t
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "n_zones": w.zones.n_zones, "n_lines": w.notes.get("n_lines"),
+                       "n_bins": w.nu_grid().n, "packets_per_step": n_sample, "threads": cores},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": "transport::step of the %s workload (full zone/line/bin sizes) with %d "
+                                       "packets per step (%.2f s, of which set_opacity %.2f s); full-step time "
+                                       "= set_opacity + propagation scaled to %d packets" %
+                                       (w.name, n_sample, t_sample, t_opac, n_full)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "sample_packets_per_s": n_sample / t_sample, "set_opacity_seconds": t_opac}
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--packets", type=int, default=10_000_000)
+    ap.add_argument("--ref-packets", type=int, default=20_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = _env_rank()
+
+    from pubsed_b200 import workloads
+
+    def wl(n):
+        return workloads.type_ia(n_packets=n)
+
+    if args.impl == "reference":
+        if world > 1 and rank != 0:
+            return
+        print(json.dumps(run_reference(args, wl, rank)), flush=True)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from pubsed_b200 import abi, engine
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    w = wl(args.packets)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def run_mode(precision, steps, warmup, record_clock=False):
+        eng = engine.Engine(w, precision=precision, device=local, seed_offset=rank)
+        for _ in range(warmup):
+            flush.fill_(1.0)
+            eng.step(1.0)
+        barrier()
+        stats = []
+        clk = ClockSampler(local)
+        t0 = time.perf_counter()
+        with (clk if record_clock else _Null()):
+            for _ in range(steps):
+                flush.fill_(float(len(stats)))
+                torch.cuda.synchronize()
+                stats.append(eng.step(1.0))
+        barrier()
+        wall = time.perf_counter() - t0
+        return eng, stats, wall, clk
+
+    # plain FP64 form (the denominator of the mixed-precision target)
+    fp64 = None
+    if not args.skip_fp64:
+        e64, st64, wall64, _ = run_mode(abi.PREC_FP64, args.steps, min(args.warmup, 3))
+        ms64 = sum(s["ms_total"] for s in st64) / len(st64)
+        fp64 = {"value": args.packets / (ms64 * 1e-3), "ms_per_step": ms64}
+        spec64 = e64.spectrum()
+        e64.close()
+
+    eng, stats, wall, clk = run_mode(abi.PREC_MIXED, args.steps, args.warmup, record_clock=True)
+    ms = [s["ms_total"] for s in stats]
+    ms_step = sum(ms) / len(ms)
+    # max over ranks
+    t_local = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    ms_max = float(t_local.item())
+    value = world * args.packets / (ms_max * 1e-3)
+    last = stats[-1]
+    kern_ms = sum(s["ms_propagate_kernel"] for s in stats) / len(stats)
+
+    # end-to-end through the C ABI with host buffers
+    e2e_times = []
+    h2d = d2h = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b_in = eng.upload_grid()
+        eng.step(1.0)
+        flux, click = eng.spectrum()
+        tal = eng.tallies()
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+        h2d = b_in
+        d2h = flux.nbytes + click.nbytes + sum(v.nbytes for v in tal.values())
+    e2e_t = sum(e2e_times) / len(e2e_times)
+    t_e2e = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.packets / float(t_e2e.item())
+
+    # roofline of the packet kernel: algorithmic bytes per segment and per
+    # packet (zone geometry 16 B, {abs,scat} 8 B (FP32), J RMW 16 B, e_abs
+    # RMW 16 B, force RMW 64 B per segment; 2 x 76 B state + 32 B spectrum +
+    # 80 B emission CDF per packet)
+    b_seg = 16 + 8 + 16 + 16 + 64
+    b_pkt = 264
+    alg_bytes = last["n_segments"] * b_seg + args.packets * b_pkt
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "propagate_kernel_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tr = json.load(f)
+        # scale the captured launch's DRAM bytes by segments processed
+        traffic = tr["dram_bytes"] * (last["n_segments"] / tr["n_segments"])
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 transport / f32 opacity tables", "data": "synthetic",
+        "config": {"workload": w.name, "n_zones": w.zones.n_zones, "n_lines": w.notes["n_lines"],
+                   "n_bins": w.nu_grid().n, "packets_per_step": args.packets, "precision": "mixed",
+                   "segments_per_step": last["n_segments"], "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "ms_opacity": last["ms_opacity"], "ms_transport": last["ms_transport"],
+        "plain_fp64": fp64,
+        "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": e2e_t * 1e3},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "propagate_kernel", "kernel_ms": kern_ms,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        try:
+            ref = run_reference(argparse.Namespace(ref_packets=args.ref_packets, warmup=1, steps=1,
+                                                     packets=args.packets), wl, rank)
+            if "unavailable" in ref:
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                        "sample": ref["unavailable"]}
+            else:
+                line["cpu_baseline"] = ref["cpu_baseline"]
+        except Exception as ex:  # report, do not hide
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": "failed: %s" % str(ex)[:200]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+if __name__ == "__main__":
+    main()

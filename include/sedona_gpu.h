@@ -73,6 +73,9 @@ typedef struct sed_transport_params {
   double fleck_alpha;            /* transport_fleck_alpha */
   int32_t max_segments;          /* per-packet segment limit; 0 = default (10^7) */
   int32_t reserved;
+  int64_t first_packet_id;       /* Philox stream id of this context's first packet:
+                                    rank r of N replicas uses r * core_n_emit, so
+                                    the N emissions form one packet ensemble */
   sed_locate_grid nu_grid;       /* transport_nu_grid */
   sed_locate_grid spec_time;     /* spectrum_time_grid */
   sed_locate_grid spec_nu;       /* spectrum_nu_grid */

@@ -78,4 +78,7 @@ for p in "${pids[@]}"; do wait "$p"; done
 $CXX "${FLAGS[@]}" "${INC[@]}" -c "$HERE/shims.cpp" -o "$OBJ/shims.o"
 $CXX "${FLAGS[@]}" "${INC[@]}" -c "$HERE/ref_harness.cpp" -o "$OBJ/ref_harness.o"
 $CXX "${FLAGS[@]}" -o "$OUT/sedona_ref" "$OBJ"/*.o "$OUT/liblua.a" -ldl -lm
+# the reference's own locate_array test program (prints value/index pairs)
+$CXX "${FLAGS[@]}" "${INC[@]}" -o "$OUT/locate_array_test" "$REF/src/utils/locate_array_test.cpp" \
+  "$OBJ/utils_locate_array.cpp.o" "$OBJ/utils_h5utils.cpp.o" "$OBJ/shims.o" -lm
 echo "built $OUT/sedona_ref"

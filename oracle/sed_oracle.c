@@ -1193,7 +1193,7 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
   for (int64_t k = 0; k < count; ++k) {
     packet p;
     memset(&p, 0, sizeof p);
-    p.pid = (uint64_t)(first + k);
+    p.pid = (uint64_t)(o->tp.first_packet_id + first + k);
     p.n = 0;
     emit_core_packet(o, &p, Ep, t_now, dt);
     p.n = K;
@@ -1214,7 +1214,10 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
   }
   o->n_escaped_acc += nesc;
   o->n_active_acc += count;
-  if (finish) finish_step(o, dt, n_emit, o->n_escaped_acc);
+  if (finish) {
+    finish_step(o, dt, n_emit, o->n_escaped_acc);
+    o->step++;  /* the next step draws from fresh streams */
+  }
   if (st) {
     memset(st, 0, sizeof *st);
     st->n_packets = count; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
@@ -1285,6 +1288,9 @@ int oracle_get_packet_records(oracle_ctx* o, int64_t n, int32_t* fate, int32_t* 
 }
 
 const char* oracle_last_error(oracle_ctx* o) { return o ? o->err : "null context"; }
+
+void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) { oracle_philox4x32_10(ctr, key, out); }
+double oracle_uniform(uint32_t seed, uint64_t pid, uint32_t step, uint32_t n) { return oracle_packet_uniform(seed, pid, step, n); }
 
 void oracle_ctx_destroy(oracle_ctx* o)
 {

@@ -42,6 +42,9 @@ int oracle_get_fuzz_bins(oracle_ctx* o, int32_t* bins);
 /* locate_array::locate / locate_within_bounds on an arbitrary grid (for tests) */
 int oracle_locate(const sed_locate_grid* g, double x);
 const char* oracle_last_error(oracle_ctx* o);
+/* Philox4x32-10 block and the packet-stream uniform (oracle/philox.h) */
+void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double oracle_uniform(uint32_t seed, uint64_t pid, uint32_t step, uint32_t n);
 void oracle_ctx_destroy(oracle_ctx* o);
 
 #ifdef __cplusplus

@@ -47,6 +47,7 @@ class TransportParams(C.Structure):
         ("core_radius", C.c_double), ("core_luminosity", C.c_double),
         ("core_temperature", C.c_double), ("core_photon_frequency", C.c_double),
         ("fleck_alpha", C.c_double), ("max_segments", C.c_int32), ("reserved", C.c_int32),
+        ("first_packet_id", C.c_int64),
         ("nu_grid", LocateGrid), ("spec_time", LocateGrid), ("spec_nu", LocateGrid),
         ("spec_mu", LocateGrid), ("spec_phi", LocateGrid),
     ]

@@ -1,0 +1,717 @@
+// sed_abi.cu -- host side of the C ABI declared in include/sedona_gpu.h.
+//
+// A sed_ctx owns one CUDA stream and every device buffer of the transport
+// step: zone state, atomic data, opacity tables, tallies.  Host-side work is
+// limited to set-up (copies, the core emission CDF, sorting line lists by
+// frequency bin); a transport step is a short sequence of kernel launches on
+// the context's stream followed by one synchronisation.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/sedona_gpu.h"
+#include "sed_internal.h"
+
+using namespace sed;
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t resize(size_t m)
+  {
+    if (m == n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (m == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, m * sizeof(T));
+    if (e == cudaSuccess) n = m;
+    return e;
+  }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// host copy of a locate_array with the same lookup rules as the device
+struct HostLoc {
+  int type = 0;
+  double min = 0, del = 0;
+  std::vector<double> x;
+  int n() const { return (int)x.size(); }
+  double left(int i) const { return i == 0 ? min : x[i - 1]; }
+  double delta(int i) const { return i == 0 ? x[0] - min : x[i] - x[i - 1]; }
+  double center(int i) const { return i == 0 ? 0.5 * (min + x[0]) : 0.5 * (x[i - 1] + x[i]); }
+  int upper(double v) const { return (int)(std::upper_bound(x.begin(), x.end(), v) - x.begin()); }
+  int locate(double v) const  // locate_array::locate (src/utils/locate_array.cpp:191-218)
+  {
+    const int nn = n();
+    if (nn == 1) return 0;
+    if (v >= x[nn - 1]) return nn;
+    if (v < min) return 0;
+    int ind;
+    if (type == LOC_FLEX) return upper(v);
+    else if (type == LOC_LIN) ind = (int)std::floor((v - min) / del);
+    else if (type == LOC_LOG) ind = (int)std::floor(std::log(v / min) / std::log(1 + del));
+    else return 0;
+    if (ind != 0 && ind != nn && (left(ind) > v || x[ind] <= v)) ind = upper(v);
+    return ind;
+  }
+  int within(double v) const { const int i = locate(v); return i == n() ? n() - 1 : i; }
+};
+
+HostLoc host_loc(const sed_locate_grid& g)
+{
+  HostLoc h;
+  h.type = g.type;
+  h.min = g.min;
+  h.del = g.del;
+  h.x.assign(g.right, g.right + g.n);
+  return h;
+}
+
+}  // namespace
+
+struct sed_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  std::string err;
+  sed_transport_params tp{};
+  HostLoc nu, st, sn, sm, sp;
+  DevBuf<double> d_nu, d_st, d_sn, d_sm, d_sp, d_core_cdf;
+  uint32_t step = 0;
+
+  // grid
+  bool have_grid = false;
+  int gtype = 0, nz = 0, nelem = 0, homologous = 1, nx = 0, ny = 0, nzz = 0;
+  double t_grid = 0;
+  HostLoc r_out, ax[3];
+  DevBuf<double> d_r_out, d_v_r, d_ax[3], d_vol, d_rho, d_T, d_egas, d_grey, d_X;
+  DevBuf<int32_t> d_eZ, d_eA;
+  std::vector<int32_t> h_eZ;
+
+  // opacity parameters and atomic data
+  sed_opacity_params op{};
+  std::vector<int32_t> zero_eps;
+  DevBuf<int32_t> d_zero_eps_atom;
+  bool have_atoms = false;
+  int natoms = 0, n_ions_total = 0, n_lev_total = 0, nfuzz = 0, nlines = 0;
+  DevBuf<int32_t> d_ion_off, d_lev_off, d_lev_ion, d_lev_g, d_lev_ic, d_photo_off, d_line_seg, d_line_l, d_line_u,
+      d_fuzz_seg, d_fz_ion;
+  DevBuf<double> d_ion_chi, d_lev_E, d_lev_Eion, d_photo_E, d_photo_s, d_line_nu, d_line_f, d_fz_nu, d_fz_gf, d_fz_El;
+  DevBuf<float> d_fz_A32, d_fz_El32, d_fz_hnu32;
+  std::vector<int32_t> fuzz_order;  // sorted position -> caller's index
+
+  // tables
+  bool have_opacity = false;
+  DevBuf<unsigned char> d_opac, d_cdf;
+  DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
+      d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
+  DevBuf<int32_t> d_solve_err;
+
+  // tallies
+  DevBuf<double> d_J, d_e_abs, d_e_rad, d_fx, d_fy, d_fz, d_fr, d_flux, d_click;
+  DevBuf<unsigned long long> d_counters;
+  int64_t nspec = 0;
+
+  // per-packet records
+  int record = 0;
+  int64_t n_rec = 0;
+  DevBuf<int32_t> d_rec_fate, d_rec_ind, d_rec_draws;
+  DevBuf<double> d_rec_state;
+};
+
+namespace {
+
+int set_err(sed_ctx* c, int code, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                       \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess)                                                                             \
+      return set_err(c, e_ == cudaErrorMemoryAllocation ? SED_ERR_NOMEM : SED_ERR_CUDA, "%s: %s (%s:%d)", \
+                     #call, cudaGetErrorString(e_), __FILE__, __LINE__);                               \
+  } while (0)
+
+template <typename T>
+cudaError_t upload(sed_ctx* c, DevBuf<T>& b, const T* src, size_t n)
+{
+  cudaError_t e = b.resize(n ? n : 1);
+  if (e != cudaSuccess) return e;
+  if (n && src) return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+  return cudaMemsetAsync(b.p, 0, (n ? n : 1) * sizeof(T), c->stream);
+}
+
+DevLoc dev_loc(const HostLoc& h, const DevBuf<double>& d)
+{
+  DevLoc g;
+  g.n = h.n();
+  g.type = h.type;
+  g.min = h.min;
+  g.del = h.del;
+  g.right = d.p;
+  return g;
+}
+
+bool valid_grid(const sed_locate_grid& g) { return g.n > 0 && g.right != nullptr; }
+
+int alloc_tallies(sed_ctx* c)
+{
+  const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
+  const size_t nj = c->tp.store_Jnu ? nn : 1;
+  CK(c->d_J.resize(nz * nj));
+  CK(c->d_e_abs.resize(nz)); CK(c->d_e_rad.resize(nz));
+  CK(c->d_fx.resize(nz)); CK(c->d_fy.resize(nz)); CK(c->d_fz.resize(nz)); CK(c->d_fr.resize(nz));
+  const size_t esz = c->tp.precision ? sizeof(float) : sizeof(double);
+  CK(c->d_opac.resize(nz * nn * 2 * esz));
+  CK(c->d_cdf.resize(nz * nn * esz));
+  CK(c->d_eps_imc.resize(nz)); CK(c->d_planck.resize(nz)); CK(c->d_ross.resize(nz)); CK(c->d_L.resize(nz));
+  CK(c->d_n_elec.resize(nz)); CK(c->d_temp_c.resize(nz)); CK(c->d_solve_err.resize(nz));
+  CK(c->d_abs64.resize(nz * nn)); CK(c->d_scat64.resize(nz * nn)); CK(c->d_emis64.resize(nz * nn));
+  CK(cudaMemsetAsync(c->d_n_elec.p, 0, nz * sizeof(double), c->stream));
+  return SED_OK;
+}
+
+int alloc_lte(sed_ctx* c)
+{
+  const size_t nz = (size_t)c->nz;
+  const size_t na = (size_t)std::max(c->nelem, 1);
+  CK(c->d_n_dens.resize(nz * na));
+  CK(c->d_mass_frac.resize(nz * na));
+  const size_t ni = (size_t)std::max(c->n_ions_total, 1), nl = (size_t)std::max(c->n_lev_total, 1);
+  CK(c->d_ion_part.resize(nz * ni));
+  CK(c->d_ion_frac.resize(nz * ni));
+  CK(c->d_lev_n.resize(nz * nl));
+  CK(c->d_boltz.resize(nz * nl));
+  return SED_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sed_version(void) { return "sedona-b200 transport 0.1 (sm_100a)"; }
+
+int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
+{
+  if (!p || !out) return SED_ERR_ARG;
+  *out = nullptr;
+  if (!valid_grid(p->nu_grid) || !valid_grid(p->spec_time) || !valid_grid(p->spec_nu) || !valid_grid(p->spec_mu) ||
+      !valid_grid(p->spec_phi))
+    return SED_ERR_ARG;
+  sed_ctx* c = new sed_ctx();
+  if (device < 0) cudaGetDevice(&c->device);
+  else c->device = device;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) { delete c; return SED_ERR_CUDA; }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return SED_ERR_CUDA; }
+  for (auto& ev : c->ev) cudaEventCreate(&ev);
+  c->tp = *p;
+  c->nu = host_loc(p->nu_grid);
+  c->st = host_loc(p->spec_time);
+  c->sn = host_loc(p->spec_nu);
+  c->sm = host_loc(p->spec_mu);
+  c->sp = host_loc(p->spec_phi);
+  // grid pointers in the copy are not retained
+  c->tp.nu_grid.right = c->tp.spec_time.right = c->tp.spec_nu.right = c->tp.spec_mu.right = c->tp.spec_phi.right = nullptr;
+  CK(upload(c, c->d_nu, c->nu.x.data(), c->nu.x.size()));
+  CK(upload(c, c->d_st, c->st.x.data(), c->st.x.size()));
+  CK(upload(c, c->d_sn, c->sn.x.data(), c->sn.x.size()));
+  CK(upload(c, c->d_sm, c->sm.x.data(), c->sm.x.size()));
+  CK(upload(c, c->d_sp, c->sp.x.data(), c->sp.x.size()));
+  // core emission CDF, transport::setup_core_emission (src/transport/transport_init.cpp:465-556)
+  const int nn = c->nu.n();
+  std::vector<double> cdf(nn);
+  for (int j = 0; j < nn; ++j) {
+    const double nu = c->nu.center(j), dnu = c->nu.delta(j);
+    double bb;
+    if (p->core_temperature <= 0) bb = 1;
+    else {
+      const double zeta = H_PLANCK * nu / K_BOLTZ / p->core_temperature;
+      bb = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (std::exp(zeta) - 1);
+    }
+    const double w = bb * dnu * 1.0;
+    cdf[j] = (j == 0) ? w : cdf[j - 1] + w;
+  }
+  for (int j = 0; j < nn; ++j) if (std::isnan(cdf[j])) cdf[j] = 0;
+  if (cdf[nn - 1] == 0) for (int j = 0; j < nn; ++j) cdf[j] = 1.0;
+  const double N = cdf[nn - 1];
+  for (int j = 0; j < nn; ++j) cdf[j] /= N;
+  CK(upload(c, c->d_core_cdf, cdf.data(), cdf.size()));
+  c->nspec = (int64_t)c->st.n() * c->sn.n() * c->sm.n() * c->sp.n();
+  CK(c->d_flux.resize(c->nspec));
+  CK(c->d_click.resize(c->nspec));
+  CK(c->d_counters.resize(C_COUNT + 1));
+  CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->op.epsilon = 1.0;
+  c->op.maximum_opacity = 1e40;
+  c->op.temp_min = 1000;
+  c->op.temp_max = 1e8;
+  *out = c;
+  return SED_OK;
+}
+
+int sed_set_grid(sed_ctx* c, const sed_grid* g)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!g || g->n_zones <= 0 || !g->vol || !g->rho || !g->T_gas) return set_err(c, SED_ERR_ARG, "sed_set_grid: missing zone arrays");
+  if (g->n_elems < 0 || (g->n_elems > 0 && (!g->X || !g->elem_A || !g->elem_Z)))
+    return set_err(c, SED_ERR_ARG, "sed_set_grid: missing composition");
+  const bool resized = (g->n_zones != c->nz) || !c->have_grid;
+  c->gtype = g->type;
+  c->nz = g->n_zones;
+  c->nelem = g->n_elems;
+  c->homologous = g->homologous;
+  c->t_grid = g->t_now;
+  const size_t nz = (size_t)g->n_zones;
+  if (g->type == SED_GRID_1D_SPHERE) {
+    if (!g->r_out) return set_err(c, SED_ERR_ARG, "sed_set_grid: 1D sphere needs r_out");
+    sed_locate_grid rg{g->n_zones, SED_LOC_FLEX, g->r_min, 0.0, g->r_out};
+    c->r_out = host_loc(rg);
+    CK(upload(c, c->d_r_out, g->r_out, nz));
+    CK(upload(c, c->d_v_r, g->v_r, g->v_r ? nz : 0));
+  } else if (g->type == SED_GRID_3D_CART) {
+    if ((int64_t)g->nx * g->ny * g->nz != g->n_zones) return set_err(c, SED_ERR_ARG, "sed_set_grid: nx*ny*nz != n_zones");
+    if (!valid_grid(g->x_axis) || !valid_grid(g->y_axis) || !valid_grid(g->z_axis) || g->x_axis.n != g->nx ||
+        g->y_axis.n != g->ny || g->z_axis.n != g->nz)
+      return set_err(c, SED_ERR_ARG, "sed_set_grid: bad 3D axes");
+    c->nx = g->nx; c->ny = g->ny; c->nzz = g->nz;
+    const sed_locate_grid* axes[3] = {&g->x_axis, &g->y_axis, &g->z_axis};
+    for (int a = 0; a < 3; ++a) {
+      c->ax[a] = host_loc(*axes[a]);
+      CK(upload(c, c->d_ax[a], c->ax[a].x.data(), c->ax[a].x.size()));
+    }
+  } else {
+    return set_err(c, SED_ERR_ARG, "sed_set_grid: unknown grid type %d", g->type);
+  }
+  CK(upload(c, c->d_vol, g->vol, nz));
+  CK(upload(c, c->d_rho, g->rho, nz));
+  CK(upload(c, c->d_T, g->T_gas, nz));
+  CK(upload(c, c->d_egas, g->e_gas, g->e_gas ? nz : 0));
+  CK(upload(c, c->d_grey, g->total_grey_opacity, g->total_grey_opacity ? nz : 0));
+  CK(upload(c, c->d_X, g->X, nz * (size_t)g->n_elems));
+  CK(upload(c, c->d_eZ, g->elem_Z, (size_t)g->n_elems));
+  CK(upload(c, c->d_eA, g->elem_A, (size_t)g->n_elems));
+  c->h_eZ.assign(g->elem_Z, g->elem_Z + g->n_elems);
+  if (resized) {
+    int rc = alloc_tallies(c);
+    if (rc) return rc;
+    c->have_opacity = false;
+  }
+  int rc = alloc_lte(c);
+  if (rc) return rc;
+  // per-atom epsilon switch
+  std::vector<int32_t> ze(std::max(c->nelem, 1), 0);
+  for (int a = 0; a < c->nelem; ++a)
+    for (int z : c->zero_eps) if (z == c->h_eZ[a]) ze[a] = 1;
+  CK(upload(c, c->d_zero_eps_atom, ze.data(), ze.size()));
+  c->have_grid = true;
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_set_opacity_params(sed_ctx* c, const sed_opacity_params* op)
+{
+  if (!c || !op) return SED_ERR_ARG;
+  c->op = *op;
+  c->zero_eps.assign(op->atom_zero_epsilon, op->atom_zero_epsilon + std::max(op->n_atom_zero_epsilon, 0));
+  c->op.atom_zero_epsilon = nullptr;
+  if (c->have_grid) {
+    std::vector<int32_t> ze(std::max(c->nelem, 1), 0);
+    for (int a = 0; a < c->nelem; ++a)
+      for (int z : c->zero_eps) if (z == c->h_eZ[a]) ze[a] = 1;
+    CK(upload(c, c->d_zero_eps_atom, ze.data(), ze.size()));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return SED_OK;
+}
+
+int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
+{
+  if (!c || !a || a->n_atoms < 0) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_set_atomic_data: call sed_set_grid first");
+  if (a->n_atoms != c->nelem) return set_err(c, SED_ERR_ARG, "sed_set_atomic_data: %d atoms for %d elements", a->n_atoms, c->nelem);
+  const int na = a->n_atoms;
+  const int nn = c->nu.n();
+  c->natoms = na;
+  c->n_ions_total = a->ion_off[na];
+  c->n_lev_total = a->lev_off[na];
+  CK(upload(c, c->d_ion_off, a->ion_off, (size_t)na + 1));
+  CK(upload(c, c->d_ion_chi, a->ion_chi, (size_t)c->n_ions_total));
+  CK(upload(c, c->d_lev_off, a->lev_off, (size_t)na + 1));
+  const size_t nl = (size_t)c->n_lev_total;
+  CK(upload(c, c->d_lev_ion, a->lev_ion, nl));
+  CK(upload(c, c->d_lev_g, a->lev_g, nl));
+  CK(upload(c, c->d_lev_ic, a->lev_ic, nl));
+  CK(upload(c, c->d_lev_E, a->lev_E, nl));
+  CK(upload(c, c->d_lev_Eion, a->lev_Eion, nl));
+  CK(upload(c, c->d_photo_off, a->photo_off, nl + 1));
+  const size_t np = (size_t)a->photo_off[nl];
+  CK(upload(c, c->d_photo_E, a->photo_E, np));
+  CK(upload(c, c->d_photo_s, a->photo_s, np));
+  // level-to-level lines: bin (AtomicData.cpp:680), stable sort by (atom, bin)
+  {
+    const int n = a->line_off[na];
+    std::vector<int> bin(n), order(n);
+    std::vector<int64_t> key(n);
+    for (int at = 0; at < na; ++at)
+      for (int k = a->line_off[at]; k < a->line_off[at + 1]; ++k) {
+        bin[k] = c->nu.within(a->line_nu[k]);
+        key[k] = (int64_t)at * nn + bin[k];
+      }
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+    std::vector<int32_t> ll(n), lu(n), seg((size_t)na * nn + 1, 0);
+    std::vector<double> lnu(n), lf(n);
+    for (int k = 0; k < n; ++k) {
+      const int s = order[k];
+      ll[k] = a->line_l[s]; lu[k] = a->line_u[s]; lnu[k] = a->line_nu[s]; lf[k] = a->line_f[s];
+      seg[key[s] + 1]++;
+    }
+    for (size_t s = 1; s < seg.size(); ++s) seg[s] += seg[s - 1];
+    c->nlines = n;
+    CK(upload(c, c->d_line_seg, seg.data(), seg.size()));
+    CK(upload(c, c->d_line_l, ll.data(), (size_t)n));
+    CK(upload(c, c->d_line_u, lu.data(), (size_t)n));
+    CK(upload(c, c->d_line_nu, lnu.data(), (size_t)n));
+    CK(upload(c, c->d_line_f, lf.data(), (size_t)n));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  // fuzz lines: bin (AtomicData.cpp:851), stable sort by (atom, bin), FP32 constants
+  {
+    const int n = a->fuzz_off[na];
+    std::vector<int64_t> key(n);
+    std::vector<int> order(n);
+    for (int at = 0; at < na; ++at)
+      for (int k = a->fuzz_off[at]; k < a->fuzz_off[at + 1]; ++k) key[k] = (int64_t)at * nn + c->nu.within(a->fuzz_nu[k]);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
+    std::vector<int32_t> ion(n), seg((size_t)na * nn + 1, 0);
+    std::vector<double> fnu(n), fgf(n), fEl(n);
+    std::vector<float> A32(n), El32(n), h32(n);
+    for (int k = 0; k < n; ++k) {
+      const int s = order[k];
+      fnu[k] = a->fuzz_nu[s]; fgf[k] = a->fuzz_gf[s]; fEl[k] = a->fuzz_El[s]; ion[k] = a->fuzz_ion[s];
+      A32[k] = (float)(SIGMA_TOT * (C_LIGHT / fnu[k]) * fgf[k]);
+      El32[k] = (float)(fEl[k] / K_EV);
+      h32[k] = (float)(H_PLANCK * fnu[k] / K_BOLTZ);
+      seg[key[s] + 1]++;
+    }
+    for (size_t s = 1; s < seg.size(); ++s) seg[s] += seg[s - 1];
+    c->nfuzz = n;
+    c->fuzz_order = order;
+    CK(upload(c, c->d_fuzz_seg, seg.data(), seg.size()));
+    CK(upload(c, c->d_fz_nu, fnu.data(), (size_t)n));
+    CK(upload(c, c->d_fz_gf, fgf.data(), (size_t)n));
+    CK(upload(c, c->d_fz_El, fEl.data(), (size_t)n));
+    CK(upload(c, c->d_fz_ion, ion.data(), (size_t)n));
+    CK(upload(c, c->d_fz_A32, A32.data(), (size_t)n));
+    CK(upload(c, c->d_fz_El32, El32.data(), (size_t)n));
+    CK(upload(c, c->d_fz_hnu32, h32.data(), (size_t)n));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->have_atoms = true;
+  int rc = alloc_lte(c);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_set_opacity(sed_ctx* c, double dt)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_set_opacity: no grid");
+  if (c->tp.steady_state) dt = 1;
+  OpacityArgs A{};
+  A.nzones = c->nz; A.n_nu = c->nu.n(); A.nelem = c->nelem;
+  A.use_es = c->op.use_electron_scattering; A.use_ff = c->op.use_free_free; A.use_bf = c->op.use_bound_free;
+  A.use_line = c->op.use_line_expansion; A.use_fuzz = c->op.use_fuzz_expansion;
+  A.radiative_eq = c->tp.radiative_eq; A.omit_scat = c->tp.omit_scattering; A.precision = c->tp.precision;
+  A.epsilon = c->op.epsilon; A.max_opacity = c->op.maximum_opacity; A.temp_min = c->op.temp_min;
+  A.temp_max = c->op.temp_max; A.fleck_alpha = c->tp.fleck_alpha; A.dt = dt; A.time = c->t_grid;
+  A.nu = dev_loc(c->nu, c->d_nu);
+  A.rho = c->d_rho.p; A.T = c->d_T.p; A.e_gas = c->d_egas.p; A.grey = c->d_grey.p; A.X = c->d_X.p;
+  A.eZ = c->d_eZ.p; A.eA = c->d_eA.p; A.zero_eps_atom = c->d_zero_eps_atom.p;
+  A.natoms = c->have_atoms ? c->natoms : 0;
+  A.ion_off = c->d_ion_off.p; A.lev_off = c->d_lev_off.p; A.lev_ion = c->d_lev_ion.p; A.lev_g = c->d_lev_g.p;
+  A.lev_ic = c->d_lev_ic.p; A.photo_off = c->d_photo_off.p; A.ion_chi = c->d_ion_chi.p; A.lev_E = c->d_lev_E.p;
+  A.lev_Eion = c->d_lev_Eion.p; A.photo_E = c->d_photo_E.p; A.photo_s = c->d_photo_s.p;
+  A.line_seg = c->d_line_seg.p; A.line_l = c->d_line_l.p; A.line_u = c->d_line_u.p; A.line_nu = c->d_line_nu.p;
+  A.line_f = c->d_line_f.p;
+  A.fuzz_seg = c->d_fuzz_seg.p; A.fz_nu = c->d_fz_nu.p; A.fz_gf = c->d_fz_gf.p; A.fz_El = c->d_fz_El.p;
+  A.fz_ion = c->d_fz_ion.p; A.fz_A32 = c->d_fz_A32.p; A.fz_El32 = c->d_fz_El32.p; A.fz_hnu32 = c->d_fz_hnu32.p;
+  A.nfuzz = c->nfuzz;
+  A.ion_part = c->d_ion_part.p; A.ion_frac = c->d_ion_frac.p; A.lev_n = c->d_lev_n.p;
+  A.n_ions_total = c->n_ions_total; A.n_lev_total = c->n_lev_total;
+  A.n_elec = c->d_n_elec.p; A.n_dens = c->d_n_dens.p; A.mass_frac = c->d_mass_frac.p; A.temp_c = c->d_temp_c.p;
+  A.solve_err = c->d_solve_err.p; A.boltz = c->d_boltz.p;
+  A.abs64 = c->d_abs64.p; A.scat64 = c->d_scat64.p; A.emis64 = c->d_emis64.p;
+  A.opac_out = c->d_opac.p; A.cdf_out = c->d_cdf.p;
+  A.eps_imc = c->d_eps_imc.p; A.planck = c->d_planck.p; A.ross = c->d_ross.p; A.L_th = c->d_L.p;
+  if (!c->have_atoms && (A.use_es || A.use_ff || A.use_bf || A.use_line || A.use_fuzz)) {
+    // zones without grey opacity would need atomic data; grey zones are fine
+  }
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  launch_opacity(A, c->num_sms, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_opacity = true;
+  return SED_OK;
+}
+
+int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const double* emis_cdf, const double* eps_imc)
+{
+  if (!c || !abs || !emis_cdf || !eps_imc) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_load_opacity: no grid");
+  const size_t n = (size_t)c->nz * c->nu.n();
+  if (c->tp.precision) {
+    std::vector<float> o(2 * n), cd(n);
+    for (size_t i = 0; i < n; ++i) { o[2 * i] = (float)abs[i]; o[2 * i + 1] = scat ? (float)scat[i] : 0.f; cd[i] = (float)emis_cdf[i]; }
+    CK(cudaMemcpyAsync(c->d_opac.p, o.data(), o.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_cdf.p, cd.data(), cd.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  } else {
+    std::vector<double> o(2 * n);
+    for (size_t i = 0; i < n; ++i) { o[2 * i] = abs[i]; o[2 * i + 1] = scat ? scat[i] : 0.0; }
+    CK(cudaMemcpyAsync(c->d_opac.p, o.data(), o.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_cdf.p, emis_cdf, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  CK(cudaMemcpyAsync(c->d_abs64.p, abs, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (scat) CK(cudaMemcpyAsync(c->d_scat64.p, scat, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_emis64.p, emis_cdf, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_eps_imc.p, eps_imc, (size_t)c->nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_opacity = true;
+  return SED_OK;
+}
+
+static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms_opacity)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_transport: no grid");
+  if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "sed_transport: opacity tables not set");
+  if (c->tp.steady_state) dt = 1;
+  // emit_inner_source packet count and energy (src/transport/emission.cpp:383-392)
+  const int64_t n_emit = (int64_t)(c->tp.core_n_emit / 1.0);
+  if (n_emit > c->tp.max_particles)
+    return set_err(c, SED_ERR_CAPACITY, "Not enough particle space: %lld packets > particles_max_total %lld",
+                   (long long)n_emit, (long long)c->tp.max_particles);
+  const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
+  const size_t nj = c->tp.store_Jnu ? nn : 1;
+  if (c->record) {
+    CK(c->d_rec_fate.resize(std::max<int64_t>(n_emit, 1)));
+    CK(c->d_rec_ind.resize(std::max<int64_t>(n_emit, 1)));
+    CK(c->d_rec_draws.resize(std::max<int64_t>(n_emit, 1)));
+    CK(c->d_rec_state.resize(std::max<int64_t>(n_emit, 1) * 9));
+    c->n_rec = n_emit;
+  }
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  // wipe_radiation (src/transport/transport_mpi.cpp:18-34) and the spectrum
+  CK(cudaMemsetAsync(c->d_J.p, 0, nz * nj * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_e_abs.p, 0, nz * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_e_rad.p, 0, nz * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_fx.p, 0, nz * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_fy.p, 0, nz * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_fz.p, 0, nz * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_fr.p, 0, nz * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_counters.p, 0, (C_COUNT + 1) * sizeof(unsigned long long), c->stream));
+
+  StepArgs A{};
+  A.steady = c->tp.steady_state; A.radiative_eq = c->tp.radiative_eq;
+  A.bound_in_reflect = c->tp.boundary_in_reflect; A.bound_out_reflect = c->tp.boundary_out_reflect;
+  A.store_Jnu = c->tp.store_Jnu; A.omit_scat = c->tp.omit_scattering; A.tally_forces = c->tp.tally_forces;
+  A.precision = c->tp.precision; A.seed = c->tp.rng_seed; A.step = c->step;
+  A.n_packets = n_emit;
+  A.first_pid = c->tp.first_packet_id;
+  A.Ep = n_emit > 0 ? c->tp.core_luminosity * dt / n_emit : 0.0;
+  A.t_now = c->t_grid; A.dt = dt; A.tstop = c->t_grid + dt;
+  A.core_radius = c->tp.core_radius; A.core_freq = c->tp.core_photon_frequency; A.core_cdf = c->d_core_cdf.p;
+  A.max_segments = c->tp.max_segments;
+  const size_t zone_smem = (size_t)5 * nz * sizeof(double);
+  A.smem_zones = (zone_smem <= 64 * 1024) ? 1 : 0;
+  A.nu = dev_loc(c->nu, c->d_nu); A.st = dev_loc(c->st, c->d_st); A.sn = dev_loc(c->sn, c->d_sn);
+  A.sm = dev_loc(c->sm, c->d_sm); A.sp = dev_loc(c->sp, c->d_sp);
+  A.a3 = c->sp.n(); A.a2 = (int64_t)c->sm.n() * A.a3; A.a1 = (int64_t)c->sn.n() * A.a2;
+  A.opac = c->d_opac.p; A.cdf = c->d_cdf.p; A.eps_imc = c->d_eps_imc.p;
+  A.rescale_lum = c->tp.core_fix_luminosity;
+  A.J = c->d_J.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
+  A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;
+  A.flux = c->d_flux.p; A.click = c->d_click.p; A.counters = c->d_counters.p;
+  if (c->record) {
+    A.rec_fate = c->d_rec_fate.p; A.rec_ind = c->d_rec_ind.p; A.rec_draws = c->d_rec_draws.p; A.rec_state = c->d_rec_state.p;
+  }
+  GridDev G{};
+  G.type = c->gtype; G.nzones = c->nz; G.homologous = c->homologous; G.t_grid = c->t_grid;
+  if (c->gtype == SED_GRID_1D_SPHERE) {
+    G.r_out = dev_loc(c->r_out, c->d_r_out);
+    G.v_r = c->d_v_r.p;
+  } else {
+    G.nx = c->nx; G.ny = c->ny; G.nz = c->nzz;
+    for (int a = 0; a < 3; ++a) G.ax[a] = dev_loc(c->ax[a], c->d_ax[a]);
+  }
+  int launches = 0;
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  if (n_emit > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[4], c->stream));
+  launches += launch_finish(A, G, c->d_vol.p, c->nspec, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[5], c->stream));
+  unsigned long long cnt[C_COUNT + 1];
+  CK(cudaMemcpyAsync(cnt, c->d_counters.p, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->step++;
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    stats->n_packets = n_emit;
+    stats->n_escaped = (int64_t)cnt[C_ESCAPED];
+    stats->n_absorbed = (int64_t)cnt[C_ABSORBED];
+    stats->n_stopped = (int64_t)cnt[C_STOPPED];
+    stats->n_segments = (int64_t)cnt[C_SEGMENTS];
+    stats->n_scatters = (int64_t)cnt[C_SCATTERS];
+    stats->n_limit = (int64_t)cnt[C_LIMIT];
+    stats->kernel_launches = launches;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
+    stats->ms_propagate_kernel = ms;
+    cudaEventElapsedTime(&ms, c->ev[2], c->ev[5]);
+    stats->ms_transport = ms;
+    stats->ms_opacity = ms_opacity;
+    stats->ms_total = ms + ms_opacity;
+  }
+  if (cnt[C_LIMIT] > 0) return set_err(c, SED_ERR_LIMIT, "%llu packets hit the segment limit", cnt[C_LIMIT]);
+  return SED_OK;
+}
+
+int sed_transport(sed_ctx* c, double dt, sed_step_stats* stats) { return transport_impl(c, dt, stats, 0.f); }
+
+int sed_step(sed_ctx* c, double dt, sed_step_stats* stats)
+{
+  int rc = sed_set_opacity(c, dt);
+  if (rc) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  rc = transport_impl(c, dt, stats, ms);
+  if (stats && rc == SED_OK) stats->kernel_launches += 3;
+  return rc;
+}
+
+int sed_get_spectrum(sed_ctx* c, double* flux, double* click)
+{
+  if (!c) return SED_ERR_ARG;
+  if (flux) CK(cudaMemcpyAsync(flux, c->d_flux.p, c->nspec * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (click) CK(cudaMemcpyAsync(click, c->d_click.p, c->nspec * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_get_zone_tallies(sed_ctx* c, double* J, double* e_abs, double* e_rad, double* fx, double* fy, double* fz,
+                         double* fr)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "no grid");
+  const size_t nz = (size_t)c->nz, nj = c->tp.store_Jnu ? (size_t)c->nu.n() : 1;
+  if (J) CK(cudaMemcpyAsync(J, c->d_J.p, nz * nj * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  struct { double* h; double* d; } z[6] = {{e_abs, c->d_e_abs.p}, {e_rad, c->d_e_rad.p}, {fx, c->d_fx.p},
+                                           {fy, c->d_fy.p}, {fz, c->d_fz.p}, {fr, c->d_fr.p}};
+  for (auto& q : z) if (q.h) CK(cudaMemcpyAsync(q.h, q.d, nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_get_opacity(sed_ctx* c, double* abs, double* scat, double* cdf, double* n_elec, double* eps_imc,
+                    double* planck, double* ross, double* L_th)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "no opacity tables");
+  const size_t nz = (size_t)c->nz, n = nz * c->nu.n();
+  if (abs) CK(cudaMemcpyAsync(abs, c->d_abs64.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (scat) CK(cudaMemcpyAsync(scat, c->d_scat64.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (cdf) CK(cudaMemcpyAsync(cdf, c->d_emis64.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  struct { double* h; double* d; } z[5] = {{n_elec, c->d_n_elec.p}, {eps_imc, c->d_eps_imc.p}, {planck, c->d_planck.p},
+                                           {ross, c->d_ross.p}, {L_th, c->d_L.p}};
+  for (auto& q : z) if (q.h) CK(cudaMemcpyAsync(q.h, q.d, nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_record_packets(sed_ctx* c, int32_t enable)
+{
+  if (!c) return SED_ERR_ARG;
+  c->record = enable ? 1 : 0;
+  return SED_OK;
+}
+
+int sed_get_packet_records(sed_ctx* c, int64_t n, int32_t* fate, int32_t* ind, int32_t* draws, double* state9)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->record || n > c->n_rec) return set_err(c, SED_ERR_STATE, "no packet records for %lld packets", (long long)n);
+  if (fate) CK(cudaMemcpyAsync(fate, c->d_rec_fate.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (ind) CK(cudaMemcpyAsync(ind, c->d_rec_ind.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (draws) CK(cudaMemcpyAsync(draws, c->d_rec_draws.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (state9) CK(cudaMemcpyAsync(state9, c->d_rec_state.p, n * 9 * 8, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int64_t sed_n_particles(sed_ctx* c) { (void)c; return 0; }
+
+const char* sed_last_error(sed_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void sed_ctx_destroy(sed_ctx* c)
+{
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
+  DevBuf<double>* dbl[] = {&c->d_nu, &c->d_st, &c->d_sn, &c->d_sm, &c->d_sp, &c->d_core_cdf, &c->d_r_out, &c->d_v_r,
+                           &c->d_ax[0], &c->d_ax[1], &c->d_ax[2], &c->d_vol, &c->d_rho, &c->d_T, &c->d_egas,
+                           &c->d_grey, &c->d_X, &c->d_ion_chi, &c->d_lev_E, &c->d_lev_Eion, &c->d_photo_E,
+                           &c->d_photo_s, &c->d_line_nu, &c->d_line_f, &c->d_fz_nu, &c->d_fz_gf, &c->d_fz_El,
+                           &c->d_eps_imc, &c->d_abs64, &c->d_scat64, &c->d_emis64, &c->d_planck, &c->d_ross, &c->d_L,
+                           &c->d_n_elec, &c->d_n_dens, &c->d_mass_frac, &c->d_temp_c, &c->d_ion_part, &c->d_ion_frac,
+                           &c->d_lev_n, &c->d_boltz, &c->d_J, &c->d_e_abs, &c->d_e_rad, &c->d_fx, &c->d_fy,
+                           &c->d_fz, &c->d_fr, &c->d_flux, &c->d_click, &c->d_rec_state};
+  for (auto* b : dbl) b->release();
+  DevBuf<int32_t>* ints[] = {&c->d_eZ, &c->d_eA, &c->d_zero_eps_atom, &c->d_ion_off, &c->d_lev_off, &c->d_lev_ion,
+                             &c->d_lev_g, &c->d_lev_ic, &c->d_photo_off, &c->d_line_seg, &c->d_line_l, &c->d_line_u,
+                             &c->d_fuzz_seg, &c->d_fz_ion, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind,
+                             &c->d_rec_draws};
+  for (auto* b : ints) b->release();
+  c->d_fz_A32.release(); c->d_fz_El32.release(); c->d_fz_hnu32.release();
+  c->d_opac.release(); c->d_cdf.release(); c->d_counters.release();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+// sed_common.cuh -- device-side building blocks shared by the kernels:
+// physical constants, the Philox4x32-10 packet streams, and the bin-edge
+// search with locate_array semantics.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sed {
+
+// physical_constants (src/utils/physical_constants.h:9-31); pi is 3.14159 there
+constexpr double PI = 3.14159;
+constexpr double C_LIGHT = 2.99792458e10;
+constexpr double H_PLANCK = 6.6260755e-27;
+constexpr double K_BOLTZ = 1.380658e-16;
+constexpr double K_EV = 8.6173324e-5;
+constexpr double MASS_P = 1.67262158e-24;
+constexpr double MASS_E = 9.10938188e-28;
+constexpr double SB = 5.6704e-5;
+constexpr double A_RAD = 7.5657e-15;
+constexpr double THOMSON = 0.66523e-24;
+constexpr double SIGMA_TOT = 0.0265400193567;
+constexpr double ERGS_TO_EV = 624150975230.2815;
+
+enum Fate : int32_t { MOVING = 0, STOPPED = 1, ESCAPED = 2, ABSORBED = 3 };
+enum LocType : int32_t { LOC_FLEX = 0, LOC_LIN = 1, LOC_LOG = 2, LOC_NONE = 3 };
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon et al., SC'11).  A packet's deviates form the stream
+// key = {seed, 0}, counter = {n >> 1, pid.lo, pid.hi, step}; draw n uses
+// output words 0,1 (n even) or 2,3 (n odd) as a 53-bit double in [0, 1).
+struct PhiloxOut { uint32_t w[4]; };
+
+__host__ __device__ inline PhiloxOut philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                   uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+#ifdef __CUDA_ARCH__
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+#else
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+    const uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+#endif
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  return PhiloxOut{{c0, c1, c2, c3}};
+}
+
+__host__ __device__ inline double u01(uint32_t a, uint32_t b)
+{
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+// Per-packet stream with a one-pair cache: odd draws reuse the Philox block
+// of the preceding even draw.
+struct PacketRng {
+  uint32_t seed, step;
+  uint64_t pid;
+  uint32_t n;
+  uint32_t cached_ctr;
+  uint32_t cw2, cw3;
+  bool have;
+
+  __device__ void init(uint32_t seed_, uint64_t pid_, uint32_t step_, uint32_t n0)
+  {
+    seed = seed_; pid = pid_; step = step_; n = n0; have = false;
+  }
+  __device__ double next()
+  {
+    const uint32_t k = n++;
+    const uint32_t ctr = k >> 1;
+    if ((k & 1u) && have && cached_ctr == ctr) return u01(cw2, cw3);
+    PhiloxOut o = philox4x32_10(ctr, (uint32_t)pid, (uint32_t)(pid >> 32), step, seed, 0u);
+    cached_ctr = ctr; cw2 = o.w[2]; cw3 = o.w[3]; have = true;
+    return (k & 1u) ? u01(o.w[2], o.w[3]) : u01(o.w[0], o.w[1]);
+  }
+};
+
+// ---------------------------------------------------------------- locate
+struct DevLoc {
+  int32_t n, type;
+  double min, del;
+  const double* right;  // device pointer, n walls
+};
+
+__device__ __forceinline__ int upper_bound_dev(const double* __restrict__ a, int n, double v)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if (__ldg(a + m) <= v) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+template <typename T>
+__device__ __forceinline__ int upper_bound_t(const T* __restrict__ a, int n, double v)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if ((double)__ldg(a + m) <= v) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+// locate_array::locate (src/utils/locate_array.cpp:191-218): fast lin/log
+// index corrected by a binary search unless it is 0 or n
+__device__ __forceinline__ int loc_locate(const DevLoc& g, double x)
+{
+  if (g.n == 1) return 0;
+  if (x >= __ldg(g.right + g.n - 1)) return g.n;
+  if (x < g.min) return 0;
+  int ind;
+  if (g.type == LOC_FLEX) return upper_bound_dev(g.right, g.n, x);
+  else if (g.type == LOC_LIN) ind = (int)floor((x - g.min) / g.del);
+  else if (g.type == LOC_LOG) ind = (int)floor(log(x / g.min) / log(1 + g.del));
+  else return 0;
+  if (ind != 0 && ind != g.n) {
+    const double left = __ldg(g.right + ind - 1), right = __ldg(g.right + ind);
+    if (left > x || right <= x) ind = upper_bound_dev(g.right, g.n, x);
+  }
+  return ind;
+}
+
+__device__ __forceinline__ int loc_within(const DevLoc& g, double x)
+{
+  const int i = loc_locate(g, x);
+  return i == g.n ? g.n - 1 : i;
+}
+
+__device__ __forceinline__ double loc_left(const DevLoc& g, int i) { return i == 0 ? g.min : __ldg(g.right + i - 1); }
+__device__ __forceinline__ double loc_delta(const DevLoc& g, int i)
+{
+  return i == 0 ? __ldg(g.right) - g.min : __ldg(g.right + i) - __ldg(g.right + i - 1);
+}
+__device__ __forceinline__ double loc_center(const DevLoc& g, int i)
+{
+  return i == 0 ? 0.5 * (g.min + __ldg(g.right)) : 0.5 * (__ldg(g.right + i - 1) + __ldg(g.right + i));
+}
+// locate_array::sample (locate_array.cpp:237-242)
+__device__ __forceinline__ double loc_sample(const DevLoc& g, int i, double r)
+{
+  if (g.n == 1) return 0;
+  if (i == 0) return g.min + (__ldg(g.right) - g.min) * r;
+  const double l = __ldg(g.right + i - 1);
+  return l + (__ldg(g.right + i) - l) * r;
+}
+
+}  // namespace sed

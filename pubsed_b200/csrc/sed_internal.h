@@ -1,0 +1,98 @@
+// sed_internal.h -- device-side argument blocks and kernel launchers shared
+// between the C-ABI layer (sed_abi.cu) and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "sed_common.cuh"
+
+namespace sed {
+
+// Zone geometry on the device (1D sphere or 3D Cartesian).
+struct GridDev {
+  int32_t type;       // 0 = 1D sphere, 1 = 3D Cartesian
+  int32_t nzones;
+  int32_t homologous;
+  int32_t nx, ny, nz;
+  double t_grid;      // homologous velocity v = x / t_grid
+  DevLoc r_out;       // 1D: zone right walls (flex), min = r_min
+  const double* v_r;  // 1D non-homologous zone velocities
+  DevLoc ax[3];       // 3D axes
+};
+
+// counters[] slots written by the packet kernel
+enum Counter { C_QUEUE = 0, C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT, C_COUNT };
+
+struct StepArgs {
+  int32_t steady, radiative_eq, bound_in_reflect, bound_out_reflect;
+  int32_t store_Jnu, omit_scat, tally_forces, precision;  // precision: 0 fp64 tables, 1 fp32
+  uint32_t seed, step;
+  int64_t n_packets;
+  int64_t first_pid;          // Philox stream id of queue entry 0
+  double Ep, t_now, dt, tstop;
+  double core_radius, core_freq;
+  const double* core_cdf;     // [n_nu] normalised core emission CDF
+  int32_t max_segments;
+  int32_t smem_zones;         // 1: per-block shared-memory zone tallies
+  DevLoc nu, st, sn, sm, sp;  // frequency grid and spectrum grids
+  int64_t a1, a2, a3;         // spectrum strides
+  const void* opac;           // [nz*n_nu] double2 {abs, scat} or float2
+  const void* cdf;            // [nz*n_nu] double or float emissivity CDF
+  const double* eps_imc;      // [nz]
+  int32_t rescale_lum;        // core_fix_luminosity (steady-state rescale)
+  int32_t pad_;
+  double* J;                  // [nz * (store_Jnu ? n_nu : 1)]
+  double *e_abs, *e_rad, *fx, *fy, *fz, *fr;
+  double *flux, *click;
+  unsigned long long* counters;  // [C_COUNT]
+  int32_t *rec_fate, *rec_ind, *rec_draws;  // optional per-packet records
+  double* rec_state;
+};
+
+// launches the persistent packet kernel; returns the number of launches
+int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s);
+// zone-scalar tally normalisation (reduce_radiation) and steady-state rescale
+int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_t nspec, cudaStream_t s);
+
+// ---------------------------------------------------------------- opacity
+struct OpacityArgs {
+  int32_t nzones, n_nu, nelem;
+  int32_t use_es, use_ff, use_bf, use_line, use_fuzz;
+  int32_t radiative_eq, omit_scat, precision;
+  double epsilon, max_opacity, temp_min, temp_max, fleck_alpha, dt, time;
+  DevLoc nu;
+  const double *rho, *T, *e_gas, *grey, *X;  // zone state
+  const int32_t *eZ, *eA;
+  const int32_t* zero_eps_atom;  // [nelem] 1 when the atom's epsilon is 0
+  // atomic data (device)
+  int32_t natoms;
+  const int32_t *ion_off, *lev_off, *lev_ion, *lev_g, *lev_ic, *photo_off;
+  const double *ion_chi, *lev_E, *lev_Eion, *photo_E, *photo_s;
+  // level-to-level lines sorted by (atom, bin): segment starts per (atom, bin)
+  const int32_t* line_seg;     // [natoms * n_nu + 1]
+  const int32_t *line_l, *line_u;
+  const double *line_nu, *line_f;
+  // fuzz lines sorted by (atom, bin): segment starts per (atom, bin)
+  const int32_t* fuzz_seg;     // [natoms * n_nu + 1]
+  const double *fz_nu, *fz_gf, *fz_El;
+  const int32_t* fz_ion;
+  const float *fz_A32, *fz_El32, *fz_hnu32;  // FP32 per-line constants
+  int32_t nfuzz;
+  // per-zone LTE state (device scratch written by the LTE kernel)
+  double *ion_part, *ion_frac, *lev_n;  // [nzones * n_ions_total] etc.
+  int32_t n_ions_total, n_lev_total;
+  double* n_elec;                        // [nz]
+  double* n_dens;                        // [nz * natoms]
+  double* mass_frac;                     // [nz * natoms]
+  double* temp_c;                        // [nz] clamped temperature
+  int32_t* solve_err;                    // [nz]
+  double* boltz;                         // [n_lev_total * nz] exp(-E/kT) per level
+  // outputs
+  double *abs64, *scat64, *emis64;       // [nz*n_nu] FP64 working tables
+  void* opac_out;                        // double2 / float2 [nz*n_nu]
+  void* cdf_out;                         // double / float [nz*n_nu]
+  double *eps_imc, *planck, *ross, *L_th;
+};
+
+int launch_opacity(const OpacityArgs& a, int num_sms, cudaStream_t s);
+
+}  // namespace sed

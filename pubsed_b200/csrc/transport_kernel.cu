@@ -1,0 +1,545 @@
+// transport_kernel.cu -- the persistent Monte Carlo packet kernel.
+//
+// One thread owns one packet at a time and pulls the next packet index from
+// a global counter when its packet escapes, is absorbed or stops, so every
+// lane stays busy no matter how uneven packet histories are.  Emission is
+// fused in: a packet is created in registers from its first Philox draws
+// (emit_inner_source, src/transport/emission.cpp:370-485) and never stored.
+// Each loop iteration is one segment of propagate_monte_carlo
+// (src/transport/transport.cpp:260-484).  Packet state stays in registers;
+// the opacity table is a zone-major array of {abs, scat} pairs (one 16 B or
+// 8 B load per segment); zone-scalar tallies go to per-block shared memory
+// when the grid has few zones, J_nu goes straight to global FP64 atomics.
+//
+// Arithmetic follows the reference expression by expression; this file is
+// compiled without FMA contraction so products and sums round as written.
+#include <cfloat>
+#include <cmath>
+#include "sed_internal.h"
+
+namespace sed {
+
+namespace {
+
+struct Pkt {
+  double x[3], D[3];
+  double t, e, nu, dvds;
+  int32_t ind;
+};
+
+// ----------------------------------------------------------- geometry
+// grid_1D_sphere::get_zone (src/grid/grid_1D_sphere.cpp:494-505) and
+// grid_3D_cart::get_zone (src/grid/grid_3D_cart.cpp:363-390)
+template <int GRID>
+__device__ __forceinline__ int get_zone(const GridDev& G, const double* x)
+{
+  if constexpr (GRID == 0) {
+    const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    if (r < G.r_out.min) return -1;
+    if (r >= __ldg(G.r_out.right + G.r_out.n - 1)) return -2;
+    return loc_within(G.r_out, r);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (x[a] < G.ax[a].min) return -2;
+      if (x[a] > __ldg(G.ax[a].right + G.ax[a].n - 1)) return -2;
+    }
+    const int i = loc_within(G.ax[0], x[0]);
+    const int j = loc_within(G.ax[1], x[1]);
+    const int k = loc_within(G.ax[2], x[2]);
+    return i * G.ny * G.nz + j * G.nz + k;
+  }
+}
+
+// grid_1D_sphere::get_next_zone (grid_1D_sphere.cpp:510-590) and
+// grid_3D_cart::get_next_zone (grid_3D_cart.cpp:396-469)
+template <int GRID>
+__device__ __forceinline__ int get_next_zone(const GridDev& G, const double* x, const double* D, int i,
+                                             double r_core, double* l)
+{
+  if constexpr (GRID == 0) {
+    const double rsq = (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    const double xdotD = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]);
+    const double r_o = __ldg(G.r_out.right + i);
+    const double l_out = -1 * xdotD + sqrt(xdotD * xdotD + r_o * r_o - rsq);
+    double r_in;
+    int ind_in;
+    if (i != 0) { r_in = __ldg(G.r_out.right + i - 1); ind_in = i - 1; }
+    else { r_in = G.r_out.min; ind_in = -1; }
+    if (r_core >= r_in) { r_in = r_core; ind_in = -1; }
+    double l_in;
+    if ((i == 0) && (r_in == 0)) l_in = -1;
+    else {
+      const double rad = xdotD * xdotD + r_in * r_in - rsq;
+      l_in = (rad < 0) ? -1 : -1 * xdotD - sqrt(rad);
+    }
+    const double tiny_offset = 1 + 1e-6;
+    int ind;
+    if ((l_out < l_in) || (l_in < 0)) {
+      ind = i + 1;
+      if (ind == G.nzones) { ind = -2; *l = l_out / tiny_offset; }
+      else *l = l_out * tiny_offset;
+    } else {
+      ind = ind_in;
+      *l = (ind_in == -1) ? l_in / tiny_offset : l_in * tiny_offset;
+    }
+    return ind;
+  } else {
+    const int nyz = G.ny * G.nz;
+    const int idx3[3] = {i / nyz, (i / G.nz) % G.ny, i % G.nz};
+    const double tiny = 1e-10;
+    double len[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double dd = loc_delta(G.ax[a], idx3[a]);
+      const double bn = (D[a] > 0) ? __ldg(G.ax[a].right + idx3[a]) + dd * tiny : loc_left(G.ax[a], idx3[a]) - dd * tiny;
+      len[a] = (bn - x[a]) / D[a];
+    }
+    int d[3] = {0, 0, 0};
+    if ((len[0] < len[1]) && (len[0] < len[2])) { d[0] = (D[0] < 0) ? -1 : 1; *l = len[0]; }
+    else if (len[1] < len[2]) { d[1] = (D[1] < 0) ? -1 : 1; *l = len[1]; }
+    else { d[2] = (D[2] < 0) ? -1 : 1; *l = len[2]; }
+    const int nx_ = idx3[0] + d[0], ny_ = idx3[1] + d[1], nz_ = idx3[2] + d[2];
+    if (nx_ < 0 || nx_ > G.nx - 1) return -2;
+    if (ny_ < 0 || ny_ > G.ny - 1) return -2;
+    if (nz_ < 0 || nz_ > G.nz - 1) return -2;
+    return nx_ * nyz + ny_ * G.nz + nz_;
+  }
+}
+
+// get_velocity (grid_1D_sphere.cpp:707-748, grid_3D_cart.cpp:513-521)
+template <int GRID>
+__device__ __forceinline__ void get_velocity(const GridDev& G, int i, const double* x, const double* D, double* v,
+                                             double* dvds)
+{
+  if (G.homologous) {
+    v[0] = x[0] / G.t_grid;
+    v[1] = x[1] / G.t_grid;
+    v[2] = x[2] / G.t_grid;
+    *dvds = 1.0 / G.t_grid;
+    return;
+  }
+  if constexpr (GRID == 0) {
+    const double rr = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    double v_0, r_0;
+    if (i == 0) { v_0 = 0; r_0 = G.r_out.min; }
+    else { v_0 = __ldg(G.v_r + i - 1); r_0 = __ldg(G.r_out.right + i - 1); }
+    const double dr = rr - r_0;
+    const double dv_dr = (__ldg(G.v_r + i) - v_0) / (__ldg(G.r_out.right + i) - r_0);
+    const double vv = v_0 + dv_dr * dr;
+    const double Ddr = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]) / rr;
+    v[0] = x[0] / rr * vv;
+    v[1] = x[1] / rr * vv;
+    v[2] = x[2] / rr * vv;
+    *dvds = Ddr * Ddr * (dv_dr - vv / rr) + vv / rr;
+    if (rr == 0) { v[0] = v[1] = v[2] = 0; *dvds = dv_dr; }
+  } else {
+    v[0] = v[1] = v[2] = 0;
+    *dvds = 0;
+  }
+}
+
+// transport::do_dshift lab -> comoving (src/transport/relativity.cpp:14-43)
+template <int GRID>
+__device__ __forceinline__ double dshift_lab_to_comoving(const GridDev& G, Pkt& p)
+{
+  double v[3], dvds;
+  get_velocity<GRID>(G, p.ind, p.x, p.D, v, &dvds);
+  const double beta2 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / C_LIGHT / C_LIGHT;
+  const double vdd = v[0] * p.D[0] + v[1] * p.D[1] + v[2] * p.D[2];
+  const double gamma = 1.0 / sqrt(1 - beta2);
+  p.dvds = dvds;
+  return gamma * (1 - vdd / C_LIGHT);
+}
+
+// transport::lorentz_transform(p, 1) (relativity.cpp:84-127)
+template <int GRID>
+__device__ __forceinline__ void comoving_to_lab(const GridDev& G, Pkt& p)
+{
+  double v[3], dvds;
+  get_velocity<GRID>(G, p.ind, p.x, p.D, v, &dvds);
+  v[0] *= -1; v[1] *= -1; v[2] *= -1;
+  const double beta2 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / C_LIGHT / C_LIGHT;
+  const double vdd = v[0] * p.D[0] + v[1] * p.D[1] + v[2] * p.D[2];
+  const double gamma = 1.0 / sqrt(1 - beta2);
+  const double dshift = gamma * (1 - vdd / C_LIGHT);
+  p.dvds = dvds;
+  p.e *= dshift;
+  p.nu *= dshift;
+  const double f = (1 - gamma * vdd / C_LIGHT / (gamma + 1));
+  p.D[0] = 1.0 / dshift * (p.D[0] - gamma * v[0] / C_LIGHT * f);
+  p.D[1] = 1.0 / dshift * (p.D[1] - gamma * v[1] / C_LIGHT * f);
+  p.D[2] = 1.0 / dshift * (p.D[2] - gamma * v[2] / C_LIGHT * f);
+  const double norm = p.D[0] * p.D[0] + p.D[1] * p.D[1] + p.D[2] * p.D[2];
+  p.D[0] /= norm;
+  p.D[1] /= norm;
+  p.D[2] /= norm;
+}
+
+template <typename CT>
+__device__ __forceinline__ int cdf_sample(const CT* __restrict__ y, int n, double u)
+{
+  if (n == 1) return 0;
+  return upper_bound_t<CT>(y, n, u);
+}
+
+// transport::isotropic_scatter (src/transport/scatter.cpp:303-351)
+template <int GRID, typename CT>
+__device__ __forceinline__ void isotropic_scatter(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng,
+                                                  int redist)
+{
+  double V[3], dvds;
+  get_velocity<GRID>(G, p.ind, p.x, p.D, V, &dvds);
+  const double vdotD = V[0] * p.D[0] + V[1] * p.D[1] + V[2] * p.D[2];
+  const double beta2 = (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]) / C_LIGHT / C_LIGHT;
+  const double gamma = 1.0 / sqrt(1 - beta2);
+  const double dshift_in = gamma * (1 - vdotD / C_LIGHT);
+  p.e = p.e * dshift_in;
+  p.nu = p.nu * dshift_in;
+  const double mu = 1 - 2.0 * rng.next();
+  const double phi = 2.0 * PI * rng.next();
+  const double smu = sqrt(1 - mu * mu);
+  double s, c;
+  sincos(phi, &s, &c);
+  const double Dn[3] = {smu * c, smu * s, mu};
+  if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
+    const int nn = A.nu.n;
+    const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
+    const int inu = cdf_sample<CT>(row, nn, rng.next());
+    p.nu = loc_sample(A.nu, inu, rng.next());
+  }
+  V[0] = -1 * V[0]; V[1] = -1 * V[1]; V[2] = -1 * V[2];
+  const double vdp = (Dn[0] * V[0] + Dn[1] * V[1] + Dn[2] * V[2]);
+  const double vd_out = gamma * (1 - vdp / C_LIGHT);
+  const double f = (1 - gamma * vdp / C_LIGHT / (gamma + 1));
+  p.D[0] = 1.0 / vd_out * (Dn[0] - gamma * V[0] / C_LIGHT * f);
+  p.D[1] = 1.0 / vd_out * (Dn[1] - gamma * V[1] / C_LIGHT * f);
+  p.D[2] = 1.0 / vd_out * (Dn[2] - gamma * V[2] / C_LIGHT * f);
+  const double norm = sqrt(p.D[0] * p.D[0] + p.D[1] * p.D[1] + p.D[2] * p.D[2]);
+  p.D[0] = p.D[0] / norm;
+  p.D[1] = p.D[1] / norm;
+  p.D[2] = p.D[2] / norm;
+  p.e = p.e * vd_out;
+  p.nu = p.nu * vd_out;
+}
+
+// transport::emit_inner_source for one packet (emission.cpp:395-480)
+template <int GRID>
+__device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng)
+{
+  const double rc = A.core_radius;
+  if (rc == 0) {
+    p.x[0] = p.x[1] = p.x[2] = 0;
+    const double mu = 1 - 2.0 * rng.next();
+    const double phi = 2.0 * PI * rng.next();
+    const double smu = sqrt(1 - mu * mu);
+    double s, c;
+    sincos(phi, &s, &c);
+    p.D[0] = smu * c;
+    p.D[1] = smu * s;
+    p.D[2] = mu;
+  } else {
+    const double phi_core = 2 * PI * rng.next();
+    double sinp, cosp;
+    sincos(phi_core, &sinp, &cosp);
+    const double cost = 1 - 2.0 * rng.next();
+    const double sint = sqrt(1 - cost * cost);
+    const double a_phot = rc + rc * 1e-10;
+    p.x[0] = a_phot * sint * cosp;
+    p.x[1] = a_phot * sint * sinp;
+    p.x[2] = a_phot * cost;
+    const double phi_loc = 2 * PI * rng.next();
+    const double cost_loc = sqrt(rng.next());
+    const double sint_loc = sqrt(1 - cost_loc * cost_loc);
+    double sl, cl;
+    sincos(phi_loc, &sl, &cl);
+    const double D_xl = sint_loc * cl, D_yl = sint_loc * sl, D_zl = cost_loc;
+    p.D[0] = cost * cosp * D_xl - sinp * D_yl + sint * cosp * D_zl;
+    p.D[1] = cost * sinp * D_xl + cosp * D_yl + sint * sinp * D_zl;
+    p.D[2] = -sint * D_xl + cost * D_zl;
+  }
+  p.e = A.Ep;
+  if (A.core_freq > 0) p.nu = A.core_freq;
+  else {
+    const int inu = cdf_sample<double>(A.core_cdf, A.nu.n, rng.next());
+    p.nu = loc_sample(A.nu, inu, rng.next());
+    p.e /= 1.0;  // emissivity_weight_ is 1 (transport_init.cpp:322-332)
+  }
+  p.ind = get_zone<GRID>(G, p.x);
+  // the reference asserts p.ind >= 0 here (relativity.cpp:86); homologous
+  // velocities do not depend on the zone, other velocity fields need one
+  if (G.homologous || p.ind >= 0) comoving_to_lab<GRID>(G, p);
+  p.t = A.t_now + rng.next() * A.dt;
+}
+
+// spectrum_array::count (src/transport/spectrum_array.cpp:215-246)
+__device__ __forceinline__ void spectrum_count(const StepArgs& A, double t, double w, double E, const double* D)
+{
+  const double mu = D[2];
+  double phi = atan2(D[1], D[0]);
+  if (phi < 0) phi += 2. * PI;
+  const int t_bin = loc_locate(A.st, t);
+  int l_bin = loc_locate(A.sn, w);
+  const int m_bin = loc_locate(A.sm, mu);
+  const int p_bin = loc_locate(A.sp, phi);
+  if (l_bin < 0) l_bin = 0;
+  if (l_bin >= A.sn.n) l_bin = 0;
+  if ((t_bin < 0) || (m_bin < 0) || (p_bin < 0)) return;
+  if (t_bin >= A.st.n || m_bin >= A.sm.n || p_bin >= A.sp.n) return;
+  const int64_t ind = t_bin * A.a1 + l_bin * A.a2 + m_bin * A.a3 + p_bin;
+  atomicAdd(A.flux + ind, E);
+  atomicAdd(A.click + ind, 1.0);
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int GRID, typename OT, typename CT>
+__global__ void __launch_bounds__(256) propagate_kernel(const StepArgs A, const GridDev G)
+{
+  extern __shared__ double s_tal[];  // [5][nz] when A.smem_zones
+  const int nz = G.nzones;
+  const int nn = A.nu.n;
+  const int nj = A.store_Jnu ? nn : 1;
+  if (A.smem_zones) {
+    for (int i = threadIdx.x; i < 5 * nz; i += blockDim.x) s_tal[i] = 0.0;
+    __syncthreads();
+  }
+  double* t_eabs = A.smem_zones ? s_tal : A.e_abs;
+  double* t_fx = A.smem_zones ? s_tal + nz : A.fx;
+  double* t_fy = A.smem_zones ? s_tal + 2 * nz : A.fy;
+  double* t_fz = A.smem_zones ? s_tal + 3 * nz : A.fz;
+  double* t_fr = A.smem_zones ? s_tal + 4 * nz : A.fr;
+  const OT* __restrict__ opac = reinterpret_cast<const OT*>(A.opac);
+  const int64_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
+  const uint32_t K = (A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u;
+
+  unsigned long long n_esc = 0, n_abs = 0, n_stop = 0, n_seg = 0, n_scat = 0, n_lim = 0;
+  for (;;) {
+    const unsigned long long pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
+    if (pid >= (unsigned long long)A.n_packets) break;
+    Pkt p;
+    PacketRng rng;
+    rng.init(A.seed, (uint64_t)A.first_pid + pid, A.step, 0);
+    emit_core<GRID>(A, G, p, rng);
+    // transport::propagate (transport.cpp:202-254)
+    int fate = MOVING;
+    p.ind = get_zone<GRID>(G, p.x);
+    if (p.ind == -1) fate = ABSORBED;
+    else if (p.ind == -2) fate = ESCAPED;
+    int64_t seg = 0;
+    while (fate == MOVING) {
+      if (seg >= limit) { fate = STOPPED; ++n_lim; break; }
+      ++seg;
+      const int iz = p.ind;
+      double d_bn = 0;
+      int new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, &d_bn);
+      const double dshift = dshift_lab_to_comoving<GRID>(G, p);
+      // transport::get_opacity (transport_opacity.cpp:268-299)
+      const double nu_cmf = p.nu * dshift;
+      const int i_nu = loc_within(A.nu, nu_cmf);
+      const OT ab = opac[(size_t)iz * nn + i_nu];
+      const double a_opac = (double)ab.x;
+      const double s_opac = A.omit_scat ? 0.0 : (double)ab.y;
+      const double op = a_opac + s_opac;
+      const double eps = (op == 0) ? 0 : a_opac / op;
+      double d_nu = loc_delta(A.nu, i_nu) / p.nu * C_LIGHT / p.dvds;
+      if (p.dvds == 0) d_nu = INFINITY;
+      if (d_nu < 0) d_nu = -1 * d_nu;
+      if (d_nu < d_bn) { d_bn = d_nu; new_ind = p.ind; }
+      const double tot_lab = op * dshift;
+      const double tau_r = -1.0 * log(1 - rng.next());
+      double d_sc = tau_r / tot_lab;
+      if (tot_lab == 0) d_sc = INFINITY;
+      double d_tm = (A.tstop - p.t) * C_LIGHT;
+      if (A.steady) d_tm = INFINITY;
+      int event;
+      double this_d;
+      if ((d_sc < d_bn) && (d_sc < d_tm)) { event = 0; this_d = d_sc; }
+      else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
+      else { event = 2; this_d = d_tm; }
+      // tallies (transport.cpp:361-392)
+      const double this_E = p.e * this_d;
+      atomicAdd(t_eabs + iz, this_E * dshift * (op) * eps * dshift * __ldg(A.eps_imc + iz));
+      atomicAdd(A.J + (size_t)iz * nj + (A.store_Jnu ? i_nu : 0), this_E);
+      if (A.tally_forces) {
+        const double w = this_E * dshift * op;
+        atomicAdd(t_fx + iz, w * p.D[0] * dshift);
+        atomicAdd(t_fy + iz, w * p.D[1] * dshift);
+        atomicAdd(t_fz + iz, w * p.D[2] * dshift);
+        const double rr = sqrt(p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+        const double xdotD = p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2];
+        atomicAdd(t_fr + iz, w * xdotD / rr * dshift);
+      }
+      p.x[0] += this_d * p.D[0];
+      p.x[1] += this_d * p.D[1];
+      p.x[2] += this_d * p.D[2];
+      p.t = p.t + this_d / C_LIGHT;
+      if (event == 1) {
+        if (new_ind == -1) {
+          if (A.bound_in_reflect) { p.D[0] *= -1; p.D[1] *= -1; p.D[2] *= -1; }
+          else { p.ind = new_ind; fate = ABSORBED; }
+        } else if (new_ind == -2) {
+          if (A.bound_out_reflect) { p.D[0] *= -1; p.D[1] *= -1; p.D[2] *= -1; }
+          else { p.ind = new_ind; fate = ESCAPED; }
+        } else {
+          p.ind = new_ind;
+        }
+      } else if (event == 0) {
+        // transport::do_scatter (scatter.cpp:12-70)
+        ++n_scat;
+        if (rng.next() > eps) isotropic_scatter<GRID, CT>(A, G, p, rng, 0);
+        else {
+          const double z2 = rng.next();
+          if ((z2 > __ldg(A.eps_imc + iz)) || A.radiative_eq) isotropic_scatter<GRID, CT>(A, G, p, rng, 1);
+          else fate = ABSORBED;
+        }
+      } else {
+        fate = STOPPED;
+      }
+    }
+    n_seg += seg;
+    if (fate == ESCAPED) {
+      const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
+      spectrum_count(A, t_obs, p.nu, p.e, p.D);
+      p.t = t_obs;
+      ++n_esc;
+    } else if (fate == ABSORBED) {
+      ++n_abs;
+    } else {
+      ++n_stop;
+    }
+    if (A.rec_fate) {
+      A.rec_fate[pid] = fate;
+      A.rec_ind[pid] = p.ind;
+      A.rec_draws[pid] = (int32_t)(rng.n - K);
+      double* s = A.rec_state + pid * 9;
+      s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
+      s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+      s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+    }
+  }
+  // counters: warp reduction, one atomic per warp
+  n_esc = warp_sum(n_esc); n_abs = warp_sum(n_abs); n_stop = warp_sum(n_stop);
+  n_seg = warp_sum(n_seg); n_scat = warp_sum(n_scat); n_lim = warp_sum(n_lim);
+  if ((threadIdx.x & 31) == 0) {
+    if (n_esc) atomicAdd(A.counters + C_ESCAPED, n_esc);
+    if (n_abs) atomicAdd(A.counters + C_ABSORBED, n_abs);
+    if (n_stop) atomicAdd(A.counters + C_STOPPED, n_stop);
+    if (n_seg) atomicAdd(A.counters + C_SEGMENTS, n_seg);
+    if (n_scat) atomicAdd(A.counters + C_SCATTERS, n_scat);
+    if (n_lim) atomicAdd(A.counters + C_LIMIT, n_lim);
+  }
+  if (A.smem_zones) {
+    __syncthreads();
+    double* g[5] = {A.e_abs, A.fx, A.fy, A.fz, A.fr};
+    for (int i = threadIdx.x; i < 5 * nz; i += blockDim.x) {
+      const double v = s_tal[i];
+      if (v != 0.0 || isnan(v)) atomicAdd(g[i / nz] + (i % nz), v);
+    }
+  }
+}
+
+// reduce_radiation normalisation (src/transport/transport_mpi.cpp:415-441),
+// preceded by the steady-state luminosity rescale (transport.cpp:94-115) whose
+// factor is formed on the device from the escape counter.  One block per zone.
+__global__ void finish_zones_kernel(const StepArgs A, const double* __restrict__ vol, int nz, int64_t n_active,
+                                    int do_rescale)
+{
+  const int iz = blockIdx.x;
+  if (iz >= nz) return;
+  const int nn = A.nu.n;
+  const double dt = A.dt;
+  const double v = vol[iz];
+  double fac = 1.0;
+  if (do_rescale) {
+    const double per_esc = (1.0 * (double)A.counters[C_ESCAPED]) / (1.0 * (double)n_active);
+    fac = 1.0 / per_esc;
+  }
+  __shared__ double red[256];
+  if (A.store_Jnu && nn > 1) {
+    double* J = A.J + (size_t)iz * nn;
+    double esum = 0;
+    for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+      double x = J[j];
+      if (do_rescale) x *= fac;
+      const double d = loc_delta(A.nu, j);
+      x /= v * dt * 4 * PI * d;
+      J[j] = x;
+      esum += x * d * 4 * PI / C_LIGHT;
+    }
+    red[threadIdx.x] = esum;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < (unsigned)s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {
+    A.e_abs[iz] /= v * dt;
+    A.fr[iz] /= v * C_LIGHT * dt;
+    if ((nn == 1) || (!A.store_Jnu)) {
+      double j0 = A.J[(size_t)iz * (A.store_Jnu ? nn : 1)];
+      if (do_rescale && A.store_Jnu) { j0 *= fac; A.J[(size_t)iz * nn] = j0; }
+      A.e_rad[iz] = j0 / (v * dt * C_LIGHT);
+    } else {
+      A.e_rad[iz] = red[0];
+    }
+  }
+}
+
+__global__ void rescale_spectrum_kernel(const StepArgs A, int64_t nspec, int64_t n_active)
+{
+  const double per_esc = (1.0 * (double)A.counters[C_ESCAPED]) / (1.0 * (double)n_active);
+  const double fac = 1.0 / per_esc;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nspec; i += (int64_t)gridDim.x * blockDim.x)
+    A.flux[i] *= fac;
+}
+
+template <int GRID, typename OT, typename CT>
+int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
+{
+  const int threads = 256;
+  const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
+  auto kern = propagate_kernel<GRID, OT, CT>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  int64_t blocks = (int64_t)num_sms * per_sm;
+  const int64_t need = (a.n_packets + threads - 1) / threads;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  kern<<<(unsigned)blocks, threads, smem, s>>>(a, g);
+  return 1;
+}
+
+}  // namespace
+
+int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
+{
+  if (g.type == 0) {
+    if (a.precision == 0) return launch_propagate_t<0, double2, double>(a, g, num_sms, s);
+    return launch_propagate_t<0, float2, float>(a, g, num_sms, s);
+  }
+  if (a.precision == 0) return launch_propagate_t<1, double2, double>(a, g, num_sms, s);
+  return launch_propagate_t<1, float2, float>(a, g, num_sms, s);
+}
+
+int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_t nspec, cudaStream_t s)
+{
+  const int rescale = (a.steady && a.rescale_lum) ? 1 : 0;
+  int n = 0;
+  if (rescale) {
+    rescale_spectrum_kernel<<<64, 256, 0, s>>>(a, nspec, a.n_packets);
+    ++n;
+  }
+  finish_zones_kernel<<<g.nzones, 256, 0, s>>>(a, vol, g.nzones, a.n_packets, rescale);
+  return n + 1;
+}
+
+}  // namespace sed

@@ -1,0 +1,98 @@
+"""Thin Python driver of the CUDA library (one sed_ctx) for a Workload.
+
+Used by the benchmark and by pubsed_b200.transport; every call goes through
+the C ABI of include/sedona_gpu.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from ._lib import lib as _load
+
+
+class Engine:
+    def __init__(self, workload, precision: int = abi.PREC_FP64, device: int = 0,
+                 n_packets: Optional[int] = None, seed_offset: int = 0):
+        self.L = _load()
+        self.w = workload
+        self.keep = abi.Keep()
+        self.tp = workload.transport_params(self.keep, precision, n_packets)
+        self.tp.rng_seed = (self.tp.rng_seed + seed_offset) & 0xFFFFFFFF
+        self.ctx = C.c_void_p()
+        self._check(self.L.sed_ctx_create(C.byref(self.tp), device, C.byref(self.ctx)), "sed_ctx_create")
+        self.nz = workload.zones.n_zones
+        self.nn = self.tp.nu_grid.n
+        self.nspec = self.tp.spec_time.n * self.tp.spec_nu.n * self.tp.spec_mu.n * self.tp.spec_phi.n
+        self.upload_grid()
+        op = workload.opacity_params(self.keep)
+        self._check(self.L.sed_set_opacity_params(self.ctx, C.byref(op)), "sed_set_opacity_params")
+        at = workload.atomic_struct(self.keep)
+        if at is not None:
+            self._check(self.L.sed_set_atomic_data(self.ctx, C.byref(at)), "sed_set_atomic_data")
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            msg = self.L.sed_last_error(self.ctx) if self.ctx else b""
+            raise RuntimeError("%s failed (%d): %s" % (what, rc, (msg or b"").decode()))
+
+    def upload_grid(self) -> int:
+        """sed_set_grid from host arrays; returns the bytes copied host->device."""
+        k = abi.Keep()
+        g = self.w.grid_struct(k)
+        self._check(self.L.sed_set_grid(self.ctx, C.byref(g)), "sed_set_grid")
+        return int(sum(a.nbytes for a in k.arrays))
+
+    def set_opacity(self, dt: float = 1.0):
+        self._check(self.L.sed_set_opacity(self.ctx, dt), "sed_set_opacity")
+
+    def transport(self, dt: float = 1.0) -> dict:
+        st = abi.StepStats()
+        self._check(self.L.sed_transport(self.ctx, dt, C.byref(st)), "sed_transport")
+        return st.as_dict()
+
+    def step(self, dt: float = 1.0) -> dict:
+        st = abi.StepStats()
+        self._check(self.L.sed_step(self.ctx, dt, C.byref(st)), "sed_step")
+        return st.as_dict()
+
+    def spectrum(self):
+        flux = np.zeros(self.nspec)
+        click = np.zeros(self.nspec)
+        self._check(self.L.sed_get_spectrum(self.ctx, flux.ctypes.data_as(abi._dp), click.ctypes.data_as(abi._dp)),
+                    "sed_get_spectrum")
+        return flux, click
+
+    def tallies(self) -> dict:
+        nj = self.nn if self.tp.store_Jnu else 1
+        out = {"J_nu": np.zeros(self.nz * nj)}
+        out.update({k: np.zeros(self.nz) for k in ("e_abs", "e_rad", "fx", "fy", "fz", "fr")})
+        P = lambda a: a.ctypes.data_as(abi._dp)
+        self._check(self.L.sed_get_zone_tallies(self.ctx, P(out["J_nu"]), P(out["e_abs"]), P(out["e_rad"]),
+                                                P(out["fx"]), P(out["fy"]), P(out["fz"]), P(out["fr"])),
+                    "sed_get_zone_tallies")
+        return out
+
+    def opacity(self) -> dict:
+        n = self.nz * self.nn
+        out = {k: np.zeros(n) for k in ("abs", "scat", "emis_cdf")}
+        out.update({k: np.zeros(self.nz) for k in ("n_elec", "eps_imc", "planck_mean", "rosseland_mean", "L_thermal")})
+        P = lambda a: a.ctypes.data_as(abi._dp)
+        self._check(self.L.sed_get_opacity(self.ctx, P(out["abs"]), P(out["scat"]), P(out["emis_cdf"]),
+                                           P(out["n_elec"]), P(out["eps_imc"]), P(out["planck_mean"]),
+                                           P(out["rosseland_mean"]), P(out["L_thermal"])), "sed_get_opacity")
+        return out
+
+    def close(self):
+        if self.ctx:
+            self.L.sed_ctx_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -16,7 +16,7 @@ from typing import Any, Optional
 import numpy as np
 
 from . import abi
-from .atomic import AtomicModel
+from .atomic import AtomicModel, add_fuzz_lines, synthetic_atoms
 from .grids import LocGrid, PI, grid_from_spec, lin_grid, lin_grid_n, log_delta_for_bins, shell_volumes
 from .params import Params
 
@@ -211,3 +211,74 @@ def lightbulb_grey(n_packets: int = 1_000_000, n_zones: int = 128, n_bins: int =
     }
     return Workload("lightbulb_grey_1d", params, z,
                     notes={"log_del": d, "v_max": 1e9, "t_days": 10.0})
+
+
+# Type Ia-like layered composition: (Z, A) and mass fractions per layer
+IA_ELEMENTS = [(6, 12), (8, 16), (14, 28), (16, 32), (20, 40), (28, 56)]
+IA_LAYERS = [  # (v_upper cm/s, mass fractions in IA_ELEMENTS order)
+    (4e8, [0.0, 0.0, 0.0, 0.0, 0.0, 1.0]),          # 56Ni
+    (1.2e9, [0.0, 0.0, 0.6, 0.3, 0.1, 0.0]),        # Si/S/Ca
+    (math.inf, [0.5, 0.5, 0.0, 0.0, 0.0, 0.0]),     # C/O
+]
+
+
+def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_000, n_bins: int = 4096,
+            n_levels_per_ion: int = 20, v_max: float = 3e9, epsilon: float = 1.0, seed: int = 0,
+            bound_free: int = 0, free_free: int = 1, spectrum_bins: int = 1024,
+            v_core: float = 1e9) -> Workload:
+    """Precision configuration: 1D Type Ia-like ejecta, 256 zones, 1.4 Msun,
+    rho ~ exp(-v / 2.7e8 cm/s), t = 20 d, layered 56Ni / Si-S-Ca / C-O
+    composition, T falling linearly from 1.2e4 K (inner) to 5e3 K (outer),
+    LTE Saha-Boltzmann populations, 5e5 synthetic fuzz lines (lambda
+    log-uniform 1000-30000 A, gf log-uniform 1e-4..1, El uniform 0-10 eV)
+    binned into 4096 log frequency bins, electron scattering and free-free,
+    a central 1.2e4 K lightbulb, radiative equilibrium (absorbed packets are
+    re-emitted from the zone emissivity), steady-state iteration.
+
+    Choices the configuration leaves open, fixed here: v_max = 3e9 cm/s;
+    Si/S/Ca = 0.6/0.3/0.1 and C/O = 0.5/0.5 by mass; five ion stages per
+    element with approximate real ionisation energies plus the bare stage,
+    `n_levels_per_ion` levels per stage (E uniform in [0, 0.8 chi), odd g);
+    each line's (element, stage) uniform over the 30 real stages; the
+    lightbulb is an inner boundary (core_radius = v_core * t, v_core = 1e9
+    cm/s, absorbing) radiating a 1.2e4 K blackbody with L = 1e43 erg/s;
+    opacity_epsilon = 1 (absorptive lines, Sedona's default).  With this line
+    list the ejecta are optically thick at every frequency; a central point
+    source costs ~5e4 segments per packet, the inner boundary ~2e3."""
+    rng = np.random.default_rng(seed)
+    t = 20 * 86400.0
+    v = np.array([(i + 1) * v_max / n_zones for i in range(n_zones)])
+    vc = np.concatenate([[0.0], v[:-1]]) * 0.5 + v * 0.5
+    Z = [e[0] for e in IA_ELEMENTS]
+    A = [e[1] for e in IA_ELEMENTS]
+    X = np.zeros((n_zones, len(Z)))
+    for i in range(n_zones):
+        for vu, frac in IA_LAYERS:
+            if vc[i] < vu:
+                X[i] = frac
+                break
+    T = np.array([1.2e4 + (5e3 - 1.2e4) * i / (n_zones - 1) for i in range(n_zones)])
+    shape = np.exp(-vc / 2.7e8)
+    z0 = sphere_model(v, t, shape, T, X, Z, A)
+    rho0 = 1.4 * M_SUN / float(np.sum(shape * z0.vol))
+    z = sphere_model(v, t, rho0 * shape, T, X, Z, A)
+    atoms = synthetic_atoms(Z, n_levels_per_ion, 0, rng)
+    add_fuzz_lines(atoms, n_lines, 1000.0, 30000.0, 1e-4, 1.0, 10.0, rng)
+    d = log_delta_for_bins(1e14, 3e15, n_bins)
+    ds = log_delta_for_bins(1e14, 3e15, spectrum_bins)
+    params = {
+        "grid_type": "grid_1D_sphere", "hydro_module": "homologous",
+        "transport_nu_grid": [1e14, 3e15, d, 1], "spectrum_nu_grid": [1e14, 3e15, ds, 1],
+        "transport_steady_iterate": 1, "transport_radiative_equilibrium": 1,
+        "opacity_grey_opacity": 0, "opacity_epsilon": epsilon,
+        "opacity_electron_scattering": 1, "opacity_fuzz_expansion": 1,
+        "opacity_free_free": int(free_free), "opacity_bound_free": int(bound_free),
+        "dont_decay_composition": 1,
+        "core_n_emit": int(n_packets), "core_radius": float(v_core * t), "core_temperature": 1.2e4,
+        "core_luminosity": 1e43,
+        "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
+        "particles_max_total": max(int(1e7), int(n_packets)),
+    }
+    return Workload("type_ia_1d", params, z, atoms,
+                    notes={"v_max": v_max, "t_days": 20.0, "rho0": rho0, "log_del": d,
+                           "n_lines": n_lines, "n_levels_per_ion": n_levels_per_ion})

@@ -1,0 +1,70 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Needs the reference harness built from the reference sources
+(oracle/ref/build_ref.sh -> oracle/_ref/sedona_ref and
+oracle/_ref/locate_array_test).  Each fixture records the workload that made
+it (generator name and arguments) so tests can rebuild the same seeded
+inputs, plus the reference's outputs:
+
+  replay_*.npz   one transport step in replay mode (per-packet fate, final
+                 zone, number of deviates drawn, final state; J_nu, e_abs,
+                 e_rad, forces, spectrum; opacity tables)
+  locate_kat.json  value/index pairs printed by the reference's own
+                 src/utils/locate_array_test.cpp
+
+usage: python tests/golden/make_golden.py
+"""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+
+from pubsed_b200 import workloads  # noqa: E402
+import run_ref  # noqa: E402
+
+CASES = {
+    "replay_grey_absorb": ("lightbulb_grey", dict(n_packets=1000, n_zones=32, n_bins=128, radiative_eq=0, seed=3)),
+    "replay_grey_radeq": ("lightbulb_grey", dict(n_packets=600, n_zones=32, n_bins=128, radiative_eq=1, seed=5)),
+    "replay_ia_lte": ("type_ia", dict(n_packets=300, n_zones=16, n_lines=5000, n_bins=256, n_levels_per_ion=6,
+                                      bound_free=1, free_free=1, seed=7)),
+}
+
+KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "J_nu", "e_abs", "e_rad", "fx_rad", "fy_rad", "fz_rad",
+        "fr_rad", "spec_flux", "spec_click", "abs", "scat", "emis_cdf", "n_elec", "eps_imc", "planck_mean",
+        "rosseland_mean", "L_thermal", "nu_right", "nu_left"]
+
+
+def make_workload(gen: str, kw: dict):
+    return getattr(workloads, gen)(**kw)
+
+
+def main():
+    if not run_ref.available():
+        raise SystemExit("build the reference harness first: oracle/ref/build_ref.sh")
+    for name, (gen, kw) in CASES.items():
+        w = make_workload(gen, kw)
+        out = run_ref.run(w, "replay", threads=1, seed=kw.get("seed", 0))
+        arrays = {k: out[k] for k in KEYS}
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
+                            n_escaped=out["n_escaped"], **arrays)
+        print(name, "packets", int(out["n_packets"]), "escaped", int(out["n_escaped"]))
+    # locate_array_test: stderr holds "value index" lines, one block of 8
+    # values per grid; the first block (20 zero walls, uninitialised minimum)
+    # is skipped
+    exe = os.path.join(ROOT, "oracle", "_ref", "locate_array_test")
+    r = subprocess.run([exe], capture_output=True, text=True, check=True)
+    pairs = [ln.split() for ln in r.stderr.strip().splitlines()]
+    with open(os.path.join(HERE, "locate_kat.json"), "w") as f:
+        json.dump({"source": "src/utils/locate_array_test.cpp", "pairs": pairs}, f, indent=0)
+    print("locate pairs", len(pairs))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,131 @@
+"""The oracle against the reference's own outputs (CPU only).
+
+The fixtures in tests/golden/ were produced by the reference code itself
+(built from its sources with MPI/GSL/HDF5 stand-ins, tests/golden/make_golden.py):
+one replayed transport step per case, where the reference and the oracle draw
+the same Philox deviates for every packet, and the value/index pairs printed
+by the reference's src/utils/locate_array_test.cpp.
+"""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+from pubsed_b200 import abi, grids, workloads
+import oracle_lib
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte"]
+
+
+def _load(name):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    w = getattr(workloads, str(d["generator"]))(**json.loads(str(d["kwargs"])))
+    return d, w
+
+
+def _rel(a, b):
+    fin = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), fin)
+    s = np.maximum(np.abs(b[fin]), 1e-300)
+    return float(np.max(np.abs(a[fin] - b[fin]) / s)) if s.size else 0.0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference_replay(name):
+    ref, w = _load(name)
+    e = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    e.set_opacity(1.0)
+    O = e.opacity()
+    # the opacity build is the same arithmetic in the same order
+    for k in ("abs", "scat", "emis_cdf", "eps_imc", "planck_mean", "rosseland_mean", "L_thermal"):
+        assert _rel(O[k], ref[k]) <= 1e-14, k
+    if w.atoms is not None:
+        assert _rel(O["n_elec"], ref["n_elec"]) <= 1e-14
+    e.record(True)
+    n = int(ref["pkt_fate"].size)
+    st = e.transport(1.0)
+    rec = e.records(n)
+    assert np.array_equal(rec["fate"], ref["pkt_fate"])
+    assert np.array_equal(rec["ind"], ref["pkt_ind"])
+    assert np.array_equal(rec["draws"], ref["pkt_draws"])
+    assert oracle_lib.state_rel(rec["state"], ref["pkt_state"].reshape(-1, 9)) <= 1e-13
+    assert st["n_escaped"] == int(ref["n_escaped"])
+    T = e.tallies()
+    for k, rk in (("J_nu", "J_nu"), ("e_abs", "e_abs"), ("e_rad", "e_rad"), ("fr", "fr_rad")):
+        assert _rel(T[k], ref[rk]) <= 1e-12, k
+    f, c = e.spectrum()
+    assert np.array_equal(c, ref["spec_click"])
+    assert _rel(f, ref["spec_flux"]) <= 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_frequency_grid_walls_match_reference(name):
+    ref, w = _load(name)
+    g = w.nu_grid()
+    assert np.array_equal(g.right, ref["nu_right"])
+    assert np.array_equal(g.left(), ref["nu_left"])
+
+
+def _locate(g: grids.LocGrid, x: float) -> int:
+    k = abi.Keep()
+    lg = abi.locate_grid(k, g)
+    return oracle_lib.oracle_lib().oracle_locate(C.byref(lg), x)
+
+
+def test_locate_known_answers():
+    """src/utils/locate_array_test.cpp, cases 2-9 (case 1 has an
+    uninitialised minimum in the reference and is skipped)."""
+    with open(os.path.join(GOLDEN, "locate_kat.json")) as f:
+        pairs = json.load(f)["pairs"]
+    vals = [-10, 0, 1, 3.3, 9, 10, 11, 20]
+    x7 = np.arange(7, dtype=np.float64)
+    cases = [
+        grids.lin_grid(1.0, 10.0, 1.0),
+        grids.log_grid(1.0, 10.0, 0.2),
+        grids.lin_grid_n(1.0, 10.0, 10),
+        grids.LocGrid(x7, -2.0, 0.0, abi.LOC_FLEX),
+        grids.LocGrid(x7[:5].copy(), -1.0, 0.0, abi.LOC_FLEX),
+        grids.lin_grid(0.0, 0.0, 0.0),
+        grids.lin_grid_n(10.0, 20.0, 2),
+        grids.lin_grid(0.0, 9.07e13, 1.234e12),
+    ]
+    k = 8  # skip the first block
+    for ci, g in enumerate(cases):
+        xs = ([3.3e13, 3.4e13] if ci == len(cases) - 1 else []) + vals
+        for x in xs:
+            v, idx = pairs[k]
+            assert float(v) == float(x)
+            assert _locate(g, float(x)) == int(idx), (ci, x)
+            k += 1
+    assert k == len(pairs)
+
+
+def test_philox_known_answer_vectors():
+    """Philox4x32-10 known-answer vectors published with the Random123
+    library (Salmon et al., SC'11)."""
+    L = oracle_lib.oracle_lib()
+    L.oracle_philox.argtypes = [C.POINTER(C.c_uint32 * 4), C.POINTER(C.c_uint32 * 2), C.POINTER(C.c_uint32 * 4)]
+    kats = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in kats:
+        c = (C.c_uint32 * 4)(*ctr)
+        kk = (C.c_uint32 * 2)(*key)
+        out = (C.c_uint32 * 4)()
+        L.oracle_philox(C.byref(c), C.byref(kk), C.byref(out))
+        assert tuple(out) == want
+
+
+def test_packet_uniforms_in_unit_interval():
+    L = oracle_lib.oracle_lib()
+    L.oracle_uniform.argtypes = [C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32]
+    L.oracle_uniform.restype = C.c_double
+    u = np.array([L.oracle_uniform(0, p, 0, n) for p in range(64) for n in range(32)])
+    assert u.min() >= 0.0 and u.max() < 1.0
+    assert abs(u.mean() - 0.5) < 0.03
