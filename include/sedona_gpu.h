@@ -236,6 +236,36 @@ void sed_ctx_destroy(sed_ctx* ctx);
 /* Library version / build string (never NULL). */
 const char* sed_version(void);
 
+/* LTE electron density of every zone (the Saha-Boltzmann / Brent solve that
+ * sed_set_opacity runs first), for callers that cannot allocate device memory
+ * when they need it -- e.g. a host code whose device memory is all handed out
+ * by its own pool allocator, or a per-step loop that cannot afford the
+ * synchronisation cudaMalloc/cudaFree bring.  No counterpart in the
+ * reference: it has no GPU and no allocation constraints.
+ *
+ * Every pointer is a DEVICE pointer owned by the caller, including the arrays
+ * inside *atoms_dev (only ion_off, ion_chi, lev_off, lev_ion, lev_g, lev_E are
+ * read; the struct itself is in host memory).  rho, T_gas: [n_zones];
+ * X: [n_zones * n_elems] mass fractions; elem_A: [n_elems]; outputs
+ * n_elec: [n_zones] (cm^-3) and solve_err: [n_zones] (0 ok, 1 root not
+ * bracketed, 2 iteration limit).  The work is queued on `stream`
+ * (cudaStream_t, NULL = legacy default stream); the call returns without
+ * waiting for it.
+ *
+ * The per-zone working set lives in a fixed 4 MiB array inside the library
+ * (every GPU that loads the library holds it until exit).  The call returns
+ * SED_ERR_CAPACITY when n_zones * (2 n_elems + 2 + 2 n_ions_total +
+ * 2 n_levels_total) exceeds 524288.  All calls on a device share that array,
+ * so calls whose work overlaps on the GPU (different streams, or other
+ * threads) race; serialise them.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture. */
+int sed_lte_electron_density_noalloc(int32_t n_zones, const double* rho, const double* T_gas,
+                                     const double* X, int32_t n_elems, const int32_t* elem_A,
+                                     const sed_atomic_data* atoms_dev, int32_t n_ions_total,
+                                     int32_t n_levels_total, double temp_min, double temp_max,
+                                     double* n_elec, int32_t* solve_err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

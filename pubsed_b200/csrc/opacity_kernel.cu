@@ -24,6 +24,8 @@
 //                       the packed tables the packet kernel reads.
 #include <cfloat>
 #include <cmath>
+#include <mutex>
+#include "../../include/sedona_gpu.h"
 #include "sed_internal.h"
 
 namespace sed {
@@ -483,3 +485,94 @@ int launch_opacity(const OpacityArgs& a, int num_sms, cudaStream_t s)
 }
 
 }  // namespace sed
+
+// ---------------------------------------------------------------------------
+// LTE electron densities without any device allocation.
+//
+// Some callers cannot allocate device memory at the point where they need
+// this result: a host code whose device memory is entirely handed out by its
+// own pool allocator, or one that runs the solve inside a per-step loop where
+// the implicit synchronisation of cudaMalloc/cudaFree is not acceptable.
+// They own the inputs and the outputs.  The per-zone working set of the
+// solve (mass fractions, number densities, clamped temperature, partition
+// functions, ion fractions, level populations, Boltzmann factors) lives in
+// the fixed array below, which is part of the library image: every GPU that
+// loads the library holds it until the process exits.
+namespace {
+constexpr size_t NOALLOC_SCRATCH_DOUBLES = size_t(1) << 19;  // 4 MiB per device
+__device__ __align__(256) double g_lte_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_addr[NOALLOC_MAX_DEVICES] = {};
+}  // namespace
+
+extern "C" int sed_lte_electron_density_noalloc(int32_t n_zones, const double* rho, const double* T_gas,
+                                                const double* X, int32_t n_elems, const int32_t* elem_A,
+                                                const sed_atomic_data* atoms_dev, int32_t n_ions_total,
+                                                int32_t n_levels_total, double temp_min, double temp_max,
+                                                double* n_elec, int32_t* solve_err, void* stream)
+{
+  using namespace sed;
+  if (n_zones <= 0 || n_elems <= 0 || n_ions_total <= 0 || n_levels_total <= 0) return SED_ERR_ARG;
+  if (!rho || !T_gas || !X || !elem_A || !atoms_dev || !n_elec || !solve_err) return SED_ERR_ARG;
+  if (atoms_dev->n_atoms != n_elems || !atoms_dev->ion_off || !atoms_dev->ion_chi || !atoms_dev->lev_off ||
+      !atoms_dev->lev_ion || !atoms_dev->lev_g || !atoms_dev->lev_E)
+    return SED_ERR_ARG;
+  const size_t nz = (size_t)n_zones, na = (size_t)n_elems;
+  const size_t ni = (size_t)n_ions_total, nl = (size_t)n_levels_total;
+  const size_t need = nz * (2 * na + 2 + 2 * ni + 2 * nl);
+  if (need > NOALLOC_SCRATCH_DOUBLES) return SED_ERR_CAPACITY;  // limit stated in include/sedona_gpu.h
+
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return SED_ERR_CUDA;
+  double* base = nullptr;
+  {
+    // first call on this device: look up the array's device address with
+    // this device current (the host-side symbol is only a stand-in)
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_lte_scratch) != cudaSuccess || !p) return SED_ERR_CUDA;
+      g_scratch_addr[dev] = static_cast<double*>(p);
+    }
+    base = g_scratch_addr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  OpacityArgs A{};
+  A.nzones = n_zones;
+  A.nelem = n_elems;
+  A.natoms = n_elems;
+  A.temp_min = temp_min;
+  A.temp_max = temp_max;
+  A.rho = rho;
+  A.T = T_gas;
+  A.X = X;
+  A.eA = elem_A;
+  A.ion_off = atoms_dev->ion_off;
+  A.ion_chi = atoms_dev->ion_chi;
+  A.lev_off = atoms_dev->lev_off;
+  A.lev_ion = atoms_dev->lev_ion;
+  A.lev_g = atoms_dev->lev_g;
+  A.lev_E = atoms_dev->lev_E;
+  A.n_ions_total = n_ions_total;
+  A.n_lev_total = n_levels_total;
+  // carve the scratch array
+  double* q = base;
+  A.mass_frac = q;  q += na * nz;
+  A.n_dens = q;     q += na * nz;
+  A.temp_c = q;     q += nz;
+  double* grey = q; q += nz;  // all zones take the microphysical path: zero grey opacity
+  A.ion_part = q;   q += ni * nz;
+  A.ion_frac = q;   q += ni * nz;
+  A.lev_n = q;      q += nl * nz;
+  A.boltz = q;      q += nl * nz;
+  A.grey = grey;
+  A.n_elec = n_elec;
+  A.solve_err = solve_err;
+  // the array keeps the previous call's contents; only the grey-opacity
+  // column must start at zero (every other entry is written before it is read)
+  if (cudaMemsetAsync(grey, 0, nz * sizeof(double), s) != cudaSuccess) return SED_ERR_CUDA;
+  zone_state_kernel<<<(unsigned)((nz + 127) / 128), 128, 0, s>>>(A, A.boltz);
+  return cudaGetLastError() == cudaSuccess ? SED_OK : SED_ERR_CUDA;
+}
