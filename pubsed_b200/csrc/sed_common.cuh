@@ -55,27 +55,40 @@ __host__ __device__ inline double u01(uint32_t a, uint32_t b)
   return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
 }
 
-// Per-packet stream with a one-pair cache: odd draws reuse the Philox block
-// of the preceding even draw.
+// Per-packet stream.  Each draw evaluates its Philox block: lanes of a warp
+// sit at different draw parities, so keeping the odd half of a block for the
+// next draw would only make half the lanes compute while the others wait.
+#ifndef SED_RNG_CACHE
+#define SED_RNG_CACHE 0
+#endif
 struct PacketRng {
   uint32_t seed, step;
   uint64_t pid;
   uint32_t n;
+#if SED_RNG_CACHE
   uint32_t cached_ctr;
   uint32_t cw2, cw3;
   bool have;
+#endif
 
   __device__ void init(uint32_t seed_, uint64_t pid_, uint32_t step_, uint32_t n0)
   {
-    seed = seed_; pid = pid_; step = step_; n = n0; have = false;
+    seed = seed_; pid = pid_; step = step_; n = n0;
+#if SED_RNG_CACHE
+    have = false;
+#endif
   }
   __device__ double next()
   {
     const uint32_t k = n++;
     const uint32_t ctr = k >> 1;
+#if SED_RNG_CACHE
     if ((k & 1u) && have && cached_ctr == ctr) return u01(cw2, cw3);
+#endif
     PhiloxOut o = philox4x32_10(ctr, (uint32_t)pid, (uint32_t)(pid >> 32), step, seed, 0u);
+#if SED_RNG_CACHE
     cached_ctr = ctr; cw2 = o.w[2]; cw3 = o.w[3]; have = true;
+#endif
     return (k & 1u) ? u01(o.w[2], o.w[3]) : u01(o.w[0], o.w[1]);
   }
 };

@@ -302,14 +302,14 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 }
 
 // Block size and minimum resident blocks per SM of the packet kernel.  The
-// kernel is latency bound (dependent FP64 chains, L2 table loads); 3 blocks
-// of 256 threads (24 warps/SM, 80 registers) beat 2 blocks at 124 registers
-// by 12% on the Type Ia workload despite a small register spill.
+// kernel is latency bound (dependent FP64 chains, L2 table loads): 8 blocks
+// of 128 threads (32 warps/SM, 64 registers) run the Type Ia step 19% faster
+// than 2 blocks of 256 at 120 registers, despite a small register spill.
 #ifndef SED_PROP_THREADS
-#define SED_PROP_THREADS 256
+#define SED_PROP_THREADS 128
 #endif
 #ifndef SED_PROP_MINB
-#define SED_PROP_MINB 3
+#define SED_PROP_MINB 8
 #endif
 
 template <int GRID, typename OT, typename CT>
@@ -333,26 +333,72 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
   const uint32_t K = (A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u;
 
   unsigned long long n_esc = 0, n_abs = 0, n_stop = 0, n_seg = 0, n_scat = 0, n_lim = 0;
+  // One loop iteration is either one segment of the lane's packet or, when
+  // that packet has finished, its bookkeeping and the emission of the next
+  // packet.  A lane therefore refills as soon as its packet ends instead of
+  // idling until the longest packet of its warp is done.
+  Pkt p;
+  PacketRng rng;
+  int fate = ABSORBED;  // no packet yet
+  bool have = false;    // a finished packet awaits its bookkeeping
+  unsigned long long pid = 0;
+  int64_t seg = 0;
+  // zone-scalar tallies of the packet's current zone, kept in registers
+  // while the packet stays in that zone and added to the shared/global
+  // tally when it leaves (the same terms, summed per visit first)
+  int acc_zone = -1;
+  double acc_eabs = 0, acc_fx = 0, acc_fy = 0, acc_fz = 0, acc_fr = 0;
   for (;;) {
-    const unsigned long long pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
-    if (pid >= (unsigned long long)A.n_packets) break;
-    Pkt p;
-    PacketRng rng;
-    rng.init(A.seed, (uint64_t)A.first_pid + pid, A.step, 0);
-    emit_core<GRID>(A, G, p, rng);
-    // transport::propagate (transport.cpp:202-254)
-    int fate = MOVING;
-    p.ind = get_zone<GRID>(G, p.x);
-    if (p.ind == -1) fate = ABSORBED;
-    else if (p.ind == -2) fate = ESCAPED;
-    int64_t seg = 0;
-    // zone-scalar tallies of the packet's current zone, kept in registers
-    // while the packet stays in that zone and added to the shared/global
-    // tally when it leaves (the same terms, summed per visit first)
-    int acc_zone = -1;
-    double acc_eabs = 0, acc_fx = 0, acc_fy = 0, acc_fz = 0, acc_fr = 0;
-    while (fate == MOVING) {
-      if (seg >= limit) { fate = STOPPED; ++n_lim; break; }
+    if (fate != MOVING) {
+      if (have) {
+        if (acc_zone >= 0) {
+          atomicAdd(t_eabs + acc_zone, acc_eabs);
+          if (A.tally_forces) {
+            atomicAdd(t_fx + acc_zone, acc_fx);
+            atomicAdd(t_fy + acc_zone, acc_fy);
+            atomicAdd(t_fz + acc_zone, acc_fz);
+            atomicAdd(t_fr + acc_zone, acc_fr);
+          }
+        }
+        n_seg += seg;
+        if (fate == ESCAPED) {
+          const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
+          spectrum_count(A, t_obs, p.nu, p.e, p.D);
+          p.t = t_obs;
+          ++n_esc;
+        } else if (fate == ABSORBED) {
+          ++n_abs;
+        } else {
+          ++n_stop;
+        }
+        if (A.rec_fate) {
+          A.rec_fate[pid] = fate;
+          A.rec_ind[pid] = p.ind;
+          A.rec_draws[pid] = (int32_t)(rng.n - K);
+          double* s = A.rec_state + pid * 9;
+          s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
+          s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+          s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+        }
+        have = false;
+      }
+      pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
+      if (pid >= (unsigned long long)A.n_packets) break;
+      rng.init(A.seed, (uint64_t)A.first_pid + pid, A.step, 0);
+      emit_core<GRID>(A, G, p, rng);
+      // transport::propagate (transport.cpp:202-254)
+      fate = MOVING;
+      p.ind = get_zone<GRID>(G, p.x);
+      if (p.ind == -1) fate = ABSORBED;
+      else if (p.ind == -2) fate = ESCAPED;
+      seg = 0;
+      acc_zone = -1;
+      acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
+      have = true;
+      if (fate != MOVING) continue;
+    }
+    {
+      if (seg >= limit) { fate = STOPPED; ++n_lim; continue; }
       ++seg;
       const int iz = p.ind;
       if (iz != acc_zone) {
@@ -437,35 +483,6 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
       } else {
         fate = STOPPED;
       }
-    }
-    if (acc_zone >= 0) {
-      atomicAdd(t_eabs + acc_zone, acc_eabs);
-      if (A.tally_forces) {
-        atomicAdd(t_fx + acc_zone, acc_fx);
-        atomicAdd(t_fy + acc_zone, acc_fy);
-        atomicAdd(t_fz + acc_zone, acc_fz);
-        atomicAdd(t_fr + acc_zone, acc_fr);
-      }
-    }
-    n_seg += seg;
-    if (fate == ESCAPED) {
-      const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
-      spectrum_count(A, t_obs, p.nu, p.e, p.D);
-      p.t = t_obs;
-      ++n_esc;
-    } else if (fate == ABSORBED) {
-      ++n_abs;
-    } else {
-      ++n_stop;
-    }
-    if (A.rec_fate) {
-      A.rec_fate[pid] = fate;
-      A.rec_ind[pid] = p.ind;
-      A.rec_draws[pid] = (int32_t)(rng.n - K);
-      double* s = A.rec_state + pid * 9;
-      s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
-      s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
-      s[6] = p.t; s[7] = p.e; s[8] = p.nu;
     }
   }
   // counters: warp reduction, one atomic per warp
