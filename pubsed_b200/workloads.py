@@ -223,7 +223,7 @@ IA_LAYERS = [  # (v_upper cm/s, mass fractions in IA_ELEMENTS order)
 
 
 def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_000, n_bins: int = 4096,
-            n_levels_per_ion: int = 20, v_max: float = 3e9, epsilon: float = 1.0, seed: int = 0,
+            n_levels_per_ion: int = 20, v_max: float = 3e9, epsilon: float = 1.0, seed: int = 0, data_seed: int = 0,
             bound_free: int = 0, free_free: int = 1, spectrum_bins: int = 1024,
             v_core: float = 1e9) -> Workload:
     """Precision configuration: 1D Type Ia-like ejecta, 256 zones, 1.4 Msun,
@@ -245,7 +245,7 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
     opacity_epsilon = 1 (absorptive lines, Sedona's default).  With this line
     list the ejecta are optically thick at every frequency; a central point
     source costs ~5e4 segments per packet, the inner boundary ~2e3."""
-    rng = np.random.default_rng(seed)
+    rng = np.random.default_rng(data_seed)  # synthetic atoms and lines; `seed` keys the packets
     t = 20 * 86400.0
     v = np.array([(i + 1) * v_max / n_zones for i in range(n_zones)])
     vc = np.concatenate([[0.0], v[:-1]]) * 0.5 + v * 0.5

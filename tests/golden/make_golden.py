@@ -36,6 +36,11 @@ CASES = {
                                       bound_free=1, free_free=1, seed=7)),
 }
 
+FREE_CASES = {
+    "free_grey_radeq": ("lightbulb_grey", dict(n_packets=200000, n_zones=128, n_bins=256, radiative_eq=1, seed=101)),
+    "free_ia": ("type_ia", dict(n_packets=60000, n_zones=64, n_lines=50000, n_bins=1024, seed=103)),
+}
+
 KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "J_nu", "e_abs", "e_rad", "fx_rad", "fy_rad", "fz_rad",
         "fr_rad", "spec_flux", "spec_click", "abs", "scat", "emis_cdf", "n_elec", "eps_imc", "planck_mean",
         "rosseland_mean", "L_thermal", "nu_right", "nu_left"]
@@ -55,6 +60,15 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
                             n_escaped=out["n_escaped"], **arrays)
         print(name, "packets", int(out["n_packets"]), "escaped", int(out["n_escaped"]))
+    # free-running reference steps (its own transport::step, OpenMP, streams
+    # independent of the per-packet replay streams) for the chi-squared tests
+    for name, (gen, kw) in FREE_CASES.items():
+        w = make_workload(gen, kw)
+        out = run_ref.run(w, "free", threads=os.cpu_count() or 1, seed=kw.get("seed", 0))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
+                            spec_flux=out["spec_flux"], spec_click=out["spec_click"], e_rad=out["e_rad"],
+                            e_abs=out["e_abs"])
+        print(name, "clicks", int(out["spec_click"].sum()))
     # locate_array_test: stderr holds "value index" lines, one block of 8
     # values per grid; the first block (20 zero walls, uninitialised minimum)
     # is skipped
