@@ -244,8 +244,11 @@ def main():
     if os.path.exists(tfile):
         with open(tfile) as f:
             tr = json.load(f)
-        # scale the captured launch's DRAM bytes by segments processed
-        traffic = tr["dram_bytes"] * (last["n_segments"] / tr["n_segments"])
+        # DRAM bytes of one launch captured with ncu on this workload; the
+        # tables stay L2-resident, so traffic does not grow with the packet
+        # count and is only reported for the captured packet count
+        if int(tr.get("packets", -1)) == args.packets and tr.get("workload") == w.name:
+            traffic = float(tr["dram_bytes"])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
