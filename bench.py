@@ -18,6 +18,11 @@ packets, run through the C ABI (include/sedona_gpu.h).
 
 Multi-GPU: packets are independent, so N ranks run N independent replicas of
 the step (weak scaling); no collective is on the data path.
+
+--workload cart3d runs the 3D configuration instead (128^3 Cartesian cells,
+1e5 lines, 2048 bins, 1e8 packets, 16 mu bins); its reference arm runs the
+reference on a 32^3 grid of the same model (the reference CPU cannot hold the
+128^3 x 2048 tables in host memory) and scales set_opacity by the zone count.
 """
 from __future__ import annotations
 
@@ -89,14 +94,16 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ reference arm
-def run_reference(args, workload_fn, rank: int) -> dict:
+def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
     sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
     import run_ref
     if not run_ref.available():
         return {"impl": "reference", "unavailable": "reference harness oracle/_ref/sedona_ref is not built"}
     cores = os.cpu_count() or 1
     n_sample = args.ref_packets
-    w = workload_fn(n_sample)
+    w_full = workload_fn(1)
+    w = (sample_fn or workload_fn)(n_sample)
+    zone_scale = w_full.zones.n_zones / w.zones.n_zones
     # warm-up (untimed), then the timed steps; each step is the reference's
     # own transport::step on a bounded packet sample
     out = run_ref.run(w, "free", threads=cores, steps=args.warmup + args.steps, timeout=3600)
@@ -106,18 +113,22 @@ def run_reference(args, workload_fn, rank: int) -> dict:
     # the opacity build is per step, propagation per packet: the reference's
     # time for the full step is t_opac + (t_sample - t_opac) * N / n_sample
     n_full = args.packets
-    t = t_opac + max(t_sample - t_opac, 0.0) * n_full / n_sample
+    t = t_opac * zone_scale + max(t_sample - t_opac, 0.0) * n_full / n_sample
     value = n_full / t
+    grid_note = "" if zone_scale == 1 else (
+        " on a reduced %d-zone grid of the same model: set_opacity scaled by the zone count (x%g), "
+        "propagation per packet measured on the reduced grid" % (w.zones.n_zones, zone_scale))
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "n_zones": w.zones.n_zones, "n_lines": w.notes.get("n_lines"),
-                       "n_bins": w.nu_grid().n, "packets_per_step": n_sample, "threads": cores},
+            "config": {"workload": w.name, "n_zones": w_full.zones.n_zones, "n_lines": w.notes.get("n_lines"),
+                       "n_bins": w.nu_grid().n, "packets_per_step": n_sample, "threads": cores,
+                       "sample_zones": w.zones.n_zones},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": "transport::step of the %s workload (full zone/line/bin sizes) with %d "
                                        "packets per step (%.2f s, of which set_opacity %.2f s); full-step time "
-                                       "= set_opacity + propagation scaled to %d packets" %
-                                       (w.name, n_sample, t_sample, t_opac, n_full)},
+                                       "= set_opacity + propagation scaled to %d packets%s" %
+                                       (w.name, n_sample, t_sample, t_opac, n_full, grid_note)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "sample_packets_per_s": n_sample / t_sample, "set_opacity_seconds": t_opac}
 
@@ -129,8 +140,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--packets", type=int, default=10_000_000)
-    ap.add_argument("--ref-packets", type=int, default=20_000)
+    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d"])
+    ap.add_argument("--packets", type=int, default=None)
+    ap.add_argument("--ref-packets", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     args = ap.parse_args()
@@ -138,13 +150,27 @@ def main():
 
     from pubsed_b200 import workloads
 
-    def wl(n):
-        return workloads.type_ia(n_packets=n)
+    sample_fn = None
+    if args.workload == "cart3d":
+        def wl(n):
+            return workloads.cart3d(n_packets=n)
+
+        def sample_fn(n):
+            return workloads.cart3d(n_packets=n, n_cells=32)
+        default_packets, default_ref = 100_000_000, 4000
+    else:
+        def wl(n):
+            return workloads.type_ia(n_packets=n)
+        default_packets, default_ref = 10_000_000, 20_000
+    if args.packets is None:
+        args.packets = default_packets
+    if args.ref_packets is None:
+        args.ref_packets = default_ref
 
     if args.impl == "reference":
         if world > 1 and rank != 0:
             return
-        print(json.dumps(run_reference(args, wl, rank)), flush=True)
+        print(json.dumps(run_reference(args, wl, rank, sample_fn)), flush=True)
         return
 
     import numpy as np
@@ -213,7 +239,9 @@ def main():
         b_in = eng.upload_grid()
         eng.step(1.0)
         flux, click = eng.spectrum()
-        tal = eng.tallies()
+        # the 3D J_nu array (n_zones x n_bins FP64, 34 GB at 128^3 x 2048) stays
+        # on the device; its zone-scalar tallies and the spectrum come back
+        tal = eng.tallies(J=(w.zones.type != abi.GRID_3D_CART))
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
         h2d = b_in
@@ -225,10 +253,10 @@ def main():
     e2e_value = world * args.packets / float(t_e2e.item())
 
     # roofline of the packet kernel: algorithmic bytes per segment and per
-    # packet (zone geometry 16 B, {abs,scat} 8 B (FP32), J RMW 16 B, e_abs
-    # RMW 16 B, force RMW 64 B per segment; 2 x 76 B state + 32 B spectrum +
-    # 80 B emission CDF per packet)
-    b_seg = 16 + 8 + 16 + 16 + 64
+    # packet (zone geometry 16 B in 1D / 24 B in 3D, {abs,scat} 8 B (FP32),
+    # J RMW 16 B, e_abs RMW 16 B, force RMW 64 B per segment; 2 x 76 B state
+    # + 32 B spectrum + 80 B emission CDF per packet)
+    b_seg = (24 if w.zones.type == abi.GRID_3D_CART else 16) + 8 + 16 + 16 + 64
     b_pkt = 264
     alg_bytes = last["n_segments"] * b_seg + args.packets * b_pkt
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
@@ -271,7 +299,7 @@ def main():
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         try:
             ref = run_reference(argparse.Namespace(ref_packets=args.ref_packets, warmup=1, steps=1,
-                                                     packets=args.packets), wl, rank)
+                                                     packets=args.packets), wl, rank, sample_fn)
             if "unavailable" in ref:
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                                         "sample": ref["unavailable"]}

@@ -146,11 +146,12 @@ _CHI = {
 
 
 def synthetic_atoms(elements, n_levels_per_ion: int, n_lines_per_ion: int,
-                    rng: np.random.Generator) -> AtomicModel:
+                    rng: np.random.Generator, E_max_eV: Optional[float] = None) -> AtomicModel:
     """Seeded synthetic ion/level model: five real stages per element (the
     ionisation energies above) plus the bare stage, `n_levels_per_ion`
-    levels per stage with E in [0, 0.8 chi) (ground level at 0) and odd g,
-    and optional level-to-level lines with A log-uniform in 1e4..1e8 s^-1."""
+    levels per stage with E in [0, 0.8 chi) (ground level at 0; the bound is
+    min(0.8 chi, E_max_eV) when E_max_eV is given) and odd g, and optional
+    level-to-level lines with A log-uniform in 1e4..1e8 s^-1."""
     atoms = []
     for Z in elements:
         chi = list(_CHI[Z]) + [99999.0]
@@ -158,7 +159,8 @@ def synthetic_atoms(elements, n_levels_per_ion: int, n_lines_per_ion: int,
         for s in range(len(chi)):
             ground.append(len(lev_ion))
             nl = 1 if s == len(chi) - 1 else n_levels_per_ion
-            Es = np.sort(rng.uniform(0.0, 0.8 * chi[s], nl - 1)) if nl > 1 else np.zeros(0)
+            top = 0.8 * chi[s] if E_max_eV is None else min(0.8 * chi[s], E_max_eV)
+            Es = np.sort(rng.uniform(0.0, top, nl - 1)) if nl > 1 else np.zeros(0)
             Es = np.concatenate([[0.0], Es])
             gs = 2 * rng.integers(0, 5, nl) + 1
             if s == len(chi) - 1:
@@ -176,6 +178,52 @@ def synthetic_atoms(elements, n_levels_per_ion: int, n_lines_per_ion: int,
                               lev_E=np.array(lev_E), line_l=np.array(ll, np.int32),
                               line_u=np.array(lu, np.int32), line_A=np.array(A)))
     return AtomicModel(atoms)
+
+
+def add_level_lines(model: AtomicModel, n_lines: int, nu_min: float, nu_max: float,
+                    rng: np.random.Generator, A_min: float = 1e4, A_max: float = 1e8) -> AtomicModel:
+    """Synthetic level-to-level line list for the Sobolev line-expansion
+    opacity: each line's (element, ion stage) uniform over the real stages
+    of the elements present, its lower/upper level a uniform pair of distinct
+    levels of that stage whose transition frequency lies strictly inside
+    (nu_min, nu_max) (pairs outside are redrawn), Einstein A log-uniform in
+    [A_min, A_max].  Exactly n_lines lines; each atom keeps its lines in
+    draw order."""
+    species = [(ai, s) for ai, a in enumerate(model.atoms) for s in range(a.n_ions - 1)]
+    out = {ai: ([], [], []) for ai in range(len(model.atoms))}
+    made = 0
+    while made < n_lines:
+        m = 2 * (n_lines - made) + 64
+        pick = rng.integers(0, len(species), m)
+        r1 = rng.random(m)
+        r2 = rng.random(m)
+        lgA = rng.uniform(np.log10(A_min), np.log10(A_max), m)
+        for k in range(m):
+            if made == n_lines:
+                break
+            ai, s = species[pick[k]]
+            a = model.atoms[ai]
+            g0 = int(a.ion_ground[s])
+            nlev = int(a.ion_ground[s + 1]) - g0
+            l = g0 + int(r1[k] * nlev)
+            u = g0 + int(r2[k] * nlev)
+            if l == u:
+                continue
+            if a.lev_E[l] > a.lev_E[u]:
+                l, u = u, l
+            nu = (float(a.lev_E[u]) - float(a.lev_E[l])) * EV_TO_ERGS / H
+            if not (nu_min < nu < nu_max):
+                continue
+            out[ai][0].append(l)
+            out[ai][1].append(u)
+            out[ai][2].append(10.0 ** lgA[k])
+            made += 1
+    for ai, a in enumerate(model.atoms):
+        ll, lu, A = out[ai]
+        a.line_l = np.array(ll, np.int32)
+        a.line_u = np.array(lu, np.int32)
+        a.line_A = np.array(A, np.float64)
+    return model
 
 
 def add_fuzz_lines(model: AtomicModel, n_lines: int, lam_min_A: float, lam_max_A: float,

@@ -18,10 +18,15 @@
 //                       the reference's list order.  In the mixed-precision
 //                       mode the per-line Sobolev sum runs in FP32 with Kahan
 //                       compensation; everything else stays FP64.
-//   zone_finish_kernel  one block per zone: emissivity CDF (sequential
-//                       prefix sum as cdf_array::set_value), opacity cap,
-//                       L_thermal, Planck/Rosseland means, Fleck factor, and
-//                       the packed tables the packet kernel reads.
+//   zone_finish_kernel  one block per zone: emissivity CDF (blocked prefix
+//                       sum in a fixed order, cdf_array::set_value), opacity
+//                       cap, L_thermal, Planck/Rosseland means, Fleck factor,
+//                       and the packed tables the packet kernel reads.
+//
+// The host runs the three kernels once per chunk of zones: per-zone inputs
+// and outputs are passed offset to the chunk, and every scratch array
+// (index * nzones + zone) is sized for one chunk, so a 128^3-zone grid with
+// thousands of bins builds its tables through a bounded working set.
 #include <cfloat>
 #include <cmath>
 #include <mutex>
@@ -409,31 +414,65 @@ __global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
       for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + st];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    double L = 0;
-    if (nn == 1) {
+  const double pm_tot = red[0][0], pn_tot = red[1][0], rm_tot = red[2][0], rn_tot = red[3][0];
+  __syncthreads();
+  // emissivity CDF: cdf_array::set_value prefix sum of emis*dnu (cdf_array.h:53-75)
+  // and L_thermal = 4 pi sum(emis*dnu).  Blocked scan in a fixed order: each
+  // thread sums a contiguous run of bins, thread 0 scans the 256 run totals,
+  // each run then adds its offset.  Non-negative terms, so every prefix is
+  // within a few ulp of the sequential sum; a NaN term propagates to the end
+  // of the CDF exactly as in the sequential sum.
+  double L = 0;
+  if (nn == 1) {
+    if (threadIdx.x == 0) {
       const double bb_int = SB * pow(A.T[z], 4) / PI;
       L += 4 * PI * ab[0] * bb_int;
       em[0] = 1;
-    } else {
-      // cdf_array::set_value prefix sum + normalize (cdf_array.h:53-75), in place
-      double run = 0;
-      for (int j = 0; j < nn; ++j) {
-        const double ednu = em[j] * loc_delta(A.nu, j);
-        run = (j == 0) ? ednu : run + ednu;
-        em[j] = run;
-        L += 4 * PI * ednu;
-      }
     }
+  } else {
+    const int per = (nn + blockDim.x - 1) / blockDim.x;
+    const int j0 = min(nn, (int)threadIdx.x * per), j1 = min(nn, j0 + per);
+    double run = 0, Lp = 0;
+    for (int j = j0; j < j1; ++j) {
+      const double ednu = em[j] * loc_delta(A.nu, j);
+      run = (j == j0) ? ednu : run + ednu;
+      em[j] = run;
+      Lp += 4 * PI * ednu;
+    }
+    red[0][threadIdx.x] = run;
+    red[1][threadIdx.x] = Lp;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double acc = 0, Lacc = 0;
+      for (int t = 0; t < (int)blockDim.x; ++t) {
+        const double v = red[0][t];
+        red[0][t] = acc;
+        acc = (t == 0) ? v : acc + v;
+        Lacc += red[1][t];
+      }
+      red[2][0] = Lacc;
+    }
+    __syncthreads();
+    const double off = red[0][threadIdx.x];
+    if (threadIdx.x > 0)
+      for (int j = j0; j < j1; ++j) em[j] = off + em[j];
+    L = red[2][0];
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nn; j += blockDim.x) if (isnan(em[j])) em[j] = 0;
+  __syncthreads();
+  const bool all_zero = (em[nn - 1] == 0);
+  __syncthreads();
+  if (all_zero) for (int j = threadIdx.x; j < nn; j += blockDim.x) em[j] = 1.0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
     A.L_th[z] = L;
-    for (int j = 0; j < nn; ++j) if (isnan(em[j])) em[j] = 0;
-    if (em[nn - 1] == 0) for (int j = 0; j < nn; ++j) em[j] = 1.0;
     if (nn == 1) {
       A.planck[z] = ab[0];
       A.ross[z] = ab[0] + sc[0];
     } else {
-      A.planck[z] = red[0][0] / red[1][0];
-      A.ross[z] = red[3][0] / red[2][0];
+      A.planck[z] = pm_tot / pn_tot;
+      A.ross[z] = rn_tot / rm_tot;
     }
     if (A.radiative_eq) A.eps_imc[z] = 1.;
     else {

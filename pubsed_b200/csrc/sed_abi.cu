@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -119,6 +120,8 @@ struct sed_ctx {
   bool have_opacity = false;
   DevBuf<unsigned char> d_opac, d_cdf, d_cdf_coarse;
   int n_coarse = 0;
+  int chunk_zones = 0;  // zones per opacity-build pass (bounds the FP64/LTE scratch)
+  int opacity_launches = 0;
   DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
       d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
   DevBuf<int32_t> d_solve_err;
@@ -165,6 +168,16 @@ cudaError_t upload(sed_ctx* c, DevBuf<T>& b, const T* src, size_t n)
   return cudaMemsetAsync(b.p, 0, (n ? n : 1) * sizeof(T), c->stream);
 }
 
+// n elements from src, or n zeros when the caller passed no array
+template <typename T>
+cudaError_t upload_or_zero(sed_ctx* c, DevBuf<T>& b, const T* src, size_t n)
+{
+  cudaError_t e = b.resize(n ? n : 1);
+  if (e != cudaSuccess) return e;
+  if (src) return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+  return cudaMemsetAsync(b.p, 0, (n ? n : 1) * sizeof(T), c->stream);
+}
+
 DevLoc dev_loc(const HostLoc& h, const DevBuf<double>& d)
 {
   DevLoc g;
@@ -196,22 +209,44 @@ int alloc_tallies(sed_ctx* c)
   CK(c->d_cdf_coarse.resize(nz * (size_t)c->n_coarse * esz));
   CK(c->d_eps_imc.resize(nz)); CK(c->d_planck.resize(nz)); CK(c->d_ross.resize(nz)); CK(c->d_L.resize(nz));
   CK(c->d_n_elec.resize(nz)); CK(c->d_temp_c.resize(nz)); CK(c->d_solve_err.resize(nz));
-  CK(c->d_abs64.resize(nz * nn)); CK(c->d_scat64.resize(nz * nn)); CK(c->d_emis64.resize(nz * nn));
   CK(cudaMemsetAsync(c->d_n_elec.p, 0, nz * sizeof(double), c->stream));
   return SED_OK;
 }
 
+// Scratch of the opacity build, sized for one pass over `chunk_zones` zones:
+// FP64 abs/scat/emissivity rows and the LTE state (mass fractions, number
+// densities, partition functions, ion fractions, level populations and
+// Boltzmann factors).  Passes of at most OPACITY_SCRATCH_BYTES keep this
+// bounded whatever the grid size, so the resident memory of a step is the
+// packed transport tables plus the tallies.  The environment variable
+// SEDONA_GPU_OPACITY_SCRATCH_BYTES lowers or raises the bound.
+constexpr size_t OPACITY_SCRATCH_BYTES = size_t(8) << 30;
+
+size_t opacity_scratch_bytes()
+{
+  const char* e = std::getenv("SEDONA_GPU_OPACITY_SCRATCH_BYTES");
+  if (e && *e) {
+    const unsigned long long v = std::strtoull(e, nullptr, 10);
+    if (v > 0) return (size_t)v;
+  }
+  return OPACITY_SCRATCH_BYTES;
+}
+
 int alloc_lte(sed_ctx* c)
 {
-  const size_t nz = (size_t)c->nz;
+  const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
   const size_t na = (size_t)std::max(c->nelem, 1);
-  CK(c->d_n_dens.resize(nz * na));
-  CK(c->d_mass_frac.resize(nz * na));
   const size_t ni = (size_t)std::max(c->n_ions_total, 1), nl = (size_t)std::max(c->n_lev_total, 1);
-  CK(c->d_ion_part.resize(nz * ni));
-  CK(c->d_ion_frac.resize(nz * ni));
-  CK(c->d_lev_n.resize(nz * nl));
-  CK(c->d_boltz.resize(nz * nl));
+  const size_t per_zone = (3 * nn + 2 * na + 2 * ni + 2 * nl) * sizeof(double);
+  const size_t cz = std::max<size_t>(1, std::min(nz, opacity_scratch_bytes() / per_zone));
+  c->chunk_zones = (int)cz;
+  CK(c->d_abs64.resize(cz * nn)); CK(c->d_scat64.resize(cz * nn)); CK(c->d_emis64.resize(cz * nn));
+  CK(c->d_n_dens.resize(cz * na));
+  CK(c->d_mass_frac.resize(cz * na));
+  CK(c->d_ion_part.resize(cz * ni));
+  CK(c->d_ion_frac.resize(cz * ni));
+  CK(c->d_lev_n.resize(cz * nl));
+  CK(c->d_boltz.resize(cz * nl));
   return SED_OK;
 }
 
@@ -302,7 +337,7 @@ int sed_set_grid(sed_ctx* c, const sed_grid* g)
     sed_locate_grid rg{g->n_zones, SED_LOC_FLEX, g->r_min, 0.0, g->r_out};
     c->r_out = host_loc(rg);
     CK(upload(c, c->d_r_out, g->r_out, nz));
-    CK(upload(c, c->d_v_r, g->v_r, g->v_r ? nz : 0));
+    CK(upload_or_zero(c, c->d_v_r, g->v_r, nz));
   } else if (g->type == SED_GRID_3D_CART) {
     if ((int64_t)g->nx * g->ny * g->nz != g->n_zones) return set_err(c, SED_ERR_ARG, "sed_set_grid: nx*ny*nz != n_zones");
     if (!valid_grid(g->x_axis) || !valid_grid(g->y_axis) || !valid_grid(g->z_axis) || g->x_axis.n != g->nx ||
@@ -320,8 +355,8 @@ int sed_set_grid(sed_ctx* c, const sed_grid* g)
   CK(upload(c, c->d_vol, g->vol, nz));
   CK(upload(c, c->d_rho, g->rho, nz));
   CK(upload(c, c->d_T, g->T_gas, nz));
-  CK(upload(c, c->d_egas, g->e_gas, g->e_gas ? nz : 0));
-  CK(upload(c, c->d_grey, g->total_grey_opacity, g->total_grey_opacity ? nz : 0));
+  CK(upload_or_zero(c, c->d_egas, g->e_gas, nz));
+  CK(upload_or_zero(c, c->d_grey, g->total_grey_opacity, nz));
   CK(upload(c, c->d_X, g->X, nz * (size_t)g->n_elems));
   CK(upload(c, c->d_eZ, g->elem_Z, (size_t)g->n_elems));
   CK(upload(c, c->d_eA, g->elem_A, (size_t)g->n_elems));
@@ -482,12 +517,24 @@ int sed_set_opacity(sed_ctx* c, double dt)
   A.opac_out = c->d_opac.p; A.cdf_out = c->d_cdf.p;
   A.cdf_coarse_out = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
   A.eps_imc = c->d_eps_imc.p; A.planck = c->d_planck.p; A.ross = c->d_ross.p; A.L_th = c->d_L.p;
-  if (!c->have_atoms && (A.use_es || A.use_ff || A.use_bf || A.use_line || A.use_fuzz)) {
-    // zones without grey opacity would need atomic data; grey zones are fine
-  }
+  // passes over chunks of zones: per-zone inputs and outputs are offset to
+  // the chunk, the scratch is reused with the chunk's zone count as stride
+  const size_t nn = (size_t)c->nu.n(), esz = c->tp.precision ? sizeof(float) : sizeof(double);
   CK(cudaEventRecord(c->ev[0], c->stream));
-  launch_opacity(A, c->num_sms, c->stream);
-  CK(cudaGetLastError());
+  c->opacity_launches = 0;
+  for (int z0 = 0; z0 < c->nz; z0 += c->chunk_zones) {
+    const size_t o = (size_t)z0;
+    OpacityArgs B = A;
+    B.nzones = std::min(c->chunk_zones, c->nz - z0);
+    B.rho += o; B.T += o; B.e_gas += o; B.grey += o; B.X += o * (size_t)c->nelem;
+    B.n_elec += o; B.temp_c += o; B.solve_err += o;
+    B.eps_imc += o; B.planck += o; B.ross += o; B.L_th += o;
+    B.opac_out = static_cast<unsigned char*>(A.opac_out) + o * nn * 2 * esz;
+    B.cdf_out = static_cast<unsigned char*>(A.cdf_out) + o * nn * esz;
+    B.cdf_coarse_out = static_cast<unsigned char*>(A.cdf_coarse_out) + o * (size_t)c->n_coarse * esz;
+    c->opacity_launches += launch_opacity(B, c->num_sms, c->stream);
+    CK(cudaGetLastError());
+  }
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_opacity = true;
@@ -522,9 +569,6 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
     CK(cudaMemcpyAsync(c->d_cdf_coarse.p, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
-  CK(cudaMemcpyAsync(c->d_abs64.p, abs, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  if (scat) CK(cudaMemcpyAsync(c->d_scat64.p, scat, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->d_emis64.p, emis_cdf, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_eps_imc.p, eps_imc, (size_t)c->nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_opacity = true;
@@ -641,7 +685,7 @@ int sed_step(sed_ctx* c, double dt, sed_step_stats* stats)
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
   rc = transport_impl(c, dt, stats, ms);
-  if (stats && rc == SED_OK) stats->kernel_launches += 3;
+  if (stats && rc == SED_OK) stats->kernel_launches += c->opacity_launches;
   return rc;
 }
 
@@ -674,9 +718,31 @@ int sed_get_opacity(sed_ctx* c, double* abs, double* scat, double* cdf, double* 
   if (!c) return SED_ERR_ARG;
   if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "no opacity tables");
   const size_t nz = (size_t)c->nz, n = nz * c->nu.n();
-  if (abs) CK(cudaMemcpyAsync(abs, c->d_abs64.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (scat) CK(cudaMemcpyAsync(scat, c->d_scat64.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  if (cdf) CK(cudaMemcpyAsync(cdf, c->d_emis64.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  // the tables the packet kernel reads: {abs, scat} pairs and the CDF, in
+  // FP64 or FP32 by the context's precision, returned widened to double
+  if (abs || scat) {
+    if (c->tp.precision) {
+      std::vector<float> o(2 * n);
+      CK(cudaMemcpyAsync(o.data(), c->d_opac.p, 2 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      for (size_t i = 0; i < n; ++i) { if (abs) abs[i] = o[2 * i]; if (scat) scat[i] = o[2 * i + 1]; }
+    } else {
+      std::vector<double> o(2 * n);
+      CK(cudaMemcpyAsync(o.data(), c->d_opac.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      for (size_t i = 0; i < n; ++i) { if (abs) abs[i] = o[2 * i]; if (scat) scat[i] = o[2 * i + 1]; }
+    }
+  }
+  if (cdf) {
+    if (c->tp.precision) {
+      std::vector<float> o(n);
+      CK(cudaMemcpyAsync(o.data(), c->d_cdf.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      for (size_t i = 0; i < n; ++i) cdf[i] = o[i];
+    } else {
+      CK(cudaMemcpyAsync(cdf, c->d_cdf.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+  }
   struct { double* h; double* d; } z[5] = {{n_elec, c->d_n_elec.p}, {eps_imc, c->d_eps_imc.p}, {planck, c->d_planck.p},
                                            {ross, c->d_ross.p}, {L_th, c->d_L.p}};
   for (auto& q : z) if (q.h) CK(cudaMemcpyAsync(q.h, q.d, nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -66,12 +66,13 @@ class Engine:
                     "sed_get_spectrum")
         return flux, click
 
-    def tallies(self) -> dict:
+    def tallies(self, J: bool = True) -> dict:
+        """Zone tallies; J=False skips the [n_zones x n_bins] J_nu array."""
         nj = self.nn if self.tp.store_Jnu else 1
-        out = {"J_nu": np.zeros(self.nz * nj)}
+        out = {"J_nu": np.zeros(self.nz * nj)} if J else {}
         out.update({k: np.zeros(self.nz) for k in ("e_abs", "e_rad", "fx", "fy", "fz", "fr")})
         P = lambda a: a.ctypes.data_as(abi._dp)
-        self._check(self.L.sed_get_zone_tallies(self.ctx, P(out["J_nu"]), P(out["e_abs"]), P(out["e_rad"]),
+        self._check(self.L.sed_get_zone_tallies(self.ctx, P(out["J_nu"]) if J else None, P(out["e_abs"]), P(out["e_rad"]),
                                                 P(out["fx"]), P(out["fy"]), P(out["fz"]), P(out["fr"])),
                     "sed_get_zone_tallies")
         return out

@@ -282,3 +282,99 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
     return Workload("type_ia_1d", params, z, atoms,
                     notes={"v_max": v_max, "t_days": 20.0, "rho0": rho0, "log_del": d,
                            "n_lines": n_lines, "n_levels_per_ion": n_levels_per_ion})
+
+
+# ---------------------------------------------------------------- 3D models
+def gaussian_random_field(n: int, corr_cells: float, rng: np.random.Generator) -> np.ndarray:
+    """Unit-variance Gaussian random field on an n^3 periodic lattice: white
+    noise filtered in Fourier space by exp(-k^2 l^2 / 2) (a Gaussian
+    two-point correlation of length l = corr_cells), rescaled to zero mean
+    and unit variance.  Indexed [i, j, k] = [x, y, z]."""
+    w = rng.standard_normal((n, n, n))
+    k = 2 * np.pi * np.fft.fftfreq(n)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    g = np.fft.ifftn(np.fft.fftn(w) * np.exp(-0.5 * k2 * corr_cells ** 2)).real
+    g -= g.mean()
+    return g / g.std()
+
+
+def cart_axis(half_width: float, n: int) -> LocGrid:
+    """Explicit cell walls -W + (i+1) 2W/n with minimum -W, as a model file's
+    x_out/y_out/z_out + rmin give them (grid_3D_cart.cpp:88-131: a `flex`
+    locate_array)."""
+    from .abi import LOC_FLEX
+    d = 2.0 * half_width / n
+    right = np.array([-half_width + (i + 1) * d for i in range(n - 1)] + [half_width], dtype=np.float64)
+    return LocGrid(right, -half_width, 0.0, LOC_FLEX)
+
+
+def cart3d(n_packets: int = 100_000_000, n_cells: int = 128, n_lines: int = 100_000, n_bins: int = 2048,
+           n_mu: int = 16, spectrum_bins: int = 1024, sigma: float = 0.5, corr_cells: float = 8.0,
+           mass_msun: float = 1.4, v_max: float = 2e9, v_e: float = 2.7e8, t_days: float = 30.0,
+           n_levels_per_ion: int = 30, epsilon: float = 1.0, v_core: float = 3e8, line_A_min: float = 1e-2,
+           line_A_max: float = 1e2, seed: int = 0, data_seed: int = 0) -> Workload:
+    """3D configuration: homologous ejecta on an n_cells^3 Cartesian grid
+    spanning +-v_max t on each axis.  rho = rho0 exp(-|v|/v_e) times a
+    lognormal clumping field exp(sigma G - sigma^2/2), G a unit-variance
+    Gaussian random field with correlation length corr_cells cells (seeded);
+    rho0 sets the mass on the grid to mass_msun.  Composition layered in |v|
+    as in the 1D Type Ia-like model; T falls linearly in |v| from 1.2e4 K at
+    the centre to 5e3 K at v_max (5e3 K beyond).  Opacity: electron
+    scattering (the grey scattering term) plus the Sobolev line-expansion
+    opacity of n_lines synthetic level-to-level lines (LTE populations),
+    opacity_epsilon = epsilon, radiative equilibrium.  n_bins log frequency
+    bins over 1e14-3e15 Hz; spectra in spectrum_bins log bins and n_mu
+    viewing-angle bins (mu = D_z).  Source: a 1.2e4 K blackbody lightbulb of
+    radius v_core t, L = 1e43 erg/s.
+
+    Choices the configuration leaves open, fixed here: the ejecta
+    parameters above; level energies below min(0.8 chi, 12 eV) so that
+    transitions fall inside the frequency grid; each line's (element, stage)
+    uniform over the real stages, its level pair uniform with the transition
+    frequency inside the grid, A log-uniform in 1e-2..1e2 s^-1 (weak lines:
+    with t = 30 d the median optical depth from the centre is ~5, so a packet
+    takes a few hundred segments rather than the ~1e4 of saturated lines)."""
+    from .atomic import add_level_lines
+    rng = np.random.default_rng(data_seed)
+    t = t_days * 86400.0
+    W = v_max * t
+    ax = cart_axis(W, n_cells)
+    n = n_cells
+    left = ax.left()
+    dx = np.array([ax.right[i] - left[i] for i in range(n)])   # locate_array::delta
+    c = 0.5 * (left + ax.right)
+    x, y, zz = np.meshgrid(c, c, c, indexing="ij")
+    vr = np.sqrt(x * x + y * y + zz * zz).reshape(-1) / t
+    vol = (dx[:, None, None] * dx[None, :, None] * dx[None, None, :]).reshape(-1)
+    G = gaussian_random_field(n, corr_cells, rng).reshape(-1)
+    shape = np.exp(-vr / v_e) * np.exp(sigma * G - 0.5 * sigma * sigma)
+    rho = mass_msun * M_SUN / float(np.sum(shape * vol)) * shape
+    T = 1.2e4 + (5e3 - 1.2e4) * np.minimum(vr / v_max, 1.0)
+    Z = [e[0] for e in IA_ELEMENTS]
+    A = [e[1] for e in IA_ELEMENTS]
+    X = np.zeros((rho.size, len(Z)))
+    for vu, frac in reversed(IA_LAYERS):
+        X[vr < vu] = frac
+    zones = ZoneModel(type=abi.GRID_3D_CART, t_now=float(t), rho=rho, T=T, X=X,
+                      elem_Z=np.asarray(Z, np.int32), elem_A=np.asarray(A, np.int32), vol=vol,
+                      axes=[ax, ax, ax], shape=(n, n, n))
+    atoms = synthetic_atoms(Z, n_levels_per_ion, 0, rng, E_max_eV=12.0)
+    add_level_lines(atoms, n_lines, 1e14, 3e15, rng, line_A_min, line_A_max)
+    d = log_delta_for_bins(1e14, 3e15, n_bins)
+    ds = log_delta_for_bins(1e14, 3e15, spectrum_bins)
+    params = {
+        "grid_type": "grid_3D_cart", "hydro_module": "homologous",
+        "transport_nu_grid": [1e14, 3e15, d, 1], "spectrum_nu_grid": [1e14, 3e15, ds, 1],
+        "spectrum_n_mu": int(n_mu),
+        "transport_steady_iterate": 1, "transport_radiative_equilibrium": 1,
+        "opacity_grey_opacity": 0, "opacity_epsilon": epsilon,
+        "opacity_electron_scattering": 1, "opacity_line_expansion": 1,
+        "dont_decay_composition": 1,
+        "core_n_emit": int(n_packets), "core_radius": float(v_core * t), "core_temperature": 1.2e4,
+        "core_luminosity": 1e43,
+        "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
+        "particles_max_total": max(int(1e7), int(n_packets)),
+    }
+    return Workload("cart3d", params, zones, atoms,
+                    notes={"v_max": v_max, "t_days": t_days, "n_cells": n, "n_lines": n_lines,
+                           "sigma": sigma, "corr_cells": corr_cells, "mass_msun": mass_msun, "v_e": v_e})

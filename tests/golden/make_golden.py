@@ -34,11 +34,15 @@ CASES = {
     "replay_grey_radeq": ("lightbulb_grey", dict(n_packets=600, n_zones=32, n_bins=128, radiative_eq=1, seed=5)),
     "replay_ia_lte": ("type_ia", dict(n_packets=300, n_zones=16, n_lines=5000, n_bins=256, n_levels_per_ion=6,
                                       bound_free=1, free_free=1, seed=7)),
+    "replay_cart3d": ("cart3d", dict(n_packets=300, n_cells=6, n_lines=1500, n_bins=128, spectrum_bins=64, n_mu=4,
+                                     seed=13)),
 }
 
 FREE_CASES = {
     "free_grey_radeq": ("lightbulb_grey", dict(n_packets=200000, n_zones=128, n_bins=256, radiative_eq=1, seed=101)),
     "free_ia": ("type_ia", dict(n_packets=60000, n_zones=64, n_lines=50000, n_bins=1024, seed=103)),
+    "free_cart3d": ("cart3d", dict(n_packets=100000, n_cells=16, n_lines=10000, n_bins=512, spectrum_bins=128,
+                                   n_mu=16, seed=109)),
 }
 
 KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "J_nu", "e_abs", "e_rad", "fx_rad", "fy_rad", "fz_rad",

@@ -46,6 +46,7 @@ def _gpu_spectrum(sed_lib, w, precision):
 @pytest.mark.parametrize("case,n_packets,seed,merge", [
     ("free_grey_radeq", 1_000_000, 9001, 2),
     ("free_ia", 600_000, 9002, 8),
+    ("free_cart3d", 400_000, 9003, 4),
 ])
 def test_free_running_spectrum_matches_reference(sed_lib, case, n_packets, seed, merge):
     ref = np.load(os.path.join(GOLDEN, case + ".npz"))

@@ -69,7 +69,10 @@ def test_grey_opacity_tables_match(sed_lib):
     o.set_opacity(1.0)
     g.set_opacity(1.0)
     Oo, Og = o.opacity(), g.opacity()
-    for k in ("abs", "scat", "emis_cdf", "eps_imc", "L_thermal"):
+    for k in ("abs", "scat", "eps_imc"):
         assert _rel(Og[k], Oo[k]) <= 1e-15, k
-    for k in ("planck_mean", "rosseland_mean"):
+    # the CDF prefix sum, L_thermal and the means are sums of the same
+    # non-negative terms in a blocked / tree order: within n * 2^-53 of the
+    # sequential sum (1024 bins)
+    for k in ("emis_cdf", "L_thermal", "planck_mean", "rosseland_mean"):
         assert _rel(Og[k], Oo[k]) <= 1e-13, k

@@ -17,7 +17,7 @@ from pubsed_b200 import abi, grids, workloads
 import oracle_lib
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte"]
+CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte", "replay_cart3d"]
 
 
 def _load(name):
