@@ -141,6 +141,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d"])
+    ap.add_argument("--cells", type=int, default=128, help="cells per axis of the cart3d workload")
     ap.add_argument("--packets", type=int, default=None)
     ap.add_argument("--ref-packets", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -153,10 +154,10 @@ def main():
     sample_fn = None
     if args.workload == "cart3d":
         def wl(n):
-            return workloads.cart3d(n_packets=n)
+            return workloads.cart3d(n_packets=n, n_cells=args.cells)
 
         def sample_fn(n):
-            return workloads.cart3d(n_packets=n, n_cells=32)
+            return workloads.cart3d(n_packets=n, n_cells=min(32, args.cells))
         default_packets, default_ref = 100_000_000, 4000
     else:
         def wl(n):

@@ -9,27 +9,32 @@
 //                       Boltzmann factors depend on T only and are computed
 //                       once per zone instead of once per Brent iteration
 //                       (same values, same rounding).
-//   bin_opacity_kernel  one thread per (zone, frequency bin): electron
-//                       scattering, free-free, bound-free, Sobolev line and
-//                       fuzz-line expansion opacity summed in the reference
-//                       order (GasState::computeOpacity, GasState_opacities.cpp:11-136).
-//                       Line lists are stored sorted by (atom, bin) with a
-//                       stable sort, so the lines of one bin are summed in
-//                       the reference's list order.  In the mixed-precision
-//                       mode the per-line Sobolev sum runs in FP32 with Kahan
-//                       compensation; everything else stays FP64.
-//   zone_finish_kernel  one block per zone: emissivity CDF (blocked prefix
-//                       sum in a fixed order, cdf_array::set_value), opacity
-//                       cap, L_thermal, Planck/Rosseland means, Fleck factor,
-//                       and the packed tables the packet kernel reads.
+//   zone_opacity_kernel one CTA per zone: electron scattering, free-free,
+//                       bound-free, Sobolev line and fuzz-line expansion
+//                       opacity per frequency bin in the reference's order
+//                       (GasState::computeOpacity, GasState_opacities.cpp:11-136),
+//                       then the opacity cap, Planck/Rosseland means,
+//                       emissivity CDF (blocked prefix sum in a fixed order,
+//                       cdf_array::set_value), L_thermal, Fleck factor and
+//                       the packed tables the packet kernel reads.  The
+//                       zone's level populations are staged in shared memory
+//                       with their reciprocals, so a line costs two
+//                       shared-memory reads, one 16 B and one 16 B (8 B in
+//                       FP32) global load and no division.  Line lists are
+//                       sorted by (bin, atom) with a stable sort, so each bin
+//                       is one contiguous run in the reference's list order.
+//                       In the mixed-precision form the per-line Sobolev sums
+//                       run in FP32 with Kahan compensation; everything else
+//                       stays FP64.
 //
-// The host runs the three kernels once per chunk of zones: per-zone inputs
-// and outputs are passed offset to the chunk, and every scratch array
+// The host runs the kernels once per chunk of zones: per-zone inputs and
+// outputs are passed offset to the chunk, and every scratch array
 // (index * nzones + zone) is sized for one chunk, so a 128^3-zone grid with
 // thousands of bins builds its tables through a bounded working set.
 #include <cfloat>
 #include <cmath>
 #include <mutex>
+#include <type_traits>
 #include "../../include/sedona_gpu.h"
 #include "sed_internal.h"
 
@@ -178,13 +183,7 @@ __global__ void zone_state_kernel(const OpacityArgs A, double* boltz_e)
   A.solve_err[z] = err;
 }
 
-// ------------------------------------------------------------ per bin
-__device__ __forceinline__ double bb_nu(double nu, double temp)
-{
-  const double ezeta = exp(1.0 * H_PLANCK * nu / K_BOLTZ / temp);
-  return 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (ezeta - 1);
-}
-
+// ------------------------------------------------------------ per zone
 // xy_array::value_at_with_zero_edges (src/utils/xy_array.cpp:42-104)
 __device__ double photo_cs(const OpacityArgs& A, int lev, double zv)
 {
@@ -210,43 +209,200 @@ __device__ double photo_cs(const OpacityArgs& A, int lev, double zv)
   return y[ind < n ? ind : n - 1] + slope * (zv - x[i1]);
 }
 
-template <bool MIXED>
-__global__ void bin_opacity_kernel(const OpacityArgs A)
+// 1 - exp(-tau), the Sobolev escape factor of one line, as the reference
+// writes it: for tau below ~1e-16 it is exactly 0 and for small tau it
+// carries the cancellation of 1 - exp(-tau), which the FP64 tables reproduce.
+__device__ __forceinline__ double sobolev_term(double tau) { return 1 - exp(-tau); }
+
+// FP32 form: below tau = 2^-7 the Taylor series to tau^5 (truncation below
+// tau^5/720, under 5e-14 relative), above it -expm1f(-tau); both free of the
+// cancellation that 1 - expf(-tau) would have in single precision.
+__device__ __forceinline__ float sobolev_term32(float tau)
 {
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int nn = A.n_nu, nz = A.nzones;
-  if (t >= (int64_t)nz * nn) return;
-  const int z = (int)(t / nn), i = (int)(t % nn);
-  const double temp = A.temp_c[z];
-  const double nu = loc_center(A.nu, i);
+  if (tau < 0.0078125f) {
+    const float t = tau;
+    return t * (1.f - t * 0.5f * (1.f - t * (1.f / 3) * (1.f - t * 0.25f * (1.f - t * 0.2f))));
+  }
+  return -expm1f(-tau);
+}
+
+// Level populations of one zone in the chunk scratch (level-major).
+struct LevView {
+  const double* p;
+  int64_t stride;
+  __device__ __forceinline__ double n(int l) const { return p[l * stride]; }
+};
+
+// Per-bin Sobolev sums of one line list (level-to-level lines, or fuzz lines
+// when FUZZ) for a tile of ZT zones: S[z][bin] = sum of (1 - exp(-tau)) over
+// the bin's lines, Se[z][bin] the same weighted by the line's atom epsilon
+// when atoms differ in epsilon (AtomicSpecies_opacities.cpp:292-375,
+// GasState_opacities.cpp:424-494).  The tile's level populations (or ion
+// populations for fuzz lines) and reciprocals are staged in shared memory
+// level-major, ZT zones contiguous; each thread takes bins j = tid, tid + 256,
+// ... and walks the bin's lines (sorted by bin, atom), loading each line
+// record once and applying it to the ZT zones.  Sums accumulate in FP64 in
+// the bin's list order.  In the mixed form the per-line arithmetic is FP32.
+// Level populations come from the LTE solve, floored at 1e-30, so they are
+// normal FP32 numbers and the reference's n_l < DBL_MIN skip never applies
+// to them; a NaN term is skipped as in the reference.
+template <bool MIXED, bool FUZZ, int ZT>
+__global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, double* S, double* Se)
+{
+  using V = typename std::conditional<MIXED, float, double>::type;
+  extern __shared__ double lsm[];
+  const int nn = A.n_nu, nz = A.nzones, na = A.natoms, tid = threadIdx.x, bd = blockDim.x;
+  const int z0 = blockIdx.x * ZT;
+  const int nzt = min(ZT, nz - z0);
+  if (nzt <= 0) return;
+  // shared: ndv[na][ZT], epsv[na], invT[ZT], pop[np][ZT], ipop[np][ZT] (V)
+  const int np = FUZZ ? A.n_ions_total : A.n_lev_total;
+  V* ndv = reinterpret_cast<V*>(lsm);
+  V* epsv = ndv + na * ZT;
+  V* invT = epsv + na;
+  V* pop = invT + ZT;
+  V* ipop = pop + (size_t)np * ZT;
+  for (int i = tid; i < na * ZT; i += bd) {
+    const int a = i / ZT, zi = i % ZT;
+    ndv[i] = (zi < nzt) ? (V)A.n_dens[(size_t)a * nz + z0 + zi] : (V)0;
+  }
+  for (int a = tid; a < na; a += bd) epsv[a] = A.zero_eps_atom[a] ? (V)0 : (V)A.epsilon;
+  for (int zi = tid; zi < ZT; zi += bd) invT[zi] = (zi < nzt) ? (V)(1.0 / A.temp_c[z0 + zi]) : (V)0;
+  for (int i = tid; i < np * ZT; i += bd) {
+    const int l = i / ZT, zi = i % ZT;
+    double v = 0;
+    if (zi < nzt) {
+      if constexpr (FUZZ) {
+        const int a = A.ion_atom[l];
+        v = A.n_dens[(size_t)a * nz + z0 + zi] * A.ion_frac[(size_t)l * nz + z0 + zi] /
+            A.ion_part[(size_t)l * nz + z0 + zi];
+      } else {
+        v = A.lev_n[(size_t)l * nz + z0 + zi];
+      }
+    }
+    pop[i] = (V)v;
+    if constexpr (!FUZZ) ipop[i] = (zi < nzt) ? (V)(1.0 / v) : (V)0;
+  }
+  __syncthreads();
+  const bool want_e = !A.uniform_eps;
+  const int32_t* seg = FUZZ ? A.fz_seg : A.ln_seg;
+  const double time = A.time;
+  for (int j = tid; j < nn; j += bd) {
+    double acc[ZT], acce[ZT];
+#pragma unroll
+    for (int q = 0; q < ZT; ++q) { acc[q] = 0; acce[q] = 0; }
+    const int k1 = seg[j + 1];
+    for (int k = seg[j]; k < k1; ++k) {
+      int atom;
+      V term[ZT];
+      if constexpr (!FUZZ) {
+        // tau = n_l n_atom sigma_tot f lambda t (1 - n_u g_l / (n_l g_u)), 0 past the laser limit
+        const int4 lv = __ldg(A.ln_lv + k);
+        atom = lv.w;
+        const V* pl = pop + (size_t)lv.x * ZT;
+        const V* il = ipop + (size_t)lv.x * ZT;
+        const V* pu = pop + (size_t)lv.y * ZT;
+        const V* nd = ndv + atom * ZT;
+        if constexpr (MIXED) {
+          const float2 c = __ldg(A.ln_c32 + k);
+          const float ct = c.x * (float)time;
+#pragma unroll
+          for (int q = 0; q < ZT; ++q) {
+            const float r = pu[q] * il[q] * c.y;
+            const float tau = (r > 1.f) ? 0.f : pl[q] * nd[q] * ct * (1.f - r);
+            const float t = sobolev_term32(tau);
+            term[q] = (t == t) ? t : 0.f;
+          }
+        } else {
+          const double2 c = __ldg(A.ln_c + k);
+#pragma unroll
+          for (int q = 0; q < ZT; ++q) {
+            const double nl = pl[q];
+            double t = 0;
+            if (!(nl < DBL_MIN)) {
+              const double r = pu[q] * il[q] * c.y;
+              const double tau = (r > 1) ? 0.0 : nl * nd[q] * c.x * time * (1 - r);
+              t = sobolev_term(tau);
+              if (isnan(t)) t = 0;
+            }
+            term[q] = t;
+          }
+        }
+      } else {
+        // n_l = n_ion exp(-E_l/kT) / Z_ion, tau = sigma_tot lambda n_l gf (1 - exp(-h nu/kT)) t
+        const int4 ia = __ldg(A.fz_ia + k);
+        atom = ia.z;
+        const V* pi = pop + (size_t)ia.x * ZT;
+        if constexpr (MIXED) {
+          const float4 c = __ldg(A.fz_c32 + k);
+          const float ct = c.x * (float)time;
+#pragma unroll
+          for (int q = 0; q < ZT; ++q) {
+            const float stim = -expm1f(-c.z * invT[q]);
+            const float tau = ct * pi[q] * expf(-c.y * invT[q]) * stim;
+            term[q] = sobolev_term32(tau);
+          }
+        } else {
+          const double2 c = __ldg(A.fz_c + k);
+          const double h = __ldg(A.fz_h + k);
+#pragma unroll
+          for (int q = 0; q < ZT; ++q) {
+            if (q < nzt) {
+              const double temp = A.temp_c[z0 + q];
+              const double nl = pi[q] * exp(-c.y / temp);
+              const double stim_cor = (1 - exp(-h / temp));
+              const double tau = c.x * nl * stim_cor * time;
+              term[q] = sobolev_term(tau);
+            } else {
+              term[q] = 0;
+            }
+          }
+        }
+      }
+      const V e = epsv[atom];
+#pragma unroll
+      for (int q = 0; q < ZT; ++q) {
+        acc[q] += (double)term[q];
+        if (want_e) acce[q] += (double)(term[q] * e);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < ZT; ++q) {
+      if (q < nzt) {
+        S[(size_t)(z0 + q) * nn + j] = acc[q];
+        if (want_e) Se[(size_t)(z0 + q) * nn + j] = acce[q];
+      }
+    }
+  }
+}
+
+// Opacity, scattering and emissivity of bin j of zone z (GasState::
+// computeOpacity, GasState_opacities.cpp:11-136, with its terms in the
+// reference's order: electron scattering, free-free, bound-free, Sobolev
+// lines, fuzz lines).  The line terms arrive as the bin's Sobolev sums
+// (ls, lse, fs, fse; the epsilon-weighted sums only when atoms differ in
+// epsilon); nu and ez = exp(h nu/kT) are shared with the caller, which reuses
+// ez for the mean opacities.
+__device__ void bin_opacity(const OpacityArgs& A, int zc, int j, double nu, double ez, double temp, double grey,
+                            double ne, double es, double ff_fac, const double* nd, const LevView& L, double ls,
+                            double lse, double fs, double fse, double& ab_o, double& sc_o, double& em_o)
+{
   double ab = 0, sc = 0, em = 0;
-  const double grey = A.grey[z];
   if (grey != 0) {  // GasState_opacities.cpp:29-41
-    const double gopac = A.rho[z] * grey;
+    const double gopac = A.rho[zc] * grey;
     ab = gopac * A.epsilon;
     sc = gopac * (1 - A.epsilon);
-    em += bb_nu(nu, temp) * ab;
+    const double bb = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (ez - 1);
+    em += bb * ab;
   } else if (A.natoms > 0) {
-    const double ne = A.n_elec[z];
-    const double dens = A.rho[z];
     if (A.use_es) {  // :49-58
-      const double es = THOMSON * ne;
       sc += es;
       ab += 1e-20 * A.epsilon * es;
     }
     if (A.use_ff) {  // GasState::free_free_opacity :152-183
-      double fac = 0;
-      for (int a = 0; a < A.natoms; ++a) {
-        const int i0 = A.ion_off[a], ni = A.ion_off[a + 1] - i0;
-        double zsq = 0;
-        for (int j = 0; j < ni; j++) zsq += A.ion_frac[(size_t)(i0 + j) * nz + z] * j * j;
-        const double n_ion = A.mass_frac[(size_t)a * nz + z] * dens / (A.eA[a] * MASS_P);
-        fac += n_ion * zsq;
-      }
-      fac *= 3.7e8 * pow(temp, -0.5) * ne;
       const double ezeta = exp(-1.0 * H_PLANCK * nu / K_BOLTZ / temp);
       const double bb = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (1.0 / ezeta - 1);
-      const double op = fac / nu / nu / nu * (1 - ezeta);
+      const double op = ff_fac / nu / nu / nu * (1 - ezeta);
       ab += op;
       em += op * bb;
     }
@@ -258,20 +414,19 @@ __global__ void bin_opacity_kernel(const OpacityArgs A)
       double so = 0, se = 0;
       for (int a = 0; a < A.natoms; ++a) {
         const int l0 = A.lev_off[a], nl = A.lev_off[a + 1] - l0;
-        const double nd = A.n_dens[(size_t)a * nz + z];
         double ao = 0, ae = 0;
-        for (int j = 0; j < nl; ++j) {
-          const int ic = A.lev_ic[l0 + j];
+        for (int q = 0; q < nl; ++q) {
+          const int ic = A.lev_ic[l0 + q];
           if (ic == -1) continue;
-          const double Eion = A.lev_Eion[l0 + j];
+          const double Eion = A.lev_Eion[l0 + q];
           if (E < Eion) continue;
-          const double nc = nd * A.lev_n[(size_t)(l0 + ic) * nz + z];
-          const double gl_o_gc = (1.0 * A.lev_g[l0 + j]) / (1.0 * A.lev_g[l0 + ic]);
+          const double nc = nd[a] * L.n(l0 + ic);
+          const double gl_o_gc = (1.0 * A.lev_g[l0 + q]) / (1.0 * A.lev_g[l0 + ic]);
           const double ncp = nc * gl_o_gc / 2. * lam_t * lam_t * lam_t;
           const double zeta_net = (Eion - E) / kt_ev;
           const double ezeta_net = exp(zeta_net);
-          const double sigma = photo_cs(A, l0 + j, E);
-          double opac_fac = nd * A.lev_n[(size_t)(l0 + j) * nz + z] - ncp * ne * ezeta_net;
+          const double sigma = photo_cs(A, l0 + q, E);
+          double opac_fac = nd[a] * L.n(l0 + q) - ncp * ne * ezeta_net;
           if (opac_fac < 0) opac_fac = 0.;
           ao += sigma * opac_fac;
           ae += emis_fac * sigma * ncp * ezeta_net;
@@ -282,156 +437,148 @@ __global__ void bin_opacity_kernel(const OpacityArgs A)
       ab += so;
       em += se * ne;
     }
-    if (A.use_line) {  // GasState::line_expansion_opacity :424-454, AtomicSpecies_opacities.cpp:331-375
-      double opac = 0, aopac = 0;
-      for (int a = 0; a < A.natoms; ++a) {
-        const double this_eps = A.zero_eps_atom[a] ? 0.0 : A.epsilon;
-        const int l0 = A.lev_off[a];
-        const double nd = A.n_dens[(size_t)a * nz + z];
-        double s = 0;
-        const int k0 = A.line_seg[(size_t)a * nn + i], k1 = A.line_seg[(size_t)a * nn + i + 1];
-        for (int k = k0; k < k1; ++k) {
-          const int ll = A.line_l[k], lu = A.line_u[k];
-          const double nl = A.lev_n[(size_t)(l0 + ll) * nz + z];
-          const double nup = A.lev_n[(size_t)(l0 + lu) * nz + z];
-          const double gl = 1.0 * A.lev_g[l0 + ll], gu = 1.0 * A.lev_g[l0 + lu];
-          if (nl < DBL_MIN) continue;
-          const double lam = C_LIGHT / A.line_nu[k];
-          double tau = nl * nd * SIGMA_TOT * A.line_f[k] * A.time * lam;
-          tau = tau * (1 - nup * gl / (nl * gu));
-          if (nup * gl > nl * gu) tau = 0;
-          const double etau = exp(-tau);
-          if (!isnan(etau)) s += (1 - etau);
-        }
-        s = s * nu / loc_delta(A.nu, i) / C_LIGHT / A.time;
-        opac += s;
-        aopac += s * this_eps;
-      }
+    const double bb = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (ez - 1);
+    const double fac = nu / loc_delta(A.nu, j) / C_LIGHT / A.time;
+    if (A.use_line) {  // GasState::line_expansion_opacity :424-454
+      const double opac = ls * fac;
+      const double aopac = (A.uniform_eps ? ls * A.epsilon : lse) * fac;
       ab += aopac;
       sc += opac - aopac;
-      em += bb_nu(nu, temp) * aopac;
+      em += bb * aopac;
     }
-    if (A.use_fuzz) {  // GasState::fuzz_expansion_opacity :464-494, AtomicSpecies_opacities.cpp:292-324
-      double opac = 0, aopac = 0;
-      for (int a = 0; a < A.natoms; ++a) {
-        const double this_eps = A.zero_eps_atom[a] ? 0.0 : A.epsilon;
-        const int i0 = A.ion_off[a];
-        const double nd = A.n_dens[(size_t)a * nz + z];
-        const int k0 = A.fuzz_seg[(size_t)a * nn + i], k1 = A.fuzz_seg[(size_t)a * nn + i + 1];
-        double s;
-        if constexpr (MIXED) {
-          // FP32 Sobolev sum with Kahan compensation; per-line constants
-          // A32 = sigma_tot*lambda*gf, El32 = El/k_ev, hnu32 = h nu/k
-          const float invT = (float)(1.0 / temp);
-          const float tm = (float)A.time;
-          float sum = 0.f, comp = 0.f;
-          for (int k = k0; k < k1; ++k) {
-            const int ion = A.fz_ion[k];
-            const float pop = (float)(nd * A.ion_frac[(size_t)(i0 + ion) * nz + z] / A.ion_part[(size_t)(i0 + ion) * nz + z]);
-            const float stim = -expm1f(-__ldg(A.fz_hnu32 + k) * invT);
-            const float tau = __ldg(A.fz_A32 + k) * pop * expf(-__ldg(A.fz_El32 + k) * invT) * stim * tm;
-            const float term = -expm1f(-tau);
-            const float y = term - comp;
-            const float tt = sum + y;
-            comp = (tt - sum) - y;
-            sum = tt;
-          }
-          s = (double)sum;
-        } else {
-          s = 0;
-          for (int k = k0; k < k1; ++k) {
-            const double fnu = A.fz_nu[k], gf = A.fz_gf[k], El = A.fz_El[k];
-            const int ion = A.fz_ion[k];
-            const double nion = nd * A.ion_frac[(size_t)(i0 + ion) * nz + z];
-            const double nl = nion * exp(-1.0 * El / K_EV / temp) / A.ion_part[(size_t)(i0 + ion) * nz + z];
-            const double lam = C_LIGHT / fnu;
-            const double stim_cor = (1 - exp(-H_PLANCK * fnu / K_BOLTZ / temp));
-            const double tau = SIGMA_TOT * lam * nl * gf * stim_cor * A.time;
-            const double etau = exp(-tau);
-            s += (1 - etau);
-          }
-        }
-        s = s * nu / loc_delta(A.nu, i) / C_LIGHT / A.time;
-        opac += s;
-        aopac += s * this_eps;
-      }
+    if (A.use_fuzz) {  // GasState::fuzz_expansion_opacity :464-494
+      const double opac = fs * fac;
+      const double aopac = (A.uniform_eps ? fs * A.epsilon : fse) * fac;
       ab += aopac;
       sc += opac - aopac;
-      em += bb_nu(nu, temp) * aopac;
+      em += bb * aopac;
     }
   }
-  A.abs64[t] = ab;
-  A.scat64[t] = sc;
-  A.emis64[t] = em;
+  ab_o = ab;
+  sc_o = sc;
+  em_o = em;
 }
 
-// emissivity CDF, cap, L_thermal, means, eps_imc (transport_opacity.cpp:152-252)
-// The CDF prefix sum and L_thermal are sequential (cdf_array::set_value
-// order); the Planck and Rosseland means are block reductions in a fixed
-// order (strided partial sums, then a tree).
+// One CTA per zone of the chunk, after line_sum_kernel: each thread builds
+// bins j = tid, tid + 256, ... from the continuum terms and the bin's
+// Sobolev sums (GasState::computeOpacity), caps them and accumulates the
+// Planck/Rosseland partial sums (GasState_opacities.cpp:564-666); then the
+// CTA forms the emissivity CDF, L_thermal and eps_imc
+// (transport_opacity.cpp:152-252) and writes the packed tables the packet
+// kernel reads.  The FP64 rows (abs, scat, emissivity) live in shared memory
+// when they fit (A.smem_rows); otherwise abs and scat overwrite the line and
+// fuzz sums of the zone in the chunk scratch (each bin is read, then written,
+// by the same thread) and the emissivity row is scratch too.
 template <bool MIXED>
-__global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
+__global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
 {
+  extern __shared__ double dsm[];
   __shared__ double red[4][256];
+  __shared__ double zs[2];  // electron scattering, free-free factor
   const int z = blockIdx.x;
   if (z >= A.nzones) return;
-  const int nn = A.n_nu;
-  double* ab = A.abs64 + (size_t)z * nn;
-  double* sc = A.scat64 + (size_t)z * nn;
-  double* em = A.emis64 + (size_t)z * nn;
-  const double max_ext = A.max_opacity * A.rho[z];
+  const int nn = A.n_nu, nz = A.nzones, na = A.natoms, tid = threadIdx.x, bd = blockDim.x;
   const double temp = A.temp_c[z];
-  // cap (element-wise) and the mean-opacity partial sums
+  const double grey = A.grey[z];
+  const double ne = A.n_elec[z];
+  const bool want_e = !A.uniform_eps;
+
+  // shared layout: nd[na] rows[3 nn]
+  double* nd = dsm;
+  double* rows = nd + na;
+  const size_t zo = (size_t)z * nn;
+  const double* LS = A.abs64 + zo;
+  const double* FS = A.scat64 + zo;
+  const double* LSe = A.epsl64 + zo;
+  const double* FSe = A.epsf64 + zo;
+  double* R0 = A.smem_rows ? rows : A.abs64 + zo;
+  double* R1 = A.smem_rows ? rows + nn : A.scat64 + zo;
+  double* R2 = A.smem_rows ? rows + 2 * nn : A.emis64 + zo;
+
+  const bool micro = (grey == 0 && na > 0);
+  if (micro) {
+    for (int a = tid; a < na; a += bd) nd[a] = A.n_dens[(size_t)a * nz + z];
+    if (tid == 0) {
+      zs[0] = THOMSON * ne;
+      double ff = 0;
+      if (A.use_ff) {  // GasState::free_free_opacity :152-183 (zone factor)
+        const double dens = A.rho[z];
+        for (int a = 0; a < na; ++a) {
+          const int i0 = A.ion_off[a], ni = A.ion_off[a + 1] - i0;
+          double zsq = 0;
+          for (int q = 0; q < ni; q++) zsq += A.ion_frac[(size_t)(i0 + q) * nz + z] * q * q;
+          const double n_ion = A.mass_frac[(size_t)a * nz + z] * dens / (A.eA[a] * MASS_P);
+          ff += n_ion * zsq;
+        }
+        ff *= 3.7e8 * pow(temp, -0.5) * ne;
+      }
+      zs[1] = ff;
+    }
+  }
+  __syncthreads();
+  LevView L;
+  L.p = A.lev_n + z;
+  L.stride = nz;
+  const double es = micro ? zs[0] : 0.0, ff_fac = micro ? zs[1] : 0.0;
+  const bool lines = micro && A.use_line, fuzz = micro && A.use_fuzz;
+
+  // bins, cap (transport_opacity.cpp:189-200) and mean-opacity partial sums
+  const double max_ext = A.max_opacity * A.rho[z];
   double pm = 0, pn = 0, rm = 0, rn = 0;
-  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
-    double s = sc[j];
-    if (A.omit_scat) s = 0;
-    else if (s > max_ext) s = max_ext;
-    sc[j] = s;
-    double a = ab[j];
-    if (a > max_ext) a = max_ext;
-    ab[j] = a;
-    // GasState::get_planck_mean / get_rosseland_mean (GasState_opacities.cpp:564-666)
+  for (int j = tid; j < nn; j += bd) {
     const double nu = loc_center(A.nu, j);
     const double zeta = H_PLANCK * nu / K_BOLTZ / temp;
-    double Bnu = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (exp(zeta) - 1);
+    const double ez = exp(zeta);
+    double ab, sc, em;
+    bin_opacity(A, z, j, nu, ez, temp, grey, ne, es, ff_fac, nd, L, lines ? LS[j] : 0.0,
+                (lines && want_e) ? LSe[j] : 0.0, fuzz ? FS[j] : 0.0, (fuzz && want_e) ? FSe[j] : 0.0, ab, sc, em);
+    if (A.omit_scat) sc = 0;
+    else if (sc > max_ext) sc = max_ext;
+    if (ab > max_ext) ab = max_ext;
+    R0[j] = ab;
+    R1[j] = sc;
+    R2[j] = em;
+    double Bnu = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (ez - 1);
     if (isnan(Bnu)) Bnu = 0;
     const double d = loc_delta(A.nu, j);
     const double W = Bnu * d;
-    pm += W * a;
+    pm += W * ab;
     pn += W;
-    const double ezeta = exp(zeta);
-    double dBdT = pow(nu, 4) * ezeta / (ezeta - 1) / (ezeta - 1);
+    double dBdT = pow(nu, 4) * ez / (ez - 1) / (ez - 1);
     if (isnan(dBdT)) dBdT = 0;
     const double Wr = dBdT * d;
-    rm += Wr / (a + s);
+    rm += Wr / (ab + sc);
     rn += Wr;
   }
-  red[0][threadIdx.x] = pm; red[1][threadIdx.x] = pn; red[2][threadIdx.x] = rm; red[3][threadIdx.x] = rn;
+  double* ab_r = R0;
+  double* sc_r = R1;
+  red[0][tid] = pm; red[1][tid] = pn; red[2][tid] = rm; red[3][tid] = rn;
   __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < (unsigned)st)
-      for (int q = 0; q < 4; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+  for (int st = bd / 2; st > 0; st >>= 1) {
+    if (tid < st)
+      for (int q = 0; q < 4; ++q) red[q][tid] += red[q][tid + st];
     __syncthreads();
   }
   const double pm_tot = red[0][0], pn_tot = red[1][0], rm_tot = red[2][0], rn_tot = red[3][0];
   __syncthreads();
-  // emissivity CDF: cdf_array::set_value prefix sum of emis*dnu (cdf_array.h:53-75)
-  // and L_thermal = 4 pi sum(emis*dnu).  Blocked scan in a fixed order: each
-  // thread sums a contiguous run of bins, thread 0 scans the 256 run totals,
-  // each run then adds its offset.  Non-negative terms, so every prefix is
-  // within a few ulp of the sequential sum; a NaN term propagates to the end
-  // of the CDF exactly as in the sequential sum.
-  double L = 0;
+
+  // emissivity CDF: cdf_array::set_value prefix sum of emis*dnu (cdf_array.h:
+  // 53-75) and L_thermal = 4 pi sum(emis*dnu).  Blocked scan in a fixed
+  // order: each thread sums a contiguous run of bins, thread 0 scans the run
+  // totals, each run then adds its offset.  Non-negative terms, so every
+  // prefix is within a few ulp of the sequential sum; a NaN term propagates
+  // to the end of the CDF exactly as in the sequential sum.
+  double* em = R2;
+  double Lth = 0;
   if (nn == 1) {
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       const double bb_int = SB * pow(A.T[z], 4) / PI;
-      L += 4 * PI * ab[0] * bb_int;
+      Lth += 4 * PI * ab_r[0] * bb_int;
       em[0] = 1;
     }
   } else {
-    const int per = (nn + blockDim.x - 1) / blockDim.x;
-    const int j0 = min(nn, (int)threadIdx.x * per), j1 = min(nn, j0 + per);
+    const int per = (nn + bd - 1) / bd;
+    const int j0 = min(nn, tid * per), j1 = min(nn, j0 + per);
     double run = 0, Lp = 0;
     for (int j = j0; j < j1; ++j) {
       const double ednu = em[j] * loc_delta(A.nu, j);
@@ -439,12 +586,12 @@ __global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
       em[j] = run;
       Lp += 4 * PI * ednu;
     }
-    red[0][threadIdx.x] = run;
-    red[1][threadIdx.x] = Lp;
+    red[0][tid] = run;
+    red[1][tid] = Lp;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       double acc = 0, Lacc = 0;
-      for (int t = 0; t < (int)blockDim.x; ++t) {
+      for (int t = 0; t < bd; ++t) {
         const double v = red[0][t];
         red[0][t] = acc;
         acc = (t == 0) ? v : acc + v;
@@ -453,23 +600,23 @@ __global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
       red[2][0] = Lacc;
     }
     __syncthreads();
-    const double off = red[0][threadIdx.x];
-    if (threadIdx.x > 0)
+    const double off = red[0][tid];
+    if (tid > 0)
       for (int j = j0; j < j1; ++j) em[j] = off + em[j];
-    L = red[2][0];
+    Lth = red[2][0];
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < nn; j += blockDim.x) if (isnan(em[j])) em[j] = 0;
+  for (int j = tid; j < nn; j += bd) if (isnan(em[j])) em[j] = 0;
   __syncthreads();
   const bool all_zero = (em[nn - 1] == 0);
   __syncthreads();
-  if (all_zero) for (int j = threadIdx.x; j < nn; j += blockDim.x) em[j] = 1.0;
+  if (all_zero) for (int j = tid; j < nn; j += bd) em[j] = 1.0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    A.L_th[z] = L;
+  if (tid == 0) {
+    A.L_th[z] = Lth;
     if (nn == 1) {
-      A.planck[z] = ab[0];
-      A.ross[z] = ab[0] + sc[0];
+      A.planck[z] = ab_r[0];
+      A.ross[z] = ab_r[0] + sc_r[0];
     } else {
       A.planck[z] = pm_tot / pn_tot;
       A.ross[z] = rn_tot / rm_tot;
@@ -483,17 +630,16 @@ __global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
       A.eps_imc[z] = 1.0 / (1.0 + f_imc);
     }
   }
-  __syncthreads();
   const double N = em[nn - 1];
   // normalised CDF, packed tables and the coarse CDF index for the packet kernel
-  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+  for (int j = tid; j < nn; j += bd) {
     const size_t k = (size_t)z * nn + j;
     const double c = em[j] / N;
     if constexpr (MIXED) {
-      reinterpret_cast<float2*>(A.opac_out)[k] = make_float2((float)ab[j], (float)sc[j]);
+      reinterpret_cast<float2*>(A.opac_out)[k] = make_float2((float)ab_r[j], (float)sc_r[j]);
       reinterpret_cast<float*>(A.cdf_out)[k] = (float)c;
     } else {
-      reinterpret_cast<double2*>(A.opac_out)[k] = make_double2(ab[j], sc[j]);
+      reinterpret_cast<double2*>(A.opac_out)[k] = make_double2(ab_r[j], sc_r[j]);
       reinterpret_cast<double*>(A.cdf_out)[k] = c;
     }
     if ((j % CDF_STRIDE) == CDF_STRIDE - 1 || j == nn - 1) {
@@ -502,25 +648,74 @@ __global__ void __launch_bounds__(256) zone_finish_kernel(const OpacityArgs A)
       else reinterpret_cast<double*>(A.cdf_coarse_out)[kc] = c;
     }
   }
-  __syncthreads();
-  for (int j = threadIdx.x; j < nn; j += blockDim.x) em[j] = em[j] / N;
+}
+
+// zone tiles of the line-sum kernel: 8 zones per CTA in FP32, 4 in FP64
+constexpr int LINE_TILE_MIXED = 8;
+constexpr int LINE_TILE_FP64 = 4;
+
+template <bool MIXED, bool FUZZ>
+int launch_line_sums(const OpacityArgs& a, double* S, double* Se, cudaStream_t s)
+{
+  constexpr int ZT = MIXED ? LINE_TILE_MIXED : LINE_TILE_FP64;
+  const size_t vs = MIXED ? sizeof(float) : sizeof(double);
+  const size_t np = FUZZ ? (size_t)a.n_ions_total : (size_t)a.n_lev_total;
+  const size_t smem = vs * ((size_t)a.natoms * ZT + a.natoms + ZT + 2 * np * ZT);
+  auto k = line_sum_kernel<MIXED, FUZZ, ZT>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+  k<<<(a.nzones + ZT - 1) / ZT, 256, smem, s>>>(a, S, Se);
+  return 1;
 }
 
 }  // namespace
+
+size_t opacity_smem_bytes(const OpacityArgs& a)
+{
+  size_t d = (size_t)a.natoms;
+  if (a.smem_rows) d += 3 * (size_t)a.n_nu;
+  return d * sizeof(double);
+}
+
+size_t line_sum_smem_bytes(int precision, int natoms, int n_pop)
+{
+  const int ZT = precision ? LINE_TILE_MIXED : LINE_TILE_FP64;
+  const size_t vs = precision ? sizeof(float) : sizeof(double);
+  return vs * ((size_t)natoms * ZT + natoms + ZT + 2 * (size_t)n_pop * ZT);
+}
 
 int launch_opacity(const OpacityArgs& a, int num_sms, cudaStream_t s)
 {
   (void)num_sms;
   const int nz = a.nzones;
+  int n = 0;
   zone_state_kernel<<<(nz + 127) / 128, 128, 0, s>>>(a, a.boltz);
-  const int64_t nt = (int64_t)nz * a.n_nu;
-  const int threads = 256;
-  const unsigned blocks = (unsigned)((nt + threads - 1) / threads);
-  if (a.precision) bin_opacity_kernel<true><<<blocks, threads, 0, s>>>(a);
-  else bin_opacity_kernel<false><<<blocks, threads, 0, s>>>(a);
-  if (a.precision) zone_finish_kernel<true><<<nz, 256, 0, s>>>(a);
-  else zone_finish_kernel<false><<<nz, 256, 0, s>>>(a);
-  return 3;
+  ++n;
+  const bool micro = a.natoms > 0;
+  int r = 0;
+  if (micro && a.use_line)
+    r = a.precision ? launch_line_sums<true, false>(a, a.abs64, a.epsl64, s)
+                    : launch_line_sums<false, false>(a, a.abs64, a.epsl64, s);
+  if (r < 0) return -1;
+  n += r;
+  r = 0;
+  if (micro && a.use_fuzz)
+    r = a.precision ? launch_line_sums<true, true>(a, a.scat64, a.epsf64, s)
+                    : launch_line_sums<false, true>(a, a.scat64, a.epsf64, s);
+  if (r < 0) return -1;
+  n += r;
+  const size_t smem = opacity_smem_bytes(a);
+  if (a.precision) {
+    if (cudaFuncSetAttribute(zone_opacity_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return -1;
+    zone_opacity_kernel<true><<<nz, 256, smem, s>>>(a);
+  } else {
+    if (cudaFuncSetAttribute(zone_opacity_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return -1;
+    zone_opacity_kernel<false><<<nz, 256, smem, s>>>(a);
+  }
+  return n + 1;
 }
 
 }  // namespace sed

@@ -109,12 +109,15 @@ struct sed_ctx {
   std::vector<int32_t> zero_eps;
   DevBuf<int32_t> d_zero_eps_atom;
   bool have_atoms = false;
+  bool any_zero_eps = false;
   int natoms = 0, n_ions_total = 0, n_lev_total = 0, nfuzz = 0, nlines = 0;
-  DevBuf<int32_t> d_ion_off, d_lev_off, d_lev_ion, d_lev_g, d_lev_ic, d_photo_off, d_line_seg, d_line_l, d_line_u,
-      d_fuzz_seg, d_fz_ion;
-  DevBuf<double> d_ion_chi, d_lev_E, d_lev_Eion, d_photo_E, d_photo_s, d_line_nu, d_line_f, d_fz_nu, d_fz_gf, d_fz_El;
-  DevBuf<float> d_fz_A32, d_fz_El32, d_fz_hnu32;
-  std::vector<int32_t> fuzz_order;  // sorted position -> caller's index
+  DevBuf<int32_t> d_ion_off, d_lev_off, d_lev_ion, d_lev_g, d_lev_ic, d_photo_off, d_ion_atom, d_ln_seg, d_fz_seg;
+  DevBuf<double> d_ion_chi, d_lev_E, d_lev_Eion, d_photo_E, d_photo_s, d_fz_h;
+  DevBuf<int4> d_ln_lv;
+  DevBuf<double2> d_ln_c, d_fz_c;
+  DevBuf<float2> d_ln_c32;
+  DevBuf<int4> d_fz_ia;
+  DevBuf<float4> d_fz_c32;
 
   // tables
   bool have_opacity = false;
@@ -122,7 +125,7 @@ struct sed_ctx {
   int n_coarse = 0;
   int chunk_zones = 0;  // zones per opacity-build pass (bounds the FP64/LTE scratch)
   int opacity_launches = 0;
-  DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
+  DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_epsl64, d_epsf64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
       d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
   DevBuf<int32_t> d_solve_err;
 
@@ -232,15 +235,31 @@ size_t opacity_scratch_bytes()
   return OPACITY_SCRATCH_BYTES;
 }
 
+// Shared memory per CTA: the per-zone opacity kernel keeps its three FP64
+// rows (abs, scat, emissivity) there when they take at most SMEM_ZONE_BYTES,
+// else in the chunk scratch; the line-sum kernel stages the populations of a
+// tile of zones and must fit in SMEM_ZONE_BYTES.
+constexpr size_t SMEM_ZONE_BYTES = 200 * 1024;
+
+bool rows_in_smem(size_t na, size_t nn) { return (na + 3 * nn) * sizeof(double) <= SMEM_ZONE_BYTES; }
+
+// Chunk scratch: per zone the line and fuzz Sobolev sums (overwritten by the
+// abs and scat rows), the emissivity row when the rows are not in shared
+// memory, two epsilon-weighted sums when atoms differ in epsilon, and the LTE
+// state.
 int alloc_lte(sed_ctx* c)
 {
   const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
   const size_t na = (size_t)std::max(c->nelem, 1);
   const size_t ni = (size_t)std::max(c->n_ions_total, 1), nl = (size_t)std::max(c->n_lev_total, 1);
-  const size_t per_zone = (3 * nn + 2 * na + 2 * ni + 2 * nl) * sizeof(double);
+  const bool smem_rows = rows_in_smem(na, nn);
+  const size_t rows = (smem_rows ? 2 : 3) * nn + (c->any_zero_eps ? 2 * nn : 0);
+  const size_t per_zone = (rows + 2 * na + 2 * ni + 2 * nl) * sizeof(double);
   const size_t cz = std::max<size_t>(1, std::min(nz, opacity_scratch_bytes() / per_zone));
   c->chunk_zones = (int)cz;
-  CK(c->d_abs64.resize(cz * nn)); CK(c->d_scat64.resize(cz * nn)); CK(c->d_emis64.resize(cz * nn));
+  CK(c->d_abs64.resize(cz * nn)); CK(c->d_scat64.resize(cz * nn));
+  CK(c->d_emis64.resize(smem_rows ? 1 : cz * nn));
+  CK(c->d_epsl64.resize(c->any_zero_eps ? cz * nn : 1)); CK(c->d_epsf64.resize(c->any_zero_eps ? cz * nn : 1));
   CK(c->d_n_dens.resize(cz * na));
   CK(c->d_mass_frac.resize(cz * na));
   CK(c->d_ion_part.resize(cz * ni));
@@ -370,8 +389,9 @@ int sed_set_grid(sed_ctx* c, const sed_grid* g)
   if (rc) return rc;
   // per-atom epsilon switch
   std::vector<int32_t> ze(std::max(c->nelem, 1), 0);
+  c->any_zero_eps = false;
   for (int a = 0; a < c->nelem; ++a)
-    for (int z : c->zero_eps) if (z == c->h_eZ[a]) ze[a] = 1;
+    for (int z : c->zero_eps) if (z == c->h_eZ[a]) { ze[a] = 1; c->any_zero_eps = true; }
   CK(upload(c, c->d_zero_eps_atom, ze.data(), ze.size()));
   c->have_grid = true;
   CK(cudaStreamSynchronize(c->stream));
@@ -386,8 +406,9 @@ int sed_set_opacity_params(sed_ctx* c, const sed_opacity_params* op)
   c->op.atom_zero_epsilon = nullptr;
   if (c->have_grid) {
     std::vector<int32_t> ze(std::max(c->nelem, 1), 0);
+    c->any_zero_eps = false;
     for (int a = 0; a < c->nelem; ++a)
-      for (int z : c->zero_eps) if (z == c->h_eZ[a]) ze[a] = 1;
+      for (int z : c->zero_eps) if (z == c->h_eZ[a]) { ze[a] = 1; c->any_zero_eps = true; }
     CK(upload(c, c->d_zero_eps_atom, ze.data(), ze.size()));
     CK(cudaStreamSynchronize(c->stream));
   }
@@ -417,65 +438,83 @@ int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
   const size_t np = (size_t)a->photo_off[nl];
   CK(upload(c, c->d_photo_E, a->photo_E, np));
   CK(upload(c, c->d_photo_s, a->photo_s, np));
-  // level-to-level lines: bin (AtomicData.cpp:680), stable sort by (atom, bin)
+  {
+    std::vector<int32_t> ia((size_t)std::max(c->n_ions_total, 1), 0);
+    for (int at = 0; at < na; ++at)
+      for (int i = a->ion_off[at]; i < a->ion_off[at + 1]; ++i) ia[i] = at;
+    CK(upload(c, c->d_ion_atom, ia.data(), ia.size()));
+  }
+  // level-to-level lines: bin (AtomicData.cpp:680), stable sort by (bin, atom)
+  // so each bin is one contiguous run in the atoms' list order; per line the
+  // absolute level indices, sigma_tot f lambda and g_l/g_u
   {
     const int n = a->line_off[na];
-    std::vector<int> bin(n), order(n);
+    std::vector<int> order(n);
     std::vector<int64_t> key(n);
+    std::vector<int> atom_of(n);
     for (int at = 0; at < na; ++at)
       for (int k = a->line_off[at]; k < a->line_off[at + 1]; ++k) {
-        bin[k] = c->nu.within(a->line_nu[k]);
-        key[k] = (int64_t)at * nn + bin[k];
+        key[k] = (int64_t)c->nu.within(a->line_nu[k]) * na + at;
+        atom_of[k] = at;
       }
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
-    std::vector<int32_t> ll(n), lu(n), seg((size_t)na * nn + 1, 0);
-    std::vector<double> lnu(n), lf(n);
+    std::vector<int4> lv(std::max(n, 1));
+    std::vector<double2> lc(std::max(n, 1));
+    std::vector<float2> lc32(std::max(n, 1));
+    std::vector<int32_t> seg((size_t)nn + 1, 0);
     for (int k = 0; k < n; ++k) {
-      const int s = order[k];
-      ll[k] = a->line_l[s]; lu[k] = a->line_u[s]; lnu[k] = a->line_nu[s]; lf[k] = a->line_f[s];
-      seg[key[s] + 1]++;
+      const int s = order[k], at = atom_of[s], l0 = a->lev_off[at];
+      const int ll = l0 + a->line_l[s], lu = l0 + a->line_u[s];
+      lv[k] = make_int4(ll, lu, (int)(key[s] / na), at);
+      const double lam = C_LIGHT / a->line_nu[s];
+      const double gr = (1.0 * a->lev_g[ll]) / (1.0 * a->lev_g[lu]);
+      lc[k] = make_double2(SIGMA_TOT * a->line_f[s] * lam, gr);
+      lc32[k] = make_float2((float)lc[k].x, (float)gr);
+      seg[key[s] / na + 1]++;
     }
-    for (size_t s = 1; s < seg.size(); ++s) seg[s] += seg[s - 1];
+    for (size_t q = 1; q < seg.size(); ++q) seg[q] += seg[q - 1];
     c->nlines = n;
-    CK(upload(c, c->d_line_seg, seg.data(), seg.size()));
-    CK(upload(c, c->d_line_l, ll.data(), (size_t)n));
-    CK(upload(c, c->d_line_u, lu.data(), (size_t)n));
-    CK(upload(c, c->d_line_nu, lnu.data(), (size_t)n));
-    CK(upload(c, c->d_line_f, lf.data(), (size_t)n));
+    CK(upload(c, c->d_ln_seg, seg.data(), seg.size()));
+    CK(upload(c, c->d_ln_lv, lv.data(), lv.size()));
+    CK(upload(c, c->d_ln_c, lc.data(), lc.size()));
+    CK(upload(c, c->d_ln_c32, lc32.data(), lc32.size()));
     CK(cudaStreamSynchronize(c->stream));
   }
-  // fuzz lines: bin (AtomicData.cpp:851), stable sort by (atom, bin), FP32 constants
+  // fuzz lines: bin (AtomicData.cpp:851), stable sort by (bin, atom); per line
+  // the absolute ion index, sigma_tot lambda gf, E_l/k_ev, h nu/k
   {
     const int n = a->fuzz_off[na];
     std::vector<int64_t> key(n);
-    std::vector<int> order(n);
+    std::vector<int> order(n), atom_of(n);
     for (int at = 0; at < na; ++at)
-      for (int k = a->fuzz_off[at]; k < a->fuzz_off[at + 1]; ++k) key[k] = (int64_t)at * nn + c->nu.within(a->fuzz_nu[k]);
+      for (int k = a->fuzz_off[at]; k < a->fuzz_off[at + 1]; ++k) {
+        key[k] = (int64_t)c->nu.within(a->fuzz_nu[k]) * na + at;
+        atom_of[k] = at;
+      }
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key[x] < key[y]; });
-    std::vector<int32_t> ion(n), seg((size_t)na * nn + 1, 0);
-    std::vector<double> fnu(n), fgf(n), fEl(n);
-    std::vector<float> A32(n), El32(n), h32(n);
+    std::vector<int4> fia(std::max(n, 1));
+    std::vector<double2> fc(std::max(n, 1));
+    std::vector<double> fh(std::max(n, 1));
+    std::vector<float4> fc32(std::max(n, 1));
+    std::vector<int32_t> seg((size_t)nn + 1, 0);
     for (int k = 0; k < n; ++k) {
-      const int s = order[k];
-      fnu[k] = a->fuzz_nu[s]; fgf[k] = a->fuzz_gf[s]; fEl[k] = a->fuzz_El[s]; ion[k] = a->fuzz_ion[s];
-      A32[k] = (float)(SIGMA_TOT * (C_LIGHT / fnu[k]) * fgf[k]);
-      El32[k] = (float)(fEl[k] / K_EV);
-      h32[k] = (float)(H_PLANCK * fnu[k] / K_BOLTZ);
-      seg[key[s] + 1]++;
+      const int s = order[k], at = atom_of[s];
+      const double fnu = a->fuzz_nu[s];
+      fia[k] = make_int4(a->ion_off[at] + a->fuzz_ion[s], (int)(key[s] / na), at, 0);
+      fc[k] = make_double2(SIGMA_TOT * (C_LIGHT / fnu) * a->fuzz_gf[s], a->fuzz_El[s] / K_EV);
+      fh[k] = H_PLANCK * fnu / K_BOLTZ;
+      fc32[k] = make_float4((float)fc[k].x, (float)fc[k].y, (float)fh[k], 0.f);
+      seg[key[s] / na + 1]++;
     }
-    for (size_t s = 1; s < seg.size(); ++s) seg[s] += seg[s - 1];
+    for (size_t q = 1; q < seg.size(); ++q) seg[q] += seg[q - 1];
     c->nfuzz = n;
-    c->fuzz_order = order;
-    CK(upload(c, c->d_fuzz_seg, seg.data(), seg.size()));
-    CK(upload(c, c->d_fz_nu, fnu.data(), (size_t)n));
-    CK(upload(c, c->d_fz_gf, fgf.data(), (size_t)n));
-    CK(upload(c, c->d_fz_El, fEl.data(), (size_t)n));
-    CK(upload(c, c->d_fz_ion, ion.data(), (size_t)n));
-    CK(upload(c, c->d_fz_A32, A32.data(), (size_t)n));
-    CK(upload(c, c->d_fz_El32, El32.data(), (size_t)n));
-    CK(upload(c, c->d_fz_hnu32, h32.data(), (size_t)n));
+    CK(upload(c, c->d_fz_seg, seg.data(), seg.size()));
+    CK(upload(c, c->d_fz_ia, fia.data(), fia.size()));
+    CK(upload(c, c->d_fz_c, fc.data(), fc.size()));
+    CK(upload(c, c->d_fz_h, fh.data(), fh.size()));
+    CK(upload(c, c->d_fz_c32, fc32.data(), fc32.size()));
     CK(cudaStreamSynchronize(c->stream));
   }
   c->have_atoms = true;
@@ -504,11 +543,26 @@ int sed_set_opacity(sed_ctx* c, double dt)
   A.ion_off = c->d_ion_off.p; A.lev_off = c->d_lev_off.p; A.lev_ion = c->d_lev_ion.p; A.lev_g = c->d_lev_g.p;
   A.lev_ic = c->d_lev_ic.p; A.photo_off = c->d_photo_off.p; A.ion_chi = c->d_ion_chi.p; A.lev_E = c->d_lev_E.p;
   A.lev_Eion = c->d_lev_Eion.p; A.photo_E = c->d_photo_E.p; A.photo_s = c->d_photo_s.p;
-  A.line_seg = c->d_line_seg.p; A.line_l = c->d_line_l.p; A.line_u = c->d_line_u.p; A.line_nu = c->d_line_nu.p;
-  A.line_f = c->d_line_f.p;
-  A.fuzz_seg = c->d_fuzz_seg.p; A.fz_nu = c->d_fz_nu.p; A.fz_gf = c->d_fz_gf.p; A.fz_El = c->d_fz_El.p;
-  A.fz_ion = c->d_fz_ion.p; A.fz_A32 = c->d_fz_A32.p; A.fz_El32 = c->d_fz_El32.p; A.fz_hnu32 = c->d_fz_hnu32.p;
-  A.nfuzz = c->nfuzz;
+  A.ion_atom = c->d_ion_atom.p;
+  A.ln_seg = c->d_ln_seg.p; A.ln_lv = c->d_ln_lv.p; A.ln_c = c->d_ln_c.p; A.ln_c32 = c->d_ln_c32.p;
+  A.fz_seg = c->d_fz_seg.p; A.fz_ia = c->d_fz_ia.p; A.fz_c = c->d_fz_c.p; A.fz_h = c->d_fz_h.p;
+  A.fz_c32 = c->d_fz_c32.p;
+  A.uniform_eps = c->any_zero_eps ? 0 : 1;
+  A.smem_rows = rows_in_smem((size_t)std::max(c->nelem, 1), (size_t)c->nu.n());
+  if (!A.uniform_eps && c->d_epsl64.n < (size_t)c->chunk_zones * c->nu.n()) {
+    int rc = alloc_lte(c);  // epsilon-weighted sums appear with the first atom of epsilon 0
+    if (rc) return rc;
+  }
+  A.epsl64 = c->d_epsl64.p; A.epsf64 = c->d_epsf64.p;
+  if (A.natoms > 0 && (A.use_line || A.use_fuzz)) {
+    const int npop = std::max(A.use_line ? c->n_lev_total : 0, A.use_fuzz ? c->n_ions_total : 0);
+    if (line_sum_smem_bytes(c->tp.precision, c->natoms, npop) > SMEM_ZONE_BYTES)
+      return set_err(c, SED_ERR_CAPACITY, "sed_set_opacity: %d populations per zone exceed the line-sum kernel's "
+                     "shared memory", npop);
+  }
+  if (A.natoms > 0 && ((A.use_line && c->nlines > 0 && !c->d_ln_seg.p) || (A.use_fuzz && !c->d_fz_seg.p)))
+    return set_err(c, SED_ERR_STATE, "sed_set_opacity: line lists not set");
+  if (A.natoms == 0) { A.use_line = 0; A.use_fuzz = 0; }
   A.ion_part = c->d_ion_part.p; A.ion_frac = c->d_ion_frac.p; A.lev_n = c->d_lev_n.p;
   A.n_ions_total = c->n_ions_total; A.n_lev_total = c->n_lev_total;
   A.n_elec = c->d_n_elec.p; A.n_dens = c->d_n_dens.p; A.mass_frac = c->d_mass_frac.p; A.temp_c = c->d_temp_c.p;
@@ -532,8 +586,10 @@ int sed_set_opacity(sed_ctx* c, double dt)
     B.opac_out = static_cast<unsigned char*>(A.opac_out) + o * nn * 2 * esz;
     B.cdf_out = static_cast<unsigned char*>(A.cdf_out) + o * nn * esz;
     B.cdf_coarse_out = static_cast<unsigned char*>(A.cdf_coarse_out) + o * (size_t)c->n_coarse * esz;
-    c->opacity_launches += launch_opacity(B, c->num_sms, c->stream);
+    const int nl = launch_opacity(B, c->num_sms, c->stream);
     CK(cudaGetLastError());
+    if (nl < 0) return set_err(c, SED_ERR_CUDA, "sed_set_opacity: opacity kernel configuration rejected");
+    c->opacity_launches += nl;
   }
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -782,18 +838,18 @@ void sed_ctx_destroy(sed_ctx* c)
   DevBuf<double>* dbl[] = {&c->d_nu, &c->d_st, &c->d_sn, &c->d_sm, &c->d_sp, &c->d_core_cdf, &c->d_r_out, &c->d_v_r,
                            &c->d_ax[0], &c->d_ax[1], &c->d_ax[2], &c->d_vol, &c->d_rho, &c->d_T, &c->d_egas,
                            &c->d_grey, &c->d_X, &c->d_ion_chi, &c->d_lev_E, &c->d_lev_Eion, &c->d_photo_E,
-                           &c->d_photo_s, &c->d_line_nu, &c->d_line_f, &c->d_fz_nu, &c->d_fz_gf, &c->d_fz_El,
-                           &c->d_eps_imc, &c->d_abs64, &c->d_scat64, &c->d_emis64, &c->d_planck, &c->d_ross, &c->d_L,
+                           &c->d_photo_s, &c->d_fz_h,
+                           &c->d_eps_imc, &c->d_abs64, &c->d_scat64, &c->d_emis64, &c->d_epsl64, &c->d_epsf64, &c->d_planck, &c->d_ross, &c->d_L,
                            &c->d_n_elec, &c->d_n_dens, &c->d_mass_frac, &c->d_temp_c, &c->d_ion_part, &c->d_ion_frac,
                            &c->d_lev_n, &c->d_boltz, &c->d_J, &c->d_e_abs, &c->d_e_rad, &c->d_fx, &c->d_fy,
                            &c->d_fz, &c->d_fr, &c->d_flux, &c->d_click, &c->d_rec_state};
   for (auto* b : dbl) b->release();
   DevBuf<int32_t>* ints[] = {&c->d_eZ, &c->d_eA, &c->d_zero_eps_atom, &c->d_ion_off, &c->d_lev_off, &c->d_lev_ion,
-                             &c->d_lev_g, &c->d_lev_ic, &c->d_photo_off, &c->d_line_seg, &c->d_line_l, &c->d_line_u,
-                             &c->d_fuzz_seg, &c->d_fz_ion, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind,
-                             &c->d_rec_draws};
+                             &c->d_lev_g, &c->d_lev_ic, &c->d_photo_off, &c->d_ion_atom, &c->d_ln_seg,
+                             &c->d_fz_seg, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind, &c->d_rec_draws};
   for (auto* b : ints) b->release();
-  c->d_fz_A32.release(); c->d_fz_El32.release(); c->d_fz_hnu32.release();
+  c->d_ln_lv.release(); c->d_ln_c.release(); c->d_ln_c32.release(); c->d_fz_ia.release(); c->d_fz_c.release();
+  c->d_fz_c32.release();
   c->d_opac.release(); c->d_cdf.release(); c->d_cdf_coarse.release(); c->d_counters.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -69,16 +69,20 @@ struct OpacityArgs {
   int32_t natoms;
   const int32_t *ion_off, *lev_off, *lev_ion, *lev_g, *lev_ic, *photo_off;
   const double *ion_chi, *lev_E, *lev_Eion, *photo_E, *photo_s;
-  // level-to-level lines sorted by (atom, bin): segment starts per (atom, bin)
-  const int32_t* line_seg;     // [natoms * n_nu + 1]
-  const int32_t *line_l, *line_u;
-  const double *line_nu, *line_f;
-  // fuzz lines sorted by (atom, bin): segment starts per (atom, bin)
-  const int32_t* fuzz_seg;     // [natoms * n_nu + 1]
-  const double *fz_nu, *fz_gf, *fz_El;
-  const int32_t* fz_ion;
-  const float *fz_A32, *fz_El32, *fz_hnu32;  // FP32 per-line constants
-  int32_t nfuzz;
+  const int32_t* ion_atom;      // [n_ions_total] atom of each ion
+  // level-to-level lines sorted by (bin, atom): bin j holds [ln_seg[j], ln_seg[j+1])
+  const int32_t* ln_seg;       // [n_nu + 1]
+  const int4* ln_lv;           // {lower level, upper level (absolute indices), bin, atom}
+  const double2* ln_c;         // {sigma_tot f lambda, g_l / g_u}
+  const float2* ln_c32;        // FP32 copy of ln_c
+  // fuzz lines sorted by (bin, atom)
+  const int32_t* fz_seg;       // [n_nu + 1]
+  const int4* fz_ia;           // {absolute ion index, bin, atom, 0}
+  const double2* fz_c;         // {sigma_tot lambda gf, E_l / k_ev}
+  const double* fz_h;          // h nu / k
+  const float4* fz_c32;        // FP32 {sigma_tot lambda gf, E_l / k_ev, h nu / k, 0}
+  int32_t uniform_eps;         // every atom has epsilon = A.epsilon
+  int32_t smem_rows;           // FP64 rows of the zone in shared memory
   // per-zone LTE state (device scratch written by the LTE kernel)
   double *ion_part, *ion_frac, *lev_n;  // [nzones * n_ions_total] etc.
   int32_t n_ions_total, n_lev_total;
@@ -89,7 +93,8 @@ struct OpacityArgs {
   int32_t* solve_err;                    // [nz]
   double* boltz;                         // [n_lev_total * nz] exp(-E/kT) per level
   // outputs
-  double *abs64, *scat64, *emis64;       // [nz*n_nu] FP64 working tables
+  double *abs64, *scat64, *emis64;       // [nz*n_nu] FP64 rows when they do not fit in shared memory
+  double *epsl64, *epsf64;               // [nz*n_nu] epsilon-weighted line / fuzz sums (same condition)
   void* opac_out;                        // double2 / float2 [nz*n_nu]
   void* cdf_out;                         // double / float [nz*n_nu]
   void* cdf_coarse_out;                  // double / float [nz*n_coarse]
@@ -97,6 +102,10 @@ struct OpacityArgs {
   double *eps_imc, *planck, *ross, *L_th;
 };
 
+// dynamic shared memory of the per-zone opacity kernel for these arguments
+size_t opacity_smem_bytes(const OpacityArgs& a);
+// dynamic shared memory of the line-sum kernel (n_pop levels or ions per zone)
+size_t line_sum_smem_bytes(int precision, int natoms, int n_pop);
 int launch_opacity(const OpacityArgs& a, int num_sms, cudaStream_t s);
 
 }  // namespace sed
