@@ -214,17 +214,20 @@ __device__ double photo_cs(const OpacityArgs& A, int lev, double zv)
 // carries the cancellation of 1 - exp(-tau), which the FP64 tables reproduce.
 __device__ __forceinline__ double sobolev_term(double tau) { return 1 - exp(-tau); }
 
-// FP32 form: below tau = 2^-7 the Taylor series to tau^5 (truncation below
-// tau^5/720, under 5e-14 relative), above it -expm1f(-tau); both free of the
-// cancellation that 1 - expf(-tau) would have in single precision.
-__device__ __forceinline__ float sobolev_term32(float tau)
+// FP32 form of 1 - exp(-x) for x >= 0, branch-free: below x = 0.1 the
+// Taylor series to x^7 (truncation below x^8/8! < 3e-12 relative), above it
+// 1 - __expf(-x), whose ~2^-22 relative error in exp(-x) stays below 3e-6
+// relative in 1 - exp(-x) for x >= 0.1.  Neither has the cancellation of
+// 1 - expf(-x) at small x.
+__device__ __forceinline__ float one_minus_exp32(float x)
 {
-  if (tau < 0.0078125f) {
-    const float t = tau;
-    return t * (1.f - t * 0.5f * (1.f - t * (1.f / 3) * (1.f - t * 0.25f * (1.f - t * 0.2f))));
-  }
-  return -expm1f(-tau);
+  const float p = x * (1.f - x * 0.5f * (1.f - x * (1.f / 3) * (1.f - x * 0.25f * (1.f - x * 0.2f *
+                 (1.f - x * (1.f / 6) * (1.f - x * (1.f / 7)))))));
+  const float e = 1.f - __expf(-x);
+  return (x < 0.1f) ? p : e;
 }
+
+__device__ __forceinline__ float sobolev_term32(float tau) { return one_minus_exp32(tau); }
 
 // Level populations of one zone in the chunk scratch (level-major).
 struct LevView {
@@ -237,12 +240,16 @@ struct LevView {
 // when FUZZ) for a tile of ZT zones: S[z][bin] = sum of (1 - exp(-tau)) over
 // the bin's lines, Se[z][bin] the same weighted by the line's atom epsilon
 // when atoms differ in epsilon (AtomicSpecies_opacities.cpp:292-375,
-// GasState_opacities.cpp:424-494).  The tile's level populations (or ion
-// populations for fuzz lines) and reciprocals are staged in shared memory
-// level-major, ZT zones contiguous; each thread takes bins j = tid, tid + 256,
-// ... and walks the bin's lines (sorted by bin, atom), loading each line
-// record once and applying it to the ZT zones.  Sums accumulate in FP64 in
-// the bin's list order.  In the mixed form the per-line arithmetic is FP32.
+// GasState_opacities.cpp:424-494).  The tile's level populations times the
+// atom's number density, n_l n_atom, and their reciprocals (or the ion
+// populations for fuzz lines) are staged in shared memory level-major, ZT
+// zones contiguous; the ratio n_u g_l / (n_l g_u) is formed from them (the
+// atom density cancels).  Thread t takes the bins order[t], order[t + 256],
+// ... where `order` lists the bins by decreasing line count, so the lanes of
+// a warp walk lists of similar length; it walks each bin's lines (sorted by
+// bin, atom), loading each line record once and applying it to the ZT zones.
+// Sums accumulate in FP64 in the bin's list order.  In the mixed form the
+// per-line arithmetic is FP32.
 // Level populations come from the LTE solve, floored at 1e-30, so they are
 // normal FP32 numbers and the reference's n_l < DBL_MIN skip never applies
 // to them; a NaN term is skipped as in the reference.
@@ -277,7 +284,7 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
         v = A.n_dens[(size_t)a * nz + z0 + zi] * A.ion_frac[(size_t)l * nz + z0 + zi] /
             A.ion_part[(size_t)l * nz + z0 + zi];
       } else {
-        v = A.lev_n[(size_t)l * nz + z0 + zi];
+        v = A.lev_n[(size_t)l * nz + z0 + zi] * A.n_dens[(size_t)A.lev_atom[l] * nz + z0 + zi];
       }
     }
     pop[i] = (V)v;
@@ -286,8 +293,10 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
   __syncthreads();
   const bool want_e = !A.uniform_eps;
   const int32_t* seg = FUZZ ? A.fz_seg : A.ln_seg;
+  const int32_t* order = FUZZ ? A.fz_order : A.ln_order;
   const double time = A.time;
-  for (int j = tid; j < nn; j += bd) {
+  for (int jj = tid; jj < nn; jj += bd) {
+    const int j = __ldg(order + jj);
     double acc[ZT], acce[ZT];
 #pragma unroll
     for (int q = 0; q < ZT; ++q) { acc[q] = 0; acce[q] = 0; }
@@ -299,17 +308,16 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
         // tau = n_l n_atom sigma_tot f lambda t (1 - n_u g_l / (n_l g_u)), 0 past the laser limit
         const int4 lv = __ldg(A.ln_lv + k);
         atom = lv.w;
-        const V* pl = pop + (size_t)lv.x * ZT;
-        const V* il = ipop + (size_t)lv.x * ZT;
-        const V* pu = pop + (size_t)lv.y * ZT;
-        const V* nd = ndv + atom * ZT;
+        const V* pl = pop + (size_t)lv.x * ZT;   // n_l n_atom
+        const V* il = ipop + (size_t)lv.x * ZT;  // 1 / (n_l n_atom)
+        const V* pu = pop + (size_t)lv.y * ZT;   // n_u n_atom
         if constexpr (MIXED) {
           const float2 c = __ldg(A.ln_c32 + k);
           const float ct = c.x * (float)time;
 #pragma unroll
           for (int q = 0; q < ZT; ++q) {
             const float r = pu[q] * il[q] * c.y;
-            const float tau = (r > 1.f) ? 0.f : pl[q] * nd[q] * ct * (1.f - r);
+            const float tau = (r > 1.f) ? 0.f : pl[q] * ct * (1.f - r);
             const float t = sobolev_term32(tau);
             term[q] = (t == t) ? t : 0.f;
           }
@@ -317,11 +325,11 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
           const double2 c = __ldg(A.ln_c + k);
 #pragma unroll
           for (int q = 0; q < ZT; ++q) {
-            const double nl = pl[q];
+            const double nln = pl[q];
             double t = 0;
-            if (!(nl < DBL_MIN)) {
+            if (!(nln < DBL_MIN)) {
               const double r = pu[q] * il[q] * c.y;
-              const double tau = (r > 1) ? 0.0 : nl * nd[q] * c.x * time * (1 - r);
+              const double tau = (r > 1) ? 0.0 : nln * c.x * time * (1 - r);
               t = sobolev_term(tau);
               if (isnan(t)) t = 0;
             }
@@ -338,8 +346,8 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
           const float ct = c.x * (float)time;
 #pragma unroll
           for (int q = 0; q < ZT; ++q) {
-            const float stim = -expm1f(-c.z * invT[q]);
-            const float tau = ct * pi[q] * expf(-c.y * invT[q]) * stim;
+            const float stim = one_minus_exp32(c.z * invT[q]);
+            const float tau = ct * pi[q] * __expf(-c.y * invT[q]) * stim;
             term[q] = sobolev_term32(tau);
           }
         } else {

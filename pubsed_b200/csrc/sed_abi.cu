@@ -111,7 +111,8 @@ struct sed_ctx {
   bool have_atoms = false;
   bool any_zero_eps = false;
   int natoms = 0, n_ions_total = 0, n_lev_total = 0, nfuzz = 0, nlines = 0;
-  DevBuf<int32_t> d_ion_off, d_lev_off, d_lev_ion, d_lev_g, d_lev_ic, d_photo_off, d_ion_atom, d_ln_seg, d_fz_seg;
+  DevBuf<int32_t> d_ion_off, d_lev_off, d_lev_ion, d_lev_g, d_lev_ic, d_photo_off, d_ion_atom, d_lev_atom, d_ln_seg,
+      d_fz_seg, d_ln_order, d_fz_order;
   DevBuf<double> d_ion_chi, d_lev_E, d_lev_Eion, d_photo_E, d_photo_s, d_fz_h;
   DevBuf<int4> d_ln_lv;
   DevBuf<double2> d_ln_c, d_fz_c;
@@ -439,11 +440,22 @@ int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
   CK(upload(c, c->d_photo_E, a->photo_E, np));
   CK(upload(c, c->d_photo_s, a->photo_s, np));
   {
-    std::vector<int32_t> ia((size_t)std::max(c->n_ions_total, 1), 0);
-    for (int at = 0; at < na; ++at)
+    std::vector<int32_t> ia((size_t)std::max(c->n_ions_total, 1), 0), la(std::max(nl, (size_t)1), 0);
+    for (int at = 0; at < na; ++at) {
       for (int i = a->ion_off[at]; i < a->ion_off[at + 1]; ++i) ia[i] = at;
+      for (int l = a->lev_off[at]; l < a->lev_off[at + 1]; ++l) la[l] = at;
+    }
     CK(upload(c, c->d_ion_atom, ia.data(), ia.size()));
+    CK(upload(c, c->d_lev_atom, la.data(), la.size()));
   }
+  // bins by decreasing line count (ties by bin): the line-sum kernel deals
+  // them to threads in this order so the lanes of a warp get similar counts
+  auto bin_order = [&](const std::vector<int32_t>& seg) {
+    std::vector<int32_t> o(nn);
+    std::iota(o.begin(), o.end(), 0);
+    std::stable_sort(o.begin(), o.end(), [&](int x, int y) { return seg[x + 1] - seg[x] > seg[y + 1] - seg[y]; });
+    return o;
+  };
   // level-to-level lines: bin (AtomicData.cpp:680), stable sort by (bin, atom)
   // so each bin is one contiguous run in the atoms' list order; per line the
   // absolute level indices, sigma_tot f lambda and g_l/g_u
@@ -475,6 +487,8 @@ int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
     }
     for (size_t q = 1; q < seg.size(); ++q) seg[q] += seg[q - 1];
     c->nlines = n;
+    const std::vector<int32_t> ord = bin_order(seg);
+    CK(upload(c, c->d_ln_order, ord.data(), ord.size()));
     CK(upload(c, c->d_ln_seg, seg.data(), seg.size()));
     CK(upload(c, c->d_ln_lv, lv.data(), lv.size()));
     CK(upload(c, c->d_ln_c, lc.data(), lc.size()));
@@ -510,6 +524,8 @@ int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
     }
     for (size_t q = 1; q < seg.size(); ++q) seg[q] += seg[q - 1];
     c->nfuzz = n;
+    const std::vector<int32_t> ord = bin_order(seg);
+    CK(upload(c, c->d_fz_order, ord.data(), ord.size()));
     CK(upload(c, c->d_fz_seg, seg.data(), seg.size()));
     CK(upload(c, c->d_fz_ia, fia.data(), fia.size()));
     CK(upload(c, c->d_fz_c, fc.data(), fc.size()));
@@ -543,7 +559,8 @@ int sed_set_opacity(sed_ctx* c, double dt)
   A.ion_off = c->d_ion_off.p; A.lev_off = c->d_lev_off.p; A.lev_ion = c->d_lev_ion.p; A.lev_g = c->d_lev_g.p;
   A.lev_ic = c->d_lev_ic.p; A.photo_off = c->d_photo_off.p; A.ion_chi = c->d_ion_chi.p; A.lev_E = c->d_lev_E.p;
   A.lev_Eion = c->d_lev_Eion.p; A.photo_E = c->d_photo_E.p; A.photo_s = c->d_photo_s.p;
-  A.ion_atom = c->d_ion_atom.p;
+  A.ion_atom = c->d_ion_atom.p; A.lev_atom = c->d_lev_atom.p;
+  A.ln_order = c->d_ln_order.p; A.fz_order = c->d_fz_order.p;
   A.ln_seg = c->d_ln_seg.p; A.ln_lv = c->d_ln_lv.p; A.ln_c = c->d_ln_c.p; A.ln_c32 = c->d_ln_c32.p;
   A.fz_seg = c->d_fz_seg.p; A.fz_ia = c->d_fz_ia.p; A.fz_c = c->d_fz_c.p; A.fz_h = c->d_fz_h.p;
   A.fz_c32 = c->d_fz_c32.p;
@@ -846,7 +863,7 @@ void sed_ctx_destroy(sed_ctx* c)
   for (auto* b : dbl) b->release();
   DevBuf<int32_t>* ints[] = {&c->d_eZ, &c->d_eA, &c->d_zero_eps_atom, &c->d_ion_off, &c->d_lev_off, &c->d_lev_ion,
                              &c->d_lev_g, &c->d_lev_ic, &c->d_photo_off, &c->d_ion_atom, &c->d_ln_seg,
-                             &c->d_fz_seg, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind, &c->d_rec_draws};
+                             &c->d_fz_seg, &c->d_lev_atom, &c->d_ln_order, &c->d_fz_order, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind, &c->d_rec_draws};
   for (auto* b : ints) b->release();
   c->d_ln_lv.release(); c->d_ln_c.release(); c->d_ln_c32.release(); c->d_fz_ia.release(); c->d_fz_c.release();
   c->d_fz_c32.release();

@@ -70,6 +70,9 @@ struct OpacityArgs {
   const int32_t *ion_off, *lev_off, *lev_ion, *lev_g, *lev_ic, *photo_off;
   const double *ion_chi, *lev_E, *lev_Eion, *photo_E, *photo_s;
   const int32_t* ion_atom;      // [n_ions_total] atom of each ion
+  const int32_t* lev_atom;      // [n_lev_total] atom of each level
+  const int32_t* ln_order;      // [n_nu] bins by decreasing level-line count
+  const int32_t* fz_order;      // [n_nu] bins by decreasing fuzz-line count
   // level-to-level lines sorted by (bin, atom): bin j holds [ln_seg[j], ln_seg[j+1])
   const int32_t* ln_seg;       // [n_nu + 1]
   const int4* ln_lv;           // {lower level, upper level (absolute indices), bin, atom}
