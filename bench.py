@@ -125,10 +125,11 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
                        "n_bins": w.nu_grid().n, "packets_per_step": n_sample, "threads": cores,
                        "sample_zones": w.zones.n_zones},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": "transport::step of the %s workload (full zone/line/bin sizes) with %d "
+                             "sample": "transport::step of the %s workload (%s sizes) with %d "
                                        "packets per step (%.2f s, of which set_opacity %.2f s); full-step time "
                                        "= set_opacity + propagation scaled to %d packets%s" %
-                                       (w.name, n_sample, t_sample, t_opac, n_full, grid_note)},
+                                       (w.name, "full zone/line/bin" if zone_scale == 1 else "full line/bin",
+                                        n_sample, t_sample, t_opac, n_full, grid_note)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "sample_packets_per_s": n_sample / t_sample, "set_opacity_seconds": t_opac}
 

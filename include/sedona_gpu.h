@@ -215,6 +215,10 @@ int sed_step(sed_ctx* ctx, double dt, sed_step_stats* stats);
 int sed_get_spectrum(sed_ctx* ctx, double* flux, double* click);
 int sed_get_zone_tallies(sed_ctx* ctx, double* J_nu, double* e_abs, double* e_rad,
                          double* fx, double* fy, double* fz, double* fr);
+/* The opacity tables the packet kernel reads (transport::abs_opacity_,
+ * scat_opacity_, emissivity_ after set_opacity, transport.h), n_zones*n_nu
+ * each, widened to double from FP32 in the mixed-precision form; emis_cdf is
+ * the normalised emissivity CDF.  Zone arrays n_zones. */
 int sed_get_opacity(sed_ctx* ctx, double* abs, double* scat, double* emis_cdf,
                     double* n_elec, double* eps_imc, double* planck_mean,
                     double* rosseland_mean, double* L_thermal);
