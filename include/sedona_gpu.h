@@ -240,6 +240,94 @@ void sed_ctx_destroy(sed_ctx* ctx);
 /* Library version / build string (never NULL). */
 const char* sed_version(void);
 
+/* ------------------------------------------------------------------ batches
+ * Many independent 1D spherical ejecta models (grid_1D_sphere, homologous)
+ * stepped together: one opacity build over all their zones and ONE packet
+ * launch over all their packets, captured into CUDA graphs (opacity build,
+ * packet kernel, normalisation) that are replayed every step.  Each model is what one reference run (one `transport` object,
+ * src/transport/transport.h:45-320) would hold: its own zones, core source,
+ * packet count, spectrum and zone tallies.  The batch shares the
+ * frequency/spectrum grids, the transport switches, the opacity parameters,
+ * the atomic data, the element list and the grid time t_now.  A model's
+ * packets use that model's Philox key and stream ids, so its results are
+ * those of a separate context with the same rng_seed and first_packet_id
+ * (tallies up to summation order). */
+typedef struct sed_batch sed_batch;
+
+/* One model: the sed_grid fields of a 1D sphere plus the core_* parameters
+ * and the Philox key/stream ids of sed_transport_params. */
+typedef struct sed_batch_model {
+  int32_t n_zones;
+  int32_t reserved;
+  double r_min;
+  const double* r_out;               /* [n_zones] */
+  const double* vol;                 /* [n_zones] */
+  const double* rho;
+  const double* T_gas;
+  const double* e_gas;               /* may be NULL (zeros) */
+  const double* total_grey_opacity;  /* may be NULL (zeros: microphysics) */
+  const double* X;                   /* [n_zones * n_elems] mass fractions */
+  int64_t core_n_emit;
+  double core_radius;
+  double core_luminosity;
+  double core_temperature;
+  uint32_t rng_seed;
+  int32_t reserved2;
+  int64_t first_packet_id;
+} sed_batch_model;
+
+/* Launch shape of the batched packet kernel: one of the compiled shapes
+ * (variant -> threads per block / minimum blocks per SM), how many blocks
+ * per SM to launch (0 = as many as fit) and how many consecutive packets a
+ * thread claims per pop of the packet queue. */
+typedef struct sed_batch_tuning {
+  int32_t variant;
+  int32_t threads;          /* output: threads per block of the variant */
+  int32_t blocks_per_sm;
+  int32_t queue_chunk;
+  float ms;                 /* autotune: kernel time of the sample with this shape */
+  int32_t n_tried;          /* autotune: shapes timed */
+} sed_batch_tuning;
+
+/* Creates a batch on `device`.  `common` supplies everything but the core_*
+ * fields, rng_seed and first_packet_id, which come per model.  Replaces one
+ * transport::init per model (transport_init.cpp:44-427). */
+int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n_elems, const int32_t* elem_Z,
+                     const int32_t* elem_A, int32_t n_models, const sed_batch_model* models, int device,
+                     sed_batch** out);
+int sed_batch_set_opacity_params(sed_batch* b, const sed_opacity_params* op);
+int sed_batch_set_atomic_data(sed_batch* b, const sed_atomic_data* atoms);
+
+/* Times the batched packet kernel on a sample of every model's packets
+ * (`sample_fraction` of each, at least one) for each compiled shape and
+ * queue chunk, keeps the fastest and returns it.  Runs an opacity build
+ * first if none exists.  Per-packet results do not depend on the choice. */
+int sed_batch_autotune(sed_batch* b, double sample_fraction, sed_batch_tuning* best);
+/* Uses the given shape instead (variant, blocks_per_sm, queue_chunk). */
+int sed_batch_set_tuning(sed_batch* b, const sed_batch_tuning* t);
+/* 1 (default): steps after the first are replays of captured CUDA graphs;
+ * 0: every step is launched kernel by kernel. */
+int sed_batch_use_graph(sed_batch* b, int32_t enable);
+
+/* transport::step of every model: opacity build, emission, propagation,
+ * spectrum and zone tallies, steady-state rescale and normalisation.
+ * `total` sums the counters over the models. */
+int sed_batch_step(sed_batch* b, double dt, sed_step_stats* total);
+
+/* Per-model results, laid out as the single-context getters lay them out. */
+int sed_batch_get_escaped(sed_batch* b, int64_t* n_escaped /* [n_models] */);
+int sed_batch_get_spectrum(sed_batch* b, int32_t model, double* flux, double* click);
+int sed_batch_get_zone_tallies(sed_batch* b, int32_t model, double* J_nu, double* e_abs, double* e_rad,
+                               double* fx, double* fy, double* fz, double* fr);
+int sed_batch_get_opacity(sed_batch* b, int32_t model, double* abs, double* scat, double* emis_cdf,
+                          double* n_elec, double* eps_imc);
+int sed_batch_record_packets(sed_batch* b, int32_t enable);
+/* Records of the model's first n packets; `ind` is the model's own zone index. */
+int sed_batch_get_packet_records(sed_batch* b, int32_t model, int64_t n, int32_t* fate, int32_t* ind,
+                                 int32_t* draws, double* state9);
+const char* sed_batch_last_error(sed_batch* b);
+void sed_batch_destroy(sed_batch* b);
+
 /* LTE electron density of every zone (the Saha-Boltzmann / Brent solve that
  * sed_set_opacity runs first), for callers that cannot allocate device memory
  * when they need it -- e.g. a host code whose device memory is all handed out

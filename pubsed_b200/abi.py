@@ -100,6 +100,25 @@ class StepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class BatchModel(C.Structure):
+    _fields_ = [
+        ("n_zones", C.c_int32), ("reserved", C.c_int32), ("r_min", C.c_double),
+        ("r_out", _dp), ("vol", _dp), ("rho", _dp), ("T_gas", _dp), ("e_gas", _dp),
+        ("total_grey_opacity", _dp), ("X", _dp),
+        ("core_n_emit", C.c_int64), ("core_radius", C.c_double), ("core_luminosity", C.c_double),
+        ("core_temperature", C.c_double), ("rng_seed", C.c_uint32), ("reserved2", C.c_int32),
+        ("first_packet_id", C.c_int64),
+    ]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("threads", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("queue_chunk", C.c_int32), ("ms", C.c_float), ("n_tried", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 @dataclass
 class Keep:
     """Holds numpy buffers referenced by C structs."""
@@ -153,6 +172,26 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         sig["transport_range"] = ([vp, C.c_double, C.c_int64, C.c_int64, C.c_int, C.POINTER(StepStats)], C.c_int)
         sig["get_fuzz_bins"] = ([vp, _ip], C.c_int)
         sig["locate"] = ([C.POINTER(LocateGrid), C.c_double], C.c_int)
+    if prefix == "sed_":
+        i64p = C.POINTER(C.c_int64)
+        sig.update({
+            "batch_create": ([C.POINTER(TransportParams), C.c_double, C.c_int32, _ip, _ip, C.c_int32,
+                              C.POINTER(BatchModel), C.c_int, C.POINTER(vp)], C.c_int),
+            "batch_set_opacity_params": ([vp, C.POINTER(OpacityParams)], C.c_int),
+            "batch_set_atomic_data": ([vp, C.POINTER(AtomicData)], C.c_int),
+            "batch_autotune": ([vp, C.c_double, C.POINTER(BatchTuning)], C.c_int),
+            "batch_set_tuning": ([vp, C.POINTER(BatchTuning)], C.c_int),
+            "batch_use_graph": ([vp, C.c_int32], C.c_int),
+            "batch_step": ([vp, C.c_double, C.POINTER(StepStats)], C.c_int),
+            "batch_get_escaped": ([vp, i64p], C.c_int),
+            "batch_get_spectrum": ([vp, C.c_int32, _dp, _dp], C.c_int),
+            "batch_get_zone_tallies": ([vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),
+            "batch_get_opacity": ([vp, C.c_int32, _dp, _dp, _dp, _dp, _dp], C.c_int),
+            "batch_record_packets": ([vp, C.c_int32], C.c_int),
+            "batch_get_packet_records": ([vp, C.c_int32, C.c_int64, _ip, _ip, _ip, _dp], C.c_int),
+            "batch_last_error": ([vp], C.c_char_p),
+            "batch_destroy": ([vp], None),
+        })
     for name, (args, res) in sig.items():
         fn = getattr(lib, prefix + name)
         fn.argtypes = args

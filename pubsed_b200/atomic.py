@@ -75,6 +75,9 @@ def _photo_table(E_ion: float, ion: int, chi_ground: float):
 class AtomicModel:
     atoms: list
 
+    def n_fuzz(self) -> int:
+        return int(sum(a.fuzz_nu.size for a in self.atoms))
+
     def selected_fuzz(self, a: AtomSpec, nu_grid: LocGrid):
         keep = (a.fuzz_ion < a.n_ions) & (a.fuzz_nu > nu_grid.min) & (a.fuzz_nu < nu_grid.right[-1])
         return keep

@@ -15,189 +15,11 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sedona_gpu.h"
-#include "sed_internal.h"
+#include "sed_ctx.h"
 
 using namespace sed;
 
 namespace {
-
-template <typename T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  cudaError_t resize(size_t m)
-  {
-    if (m == n && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    if (m == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, m * sizeof(T));
-    if (e == cudaSuccess) n = m;
-    return e;
-  }
-  void release()
-  {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-};
-
-// host copy of a locate_array with the same lookup rules as the device
-struct HostLoc {
-  int type = 0;
-  double min = 0, del = 0;
-  std::vector<double> x;
-  int n() const { return (int)x.size(); }
-  double left(int i) const { return i == 0 ? min : x[i - 1]; }
-  double delta(int i) const { return i == 0 ? x[0] - min : x[i] - x[i - 1]; }
-  double center(int i) const { return i == 0 ? 0.5 * (min + x[0]) : 0.5 * (x[i - 1] + x[i]); }
-  int upper(double v) const { return (int)(std::upper_bound(x.begin(), x.end(), v) - x.begin()); }
-  int locate(double v) const  // locate_array::locate (src/utils/locate_array.cpp:191-218)
-  {
-    const int nn = n();
-    if (nn == 1) return 0;
-    if (v >= x[nn - 1]) return nn;
-    if (v < min) return 0;
-    int ind;
-    if (type == LOC_FLEX) return upper(v);
-    else if (type == LOC_LIN) ind = (int)std::floor((v - min) / del);
-    else if (type == LOC_LOG) ind = (int)std::floor(std::log(v / min) / std::log(1 + del));
-    else return 0;
-    if (ind != 0 && ind != nn && (left(ind) > v || x[ind] <= v)) ind = upper(v);
-    return ind;
-  }
-  int within(double v) const { const int i = locate(v); return i == n() ? n() - 1 : i; }
-};
-
-HostLoc host_loc(const sed_locate_grid& g)
-{
-  HostLoc h;
-  h.type = g.type;
-  h.min = g.min;
-  h.del = g.del;
-  h.x.assign(g.right, g.right + g.n);
-  return h;
-}
-
-}  // namespace
-
-struct sed_ctx {
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev[6] = {};
-  std::string err;
-  sed_transport_params tp{};
-  HostLoc nu, st, sn, sm, sp;
-  DevBuf<double> d_nu, d_st, d_sn, d_sm, d_sp, d_core_cdf;
-  uint32_t step = 0;
-
-  // grid
-  bool have_grid = false;
-  int gtype = 0, nz = 0, nelem = 0, homologous = 1, nx = 0, ny = 0, nzz = 0;
-  double t_grid = 0;
-  HostLoc r_out, ax[3];
-  DevBuf<double> d_r_out, d_v_r, d_ax[3], d_vol, d_rho, d_T, d_egas, d_grey, d_X;
-  DevBuf<int32_t> d_eZ, d_eA;
-  std::vector<int32_t> h_eZ;
-
-  // opacity parameters and atomic data
-  sed_opacity_params op{};
-  std::vector<int32_t> zero_eps;
-  DevBuf<int32_t> d_zero_eps_atom;
-  bool have_atoms = false;
-  bool any_zero_eps = false;
-  int natoms = 0, n_ions_total = 0, n_lev_total = 0, nfuzz = 0, nlines = 0;
-  DevBuf<int32_t> d_ion_off, d_lev_off, d_lev_ion, d_lev_g, d_lev_ic, d_photo_off, d_ion_atom, d_lev_atom, d_ln_seg,
-      d_fz_seg, d_ln_order, d_fz_order;
-  DevBuf<double> d_ion_chi, d_lev_E, d_lev_Eion, d_photo_E, d_photo_s, d_fz_h;
-  DevBuf<int4> d_ln_lv;
-  DevBuf<double2> d_ln_c, d_fz_c;
-  DevBuf<float2> d_ln_c32;
-  DevBuf<int4> d_fz_ia;
-  DevBuf<float4> d_fz_c32;
-
-  // tables
-  bool have_opacity = false;
-  DevBuf<unsigned char> d_opac, d_cdf, d_cdf_coarse;
-  int n_coarse = 0;
-  int chunk_zones = 0;  // zones per opacity-build pass (bounds the FP64/LTE scratch)
-  int opacity_launches = 0;
-  DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_epsl64, d_epsf64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
-      d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
-  DevBuf<int32_t> d_solve_err;
-
-  // tallies
-  DevBuf<double> d_J, d_e_abs, d_e_rad, d_fx, d_fy, d_fz, d_fr, d_flux, d_click;
-  DevBuf<unsigned long long> d_counters;
-  int64_t nspec = 0;
-
-  // per-packet records
-  int record = 0;
-  int64_t n_rec = 0;
-  DevBuf<int32_t> d_rec_fate, d_rec_ind, d_rec_draws;
-  DevBuf<double> d_rec_state;
-};
-
-namespace {
-
-int set_err(sed_ctx* c, int code, const char* fmt, ...)
-{
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  if (c) c->err = buf;
-  return code;
-}
-
-#define CK(call)                                                                                       \
-  do {                                                                                                 \
-    cudaError_t e_ = (call);                                                                           \
-    if (e_ != cudaSuccess)                                                                             \
-      return set_err(c, e_ == cudaErrorMemoryAllocation ? SED_ERR_NOMEM : SED_ERR_CUDA, "%s: %s (%s:%d)", \
-                     #call, cudaGetErrorString(e_), __FILE__, __LINE__);                               \
-  } while (0)
-
-template <typename T>
-cudaError_t upload(sed_ctx* c, DevBuf<T>& b, const T* src, size_t n)
-{
-  cudaError_t e = b.resize(n ? n : 1);
-  if (e != cudaSuccess) return e;
-  if (n && src) return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream);
-  return cudaMemsetAsync(b.p, 0, (n ? n : 1) * sizeof(T), c->stream);
-}
-
-// n elements from src, or n zeros when the caller passed no array
-template <typename T>
-cudaError_t upload_or_zero(sed_ctx* c, DevBuf<T>& b, const T* src, size_t n)
-{
-  cudaError_t e = b.resize(n ? n : 1);
-  if (e != cudaSuccess) return e;
-  if (src) return cudaMemcpyAsync(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream);
-  return cudaMemsetAsync(b.p, 0, (n ? n : 1) * sizeof(T), c->stream);
-}
-
-DevLoc dev_loc(const HostLoc& h, const DevBuf<double>& d)
-{
-  DevLoc g;
-  g.n = h.n();
-  g.type = h.type;
-  g.min = h.min;
-  g.del = h.del;
-  g.right = d.p;
-  g.inv_step = 0.f;
-  if (h.type == LOC_LOG && h.del > 0) g.inv_step = (float)(1.0 / std::log2(1.0 + h.del));
-  else if (h.type == LOC_LIN && h.del > 0) g.inv_step = (float)(1.0 / h.del);
-  g.pad_ = 0;
-  return g;
-}
-
-bool valid_grid(const sed_locate_grid& g) { return g.n > 0 && g.right != nullptr; }
 
 int alloc_tallies(sed_ctx* c)
 {
@@ -272,6 +94,30 @@ int alloc_lte(sed_ctx* c)
 
 }  // namespace
 
+
+// core emission CDF, transport::setup_core_emission (src/transport/transport_init.cpp:465-556)
+std::vector<double> sed::core_emission_cdf(const HostLoc& nug, double T)
+{
+  const int nn = nug.n();
+  std::vector<double> cdf(nn);
+  for (int j = 0; j < nn; ++j) {
+    const double nu = nug.center(j), dnu = nug.delta(j);
+    double bb;
+    if (T <= 0) bb = 1;
+    else {
+      const double zeta = H_PLANCK * nu / K_BOLTZ / T;
+      bb = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (std::exp(zeta) - 1);
+    }
+    const double w = bb * dnu * 1.0;
+    cdf[j] = (j == 0) ? w : cdf[j - 1] + w;
+  }
+  for (int j = 0; j < nn; ++j) if (std::isnan(cdf[j])) cdf[j] = 0;
+  if (cdf[nn - 1] == 0) for (int j = 0; j < nn; ++j) cdf[j] = 1.0;
+  const double N = cdf[nn - 1];
+  for (int j = 0; j < nn; ++j) cdf[j] /= N;
+  return cdf;
+}
+
 extern "C" {
 
 const char* sed_version(void) { return "sedona-b200 transport 0.1 (sm_100a)"; }
@@ -305,24 +151,7 @@ int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
   CK(upload(c, c->d_sn, c->sn.x.data(), c->sn.x.size()));
   CK(upload(c, c->d_sm, c->sm.x.data(), c->sm.x.size()));
   CK(upload(c, c->d_sp, c->sp.x.data(), c->sp.x.size()));
-  // core emission CDF, transport::setup_core_emission (src/transport/transport_init.cpp:465-556)
-  const int nn = c->nu.n();
-  std::vector<double> cdf(nn);
-  for (int j = 0; j < nn; ++j) {
-    const double nu = c->nu.center(j), dnu = c->nu.delta(j);
-    double bb;
-    if (p->core_temperature <= 0) bb = 1;
-    else {
-      const double zeta = H_PLANCK * nu / K_BOLTZ / p->core_temperature;
-      bb = 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (std::exp(zeta) - 1);
-    }
-    const double w = bb * dnu * 1.0;
-    cdf[j] = (j == 0) ? w : cdf[j - 1] + w;
-  }
-  for (int j = 0; j < nn; ++j) if (std::isnan(cdf[j])) cdf[j] = 0;
-  if (cdf[nn - 1] == 0) for (int j = 0; j < nn; ++j) cdf[j] = 1.0;
-  const double N = cdf[nn - 1];
-  for (int j = 0; j < nn; ++j) cdf[j] /= N;
+  const std::vector<double> cdf = core_emission_cdf(c->nu, p->core_temperature);
   CK(upload(c, c->d_core_cdf, cdf.data(), cdf.size()));
   c->nspec = (int64_t)c->st.n() * c->sn.n() * c->sm.n() * c->sp.n();
   CK(c->d_flux.resize(c->nspec));
@@ -540,7 +369,9 @@ int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
   return SED_OK;
 }
 
-int sed_set_opacity(sed_ctx* c, double dt)
+}  // extern "C"
+
+int sed::enqueue_opacity(sed_ctx* c, double dt)
 {
   if (!c) return SED_ERR_ARG;
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_set_opacity: no grid");
@@ -608,6 +439,16 @@ int sed_set_opacity(sed_ctx* c, double dt)
     if (nl < 0) return set_err(c, SED_ERR_CUDA, "sed_set_opacity: opacity kernel configuration rejected");
     c->opacity_launches += nl;
   }
+  return SED_OK;
+}
+
+extern "C" {
+
+int sed_set_opacity(sed_ctx* c, double dt)
+{
+  if (!c) return SED_ERR_ARG;
+  int rc = enqueue_opacity(c, dt);
+  if (rc) return rc;
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_opacity = true;

@@ -19,6 +19,8 @@ struct GridDev {
   DevLoc ax[3];       // 3D axes
 };
 
+struct BatchModel;
+
 // counters[] slots written by the packet kernel
 enum Counter { C_QUEUE = 0, C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT, C_COUNT };
 
@@ -48,12 +50,42 @@ struct StepArgs {
   unsigned long long* counters;  // [C_COUNT]
   int32_t *rec_fate, *rec_ind, *rec_draws;  // optional per-packet records
   double* rec_state;
+  // ---- batch of independent 1D models (batched kernels only) ----
+  const BatchModel* models;         // [n_models], ordered by pkt_off
+  int32_t n_models;
+  int32_t queue_chunk;               // packets a thread claims per queue pop
+  const int4* zone_nbr;              // [zones] {inner neighbour or -1, outer or -2, no-inner flag, model}
+  const double* zone_rin;            // [zones] inner wall after the core substitution
+  unsigned long long* model_escaped; // [n_models] escaped packets per model
+  uint32_t* step_dev;                // step counter on the device (advanced by the finish kernel)
+};
+
+// One model of a batch: its packets are global queue entries
+// [pkt_off, pkt_off + n_packets), its zones [zone_off, zone_off + n_zones)
+// of the concatenated zone arrays, its spectrum at flux + spec_off.
+struct BatchModel {
+  int64_t pkt_off, n_packets, first_pid, spec_off;
+  int32_t zone_off, n_zones;
+  uint32_t seed, emit_draws;         // Philox key; deviates drawn by the emission
+  double r_min, core_radius, Ep;
+  const double* core_cdf;            // [n_nu] normalised core emission CDF
 };
 
 // launches the persistent packet kernel; returns the number of launches
 int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s);
 // zone-scalar tally normalisation (reduce_radiation) and steady-state rescale
 int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_t nspec, cudaStream_t s);
+
+// Batched packet kernel: compiled shapes {threads per block, min blocks per
+// SM} selectable at run time (the autotuner times each).  `blocks_per_sm`
+// 0 = as many as fit.
+constexpr int BATCH_VARIANTS = 4;
+void batch_variant_shape(int variant, int* threads, int* min_blocks);
+int launch_propagate_batch(const StepArgs& a, const GridDev& g, int variant, int blocks_per_sm, int num_sms,
+                           int64_t total_packets, cudaStream_t s);
+// per-model steady-state rescale of the spectra, per-zone normalisation with
+// the zone's model factor, then the device step counter advances
+int launch_finish_batch(const StepArgs& a, const double* vol, int nz_total, int64_t nspec, cudaStream_t s);
 
 // ---------------------------------------------------------------- opacity
 struct OpacityArgs {

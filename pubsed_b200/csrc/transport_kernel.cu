@@ -176,6 +176,73 @@ __device__ __forceinline__ void comoving_to_lab(const GridDev& G, Pkt& p)
   p.D[2] /= norm;
 }
 
+// ----------------------------------------------------------- batches
+// get_next_zone of grid_1D_sphere for a zone of one model of a batch.  The
+// model's walls sit in the concatenated r_out array; per zone the host has
+// precomputed what the reference derives from the zone index, r_min and the
+// core radius (grid_1D_sphere.cpp:527-546): the inner wall after the core
+// substitution, the inner neighbour (-1 at the core or the model's first
+// zone), the outer neighbour (-2 past the model's last zone) and whether
+// zone 0 starts at r = 0.  Values and branches are the single-model ones.
+__device__ __forceinline__ int get_next_zone_batch(const StepArgs& A, const GridDev& G, const double* x, const double* D,
+                                                   int i, double* l)
+{
+  const double rsq = (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  const double xdotD = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]);
+  const double r_o = __ldg(G.r_out.right + i);
+  const double l_out = -1 * xdotD + sqrt(xdotD * xdotD + r_o * r_o - rsq);
+  const int4 nb = __ldg(A.zone_nbr + i);
+  const double r_in = __ldg(A.zone_rin + i);
+  double l_in;
+  if (nb.z) l_in = -1;
+  else {
+    const double rad = xdotD * xdotD + r_in * r_in - rsq;
+    l_in = (rad < 0) ? -1 : -1 * xdotD - sqrt(rad);
+  }
+  const double tiny_offset = 1 + 1e-6;
+  int ind;
+  if ((l_out < l_in) || (l_in < 0)) {
+    ind = nb.y;
+    *l = (ind == -2) ? l_out / tiny_offset : l_out * tiny_offset;
+  } else {
+    ind = nb.x;
+    *l = (ind == -1) ? l_in / tiny_offset : l_in * tiny_offset;
+  }
+  return ind;
+}
+
+// model holding global queue entry `q`: the last model whose first entry is
+// at or before q (models without packets share their successor's offset)
+__device__ __forceinline__ int find_model(const BatchModel* __restrict__ M, int n, int64_t q)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if ((int64_t)__ldg(reinterpret_cast<const long long*>(&M[mid].pkt_off)) <= q) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo - 1;
+}
+
+// grid_1D_sphere::get_zone over one model's slice of the walls
+struct BatchZoneOf {
+  DevLoc slice;  // n = model zones, min = r_min, right = first wall of the model
+  int zone_off;
+  __device__ int operator()(const double* x) const
+  {
+    const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    if (r < slice.min) return -1;
+    if (r >= __ldg(slice.right + slice.n - 1)) return -2;
+    return zone_off + loc_within(slice, r);
+  }
+};
+
+template <int GRID>
+struct GridZoneOf {
+  const GridDev& G;
+  __device__ int operator()(const double* x) const { return get_zone<GRID>(G, x); }
+};
+
 template <typename CT>
 __device__ __forceinline__ int cdf_sample(const CT* __restrict__ y, int n, double u)
 {
@@ -226,11 +293,13 @@ __device__ __forceinline__ void isotropic_scatter(const StepArgs& A, const GridD
   p.nu = p.nu * vd_out;
 }
 
-// transport::emit_inner_source for one packet (emission.cpp:395-480)
-template <int GRID>
-__device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng)
+// transport::emit_inner_source for one packet (emission.cpp:395-480).  The
+// source (core radius, packet energy, core CDF) and the zone lookup are
+// arguments so one model of a batch can supply its own.
+template <int GRID, class ZoneOf>
+__device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng, double rc,
+                                          double Ep, const double* core_cdf, const ZoneOf& zone_of)
 {
-  const double rc = A.core_radius;
   if (rc == 0) {
     p.x[0] = p.x[1] = p.x[2] = 0;
     const double mu = 1 - 2.0 * rng.next();
@@ -261,14 +330,14 @@ __device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, P
     p.D[1] = cost * sinp * D_xl + cosp * D_yl + sint * sinp * D_zl;
     p.D[2] = -sint * D_xl + cost * D_zl;
   }
-  p.e = A.Ep;
+  p.e = Ep;
   if (A.core_freq > 0) p.nu = A.core_freq;
   else {
-    const int inu = cdf_sample<double>(A.core_cdf, A.nu.n, rng.next());
+    const int inu = cdf_sample<double>(core_cdf, A.nu.n, rng.next());
     p.nu = loc_sample(A.nu, inu, rng.next());
     p.e /= 1.0;  // emissivity_weight_ is 1 (transport_init.cpp:322-332)
   }
-  p.ind = get_zone<GRID>(G, p.x);
+  p.ind = zone_of(p.x);
   // the reference asserts p.ind >= 0 here (relativity.cpp:86); homologous
   // velocities do not depend on the zone, other velocity fields need one
   if (G.homologous || p.ind >= 0) comoving_to_lab<GRID>(G, p);
@@ -276,7 +345,8 @@ __device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, P
 }
 
 // spectrum_array::count (src/transport/spectrum_array.cpp:215-246)
-__device__ __forceinline__ void spectrum_count(const StepArgs& A, double t, double w, double E, const double* D)
+__device__ __forceinline__ void spectrum_count(const StepArgs& A, double* flux, double* click, double t, double w,
+                                               double E, const double* D)
 {
   const double mu = D[2];
   double phi = atan2(D[1], D[0]);
@@ -290,8 +360,8 @@ __device__ __forceinline__ void spectrum_count(const StepArgs& A, double t, doub
   if ((t_bin < 0) || (m_bin < 0) || (p_bin < 0)) return;
   if (t_bin >= A.st.n || m_bin >= A.sm.n || p_bin >= A.sp.n) return;
   const int64_t ind = t_bin * A.a1 + l_bin * A.a2 + m_bin * A.a3 + p_bin;
-  atomicAdd(A.flux + ind, E);
-  atomicAdd(A.click + ind, 1.0);
+  atomicAdd(flux + ind, E);
+  atomicAdd(click + ind, 1.0);
 }
 
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
@@ -312,8 +382,13 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 #define SED_PROP_MINB 8
 #endif
 
-template <int GRID, typename OT, typename CT>
-__global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_kernel(const StepArgs A, const GridDev G)
+// BATCH = 1: the queue spans every packet of a batch of 1D models; a thread
+// claims `queue_chunk` consecutive entries per pop, finds each entry's model
+// and emits the packet from that model's source, Philox key and stream id;
+// zone walks use the per-zone neighbour tables.  The step number is read
+// from device memory so a captured graph can be replayed step after step.
+template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs A, const GridDev G)
 {
   extern __shared__ double s_tal[];  // [5][nz] when A.smem_zones
   const int nz = G.nzones;
@@ -330,7 +405,14 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
   double* t_fr = A.smem_zones ? s_tal + 4 * nz : A.fr;
   const OT* __restrict__ opac = reinterpret_cast<const OT*>(A.opac);
   const int64_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
-  const uint32_t K = (A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u;
+  uint32_t K = (A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u;
+  uint32_t step = A.step;
+  if constexpr (BATCH) step = *A.step_dev;
+  // batch: claimed queue entries [q_next, q_end), the current packet's model,
+  // and escapes counted per model until the model changes
+  int64_t q_next = 0, q_end = 0;
+  int m = 0, esc_model = -1;
+  unsigned long long esc_count = 0;
 
   unsigned long long n_esc = 0, n_abs = 0, n_stop = 0, n_seg = 0, n_scat = 0, n_lim = 0;
   // One loop iteration is either one segment of the lane's packet or, when
@@ -363,7 +445,18 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
         n_seg += seg;
         if (fate == ESCAPED) {
           const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
-          spectrum_count(A, t_obs, p.nu, p.e, p.D);
+          if constexpr (BATCH) {
+            const int64_t so = A.models[m].spec_off;
+            spectrum_count(A, A.flux + so, A.click + so, t_obs, p.nu, p.e, p.D);
+            if (m != esc_model) {
+              if (esc_model >= 0) atomicAdd(A.model_escaped + esc_model, esc_count);
+              esc_model = m;
+              esc_count = 0;
+            }
+            ++esc_count;
+          } else {
+            spectrum_count(A, A.flux, A.click, t_obs, p.nu, p.e, p.D);
+          }
           p.t = t_obs;
           ++n_esc;
         } else if (fate == ABSORBED) {
@@ -382,13 +475,34 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
         }
         have = false;
       }
-      pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
-      if (pid >= (unsigned long long)A.n_packets) break;
-      rng.init(A.seed, (uint64_t)A.first_pid + pid, A.step, 0);
-      emit_core<GRID>(A, G, p, rng);
-      // transport::propagate (transport.cpp:202-254)
+      if constexpr (BATCH) {
+        if (q_next >= q_end) {
+          q_next = (int64_t)atomicAdd(A.counters + C_QUEUE, (unsigned long long)A.queue_chunk);
+          q_end = q_next + A.queue_chunk;
+          if (q_end > A.n_packets) q_end = A.n_packets;
+        }
+        if (q_next >= A.n_packets) break;
+        pid = (unsigned long long)q_next++;
+        m = find_model(A.models, A.n_models, (int64_t)pid);
+        const BatchModel& M = A.models[m];
+        K = M.emit_draws;
+        rng.init(M.seed, (uint64_t)(M.first_pid + ((int64_t)pid - M.pkt_off)), step, 0);
+        BatchZoneOf zf;
+        zf.slice = G.r_out;
+        zf.slice.n = M.n_zones;
+        zf.slice.min = M.r_min;
+        zf.slice.right = G.r_out.right + M.zone_off;
+        zf.zone_off = M.zone_off;
+        emit_core<GRID>(A, G, p, rng, M.core_radius, M.Ep, M.core_cdf, zf);
+      } else {
+        pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
+        if (pid >= (unsigned long long)A.n_packets) break;
+        rng.init(A.seed, (uint64_t)A.first_pid + pid, step, 0);
+        emit_core<GRID>(A, G, p, rng, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<GRID>{G});
+      }
+      // transport::propagate (transport.cpp:202-254): its get_zone of the
+      // emitted position is the p.ind emit_core set (x has not moved since)
       fate = MOVING;
-      p.ind = get_zone<GRID>(G, p.x);
       if (p.ind == -1) fate = ABSORBED;
       else if (p.ind == -2) fate = ESCAPED;
       seg = 0;
@@ -415,7 +529,9 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
         acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
       }
       double d_bn = 0;
-      int new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, &d_bn);
+      int new_ind;
+      if constexpr (BATCH) new_ind = get_next_zone_batch(A, G, p.x, p.D, iz, &d_bn);
+      else new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, &d_bn);
       const double dshift = dshift_lab_to_comoving<GRID>(G, p);
       // transport::get_opacity (transport_opacity.cpp:268-299)
       const double nu_cmf = p.nu * dshift;
@@ -485,6 +601,9 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
       }
     }
   }
+  if constexpr (BATCH) {
+    if (esc_model >= 0 && esc_count) atomicAdd(A.model_escaped + esc_model, esc_count);
+  }
   // counters: warp reduction, one atomic per warp
   n_esc = warp_sum(n_esc); n_abs = warp_sum(n_abs); n_stop = warp_sum(n_stop);
   n_seg = warp_sum(n_seg); n_scat = warp_sum(n_scat); n_lim = warp_sum(n_lim);
@@ -506,22 +625,15 @@ __global__ void __launch_bounds__(SED_PROP_THREADS, SED_PROP_MINB) propagate_ker
   }
 }
 
-// reduce_radiation normalisation (src/transport/transport_mpi.cpp:415-441),
-// preceded by the steady-state luminosity rescale (transport.cpp:94-115) whose
-// factor is formed on the device from the escape counter.  One block per zone.
-__global__ void finish_zones_kernel(const StepArgs A, const double* __restrict__ vol, int nz, int64_t n_active,
-                                    int do_rescale)
+// reduce_radiation normalisation (src/transport/transport_mpi.cpp:415-441)
+// of zone iz, after the steady-state luminosity rescale (transport.cpp:94-115)
+// by `fac` when do_rescale.  Run by one block per zone.
+__device__ __forceinline__ void finish_zone(const StepArgs& A, const double* __restrict__ vol, int iz, double fac,
+                                            int do_rescale)
 {
-  const int iz = blockIdx.x;
-  if (iz >= nz) return;
   const int nn = A.nu.n;
   const double dt = A.dt;
   const double v = vol[iz];
-  double fac = 1.0;
-  if (do_rescale) {
-    const double per_esc = (1.0 * (double)A.counters[C_ESCAPED]) / (1.0 * (double)n_active);
-    fac = 1.0 / per_esc;
-  }
   __shared__ double red[256];
   if (A.store_Jnu && nn > 1) {
     double* J = A.J + (size_t)iz * nn;
@@ -554,30 +666,97 @@ __global__ void finish_zones_kernel(const StepArgs A, const double* __restrict__
   }
 }
 
+// steady-state rescale factor L / (escaped energy fraction): transport.cpp:94-115
+__device__ __forceinline__ double rescale_factor(unsigned long long escaped, int64_t n_active)
+{
+  const double per_esc = (1.0 * (double)escaped) / (1.0 * (double)n_active);
+  return 1.0 / per_esc;
+}
+
+// The factor is formed on the device from the escape counter.
+__global__ void finish_zones_kernel(const StepArgs A, const double* __restrict__ vol, int nz, int64_t n_active,
+                                    int do_rescale)
+{
+  const int iz = blockIdx.x;
+  if (iz >= nz) return;
+  const double fac = do_rescale ? rescale_factor(A.counters[C_ESCAPED], n_active) : 1.0;
+  finish_zone(A, vol, iz, fac, do_rescale);
+}
+
 __global__ void rescale_spectrum_kernel(const StepArgs A, int64_t nspec, int64_t n_active)
 {
-  const double per_esc = (1.0 * (double)A.counters[C_ESCAPED]) / (1.0 * (double)n_active);
-  const double fac = 1.0 / per_esc;
+  const double fac = rescale_factor(A.counters[C_ESCAPED], n_active);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nspec; i += (int64_t)gridDim.x * blockDim.x)
     A.flux[i] *= fac;
+}
+
+// Batch: each zone and each spectrum is rescaled with its own model's factor
+// (a model without packets keeps factor 1); the last block to finish is not
+// needed for the step counter, block 0 advances it once everything of the
+// step has been queued before this kernel.
+__global__ void finish_zones_batch_kernel(const StepArgs A, const double* __restrict__ vol, int nz, int do_rescale)
+{
+  const int iz = blockIdx.x;
+  if (iz >= nz) return;
+  double fac = 1.0;
+  if (do_rescale) {
+    const int m = __ldg(A.zone_nbr + iz).w;
+    const int64_t n = A.models[m].n_packets;
+    if (n > 0) fac = rescale_factor(A.model_escaped[m], n);
+  }
+  finish_zone(A, vol, iz, fac, do_rescale);
+  if (iz == 0 && threadIdx.x == 0) *A.step_dev += 1u;
+}
+
+__global__ void rescale_spectrum_batch_kernel(const StepArgs A, int64_t nspec)
+{
+  const int64_t total = nspec * A.n_models;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int m = (int)(i / nspec);
+    const int64_t n = A.models[m].n_packets;
+    if (n > 0) A.flux[i] *= rescale_factor(A.model_escaped[m], n);
+  }
+}
+
+template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB>
+int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
+                    cudaStream_t s)
+{
+  const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
+  auto kern = propagate_kernel<GRID, OT, CT, BATCH, THREADS, MINB>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
+  if (per_sm < 1) per_sm = 1;
+  if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+  int64_t blocks = (int64_t)num_sms * per_sm;
+  const int64_t need = (total + THREADS - 1) / THREADS;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  kern<<<(unsigned)blocks, THREADS, smem, s>>>(a, g);
+  return 1;
 }
 
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
-  const int threads = SED_PROP_THREADS;
-  const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
-  auto kern = propagate_kernel<GRID, OT, CT>;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-  if (per_sm < 1) per_sm = 1;
-  int64_t blocks = (int64_t)num_sms * per_sm;
-  const int64_t need = (a.n_packets + threads - 1) / threads;
-  if (blocks > need) blocks = need;
-  if (blocks < 1) blocks = 1;
-  kern<<<(unsigned)blocks, threads, smem, s>>>(a, g);
-  return 1;
+  return launch_kernel_t<GRID, OT, CT, 0, SED_PROP_THREADS, SED_PROP_MINB>(a, g, 0, num_sms, a.n_packets, s);
+}
+
+// batched kernel shapes {threads, min blocks per SM}: 32 or 24 warps per SM
+// (64 or 80 registers per thread) in blocks of 4 or 8 warps
+constexpr int BATCH_SHAPES[BATCH_VARIANTS][2] = {{128, 8}, {256, 4}, {128, 6}, {256, 3}};
+
+template <typename OT, typename CT>
+int launch_batch_t(const StepArgs& a, const GridDev& g, int variant, int bps, int num_sms, int64_t total,
+                   cudaStream_t s)
+{
+  switch (variant) {
+    case 1: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[1][0], BATCH_SHAPES[1][1]>(a, g, bps, num_sms, total, s);
+    case 2: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[2][0], BATCH_SHAPES[2][1]>(a, g, bps, num_sms, total, s);
+    case 3: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[3][0], BATCH_SHAPES[3][1]>(a, g, bps, num_sms, total, s);
+    default: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[0][0], BATCH_SHAPES[0][1]>(a, g, bps, num_sms, total, s);
+  }
 }
 
 }  // namespace
@@ -601,6 +780,32 @@ int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_
     ++n;
   }
   finish_zones_kernel<<<g.nzones, 256, 0, s>>>(a, vol, g.nzones, a.n_packets, rescale);
+  return n + 1;
+}
+
+void batch_variant_shape(int variant, int* threads, int* min_blocks)
+{
+  if (variant < 0 || variant >= BATCH_VARIANTS) variant = 0;
+  *threads = BATCH_SHAPES[variant][0];
+  *min_blocks = BATCH_SHAPES[variant][1];
+}
+
+int launch_propagate_batch(const StepArgs& a, const GridDev& g, int variant, int blocks_per_sm, int num_sms,
+                           int64_t total_packets, cudaStream_t s)
+{
+  if (a.precision == 0) return launch_batch_t<double2, double>(a, g, variant, blocks_per_sm, num_sms, total_packets, s);
+  return launch_batch_t<float2, float>(a, g, variant, blocks_per_sm, num_sms, total_packets, s);
+}
+
+int launch_finish_batch(const StepArgs& a, const double* vol, int nz_total, int64_t nspec, cudaStream_t s)
+{
+  const int rescale = (a.steady && a.rescale_lum) ? 1 : 0;
+  int n = 0;
+  if (rescale) {
+    rescale_spectrum_batch_kernel<<<148, 256, 0, s>>>(a, nspec);
+    ++n;
+  }
+  finish_zones_batch_kernel<<<nz_total, 256, 0, s>>>(a, vol, nz_total, rescale);
   return n + 1;
 }
 

@@ -378,3 +378,103 @@ def cart3d(n_packets: int = 100_000_000, n_cells: int = 128, n_lines: int = 100_
     return Workload("cart3d", params, zones, atoms,
                     notes={"v_max": v_max, "t_days": t_days, "n_cells": n, "n_lines": n_lines,
                            "sigma": sigma, "corr_cells": corr_cells, "mass_msun": mass_msun, "v_e": v_e})
+
+
+# ---------------------------------------------------------------- batches
+@dataclass
+class BatchWorkload:
+    """Independent 1D models stepped as one batch.  Every model is a complete
+    Workload (so it can also run on its own context); the models share the
+    frequency and spectrum grids, transport and opacity switches, atomic data,
+    element list and grid time, and differ in zones, core source, packet
+    count and Philox key."""
+    name: str
+    models: list
+    notes: dict[str, Any] = field(default_factory=dict)
+
+    @property
+    def n_packets(self) -> int:
+        return int(sum(m.n_packets for m in self.models))
+
+    @property
+    def n_zones(self) -> int:
+        return int(sum(m.zones.n_zones for m in self.models))
+
+
+def batch_model(n_zones: int, n_packets: int, v_max: float, mass_msun: float, atoms: AtomicModel,
+                seed: int, t_days: float = 20.0, v_e_frac: float = 0.125, v_core_frac: float = 0.25,
+                T_core: float = 1.2e4, L_core: float = 1e43, n_bins: int = 2048, spectrum_bins: int = 1024,
+                epsilon: float = 1.0) -> Workload:
+    """One ejecta model of a batch: homologous 1D sphere of `n_zones` zones to
+    v_max at t_days, rho = rho0 exp(-v / v_e) with v_e = v_e_frac v_max and
+    rho0 set by mass_msun, Type Ia-like layers at fixed fractions of v_max
+    (56Ni below 0.15, Si/S/Ca below 0.45, C/O beyond), T linear from 1.2e4 K
+    to 5e3 K, electron scattering + free-free + fuzz line expansion from the
+    shared `atoms`, radiative equilibrium, an absorbing inner boundary at
+    v_core_frac v_max radiating a T_core blackbody of luminosity L_core."""
+    t = t_days * 86400.0
+    v = np.array([(i + 1) * v_max / n_zones for i in range(n_zones)])
+    vc = np.concatenate([[0.0], v[:-1]]) * 0.5 + v * 0.5
+    Z = [e[0] for e in IA_ELEMENTS]
+    A = [e[1] for e in IA_ELEMENTS]
+    X = np.zeros((n_zones, len(Z)))
+    layers = [(0.15 * v_max, IA_LAYERS[0][1]), (0.45 * v_max, IA_LAYERS[1][1]), (math.inf, IA_LAYERS[2][1])]
+    for i in range(n_zones):
+        for vu, frac in layers:
+            if vc[i] < vu:
+                X[i] = frac
+                break
+    T = np.array([1.2e4 + (5e3 - 1.2e4) * i / max(n_zones - 1, 1) for i in range(n_zones)])
+    shape = np.exp(-vc / (v_e_frac * v_max))
+    z0 = sphere_model(v, t, shape, T, X, Z, A)
+    rho0 = mass_msun * M_SUN / float(np.sum(shape * z0.vol))
+    z = sphere_model(v, t, rho0 * shape, T, X, Z, A)
+    d = log_delta_for_bins(1e14, 3e15, n_bins)
+    ds = log_delta_for_bins(1e14, 3e15, spectrum_bins)
+    params = {
+        "grid_type": "grid_1D_sphere", "hydro_module": "homologous",
+        "transport_nu_grid": [1e14, 3e15, d, 1], "spectrum_nu_grid": [1e14, 3e15, ds, 1],
+        "transport_steady_iterate": 1, "transport_radiative_equilibrium": 1,
+        "opacity_grey_opacity": 0, "opacity_epsilon": epsilon,
+        "opacity_electron_scattering": 1, "opacity_fuzz_expansion": 1, "opacity_free_free": 1,
+        "dont_decay_composition": 1,
+        "core_n_emit": int(n_packets), "core_radius": float(v_core_frac * v_max * t),
+        "core_temperature": float(T_core), "core_luminosity": float(L_core),
+        "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
+        "particles_max_total": max(int(1e7), int(n_packets)),
+    }
+    return Workload("batch_model", params, z, atoms,
+                    notes={"v_max": v_max, "t_days": t_days, "mass_msun": mass_msun, "n_lines": atoms.n_fuzz()})
+
+
+def batch64(n_models: int = 64, zones: tuple = (64, 512), packets: tuple = (1e5, 1e7), v_max: tuple = (5e8, 2e9),
+            mass_msun: tuple = (0.2, 1.0), n_lines: int = 30_000, n_bins: int = 2048, packet_scale: float = 1.0,
+            n_levels_per_ion: int = 20, seed: int = 0, data_seed: int = 0) -> BatchWorkload:
+    """Batching configuration: `n_models` independent 1D ejecta models, zone
+    counts uniform in zones[0]..zones[1], packet counts log-uniform in
+    packets[0]..packets[1] (times packet_scale), v_max uniform in
+    v_max[0]..v_max[1] cm/s, each with a seeded exponential density (mass
+    uniform in mass_msun) and electron-scattering + line opacity from one
+    shared synthetic fuzz list of n_lines lines.  Model m uses Philox key
+    seed + m.  Open choices fixed here: t = 20 d for every model (one grid
+    time per batch), v_e = v_max / 8, layers and temperatures as in
+    batch_model, core T uniform 1.0e4-1.5e4 K and L log-uniform 0.5e43-2e43
+    erg/s, 3e4 lines (a model then costs ~300 segments per packet, most of
+    them zone and frequency-bin crossings)."""
+    rng = np.random.default_rng(data_seed)
+    Z = [e[0] for e in IA_ELEMENTS]
+    atoms = synthetic_atoms(Z, n_levels_per_ion, 0, rng)
+    add_fuzz_lines(atoms, n_lines, 1000.0, 30000.0, 1e-4, 1.0, 10.0, rng)
+    models = []
+    for m in range(n_models):
+        nz = int(rng.integers(zones[0], zones[1] + 1))
+        npk = int(10 ** rng.uniform(math.log10(packets[0]), math.log10(packets[1])))
+        npk = max(1, int(npk * packet_scale))
+        vm = float(rng.uniform(v_max[0], v_max[1]))
+        ms = float(rng.uniform(mass_msun[0], mass_msun[1]))
+        Tc = float(rng.uniform(1.0e4, 1.5e4))
+        Lc = float(10 ** rng.uniform(math.log10(0.5e43), math.log10(2e43)))
+        models.append(batch_model(nz, npk, vm, ms, atoms, seed + m, T_core=Tc, L_core=Lc, n_bins=n_bins))
+    return BatchWorkload("batch64_1d", models,
+                         notes={"n_models": n_models, "n_lines": n_lines, "n_bins": n_bins,
+                                "packet_scale": packet_scale})
