@@ -19,6 +19,12 @@ packets, run through the C ABI (include/sedona_gpu.h).
 Multi-GPU: packets are independent, so N ranks run N independent replicas of
 the step (weak scaling); no collective is on the data path.
 
+--workload batch64 runs the batching configuration: 64 independent 1D models
+(64-512 zones, 1e5-1e7 packets each) stepped as one batch (one opacity build,
+one packet launch, CUDA graphs, autotuned launch shape), against the same
+models run as 64 separate plain-FP64 contexts; its reference arm runs the
+reference once per model on a packet sample.
+
 --workload cart3d runs the 3D configuration instead (128^3 Cartesian cells,
 1e5 lines, 2048 bins, 1e8 packets, 16 mu bins); its reference arm runs the
 reference on a 32^3 grid of the same model (the reference CPU cannot hold the
@@ -34,6 +40,8 @@ import subprocess
 import sys
 import threading
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -134,6 +142,177 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
             "sample_packets_per_s": n_sample / t_sample, "set_opacity_seconds": t_opac}
 
 
+# ------------------------------------------------------------------ batches
+def _chi2_per_dof(fa, ca, fb, cb, min_clicks=10):
+    """chi^2 / dof between two binned spectra, sigma^2 = F^2 / clicks per run,
+    over bins with at least `min_clicks` packets in both."""
+    use = (ca >= min_clicks) & (cb >= min_clicks)
+    if not use.any():
+        return None
+    va = fa[use] ** 2 / ca[use]
+    vb = fb[use] ** 2 / cb[use]
+    return float(np.sum((fa[use] - fb[use]) ** 2 / (va + vb)) / use.sum())
+
+
+def reference_batch(bw, n_sample: int, cores: int) -> dict:
+    """The reference's own transport::step per model on `n_sample` packets
+    (full zones, lines and bins); full-batch time = sum over models of
+    set_opacity + propagation scaled to the model's packet count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+    import run_ref
+    if not run_ref.available():
+        return {"unavailable": "reference harness oracle/_ref/sedona_ref is not built"}
+    total = t_opac_sum = 0.0
+    sample_t = 0.0
+    for w in bw.models:
+        out = run_ref.run(w, "free", n_packets=n_sample, threads=cores, steps=1, timeout=3600)
+        t_step = float(out["step_seconds"][0])
+        t_opac = float(out["set_opacity_seconds"][0])
+        total += t_opac + max(t_step - t_opac, 0.0) * w.n_packets / n_sample
+        t_opac_sum += t_opac
+        sample_t += t_step
+    return {"seconds": total, "set_opacity_seconds": t_opac_sum, "sample_seconds": sample_t}
+
+
+def main_batch(args, rank: int, world: int, local: int):
+    """Batching configuration: 64 independent 1D models in one batch."""
+    from pubsed_b200 import workloads
+    bw = workloads.batch64(packet_scale=args.packet_scale)
+    n_total = bw.n_packets
+    cores = os.cpu_count() or 1
+    n_ref = args.ref_packets or 500
+    cfg = {"workload": bw.name, "n_models": len(bw.models), "zones_total": bw.n_zones,
+           "n_lines": bw.notes["n_lines"], "n_bins": bw.notes["n_bins"], "packets_per_step": n_total}
+    ref_sample = ("transport::step of each of the %d models with %d packets (full zones, lines, bins); batch time = "
+                  "sum over models of set_opacity + propagation scaled to the model's packets" % (len(bw.models), n_ref))
+    if args.impl == "reference":
+        if world > 1 and rank != 0:
+            return
+        r = reference_batch(bw, n_ref, cores)
+        if "unavailable" in r:
+            print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}), flush=True)
+            return
+        v = n_total / r["seconds"]
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+                          "steps": 1, "warmup": 0, "ms_per_step": r["seconds"] * 1e3, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                                           "sample": ref_sample},
+                          "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+
+    import torch
+    from pubsed_b200 import abi, engine
+    from pubsed_b200.batch import BatchEngine
+    torch.cuda.set_device(local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed_batch(precision, steps, warmup, tune=True, clock=False):
+        be = BatchEngine(bw, precision=precision, device=local, graph=True)
+        tuning = be.autotune(0.02) if tune else None
+        for _ in range(warmup):
+            flush.fill_(1.0)
+            be.step(1.0)
+        stats = []
+        clk = ClockSampler(local)
+        with (clk if clock else _Null()):
+            for i in range(steps):
+                flush.fill_(float(i))
+                torch.cuda.synchronize()
+                stats.append(be.step(1.0))
+        return be, stats, tuning, clk
+
+    be, stats, tuning, clk = timed_batch(abi.PREC_MIXED, args.steps, args.warmup, clock=True)
+    ms = sum(s["ms_total"] for s in stats) / len(stats)
+    kern_ms = sum(s["ms_propagate_kernel"] for s in stats) / len(stats)
+    value = n_total / (ms * 1e-3)
+    last = stats[-1]
+    spec_b = [be.spectrum(m) for m in range(len(bw.models))]
+
+    # end to end: every model's zone state host->device, the batched step,
+    # every model's spectrum and zone tallies device->host
+    e2e_t = []
+    h2d = d2h = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h2d = sum(be.set_zone_state(m, w.zones.rho, w.zones.T) for m, w in enumerate(bw.models))
+        be.step(1.0)
+        d2h = 0
+        for m in range(len(bw.models)):
+            f, c = be.spectrum(m)
+            tal = be.tallies(m)
+            d2h += f.nbytes + c.nbytes + sum(v.nbytes for v in tal.values())
+        torch.cuda.synchronize()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e = sum(e2e_t) / len(e2e_t)
+    be.close()
+
+    # the same models as separate contexts, one after another: plain FP64
+    # (the denominator of the mixed/batched target) and mixed precision
+    def separate(precision):
+        tot_ms, specs = 0.0, []
+        for w in bw.models:
+            e = engine.Engine(w, precision=precision, device=local)
+            flush.fill_(1.0)
+            e.step(1.0)
+            flush.fill_(2.0)
+            torch.cuda.synchronize()
+            tot_ms += e.step(1.0)["ms_total"]
+            specs.append(e.spectrum())
+            e.close()
+        return tot_ms, specs
+
+    ms64, spec64 = separate(abi.PREC_FP64)
+    chi2 = [_chi2_per_dof(fb, cb, f6, c6) for (fb, cb), (f6, c6) in zip(spec_b, spec64)]
+    chi2 = [c for c in chi2 if c is not None]
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64 transport / f32 opacity tables", "data": "synthetic",
+           "config": dict(cfg, precision="mixed", batched=True, segments_per_step=last["n_segments"],
+                          l2="flushed between steps (256 MiB write)", tuning=tuning),
+           "ms_opacity": last["ms_opacity"], "ms_transport": last["ms_transport"],
+           "plain_fp64": {"value": n_total / (ms64 * 1e-3), "ms_per_step": ms64,
+                          "form": "64 separate contexts, FP64 tables, one after another"},
+           "chi2_per_dof_vs_plain_fp64": {"median": float(np.median(chi2)) if chi2 else None,
+                                          "max": float(np.max(chi2)) if chi2 else None, "models": len(chi2)},
+           "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+           "e2e": {"value": n_total / e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e * 1e3}}
+    if not args.skip_fp64:
+        ms_sm, _ = separate(abi.PREC_MIXED)
+        out["separate_mixed"] = {"value": n_total / (ms_sm * 1e-3), "ms_per_step": ms_sm}
+        b64, st64, _, _ = timed_batch(abi.PREC_FP64, max(1, min(args.steps, 2)), 1)
+        m64 = sum(s["ms_total"] for s in st64) / len(st64)
+        out["batched_fp64"] = {"value": n_total / (m64 * 1e-3), "ms_per_step": m64}
+        b64.close()
+    b_seg, b_pkt = 16 + 8 + 16 + 16 + 64, 264
+    achieved = (last["n_segments"] * b_seg + n_total * b_pkt) / (kern_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "traffic": None, "kernel": "propagate_kernel (batched)", "kernel_ms": kern_ms,
+                       "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    out["clocks"] = clk.summary()
+    if not args.no_cpu_baseline:
+        try:
+            r = reference_batch(bw, n_ref, cores)
+            out["cpu_baseline"] = ({"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                                    "sample": r["unavailable"]} if "unavailable" in r else
+                                   {"value": n_total / r["seconds"], "unit": UNIT, "cores": cores,
+                                    "kind": "reference", "sample": ref_sample})
+        except Exception as ex:  # report, do not hide
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference",
+                                   "sample": "failed: %s" % str(ex)[:200]}
+    print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -141,7 +320,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d"])
+    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d", "batch64"])
+    ap.add_argument("--packet-scale", type=float, default=1.0, help="batch64: scales every model's packet count")
     ap.add_argument("--cells", type=int, default=128, help="cells per axis of the cart3d workload")
     ap.add_argument("--packets", type=int, default=None)
     ap.add_argument("--ref-packets", type=int, default=None)
@@ -149,6 +329,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     args = ap.parse_args()
     rank, world, local = _env_rank()
+    if args.workload == "batch64":
+        return main_batch(args, rank, world, local)
 
     from pubsed_b200 import workloads
 

@@ -314,6 +314,11 @@ int sed_batch_use_graph(sed_batch* b, int32_t enable);
  * `total` sums the counters over the models. */
 int sed_batch_step(sed_batch* b, double dt, sed_step_stats* total);
 
+/* Replaces the density and gas temperature of one model's zones (what the
+ * next step's opacity build reads; the reference's hydro and temperature
+ * solve update grid->z[i].rho / T_gas between steps).  NULL skips an array. */
+int sed_batch_set_zone_state(sed_batch* b, int32_t model, const double* rho, const double* T_gas);
+
 /* Per-model results, laid out as the single-context getters lay them out. */
 int sed_batch_get_escaped(sed_batch* b, int64_t* n_escaped /* [n_models] */);
 int sed_batch_get_spectrum(sed_batch* b, int32_t model, double* flux, double* click);

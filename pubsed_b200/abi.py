@@ -183,6 +183,7 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
             "batch_set_tuning": ([vp, C.POINTER(BatchTuning)], C.c_int),
             "batch_use_graph": ([vp, C.c_int32], C.c_int),
             "batch_step": ([vp, C.c_double, C.POINTER(StepStats)], C.c_int),
+            "batch_set_zone_state": ([vp, C.c_int32, _dp, _dp], C.c_int),
             "batch_get_escaped": ([vp, i64p], C.c_int),
             "batch_get_spectrum": ([vp, C.c_int32, _dp, _dp], C.c_int),
             "batch_get_zone_tallies": ([vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp], C.c_int),

@@ -93,6 +93,12 @@ class BatchEngine:
         self._check(self.L.sed_batch_step(self.b, dt, C.byref(st)), "sed_batch_step")
         return st.as_dict()
 
+    def set_zone_state(self, m: int, rho=None, T=None) -> int:
+        """Copies model m's density / temperature to the device; returns the bytes copied."""
+        k = abi.Keep()
+        self._check(self.L.sed_batch_set_zone_state(self.b, m, k.d(rho), k.d(T)), "sed_batch_set_zone_state")
+        return int(sum(a.nbytes for a in k.arrays))
+
     def escaped(self) -> np.ndarray:
         out = np.zeros(len(self.bw.models), np.int64)
         self._check(self.L.sed_batch_get_escaped(self.b, out.ctypes.data_as(C.POINTER(C.c_int64))),

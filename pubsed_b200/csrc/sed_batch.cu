@@ -494,6 +494,18 @@ int sed_batch_step(sed_batch* b, double dt, sed_step_stats* st)
   return SED_OK;
 }
 
+int sed_batch_set_zone_state(sed_batch* b, int32_t m, const double* rho, const double* T)
+{
+  if (!b) return SED_ERR_ARG;
+  if (m < 0 || m >= b->n_models) return bset_err(b, SED_ERR_ARG, "model %d out of range", m);
+  sed_ctx* c = b->inner;
+  const size_t zo = (size_t)b->models[m].zone_off, nz = (size_t)b->models[m].n_zones;
+  if (rho) BCK(cudaMemcpyAsync(c->d_rho.p + zo, rho, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (T) BCK(cudaMemcpyAsync(c->d_T.p + zo, T, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  BCK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
 int sed_batch_get_escaped(sed_batch* b, int64_t* n_escaped)
 {
   if (!b || !n_escaped) return SED_ERR_ARG;
