@@ -240,6 +240,39 @@ void sed_ctx_destroy(sed_ctx* ctx);
 /* Library version / build string (never NULL). */
 const char* sed_version(void);
 
+/* Sets the Philox step number the next transport (or weighted forward) of
+ * the context draws with; each step advances it by one.  Runs given the same
+ * step number consume the same deviates (common random numbers), as
+ * transport_fix_rng_seed does for the reference's GSL streams
+ * (src/transport/transport_init.cpp:93-104). */
+int sed_set_rng_step(sed_ctx* ctx, uint32_t step);
+
+/* ------------------------------------------------------------ differentiation
+ * Gradient of the binned emergent spectrum with respect to the absorption
+ * opacity, per zone and frequency band, by path replay.  No counterpart in
+ * the reference (it has no adjoint); the checks are central finite
+ * differences of the weighted forward itself with common random numbers.
+ *
+ * The weighted forward is the same transport step (1D sphere, after
+ * sed_set_opacity or sed_load_opacity) with one change of estimator:
+ * interactions are sampled from the scattering opacity alone and absorption
+ * is a continuous weight exp(-a dshift l) on each segment.  Its expected
+ * spectrum is the reference's (radiative_eq = 0, fleck_alpha = 0, no
+ * steady-state luminosity rescale are required), and for fixed deviates it
+ * is a smooth function of the absorption opacity.  The absorption of zone z
+ * in bin i is multiplied by abs_scale[z * n_bands + band], band = i * n_bands
+ * / n_nu (NULL = all ones); gradients are with respect to those factors.
+ * Spectrum and tallies are read with sed_get_spectrum / sed_get_zone_tallies
+ * (tallies use each segment's average weight). */
+int sed_diff_forward(sed_ctx* ctx, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* stats);
+/* Vector-Jacobian product of the last weighted forward: grad_scale[z * n_bands
+ * + k] = sum_s grad_flux[s] d flux[s] / d abs_scale[z, k].  Replays every
+ * escaped packet from its Philox stream (nothing of its path was stored). */
+int sed_diff_vjp(sed_ctx* ctx, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
+/* Full Jacobian of the last weighted forward: jac[(s * n_zones + z) * n_bands
+ * + k] = d flux[s] / d abs_scale[z, k], s over the n_spec spectrum bins. */
+int sed_diff_jacobian(sed_ctx* ctx, double* jac, sed_step_stats* stats);
+
 /* ------------------------------------------------------------------ batches
  * Many independent 1D spherical ejecta models (grid_1D_sphere, homologous)
  * stepped together: one opacity build over all their zones and ONE packet

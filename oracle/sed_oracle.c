@@ -88,6 +88,11 @@ struct oracle_ctx {
   int32_t *r_fate, *r_ind, *r_draws;
   double* r_state;
   uint32_t step;
+  /* differentiable transport: exact Jacobian of the last weighted forward,
+   * accumulated forward-mode per packet ([nspec][nzones][bands]) */
+  double* jac;
+  int64_t jac_n;
+  int diff_bands;
   char err[256];
 };
 
@@ -1004,8 +1009,9 @@ static void emit_core_packet(const oracle_ctx* o, packet* p, double Ep, double t
   p->t = t_now + draw(o, p) * dt;
 }
 
-/* spectrum_array::count, src/transport/spectrum_array.cpp:215-246 */
-static void spectrum_count(oracle_ctx* o, double t, double w, double E, const double* D)
+/* spectrum_array::count, src/transport/spectrum_array.cpp:215-246; returns
+ * the index counted into, -1 when the packet is dropped */
+static int64_t spectrum_count(oracle_ctx* o, double t, double w, double E, const double* D)
 {
   double mu = D[2];
   double phi = atan2(D[1], D[0]);
@@ -1016,14 +1022,15 @@ static void spectrum_count(oracle_ctx* o, double t, double w, double E, const do
   int p_bin = lg_locate(&o->sp, phi);
   if (l_bin < 0) l_bin = 0;
   if (l_bin >= o->sn.n) l_bin = 0;
-  if ((t_bin < 0) || (l_bin < 0) || (m_bin < 0) || (p_bin < 0)) return;
-  if (t_bin >= o->st.n) return;
-  if (m_bin >= o->sm.n) return;
-  if (p_bin >= o->sp.n) return;
+  if ((t_bin < 0) || (l_bin < 0) || (m_bin < 0) || (p_bin < 0)) return -1;
+  if (t_bin >= o->st.n) return -1;
+  if (m_bin >= o->sm.n) return -1;
+  if (p_bin >= o->sp.n) return -1;
   int64_t a3 = o->sp.n, a2 = (int64_t)o->sm.n * a3, a1 = (int64_t)o->sn.n * a2;
   int64_t ind = t_bin * a1 + l_bin * a2 + m_bin * a3 + p_bin;
   o->flux[ind] += E;
   o->click[ind] += 1;
+  return ind;
 }
 
 /* transport::propagate + propagate_monte_carlo, src/transport/transport.cpp:202-484 */
@@ -1232,6 +1239,215 @@ int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
   return oracle_transport_range(o, dt, 0, (int64_t)(o->tp.core_n_emit / 1.0), 1, st);
 }
 
+/* ---------------------------------------------------------------- differentiation
+ * No reference counterpart.  The weighted forward is propagate() with one
+ * change of estimator: interactions are sampled from the scattering opacity
+ * alone and the absorption a (times abs_scale of the zone's band) is a
+ * continuous weight exp(-a dshift l) on every segment; tallies use the
+ * segment-averaged weight e (1 - exp(-tau_a)) / tau_a.  The derivative of the
+ * escaping energy W with respect to the band factor theta of (zone, band) is
+ * -W sum a0 dshift l over the packet's segments in that (zone, band); here it
+ * is accumulated forward, per packet, into the dense Jacobian. */
+typedef struct {
+  double* acc;     /* [nzones * bands] sum of a0 dshift l of the current packet */
+  int64_t* touched;
+  int64_t n_touched;
+} diff_acc;
+
+static int propagate_weighted(oracle_ctx* o, packet* p, double t_now, double dt, const double* abs_scale,
+                              int n_bands, diff_acc* da, int64_t* nseg, int64_t* nscat)
+{
+  int nn = o->nu.n;
+  int nj = o->tp.store_Jnu ? nn : 1;
+  p->ind = get_zone(o, p->x);
+  if (p->ind == -1) return F_ABSORBED;
+  if (p->ind == -2) return F_ESCAPED;
+  double tstop = t_now + dt;
+  int fate = F_MOVING;
+  int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
+  int64_t seg = 0;
+  while (fate == F_MOVING) {
+    if (seg++ >= limit) { fate = F_STOPPED; break; }
+    int iz = p->ind;
+    double d_bn = 0;
+    int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);
+    double dshift = dshift_lab_to_comoving(o, p);
+    double nu_cmf = p->nu * dshift;
+    int i_nu = lg_locate_wb(&o->nu, nu_cmf);
+    double a0 = o->abs[(size_t)iz * nn + i_nu];
+    double a_opac = a0;
+    double s_opac = 0;
+    if (!o->tp.omit_scattering) s_opac = o->scat[(size_t)iz * nn + i_nu];
+    int band = (int)(((int64_t)i_nu * n_bands) / nn);
+    if (abs_scale) a_opac *= abs_scale[(size_t)iz * n_bands + band];
+    double opac = a_opac + s_opac;
+    double d_nu = lg_delta(&o->nu, i_nu) / p->nu * PC_C / p->dvds;
+    if (p->dvds == 0) d_nu = INFINITY;
+    if (d_nu < 0) d_nu = -1 * d_nu;
+    if (d_nu < d_bn) { d_bn = d_nu; new_ind = p->ind; }
+    double tot_lab = s_opac * dshift;
+    double tau_r = -1.0 * log(1 - draw(o, p));
+    double d_sc = tau_r / tot_lab;
+    if (tot_lab == 0) d_sc = INFINITY;
+    double d_tm = (tstop - p->t) * PC_C;
+    if (o->tp.steady_state) d_tm = INFINITY;
+    int event;
+    double this_d;
+    if ((d_sc < d_bn) && (d_sc < d_tm)) { event = 0; this_d = d_sc; }
+    else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
+    else { event = 2; this_d = d_tm; }
+    double tau_a = a_opac * dshift * this_d;
+    double att = exp(-tau_a);
+    double em1 = expm1(-tau_a);
+    double this_E = (tau_a > 0 ? p->e * (-em1 / tau_a) : p->e) * this_d;
+    if (da) {
+      int64_t key = (int64_t)iz * n_bands + band;
+      if (da->acc[key] == 0) da->touched[da->n_touched++] = key;
+      da->acc[key] += a0 * dshift * this_d;
+    }
+    o->e_abs[iz] += this_E * dshift * a_opac * dshift * o->eps_imc[iz];
+    if (o->tp.store_Jnu) o->J[(size_t)iz * nj + i_nu] += this_E;
+    else o->J[(size_t)iz * nj] += this_E;
+    if (o->tp.tally_forces) {
+      o->fx[iz] += this_E * dshift * opac * p->D[0] * dshift;
+      o->fy[iz] += this_E * dshift * opac * p->D[1] * dshift;
+      o->fz[iz] += this_E * dshift * opac * p->D[2] * dshift;
+      double rr = sqrt(p->x[0] * p->x[0] + p->x[1] * p->x[1] + p->x[2] * p->x[2]);
+      double xdotD = p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2];
+      o->fr[iz] += this_E * dshift * opac * xdotD / rr * dshift;
+    }
+    p->x[0] += this_d * p->D[0];
+    p->x[1] += this_d * p->D[1];
+    p->x[2] += this_d * p->D[2];
+    p->t = p->t + this_d / PC_C;
+    p->e *= att;
+    if (event == 1) {
+      if (new_ind == -1) {
+        if (o->tp.boundary_in_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
+        else { p->ind = new_ind; fate = F_ABSORBED; }
+      } else if (new_ind == -2) {
+        if (o->tp.boundary_out_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
+        else { p->ind = new_ind; fate = F_ESCAPED; }
+      } else {
+        p->ind = new_ind;
+      }
+    } else if (event == 0) {
+      (*nscat)++;
+      isotropic_scatter(o, p, 0);
+    } else {
+      fate = F_STOPPED;
+    }
+  }
+  *nseg += seg;
+  return fate;
+}
+
+int oracle_set_rng_step(oracle_ctx* o, uint32_t step)
+{
+  if (!o) return SED_ERR_ARG;
+  o->step = step;
+  return SED_OK;
+}
+
+int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* st)
+{
+  if (!o || !o->have_grid) return SED_ERR_STATE;
+  if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
+  if (o->gtype != SED_GRID_1D_SPHERE || o->tp.radiative_eq || o->tp.fleck_alpha != 0 ||
+      (o->tp.steady_state && o->tp.core_fix_luminosity))
+    return fail(o, SED_ERR_ARG, "differentiable transport: unsupported configuration");
+  if (n_bands < 1 || n_bands > o->nu.n) return fail(o, SED_ERR_ARG, "bad band count");
+  if (o->tp.steady_state) dt = 1;
+  double t_now = o->t_grid;
+  int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
+  if (n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
+  wipe_tallies(o);
+  memset(o->flux, 0, (size_t)o->nspec * sizeof(double));
+  memset(o->click, 0, (size_t)o->nspec * sizeof(double));
+  size_t nzb = (size_t)o->nzones * (size_t)n_bands;
+  free(o->jac);
+  o->jac_n = o->nspec * (int64_t)nzb;
+  o->jac = (double*)calloc((size_t)o->jac_n, sizeof(double));
+  o->diff_bands = n_bands;
+  diff_acc da;
+  da.acc = (double*)calloc(nzb, sizeof(double));
+  da.touched = (int64_t*)malloc(nzb * sizeof(int64_t));
+  if (!o->jac || !da.acc || !da.touched) { free(da.acc); free(da.touched); return fail(o, SED_ERR_NOMEM, "out of memory"); }
+  double Ep = o->tp.core_luminosity * dt / n_emit;
+  uint32_t K = draws_per_emission(o);
+  if (o->record) {
+    free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state);
+    o->nrec = n_emit;
+    o->r_fate = (int32_t*)calloc((size_t)n_emit + 1, 4);
+    o->r_ind = (int32_t*)calloc((size_t)n_emit + 1, 4);
+    o->r_draws = (int32_t*)calloc((size_t)n_emit + 1, 4);
+    o->r_state = (double*)calloc((size_t)n_emit * 9 + 1, 8);
+  }
+  int64_t nseg = 0, nscat = 0, nesc = 0, nabs = 0, nstop = 0;
+  for (int64_t k = 0; k < n_emit; ++k) {
+    packet p;
+    memset(&p, 0, sizeof p);
+    p.pid = (uint64_t)(o->tp.first_packet_id + k);
+    p.n = 0;
+    emit_core_packet(o, &p, Ep, t_now, dt);
+    p.n = K;
+    da.n_touched = 0;
+    int fate = propagate_weighted(o, &p, t_now, dt, abs_scale, n_bands, &da, &nseg, &nscat);
+    if (fate == F_ESCAPED) {
+      double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / PC_C;
+      int64_t s = spectrum_count(o, t_obs, p.nu, p.e, p.D);
+      if (s >= 0)
+        for (int64_t q = 0; q < da.n_touched; ++q) {
+          int64_t key = da.touched[q];
+          o->jac[s * (int64_t)nzb + key] -= p.e * da.acc[key];
+        }
+      p.t = t_obs;
+      nesc++;
+    } else if (fate == F_ABSORBED) nabs++;
+    else nstop++;
+    for (int64_t q = 0; q < da.n_touched; ++q) da.acc[da.touched[q]] = 0;
+    if (o->record) {
+      o->r_fate[k] = fate; o->r_ind[k] = p.ind; o->r_draws[k] = (int32_t)(p.n - K);
+      double* sv = o->r_state + (size_t)k * 9;
+      sv[0] = p.x[0]; sv[1] = p.x[1]; sv[2] = p.x[2]; sv[3] = p.D[0]; sv[4] = p.D[1]; sv[5] = p.D[2];
+      sv[6] = p.t; sv[7] = p.e; sv[8] = p.nu;
+    }
+  }
+  free(da.acc);
+  free(da.touched);
+  finish_step(o, dt, n_emit, nesc);
+  o->step++;
+  if (st) {
+    memset(st, 0, sizeof *st);
+    st->n_packets = n_emit; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
+    st->n_segments = nseg; st->n_scatters = nscat;
+  }
+  return SED_OK;
+}
+
+int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* st)
+{
+  if (!o || !grad_flux || !grad_scale) return SED_ERR_ARG;
+  if (!o->jac) return fail(o, SED_ERR_STATE, "no weighted forward");
+  size_t nzb = (size_t)o->nzones * (size_t)o->diff_bands;
+  for (size_t q = 0; q < nzb; ++q) grad_scale[q] = 0;
+  for (int64_t s = 0; s < o->nspec; ++s) {
+    if (grad_flux[s] == 0) continue;
+    for (size_t q = 0; q < nzb; ++q) grad_scale[q] += grad_flux[s] * o->jac[(size_t)s * nzb + q];
+  }
+  if (st) memset(st, 0, sizeof *st);
+  return SED_OK;
+}
+
+int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* st)
+{
+  if (!o || !jac) return SED_ERR_ARG;
+  if (!o->jac) return fail(o, SED_ERR_STATE, "no weighted forward");
+  memcpy(jac, o->jac, (size_t)o->jac_n * sizeof(double));
+  if (st) memset(st, 0, sizeof *st);
+  return SED_OK;
+}
+
 int oracle_get_spectrum(oracle_ctx* o, double* flux, double* click)
 {
   if (!o) return SED_ERR_ARG;
@@ -1306,5 +1522,6 @@ void oracle_ctx_destroy(oracle_ctx* o)
     free(o->fuzz_off); free(o->fuzz_ion); free(o->fuzz_bin); free(o->fuzz_nu); free(o->fuzz_gf); free(o->fuzz_El);
   }
   free(o->zero_eps);
+  free(o->jac);
   free(o);
 }

@@ -41,6 +41,12 @@ int oracle_get_packet_records(oracle_ctx* o, int64_t n, int32_t* fate, int32_t* 
 int oracle_get_fuzz_bins(oracle_ctx* o, int32_t* bins);
 /* locate_array::locate / locate_within_bounds on an arbitrary grid (for tests) */
 int oracle_locate(const sed_locate_grid* g, double x);
+/* common random numbers and the differentiable transport (weighted forward,
+ * its exact Jacobian accumulated forward-mode per packet, and the VJP) */
+int oracle_set_rng_step(oracle_ctx* o, uint32_t step);
+int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* stats);
+int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
+int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
 const char* oracle_last_error(oracle_ctx* o);
 /* Philox4x32-10 block and the packet-stream uniform (oracle/philox.h) */
 void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

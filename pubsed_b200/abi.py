@@ -172,6 +172,12 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         sig["transport_range"] = ([vp, C.c_double, C.c_int64, C.c_int64, C.c_int, C.POINTER(StepStats)], C.c_int)
         sig["get_fuzz_bins"] = ([vp, _ip], C.c_int)
         sig["locate"] = ([C.POINTER(LocateGrid), C.c_double], C.c_int)
+    sig.update({
+        "set_rng_step": ([vp, C.c_uint32], C.c_int),
+        "diff_forward": ([vp, C.c_double, _dp, C.c_int32, C.POINTER(StepStats)], C.c_int),
+        "diff_vjp": ([vp, _dp, _dp, C.POINTER(StepStats)], C.c_int),
+        "diff_jacobian": ([vp, _dp, C.POINTER(StepStats)], C.c_int),
+    })
     if prefix == "sed_":
         i64p = C.POINTER(C.c_int64)
         sig.update({

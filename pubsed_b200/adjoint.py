@@ -1,0 +1,136 @@
+"""Gradient of the emergent spectrum with respect to absorption opacity, by
+path replay (sed_diff_* in include/sedona_gpu.h), exposed to torch.
+
+`DiffEngine` drives one context: `forward(theta)` runs the weighted
+transport with the absorption opacity of zone z in frequency band k scaled by
+theta[z, k] and returns the binned emergent spectrum; `vjp(g)` and
+`jacobian()` replay the escaped packets of that forward.
+
+`spectrum_from_absorption(theta, engine, step)` is the same forward as a
+torch.autograd.Function (SpectrumFromAbsorption, from autograd_function()):
+its backward is the path-replay vector-Jacobian product.  `step` fixes the
+Philox step number, so every evaluation with the same step uses the same
+deviates (common random numbers) and the spectrum is a smooth function of
+theta.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .engine import Engine
+
+
+class DiffEngine(Engine):
+    """One context running the weighted forward and its adjoint replay."""
+
+    def __init__(self, workload, n_bands: int, precision: int = abi.PREC_FP64, device: int = 0,
+                 n_packets: Optional[int] = None):
+        super().__init__(workload, precision=precision, device=device, n_packets=n_packets)
+        self.n_bands = int(n_bands)
+        self.forward_id = 0          # increments with every forward
+        self._have_tables = False
+
+    def tables(self, dt: float = 1.0):
+        """Opacity build (sed_set_opacity); the forward runs on these tables."""
+        self.set_opacity(dt)
+        self._have_tables = True
+
+    def forward(self, theta: Optional[np.ndarray] = None, step: Optional[int] = None, dt: float = 1.0):
+        """Weighted forward; returns (flux, click, stats)."""
+        if not self._have_tables:
+            self.tables(dt)
+        if step is not None:
+            self._check(self.L.sed_set_rng_step(self.ctx, int(step) & 0xFFFFFFFF), "sed_set_rng_step")
+        k = abi.Keep()
+        th = None
+        if theta is not None:
+            theta = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+            if theta.size != self.nz * self.n_bands:
+                raise ValueError("theta has %d entries, expected %d x %d" % (theta.size, self.nz, self.n_bands))
+            th = k.d(theta)
+        st = abi.StepStats()
+        self._check(self.L.sed_diff_forward(self.ctx, dt, th, self.n_bands, C.byref(st)), "sed_diff_forward")
+        self.forward_id += 1
+        flux, click = self.spectrum()
+        return flux, click, st.as_dict()
+
+    def vjp(self, grad_flux: np.ndarray) -> np.ndarray:
+        g = np.ascontiguousarray(grad_flux, dtype=np.float64).reshape(-1)
+        if g.size != self.nspec:
+            raise ValueError("grad_flux has %d entries, expected %d" % (g.size, self.nspec))
+        out = np.zeros(self.nz * self.n_bands)
+        st = abi.StepStats()
+        self._check(self.L.sed_diff_vjp(self.ctx, g.ctypes.data_as(abi._dp), out.ctypes.data_as(abi._dp),
+                                        C.byref(st)), "sed_diff_vjp")
+        self.last_replay = st.as_dict()
+        return out.reshape(self.nz, self.n_bands)
+
+    def jacobian(self) -> np.ndarray:
+        out = np.zeros(self.nspec * self.nz * self.n_bands)
+        st = abi.StepStats()
+        self._check(self.L.sed_diff_jacobian(self.ctx, out.ctypes.data_as(abi._dp), C.byref(st)),
+                    "sed_diff_jacobian")
+        self.last_replay = st.as_dict()
+        return out.reshape(self.nspec, self.nz, self.n_bands)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _make_function():
+    torch = _torch()
+
+    class SpectrumFromAbsorption(torch.autograd.Function):
+        """flux = F(theta): the weighted transport's binned emergent spectrum
+        (float64, [n_spec]) as a function of the (zone, band) absorption
+        factors theta ([n_zones, n_bands], float64).  Backward replays the
+        packets of the forward; if another forward ran on the engine since,
+        this forward is run again first (same theta, same step)."""
+
+        @staticmethod
+        def forward(ctx, theta, engine: DiffEngine, step: int):
+            th = theta.detach().to("cpu", torch.float64).numpy()
+            flux, _, _ = engine.forward(th, step=step)
+            ctx.engine = engine
+            ctx.step = step
+            ctx.fid = engine.forward_id
+            ctx.save_for_backward(theta)
+            return torch.from_numpy(flux).to(theta.device)
+
+        @staticmethod
+        def backward(ctx, grad_flux):
+            (theta,) = ctx.saved_tensors
+            eng = ctx.engine
+            if eng.forward_id != ctx.fid:
+                eng.forward(theta.detach().to("cpu", torch.float64).numpy(), step=ctx.step)
+            g = grad_flux.detach().to("cpu", torch.float64).numpy()
+            grad = eng.vjp(g)
+            return torch.from_numpy(grad).to(theta.device, theta.dtype), None, None
+
+    return SpectrumFromAbsorption
+
+
+_FN = None
+
+
+def spectrum_from_absorption(theta, engine: DiffEngine, step: int = 0):
+    """torch entry point: the differentiable spectrum for `theta`."""
+    global _FN
+    if _FN is None:
+        _FN = _make_function()
+    return _FN.apply(theta, engine, step)
+
+
+def autograd_function():
+    """The torch.autograd.Function class SpectrumFromAbsorption (built on
+    first use, so importing this module does not import torch)."""
+    global _FN
+    if _FN is None:
+        _FN = _make_function()
+    return _FN

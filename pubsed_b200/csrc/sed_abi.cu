@@ -95,6 +95,51 @@ int alloc_lte(sed_ctx* c)
 }  // namespace
 
 
+// Kernel arguments of a transport step of this context (transport.cpp:46-124):
+// switches, packet count and energy (emission.cpp:383-392), grids, tables
+// and tallies; per-packet records are left off.
+StepArgs sed::make_step_args(sed_ctx* c, double dt, int64_t n_emit)
+{
+  const size_t nz = (size_t)c->nz;
+  StepArgs A{};
+  A.steady = c->tp.steady_state; A.radiative_eq = c->tp.radiative_eq;
+  A.bound_in_reflect = c->tp.boundary_in_reflect; A.bound_out_reflect = c->tp.boundary_out_reflect;
+  A.store_Jnu = c->tp.store_Jnu; A.omit_scat = c->tp.omit_scattering; A.tally_forces = c->tp.tally_forces;
+  A.precision = c->tp.precision; A.seed = c->tp.rng_seed; A.step = c->step;
+  A.n_packets = n_emit;
+  A.first_pid = c->tp.first_packet_id;
+  A.Ep = n_emit > 0 ? c->tp.core_luminosity * dt / n_emit : 0.0;
+  A.t_now = c->t_grid; A.dt = dt; A.tstop = c->t_grid + dt;
+  A.core_radius = c->tp.core_radius; A.core_freq = c->tp.core_photon_frequency; A.core_cdf = c->d_core_cdf.p;
+  A.max_segments = c->tp.max_segments;
+  const size_t zone_smem = (size_t)5 * nz * sizeof(double);
+  A.smem_zones = (zone_smem <= 64 * 1024) ? 1 : 0;
+  A.nu = dev_loc(c->nu, c->d_nu); A.st = dev_loc(c->st, c->d_st); A.sn = dev_loc(c->sn, c->d_sn);
+  A.sm = dev_loc(c->sm, c->d_sm); A.sp = dev_loc(c->sp, c->d_sp);
+  A.a3 = c->sp.n(); A.a2 = (int64_t)c->sm.n() * A.a3; A.a1 = (int64_t)c->sn.n() * A.a2;
+  A.opac = c->d_opac.p; A.cdf = c->d_cdf.p; A.eps_imc = c->d_eps_imc.p;
+  A.cdf_coarse = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
+  A.rescale_lum = c->tp.core_fix_luminosity;
+  A.J = c->d_J.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
+  A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;
+  A.flux = c->d_flux.p; A.click = c->d_click.p; A.counters = c->d_counters.p;
+  return A;
+}
+
+GridDev sed::make_grid_dev(sed_ctx* c)
+{
+  GridDev G{};
+  G.type = c->gtype; G.nzones = c->nz; G.homologous = c->homologous; G.t_grid = c->t_grid;
+  if (c->gtype == SED_GRID_1D_SPHERE) {
+    G.r_out = dev_loc(c->r_out, c->d_r_out);
+    G.v_r = c->d_v_r.p;
+  } else {
+    G.nx = c->nx; G.ny = c->ny; G.nz = c->nzz;
+    for (int a = 0; a < 3; ++a) G.ax[a] = dev_loc(c->ax[a], c->d_ax[a]);
+  }
+  return G;
+}
+
 // core emission CDF, transport::setup_core_emission (src/transport/transport_init.cpp:465-556)
 std::vector<double> sed::core_emission_cdf(const HostLoc& nug, double T)
 {
@@ -522,40 +567,11 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_counters.p, 0, (C_COUNT + 1) * sizeof(unsigned long long), c->stream));
 
-  StepArgs A{};
-  A.steady = c->tp.steady_state; A.radiative_eq = c->tp.radiative_eq;
-  A.bound_in_reflect = c->tp.boundary_in_reflect; A.bound_out_reflect = c->tp.boundary_out_reflect;
-  A.store_Jnu = c->tp.store_Jnu; A.omit_scat = c->tp.omit_scattering; A.tally_forces = c->tp.tally_forces;
-  A.precision = c->tp.precision; A.seed = c->tp.rng_seed; A.step = c->step;
-  A.n_packets = n_emit;
-  A.first_pid = c->tp.first_packet_id;
-  A.Ep = n_emit > 0 ? c->tp.core_luminosity * dt / n_emit : 0.0;
-  A.t_now = c->t_grid; A.dt = dt; A.tstop = c->t_grid + dt;
-  A.core_radius = c->tp.core_radius; A.core_freq = c->tp.core_photon_frequency; A.core_cdf = c->d_core_cdf.p;
-  A.max_segments = c->tp.max_segments;
-  const size_t zone_smem = (size_t)5 * nz * sizeof(double);
-  A.smem_zones = (zone_smem <= 64 * 1024) ? 1 : 0;
-  A.nu = dev_loc(c->nu, c->d_nu); A.st = dev_loc(c->st, c->d_st); A.sn = dev_loc(c->sn, c->d_sn);
-  A.sm = dev_loc(c->sm, c->d_sm); A.sp = dev_loc(c->sp, c->d_sp);
-  A.a3 = c->sp.n(); A.a2 = (int64_t)c->sm.n() * A.a3; A.a1 = (int64_t)c->sn.n() * A.a2;
-  A.opac = c->d_opac.p; A.cdf = c->d_cdf.p; A.eps_imc = c->d_eps_imc.p;
-  A.cdf_coarse = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
-  A.rescale_lum = c->tp.core_fix_luminosity;
-  A.J = c->d_J.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
-  A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;
-  A.flux = c->d_flux.p; A.click = c->d_click.p; A.counters = c->d_counters.p;
+  StepArgs A = make_step_args(c, dt, n_emit);
   if (c->record) {
     A.rec_fate = c->d_rec_fate.p; A.rec_ind = c->d_rec_ind.p; A.rec_draws = c->d_rec_draws.p; A.rec_state = c->d_rec_state.p;
   }
-  GridDev G{};
-  G.type = c->gtype; G.nzones = c->nz; G.homologous = c->homologous; G.t_grid = c->t_grid;
-  if (c->gtype == SED_GRID_1D_SPHERE) {
-    G.r_out = dev_loc(c->r_out, c->d_r_out);
-    G.v_r = c->d_v_r.p;
-  } else {
-    G.nx = c->nx; G.ny = c->ny; G.nz = c->nzz;
-    for (int a = 0; a < 3; ++a) G.ax[a] = dev_loc(c->ax[a], c->d_ax[a]);
-  }
+  const GridDev G = make_grid_dev(c);
   int launches = 0;
   CK(cudaEventRecord(c->ev[3], c->stream));
   if (n_emit > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
@@ -700,11 +716,13 @@ void sed_ctx_destroy(sed_ctx* c)
                            &c->d_eps_imc, &c->d_abs64, &c->d_scat64, &c->d_emis64, &c->d_epsl64, &c->d_epsf64, &c->d_planck, &c->d_ross, &c->d_L,
                            &c->d_n_elec, &c->d_n_dens, &c->d_mass_frac, &c->d_temp_c, &c->d_ion_part, &c->d_ion_frac,
                            &c->d_lev_n, &c->d_boltz, &c->d_J, &c->d_e_abs, &c->d_e_rad, &c->d_fx, &c->d_fy,
-                           &c->d_fz, &c->d_fr, &c->d_flux, &c->d_click, &c->d_rec_state};
+                           &c->d_fz, &c->d_fr, &c->d_flux, &c->d_click, &c->d_rec_state,
+                           &c->d_esc_e, &c->d_abs_scale, &c->d_adj_g, &c->d_adj_out};
   for (auto* b : dbl) b->release();
   DevBuf<int32_t>* ints[] = {&c->d_eZ, &c->d_eA, &c->d_zero_eps_atom, &c->d_ion_off, &c->d_lev_off, &c->d_lev_ion,
                              &c->d_lev_g, &c->d_lev_ic, &c->d_photo_off, &c->d_ion_atom, &c->d_ln_seg,
-                             &c->d_fz_seg, &c->d_lev_atom, &c->d_ln_order, &c->d_fz_order, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind, &c->d_rec_draws};
+                             &c->d_fz_seg, &c->d_lev_atom, &c->d_ln_order, &c->d_fz_order, &c->d_solve_err, &c->d_rec_fate, &c->d_rec_ind, &c->d_rec_draws,
+                             &c->d_esc_bin};
   for (auto* b : ints) b->release();
   c->d_ln_lv.release(); c->d_ln_c.release(); c->d_ln_c32.release(); c->d_fz_ia.release(); c->d_fz_c.release();
   c->d_fz_c32.release();

@@ -132,6 +132,17 @@ struct sed_ctx {
   DevBuf<unsigned long long> d_counters;
   int64_t nspec = 0;
 
+  // differentiable transport: escape records of the last weighted forward
+  // (its Philox step, band count, whether a scale array was applied)
+  bool have_diff = false;
+  uint32_t diff_step = 0;
+  double diff_dt = 1;
+  int diff_bands = 0;
+  bool diff_scaled = false;
+  int64_t diff_n = 0;
+  DevBuf<int32_t> d_esc_bin;
+  DevBuf<double> d_esc_e, d_abs_scale, d_adj_g, d_adj_out;
+
   // per-packet records
   int record = 0;
   int64_t n_rec = 0;
@@ -201,6 +212,10 @@ inline bool valid_grid(const sed_locate_grid& g) { return g.n > 0 && g.right != 
 // (transport::set_opacity) without synchronising; used directly by the
 // batched step, which captures it into a CUDA graph.
 int enqueue_opacity(sed_ctx* c, double dt);
+
+// kernel arguments and device grid of a transport step of this context
+StepArgs make_step_args(sed_ctx* c, double dt, int64_t n_emit);
+GridDev make_grid_dev(sed_ctx* c);
 
 // normalised core emission CDF of a blackbody at T over the bins of `nu`
 // (transport::setup_core_emission, src/transport/transport_init.cpp:465-556)

@@ -58,6 +58,14 @@ struct StepArgs {
   const double* zone_rin;            // [zones] inner wall after the core substitution
   unsigned long long* model_escaped; // [n_models] escaped packets per model
   uint32_t* step_dev;                // step counter on the device (advanced by the finish kernel)
+  // ---- differentiable transport (weighted forward and adjoint replay kernels only) ----
+  const double* abs_scale;           // [nz * n_bands] factor on the absorption opacity, or null
+  int32_t n_bands;                   // band of bin i = i * n_bands / n_nu
+  int32_t adj_jacobian;              // adjoint: 1 = full Jacobian rows, 0 = vector-Jacobian product
+  int32_t* esc_bin;                  // [n_packets] spectrum index of an escaped, counted packet; -1 otherwise
+  double* esc_e;                     // [n_packets] its energy at escape
+  const double* adj_g;               // [nspec] d(loss)/d(flux) for the vector-Jacobian product
+  double* adj_out;                   // VJP [nz * n_bands]; Jacobian [nspec * nz * n_bands]
 };
 
 // One model of a batch: its packets are global queue entries
@@ -75,6 +83,11 @@ struct BatchModel {
 int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s);
 // zone-scalar tally normalisation (reduce_radiation) and steady-state rescale
 int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_t nspec, cudaStream_t s);
+
+// Differentiable transport on a 1D grid: mode 1 = forward with absorption as
+// a continuous weight (interactions sampled from scattering only), mode 2 =
+// adjoint replay of the escaped packets of the last mode-1 launch.
+int launch_propagate_diff(const StepArgs& a, const GridDev& g, int mode, int num_sms, cudaStream_t s);
 
 // Batched packet kernel: compiled shapes {threads per block, min blocks per
 // SM} selectable at run time (the autotuner times each).  `blocks_per_sm`

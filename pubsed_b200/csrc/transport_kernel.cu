@@ -345,8 +345,9 @@ __device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, P
 }
 
 // spectrum_array::count (src/transport/spectrum_array.cpp:215-246)
-__device__ __forceinline__ void spectrum_count(const StepArgs& A, double* flux, double* click, double t, double w,
-                                               double E, const double* D)
+// Returns the spectrum index the packet was counted in, -1 when dropped.
+__device__ __forceinline__ int64_t spectrum_count(const StepArgs& A, double* flux, double* click, double t, double w,
+                                                  double E, const double* D)
 {
   const double mu = D[2];
   double phi = atan2(D[1], D[0]);
@@ -357,11 +358,12 @@ __device__ __forceinline__ void spectrum_count(const StepArgs& A, double* flux, 
   const int p_bin = loc_locate(A.sp, phi);
   if (l_bin < 0) l_bin = 0;
   if (l_bin >= A.sn.n) l_bin = 0;
-  if ((t_bin < 0) || (m_bin < 0) || (p_bin < 0)) return;
-  if (t_bin >= A.st.n || m_bin >= A.sm.n || p_bin >= A.sp.n) return;
+  if ((t_bin < 0) || (m_bin < 0) || (p_bin < 0)) return -1;
+  if (t_bin >= A.st.n || m_bin >= A.sm.n || p_bin >= A.sp.n) return -1;
   const int64_t ind = t_bin * A.a1 + l_bin * A.a2 + m_bin * A.a3 + p_bin;
   atomicAdd(flux + ind, E);
   atomicAdd(click + ind, 1.0);
+  return ind;
 }
 
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
@@ -387,7 +389,16 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 // and emits the packet from that model's source, Philox key and stream id;
 // zone walks use the per-zone neighbour tables.  The step number is read
 // from device memory so a captured graph can be replayed step after step.
-template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB>
+// MODE 0 follows the reference's estimator.  MODE 1 (differentiable
+// forward) samples interactions from the scattering opacity only and carries
+// absorption as a continuous weight exp(-a dshift l) per segment, so for
+// fixed deviates the path does not depend on the absorption opacity and the
+// spectrum is a smooth function of it; tallies use the segment-averaged
+// weight.  MODE 2 replays the escaped packets of a MODE-1 launch (same
+// deviates, same path) and adds -w a0 dshift l per segment into the
+// gradient with respect to the (zone, band) absorption factors, where w is
+// the packet's escaping energy times d(loss)/d(its spectrum bin).
+template <int GRID, typename OT, typename CT, int BATCH, int MODE, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs A, const GridDev G)
 {
   extern __shared__ double s_tal[];  // [5][nz] when A.smem_zones
@@ -413,6 +424,10 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   int64_t q_next = 0, q_end = 0;
   int m = 0, esc_model = -1;
   unsigned long long esc_count = 0;
+  // adjoint replay: the packet's weight and Jacobian row, and the sum over
+  // consecutive segments in one (zone, band) before its atomic add
+  double adj_w = 0, acc_g = 0;
+  int64_t adj_row = 0, acc_key = -1;
 
   unsigned long long n_esc = 0, n_abs = 0, n_stop = 0, n_seg = 0, n_scat = 0, n_lim = 0;
   // One loop iteration is either one segment of the lane's packet or, when
@@ -432,6 +447,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   double acc_eabs = 0, acc_fx = 0, acc_fy = 0, acc_fz = 0, acc_fr = 0;
   for (;;) {
     if (fate != MOVING) {
+      if (have && MODE == 2) {
+        if (acc_key >= 0) atomicAdd(A.adj_out + acc_key, -adj_w * acc_g);
+        n_seg += seg;
+        have = false;
+      }
       if (have) {
         if (acc_zone >= 0) {
           atomicAdd(t_eabs + acc_zone, acc_eabs);
@@ -455,7 +475,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
             }
             ++esc_count;
           } else {
-            spectrum_count(A, A.flux, A.click, t_obs, p.nu, p.e, p.D);
+            const int64_t si = spectrum_count(A, A.flux, A.click, t_obs, p.nu, p.e, p.D);
+            if constexpr (MODE == 1) {
+              A.esc_bin[pid] = (int32_t)si;
+              A.esc_e[pid] = p.e;
+            }
           }
           p.t = t_obs;
           ++n_esc;
@@ -463,6 +487,9 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
           ++n_abs;
         } else {
           ++n_stop;
+        }
+        if constexpr (MODE == 1) {
+          if (fate != ESCAPED) A.esc_bin[pid] = -1;
         }
         if (A.rec_fate) {
           A.rec_fate[pid] = fate;
@@ -497,6 +524,16 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       } else {
         pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
         if (pid >= (unsigned long long)A.n_packets) break;
+        if constexpr (MODE == 2) {
+          // only packets that reached the spectrum carry a gradient
+          const int32_t sb = A.esc_bin[pid];
+          adj_w = 0;
+          if (sb >= 0) adj_w = A.adj_jacobian ? A.esc_e[pid] : A.adj_g[sb] * A.esc_e[pid];
+          if (adj_w == 0) continue;  // fate is not MOVING: pull the next packet
+          adj_row = A.adj_jacobian ? (int64_t)sb * nz * A.n_bands : 0;
+          acc_key = -1;
+          acc_g = 0;
+        }
         rng.init(A.seed, (uint64_t)A.first_pid + pid, step, 0);
         emit_core<GRID>(A, G, p, rng, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<GRID>{G});
       }
@@ -515,7 +552,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       if (seg >= limit) { fate = STOPPED; ++n_lim; continue; }
       ++seg;
       const int iz = p.ind;
-      if (iz != acc_zone) {
+      if (MODE != 2 && iz != acc_zone) {
         if (acc_zone >= 0) {
           atomicAdd(t_eabs + acc_zone, acc_eabs);
           if (A.tally_forces) {
@@ -537,15 +574,20 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       const double nu_cmf = p.nu * dshift;
       const int i_nu = loc_within_fast(A.nu, nu_cmf);
       const OT ab = opac[(size_t)iz * nn + i_nu];
-      const double a_opac = (double)ab.x;
+      double a_opac = (double)ab.x;
       const double s_opac = A.omit_scat ? 0.0 : (double)ab.y;
+      int band = 0;
+      if constexpr (MODE != 0) {
+        band = (int)(((int64_t)i_nu * A.n_bands) / nn);
+        if (A.abs_scale) a_opac *= __ldg(A.abs_scale + (size_t)iz * A.n_bands + band);
+      }
       const double op = a_opac + s_opac;
       const double eps = (op == 0) ? 0 : a_opac / op;
       double d_nu = loc_delta(A.nu, i_nu) / p.nu * C_LIGHT / p.dvds;
       if (p.dvds == 0) d_nu = INFINITY;
       if (d_nu < 0) d_nu = -1 * d_nu;
       if (d_nu < d_bn) { d_bn = d_nu; new_ind = p.ind; }
-      const double tot_lab = op * dshift;
+      const double tot_lab = (MODE == 0 ? op : s_opac) * dshift;
       const double tau_r = -1.0 * log(1 - rng.next());
       double d_sc = tau_r / tot_lab;
       if (tot_lab == 0) d_sc = INFINITY;
@@ -557,11 +599,30 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
       else { event = 2; this_d = d_tm; }
       // tallies (transport.cpp:361-392)
-      const double this_E = p.e * this_d;
+      double this_E = p.e * this_d;
+      double att = 1.0;
+      if constexpr (MODE == 1) {
+        // absorption over the segment: the weight falls by exp(-tau_a); the
+        // tallies use its segment average e (1 - exp(-tau_a)) / tau_a
+        const double tau_a = a_opac * dshift * this_d;
+        att = exp(-tau_a);
+        const double em1 = expm1(-tau_a);
+        this_E = (tau_a > 0 ? p.e * (-em1 / tau_a) : p.e) * this_d;
+      }
+      if constexpr (MODE == 2) {
+        const int64_t key = adj_row + (int64_t)iz * A.n_bands + band;
+        if (key != acc_key) {
+          if (acc_key >= 0) atomicAdd(A.adj_out + acc_key, -adj_w * acc_g);
+          acc_key = key;
+          acc_g = 0;
+        }
+        acc_g += (double)ab.x * dshift * this_d;  // d(theta a0 dshift l) / d theta
+      }
       const double eps_imc = __ldg(A.eps_imc + iz);
-      acc_eabs += this_E * dshift * (op) * eps * dshift * eps_imc;
-      atomicAdd(A.J + (size_t)iz * nj + (A.store_Jnu ? i_nu : 0), this_E);
-      if (A.tally_forces) {
+      if constexpr (MODE == 0) acc_eabs += this_E * dshift * (op) * eps * dshift * eps_imc;
+      if constexpr (MODE == 1) acc_eabs += this_E * dshift * a_opac * dshift * eps_imc;
+      if constexpr (MODE != 2) atomicAdd(A.J + (size_t)iz * nj + (A.store_Jnu ? i_nu : 0), this_E);
+      if (MODE != 2 && A.tally_forces) {
         const double w = this_E * dshift * op;
         acc_fx += w * p.D[0] * dshift;
         acc_fy += w * p.D[1] * dshift;
@@ -574,6 +635,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       p.x[1] += this_d * p.D[1];
       p.x[2] += this_d * p.D[2];
       p.t = p.t + this_d / C_LIGHT;
+      if constexpr (MODE == 1) p.e *= att;
       if (event == 1) {
         if (new_ind == -1) {
           if (A.bound_in_reflect) { p.D[0] *= -1; p.D[1] *= -1; p.D[2] *= -1; }
@@ -590,10 +652,12 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         // one call site keeps a single inlined copy of isotropic_scatter
         ++n_scat;
         int redist = 0;
-        if (!(rng.next() > eps)) {
-          const double z2 = rng.next();
-          if ((z2 > eps_imc) || A.radiative_eq) redist = 1;
-          else fate = ABSORBED;
+        if constexpr (MODE == 0) {
+          if (!(rng.next() > eps)) {
+            const double z2 = rng.next();
+            if ((z2 > eps_imc) || A.radiative_eq) redist = 1;
+            else fate = ABSORBED;
+          }
         }
         if (fate == MOVING) isotropic_scatter<GRID, CT>(A, G, p, rng, redist);
       } else {
@@ -615,7 +679,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
     if (n_scat) atomicAdd(A.counters + C_SCATTERS, n_scat);
     if (n_lim) atomicAdd(A.counters + C_LIMIT, n_lim);
   }
-  if (A.smem_zones) {
+  if (MODE != 2 && A.smem_zones) {
     __syncthreads();
     double* g[5] = {A.e_abs, A.fx, A.fy, A.fz, A.fr};
     for (int i = threadIdx.x; i < 5 * nz; i += blockDim.x) {
@@ -718,12 +782,12 @@ __global__ void rescale_spectrum_batch_kernel(const StepArgs A, int64_t nspec)
   }
 }
 
-template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB>
+template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB, int MODE = 0>
 int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
                     cudaStream_t s)
 {
   const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
-  auto kern = propagate_kernel<GRID, OT, CT, BATCH, THREADS, MINB>;
+  auto kern = propagate_kernel<GRID, OT, CT, BATCH, MODE, THREADS, MINB>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
@@ -781,6 +845,19 @@ int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_
   }
   finish_zones_kernel<<<g.nzones, 256, 0, s>>>(a, vol, g.nzones, a.n_packets, rescale);
   return n + 1;
+}
+
+int launch_propagate_diff(const StepArgs& a, const GridDev& g, int mode, int num_sms, cudaStream_t s)
+{
+  constexpr int T = SED_PROP_THREADS, B = SED_PROP_MINB;
+  if (g.type != 0 || (mode != 1 && mode != 2)) return -1;
+  StepArgs b = a;
+  if (mode == 2) b.smem_zones = 0;  // the replay tallies nothing per zone
+  if (a.precision == 0)
+    return mode == 1 ? launch_kernel_t<0, double2, double, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
+                     : launch_kernel_t<0, double2, double, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
+  return mode == 1 ? launch_kernel_t<0, float2, float, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
+                   : launch_kernel_t<0, float2, float, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
 }
 
 void batch_variant_shape(int variant, int* threads, int* min_blocks)

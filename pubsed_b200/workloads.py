@@ -225,7 +225,7 @@ IA_LAYERS = [  # (v_upper cm/s, mass fractions in IA_ELEMENTS order)
 def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_000, n_bins: int = 4096,
             n_levels_per_ion: int = 20, v_max: float = 3e9, epsilon: float = 1.0, seed: int = 0, data_seed: int = 0,
             bound_free: int = 0, free_free: int = 1, spectrum_bins: int = 1024,
-            v_core: float = 1e9) -> Workload:
+            v_core: float = 1e9, radiative_eq: int = 1) -> Workload:
     """Precision configuration: 1D Type Ia-like ejecta, 256 zones, 1.4 Msun,
     rho ~ exp(-v / 2.7e8 cm/s), t = 20 d, layered 56Ni / Si-S-Ca / C-O
     composition, T falling linearly from 1.2e4 K (inner) to 5e3 K (outer),
@@ -244,7 +244,9 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
     cm/s, absorbing) radiating a 1.2e4 K blackbody with L = 1e43 erg/s;
     opacity_epsilon = 1 (absorptive lines, Sedona's default).  With this line
     list the ejecta are optically thick at every frequency; a central point
-    source costs ~5e4 segments per packet, the inner boundary ~2e3."""
+    source costs ~5e4 segments per packet, the inner boundary ~2e3.
+    radiative_eq = 0 makes absorption final (the form the differentiable
+    transport needs)."""
     rng = np.random.default_rng(data_seed)  # synthetic atoms and lines; `seed` keys the packets
     t = 20 * 86400.0
     v = np.array([(i + 1) * v_max / n_zones for i in range(n_zones)])
@@ -269,7 +271,7 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
     params = {
         "grid_type": "grid_1D_sphere", "hydro_module": "homologous",
         "transport_nu_grid": [1e14, 3e15, d, 1], "spectrum_nu_grid": [1e14, 3e15, ds, 1],
-        "transport_steady_iterate": 1, "transport_radiative_equilibrium": 1,
+        "transport_steady_iterate": 1, "transport_radiative_equilibrium": int(radiative_eq),
         "opacity_grey_opacity": 0, "opacity_epsilon": epsilon,
         "opacity_electron_scattering": 1, "opacity_fuzz_expansion": 1,
         "opacity_free_free": int(free_free), "opacity_bound_free": int(bound_free),

@@ -12,7 +12,7 @@ inputs, plus the reference's outputs:
   locate_kat.json  value/index pairs printed by the reference's own
                  src/utils/locate_array_test.cpp
 
-usage: python tests/golden/make_golden.py
+usage: python tests/golden/make_golden.py [fixture names ...]   (default: all)
 """
 import json
 import os
@@ -43,6 +43,10 @@ FREE_CASES = {
     "free_ia": ("type_ia", dict(n_packets=60000, n_zones=64, n_lines=50000, n_bins=1024, seed=103)),
     "free_cart3d": ("cart3d", dict(n_packets=100000, n_cells=16, n_lines=10000, n_bins=512, spectrum_bins=128,
                                    n_mu=16, seed=109)),
+    # absorption final, lines almost pure scattering: the configuration of the
+    # differentiable (weighted) transport
+    "free_ia_absorb": ("type_ia", dict(n_packets=150000, n_zones=64, n_lines=50000, n_bins=1024, spectrum_bins=256,
+                                       epsilon=1e-4, radiative_eq=0, seed=107)),
 }
 
 KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "J_nu", "e_abs", "e_rad", "fx_rad", "fy_rad", "fz_rad",
@@ -57,7 +61,10 @@ def make_workload(gen: str, kw: dict):
 def main():
     if not run_ref.available():
         raise SystemExit("build the reference harness first: oracle/ref/build_ref.sh")
+    only = set(sys.argv[1:])
     for name, (gen, kw) in CASES.items():
+        if only and name not in only:
+            continue
         w = make_workload(gen, kw)
         out = run_ref.run(w, "replay", threads=1, seed=kw.get("seed", 0))
         arrays = {k: out[k] for k in KEYS}
@@ -67,6 +74,8 @@ def main():
     # free-running reference steps (its own transport::step, OpenMP, streams
     # independent of the per-packet replay streams) for the chi-squared tests
     for name, (gen, kw) in FREE_CASES.items():
+        if only and name not in only:
+            continue
         w = make_workload(gen, kw)
         out = run_ref.run(w, "free", threads=os.cpu_count() or 1, seed=kw.get("seed", 0))
         np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
@@ -76,6 +85,8 @@ def main():
     # locate_array_test: stderr holds "value index" lines, one block of 8
     # values per grid; the first block (20 zero walls, uninitialised minimum)
     # is skipped
+    if only and "locate_kat" not in only:
+        return
     exe = os.path.join(ROOT, "oracle", "_ref", "locate_array_test")
     r = subprocess.run([exe], capture_output=True, text=True, check=True)
     pairs = [ln.split() for ln in r.stderr.strip().splitlines()]

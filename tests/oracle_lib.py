@@ -191,3 +191,50 @@ def check_states(Sg: np.ndarray, So: np.ndarray) -> dict:
     assert q <= STATE_RTOL, out
     assert out["max"] <= STATE_RTOL_MAX, out
     return out
+
+
+# ---------------------------------------------------------------- weighted transport
+def diff_forward(eng: Engine, theta, n_bands: int, step: int = 0) -> dict:
+    """Weighted forward on either library (sed_diff_forward / oracle_diff_forward)
+    at Philox step `step`; returns the step counters."""
+    k = abi.Keep()
+    eng.check(eng.fn("set_rng_step")(eng.ctx, step), "set_rng_step")
+    st = abi.StepStats()
+    eng.check(eng.fn("diff_forward")(eng.ctx, 1.0, k.d(theta), n_bands, C.byref(st)), "diff_forward")
+    return st.as_dict()
+
+
+def diff_jacobian(eng: Engine, n_bands: int) -> np.ndarray:
+    out = np.zeros(eng.nspec * eng.nz * n_bands)
+    eng.check(eng.fn("diff_jacobian")(eng.ctx, out.ctypes.data_as(abi._dp), None), "diff_jacobian")
+    return out.reshape(eng.nspec, eng.nz * n_bands)
+
+
+def diff_vjp(eng: Engine, g: np.ndarray, n_bands: int) -> np.ndarray:
+    out = np.zeros(eng.nz * n_bands)
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    eng.check(eng.fn("diff_vjp")(eng.ctx, g.ctypes.data_as(abi._dp), out.ctypes.data_as(abi._dp), None), "diff_vjp")
+    return out
+
+
+def spectrum_second_moment(eng: Engine, w, n: int) -> tuple:
+    """Per-bin sum of escaping weights and of their squares, from the packet
+    records of a 1-time-bin, 1-mu, 1-phi spectrum (the bin of a record is
+    locate(spectrum nu grid, nu), out-of-range frequencies counted in bin 0 as
+    spectrum_array::count does)."""
+    r = eng.records(n)
+    esc = r["fate"] == abi.FATE_ESCAPED
+    tg, ng, mg, pg = w.spectrum_grids()
+    assert tg.n == 1 and mg.n == 1 and pg.n == 1
+    k = abi.Keep()
+    g = abi.locate_grid(k, ng)
+    loc = oracle_lib().oracle_locate
+    s1 = np.zeros(ng.n)
+    s2 = np.zeros(ng.n)
+    for nu, e in zip(r["state"][esc, 8], r["state"][esc, 7]):
+        b = loc(C.byref(g), float(nu))
+        if b < 0 or b >= ng.n:
+            b = 0
+        s1[b] += e
+        s2[b] += e * e
+    return s1, s2
