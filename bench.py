@@ -25,6 +25,10 @@ one packet launch, CUDA graphs, autotuned launch shape), against the same
 models run as 64 separate plain-FP64 contexts; its reference arm runs the
 reference once per model on a packet sample.
 
+--workload adjoint runs the differentiation configuration: weighted forward +
+path-replay vector-Jacobian product on the 256-zone Type Ia-like model with
+absorption final, and a central-difference check of the adjoint.
+
 --workload cart3d runs the 3D configuration instead (128^3 Cartesian cells,
 1e5 lines, 2048 bins, 1e8 packets, 16 mu bins); its reference arm runs the
 reference on a 32^3 grid of the same model (the reference CPU cannot hold the
@@ -313,6 +317,118 @@ def main_batch(args, rank: int, world: int, local: int):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------ adjoint
+def main_adjoint(args, rank: int, world: int, local: int):
+    """Differentiation configuration: the 256-zone Type Ia-like model with
+    absorption final (radiative_eq = 0, line epsilon 1e-4), 1e7 packets,
+    1024-bin spectrum, 64 frequency bands.  A step is one weighted forward
+    plus the path-replay vector-Jacobian product; --fd-entries checks the
+    adjoint against central differences (relative step 1e-3, common random
+    numbers) on that many random (zone, band) entries."""
+    from pubsed_b200 import workloads
+
+    def wl(n):
+        return workloads.type_ia(n_packets=n, epsilon=1e-4, radiative_eq=0, spectrum_bins=1024)
+    n = args.packets or 10_000_000
+    n_bands = 64
+    cores = os.cpu_count() or 1
+    cfg = {"workload": "type_ia_absorbing_adjoint", "n_zones": 256, "n_lines": 500000, "n_bins": 4096,
+           "spectrum_bins": 1024, "n_bands": n_bands, "packets_per_step": n, "line_epsilon": 1e-4}
+    if args.impl == "reference" or not args.no_cpu_baseline:
+        ref = run_reference(argparse.Namespace(ref_packets=args.ref_packets or 20_000, warmup=1, steps=1,
+                                               packets=n), wl, rank)
+        if args.impl == "reference":
+            if world > 1 and rank != 0:
+                return
+            ref["config"] = dict(cfg, note="reference forward only: it has no adjoint")
+            print(json.dumps(ref), flush=True)
+            return
+    import torch
+    from pubsed_b200 import abi
+    from pubsed_b200.adjoint import DiffEngine
+    torch.cuda.set_device(local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    w = wl(n)
+    eng = DiffEngine(w, n_bands=n_bands, precision=abi.PREC_MIXED, device=local)
+    theta = np.ones((eng.nz, n_bands))
+    g = np.linspace(0.5, 1.5, eng.nspec)
+    clk = ClockSampler(local)
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        eng.forward(theta, step=0)
+        eng.vjp(g)
+    fw, bw, fk = [], [], []
+    with clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            _, _, st = eng.forward(theta, step=i)
+            eng.vjp(g)
+            fw.append(st["ms_total"])
+            fk.append(st["ms_propagate_kernel"])
+            bw.append(eng.last_replay["ms_total"])
+    ms_f, ms_b, ms_k = (sum(x) / len(x) for x in (fw, bw, fk))
+    seg = st["n_segments"]
+    # end to end through the Python/C ABI with host arrays: theta in, spectrum
+    # out, gradient in, theta-gradient out
+    t0 = time.perf_counter()
+    flux, click, _ = eng.forward(theta, step=0)
+    grad = eng.vjp(g)
+    e2e = time.perf_counter() - t0
+    # full Jacobian once, then central differences on random entries
+    eng.forward(theta, step=0)
+    t0 = time.perf_counter()
+    jac = eng.jacobian().reshape(eng.nspec, -1)
+    ms_jac = eng.last_replay["ms_total"]
+    fd = None
+    if args.fd_entries > 0:
+        cols = np.flatnonzero(np.abs(jac).max(axis=0) > 1e-6 * np.abs(jac).max())
+        rng = np.random.default_rng(2024)
+        errs = []
+        flat = theta.reshape(-1)
+        for q in rng.choice(cols, min(args.fd_entries, cols.size), replace=False):
+            tp, tm = flat.copy(), flat.copy()
+            tp[q] += 1e-3
+            tm[q] -= 1e-3
+            fp, _, _ = eng.forward(tp, step=0)
+            fm, _, _ = eng.forward(tm, step=0)
+            d = (fp - fm) / 2e-3
+            a = jac[:, q]
+            errs.append(float(np.linalg.norm(d - a) / np.linalg.norm(a)))
+        fd = {"entries": len(errs), "relative_step": 1e-3, "common_random_numbers": True,
+              "rel_err_max": max(errs), "rel_err_median": float(np.median(errs)),
+              "norm": "||fd - adjoint||_2 / ||adjoint||_2 over the 1024 spectrum bins of a (zone, band) column"}
+    value = n / ((ms_f + ms_b) * 1e-3)
+    b_seg, b_pkt = 16 + 8 + 16 + 16 + 64, 264
+    achieved = (seg * b_seg + n * b_pkt) / (ms_k * 1e-3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    out = {"metric": METRIC + " (forward + adjoint)", "value": value, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_f + ms_b, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64 transport / f32 opacity tables",
+           "data": "synthetic", "config": dict(cfg, segments_per_forward=seg, l2="flushed between steps (256 MiB write)"),
+           "ms_forward": ms_f, "ms_adjoint_vjp": ms_b, "ms_jacobian": ms_jac,
+           "escaped_fraction": float(click.sum()) / n, "fd_check": fd,
+           "gpu_launches": 3 * args.steps,
+           "e2e": {"value": n / e2e, "unit": UNIT, "h2d_bytes_per_step": int(theta.nbytes + g.nbytes),
+                   "d2h_bytes_per_step": int(flux.nbytes + click.nbytes + grad.nbytes), "ms_per_step": e2e * 1e3},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": None, "kernel": "propagate_kernel (weighted forward)", "kernel_ms": ms_k,
+                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+           "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = ref.get("cpu_baseline", {"value": None, "sample": ref.get("unavailable")})
+        out["cpu_baseline"]["sample"] = "reference forward (discrete absorption, no adjoint): " + \
+            str(out["cpu_baseline"].get("sample"))
+    print(json.dumps(out), flush=True)
+    eng.close()
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -320,7 +436,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d", "batch64"])
+    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d", "batch64", "adjoint"])
+    ap.add_argument("--fd-entries", type=int, default=32, help="adjoint: (zone, band) entries checked by central FD")
     ap.add_argument("--packet-scale", type=float, default=1.0, help="batch64: scales every model's packet count")
     ap.add_argument("--cells", type=int, default=128, help="cells per axis of the cart3d workload")
     ap.add_argument("--packets", type=int, default=None)
@@ -331,6 +448,8 @@ def main():
     rank, world, local = _env_rank()
     if args.workload == "batch64":
         return main_batch(args, rank, world, local)
+    if args.workload == "adjoint":
+        return main_adjoint(args, rank, world, local)
 
     from pubsed_b200 import workloads
 
