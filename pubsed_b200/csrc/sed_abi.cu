@@ -110,6 +110,12 @@ StepArgs sed::make_step_args(sed_ctx* c, double dt, int64_t n_emit)
   A.first_pid = c->tp.first_packet_id;
   A.Ep = n_emit > 0 ? c->tp.core_luminosity * dt / n_emit : 0.0;
   A.t_now = c->t_grid; A.dt = dt; A.tstop = c->t_grid + dt;
+  if (c->t_grid > 0) {
+    A.inv_t = 1.0 / c->t_grid;
+    A.ct = C_LIGHT * c->t_grid;
+    A.inv_ct = 1.0 / A.ct;
+    A.inv_ct2 = A.inv_ct * A.inv_ct;
+  }
   A.core_radius = c->tp.core_radius; A.core_freq = c->tp.core_photon_frequency; A.core_cdf = c->d_core_cdf.p;
   A.max_segments = c->tp.max_segments;
   const size_t zone_smem = (size_t)5 * nz * sizeof(double);

@@ -125,6 +125,12 @@ StepArgs step_args(sed_batch* b, double dt, const BatchModel* models, int64_t to
   A.precision = c->tp.precision;
   A.n_packets = total;
   A.t_now = c->t_grid; A.dt = dt; A.tstop = c->t_grid + dt;
+  if (c->t_grid > 0) {
+    A.inv_t = 1.0 / c->t_grid;
+    A.ct = C_LIGHT * c->t_grid;
+    A.inv_ct = 1.0 / A.ct;
+    A.inv_ct2 = A.inv_ct * A.inv_ct;
+  }
   A.core_freq = c->tp.core_photon_frequency;
   A.max_segments = c->tp.max_segments;
   A.smem_zones = ((size_t)5 * c->nz * sizeof(double) <= 64 * 1024) ? 1 : 0;

@@ -99,7 +99,7 @@ struct DevLoc {
   double min, del;
   const double* right;  // device pointer, n walls
   float inv_step;       // log grids: 1/log2(1+del); lin grids: 1/del (index estimate only)
-  int32_t pad_;
+  float lmin_step;      // log grids: log2(min) * inv_step (index estimate without a division)
 };
 
 __device__ __forceinline__ int upper_bound_dev(const double* __restrict__ a, int n, double v)
@@ -172,14 +172,20 @@ __device__ __forceinline__ int loc_within(const DevLoc& g, double x)
 // n maps to n-1), found here from a float estimate and a wall check.  For
 // bins 0 and 1 the reference's own fast index is evaluated, because an
 // uncorrected fast index of 0 is what it returns.
+// NODIV: the log-grid estimate log2(x) * inv_step - lmin_step instead of
+// log2(x / min) * inv_step (no FP64 division; the wall checks below make
+// the result the same).
+template <bool NODIV = false>
 __device__ __forceinline__ int loc_within_fast(const DevLoc& g, double x)
 {
   if (g.n == 1) return 0;
   if (x >= __ldg(g.right + g.n - 1)) return g.n - 1;
   if (x < g.min) return 0;
   if (g.type != LOC_LOG && g.type != LOC_LIN) return loc_within(g, x);
-  const float est = (g.type == LOC_LOG) ? __log2f((float)(x / g.min)) * g.inv_step
-                                        : (float)(x - g.min) * g.inv_step;
+  float est;
+  if (g.type == LOC_LOG) est = NODIV ? __log2f((float)x) * g.inv_step - g.lmin_step
+                                     : __log2f((float)(x / g.min)) * g.inv_step;
+  else est = (float)(x - g.min) * g.inv_step;
   int i = (int)est;
   i = max(0, min(i, g.n - 1));
   while (i < g.n - 1 && x >= __ldg(g.right + i)) ++i;

@@ -202,7 +202,7 @@ inline DevLoc dev_loc(const HostLoc& h, const DevBuf<double>& d)
   g.inv_step = 0.f;
   if (h.type == LOC_LOG && h.del > 0) g.inv_step = (float)(1.0 / std::log2(1.0 + h.del));
   else if (h.type == LOC_LIN && h.del > 0) g.inv_step = (float)(1.0 / h.del);
-  g.pad_ = 0;
+  g.lmin_step = (h.type == LOC_LOG && h.min > 0) ? (float)(std::log2(h.min) * g.inv_step) : 0.f;
   return g;
 }
 

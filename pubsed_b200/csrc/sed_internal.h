@@ -31,6 +31,7 @@ struct StepArgs {
   int64_t n_packets;
   int64_t first_pid;          // Philox stream id of queue entry 0
   double Ep, t_now, dt, tstop;
+  double inv_t, ct, inv_ct, inv_ct2;  // 1/t_grid, c t_grid, 1/(c t_grid), its square (homologous flow)
   double core_radius, core_freq;
   const double* core_cdf;     // [n_nu] normalised core emission CDF
   int32_t max_segments;

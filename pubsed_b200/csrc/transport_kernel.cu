@@ -53,13 +53,12 @@ __device__ __forceinline__ int get_zone(const GridDev& G, const double* x)
 
 // grid_1D_sphere::get_next_zone (grid_1D_sphere.cpp:510-590) and
 // grid_3D_cart::get_next_zone (grid_3D_cart.cpp:396-469)
+// (1D: rsq = x.x and xdotD = D.x come from the caller)
 template <int GRID>
 __device__ __forceinline__ int get_next_zone(const GridDev& G, const double* x, const double* D, int i,
-                                             double r_core, double* l)
+                                             double r_core, double rsq, double xdotD, double* l)
 {
   if constexpr (GRID == 0) {
-    const double rsq = (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-    const double xdotD = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]);
     const double r_o = __ldg(G.r_out.right + i);
     const double l_out = -1 * xdotD + sqrt(xdotD * xdotD + r_o * r_o - rsq);
     double r_in;
@@ -73,7 +72,7 @@ __device__ __forceinline__ int get_next_zone(const GridDev& G, const double* x, 
       const double rad = xdotD * xdotD + r_in * r_in - rsq;
       l_in = (rad < 0) ? -1 : -1 * xdotD - sqrt(rad);
     }
-    const double tiny_offset = 1 + 1e-6;
+    constexpr double tiny_offset = 1 + 1e-6;
     int ind;
     if ((l_out < l_in) || (l_in < 0)) {
       ind = i + 1;
@@ -184,11 +183,9 @@ __device__ __forceinline__ void comoving_to_lab(const GridDev& G, Pkt& p)
 // substitution, the inner neighbour (-1 at the core or the model's first
 // zone), the outer neighbour (-2 past the model's last zone) and whether
 // zone 0 starts at r = 0.  Values and branches are the single-model ones.
-__device__ __forceinline__ int get_next_zone_batch(const StepArgs& A, const GridDev& G, const double* x, const double* D,
-                                                   int i, double* l)
+__device__ __forceinline__ int get_next_zone_batch(const StepArgs& A, const GridDev& G, int i, double rsq,
+                                                   double xdotD, double* l)
 {
-  const double rsq = (x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-  const double xdotD = (D[0] * x[0] + D[1] * x[1] + D[2] * x[2]);
   const double r_o = __ldg(G.r_out.right + i);
   const double l_out = -1 * xdotD + sqrt(xdotD * xdotD + r_o * r_o - rsq);
   const int4 nb = __ldg(A.zone_nbr + i);
@@ -289,6 +286,61 @@ __device__ __forceinline__ void isotropic_scatter(const StepArgs& A, const GridD
   p.D[0] = p.D[0] / norm;
   p.D[1] = p.D[1] / norm;
   p.D[2] = p.D[2] / norm;
+  p.e = p.e * vd_out;
+  p.nu = p.nu * vd_out;
+}
+
+// ------------------------------------------------ mixed form, homologous flow
+// The mixed form is held to the reference's spectra within Monte Carlo
+// noise, not to its bits, so with homologous velocities v = x / t it
+// evaluates the same FP64 transforms without divisions: beta = x / (c t),
+// gamma = rsqrt(1 - beta^2), reciprocals and rsqrt for the normalisations.
+// Position, time, frequency and the Lorentz transforms stay FP64.
+
+// transport::do_dshift, lab -> comoving, from rsq = x.x and xdotD = D.x
+__device__ __forceinline__ double dshift_fast(const StepArgs& A, double rsq, double xdotD)
+{
+  const double gamma = rsqrt(1 - rsq * A.inv_ct2);
+  return gamma * (1 - xdotD * A.inv_ct);
+}
+
+// transport::isotropic_scatter (scatter.cpp:303-351), homologous flow
+template <typename CT>
+__device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p, PacketRng& rng, int redist)
+{
+  const double b0 = p.x[0] * A.inv_ct, b1 = p.x[1] * A.inv_ct, b2 = p.x[2] * A.inv_ct;  // v / c
+  const double bdotD = fma(b0, p.D[0], fma(b1, p.D[1], b2 * p.D[2]));
+  const double gamma = rsqrt(1 - fma(b0, b0, fma(b1, b1, b2 * b2)));
+  const double dshift_in = gamma * (1 - bdotD);
+  p.e = p.e * dshift_in;
+  p.nu = p.nu * dshift_in;
+  const double mu = 1 - 2.0 * rng.next();
+  const double phi = 2.0 * PI * rng.next();
+  const double smu = sqrt(1 - mu * mu);
+  double s, c;
+  sincos(phi, &s, &c);
+  const double Dn[3] = {smu * c, smu * s, mu};
+  if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
+    const int nn = A.nu.n;
+    const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
+    const CT* crow = reinterpret_cast<const CT*>(A.cdf_coarse) + (size_t)p.ind * A.n_coarse;
+    const double u = rng.next();
+    const int inu = (nn == 1) ? 0 : upper_bound_2level<CT>(row, crow, nn, A.n_coarse, u);
+    p.nu = loc_sample(A.nu, inu, rng.next());
+  }
+  // comoving -> lab with the velocity reversed: beta' = -beta
+  const double bdp = -fma(b0, Dn[0], fma(b1, Dn[1], b2 * Dn[2]));
+  const double vd_out = gamma * (1 - bdp);
+  const double f = 1 - gamma * bdp / (gamma + 1);
+  const double gf = gamma * f;
+  const double inv_vd = 1.0 / vd_out;
+  p.D[0] = inv_vd * fma(gf, b0, Dn[0]);
+  p.D[1] = inv_vd * fma(gf, b1, Dn[1]);
+  p.D[2] = inv_vd * fma(gf, b2, Dn[2]);
+  const double inv_norm = rsqrt(fma(p.D[0], p.D[0], fma(p.D[1], p.D[1], p.D[2] * p.D[2])));
+  p.D[0] *= inv_norm;
+  p.D[1] *= inv_norm;
+  p.D[2] *= inv_norm;
   p.e = p.e * vd_out;
   p.nu = p.nu * vd_out;
 }
@@ -398,7 +450,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 // deviates, same path) and adds -w a0 dshift l per segment into the
 // gradient with respect to the (zone, band) absorption factors, where w is
 // the packet's escaping energy times d(loss)/d(its spectrum bin).
-template <int GRID, typename OT, typename CT, int BATCH, int MODE, int THREADS, int MINB>
+// FAST (mixed form on a homologous grid): the division-free transforms above.
+template <int GRID, typename OT, typename CT, int BATCH, int MODE, bool FAST, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs A, const GridDev G)
 {
   extern __shared__ double s_tal[];  // [5][nz] when A.smem_zones
@@ -415,6 +468,9 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   double* t_fz = A.smem_zones ? s_tal + 3 * nz : A.fz;
   double* t_fr = A.smem_zones ? s_tal + 4 * nz : A.fr;
   const OT* __restrict__ opac = reinterpret_cast<const OT*>(A.opac);
+  // the mixed form takes the division-free transforms on homologous grids;
+  // the FP64 form keeps the reference's expressions
+  constexpr bool fast = FAST;
   const int64_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
   uint32_t K = (A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u;
   uint32_t step = A.step;
@@ -566,13 +622,27 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
       }
       double d_bn = 0;
+      double rsq, xdotD;
+      if (fast) {
+        rsq = fma(p.x[0], p.x[0], fma(p.x[1], p.x[1], p.x[2] * p.x[2]));
+        xdotD = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
+      } else {
+        rsq = (p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+        xdotD = (p.D[0] * p.x[0] + p.D[1] * p.x[1] + p.D[2] * p.x[2]);
+      }
       int new_ind;
-      if constexpr (BATCH) new_ind = get_next_zone_batch(A, G, p.x, p.D, iz, &d_bn);
-      else new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, &d_bn);
-      const double dshift = dshift_lab_to_comoving<GRID>(G, p);
+      if constexpr (BATCH) new_ind = get_next_zone_batch(A, G, iz, rsq, xdotD, &d_bn);
+      else new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, rsq, xdotD, &d_bn);
+      double dshift;
+      if (fast) {
+        dshift = dshift_fast(A, rsq, xdotD);
+        p.dvds = A.inv_t;
+      } else {
+        dshift = dshift_lab_to_comoving<GRID>(G, p);
+      }
       // transport::get_opacity (transport_opacity.cpp:268-299)
       const double nu_cmf = p.nu * dshift;
-      const int i_nu = loc_within_fast(A.nu, nu_cmf);
+      const int i_nu = (fast) ? loc_within_fast<true>(A.nu, nu_cmf) : loc_within_fast<false>(A.nu, nu_cmf);
       const OT ab = opac[(size_t)iz * nn + i_nu];
       double a_opac = (double)ab.x;
       const double s_opac = A.omit_scat ? 0.0 : (double)ab.y;
@@ -582,9 +652,14 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         if (A.abs_scale) a_opac *= __ldg(A.abs_scale + (size_t)iz * A.n_bands + band);
       }
       const double op = a_opac + s_opac;
-      const double eps = (op == 0) ? 0 : a_opac / op;
-      double d_nu = loc_delta(A.nu, i_nu) / p.nu * C_LIGHT / p.dvds;
-      if (p.dvds == 0) d_nu = INFINITY;
+      double eps = 0;
+      if (!(fast)) eps = (op == 0) ? 0 : a_opac / op;
+      double d_nu;
+      if (fast) d_nu = loc_delta(A.nu, i_nu) * A.ct / p.nu;
+      else {
+        d_nu = loc_delta(A.nu, i_nu) / p.nu * C_LIGHT / p.dvds;
+        if (p.dvds == 0) d_nu = INFINITY;
+      }
       if (d_nu < 0) d_nu = -1 * d_nu;
       if (d_nu < d_bn) { d_bn = d_nu; new_ind = p.ind; }
       const double tot_lab = (MODE == 0 ? op : s_opac) * dshift;
@@ -619,7 +694,10 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         acc_g += (double)ab.x * dshift * this_d;  // d(theta a0 dshift l) / d theta
       }
       const double eps_imc = __ldg(A.eps_imc + iz);
-      if constexpr (MODE == 0) acc_eabs += this_E * dshift * (op) * eps * dshift * eps_imc;
+      if constexpr (MODE == 0) {
+        if (fast) acc_eabs += this_E * dshift * dshift * a_opac * eps_imc;
+        else acc_eabs += this_E * dshift * (op) * eps * dshift * eps_imc;
+      }
       if constexpr (MODE == 1) acc_eabs += this_E * dshift * a_opac * dshift * eps_imc;
       if constexpr (MODE != 2) atomicAdd(A.J + (size_t)iz * nj + (A.store_Jnu ? i_nu : 0), this_E);
       if (MODE != 2 && A.tally_forces) {
@@ -627,14 +705,16 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         acc_fx += w * p.D[0] * dshift;
         acc_fy += w * p.D[1] * dshift;
         acc_fz += w * p.D[2] * dshift;
-        const double rr = sqrt(p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
-        const double xdotD = p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2];
-        acc_fr += w * xdotD / rr * dshift;
+        // |x| and x.D before the move: the segment's rsq and xdotD
+        if (fast) acc_fr += w * xdotD * rsqrt(rsq) * dshift;
+        else acc_fr += w * xdotD / sqrt(rsq) * dshift;
       }
       p.x[0] += this_d * p.D[0];
       p.x[1] += this_d * p.D[1];
       p.x[2] += this_d * p.D[2];
-      p.t = p.t + this_d / C_LIGHT;
+      constexpr double INV_C = 1.0 / C_LIGHT;
+      if (fast) p.t = p.t + this_d * INV_C;
+      else p.t = p.t + this_d / C_LIGHT;
       if constexpr (MODE == 1) p.e *= att;
       if (event == 1) {
         if (new_ind == -1) {
@@ -653,13 +733,17 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         ++n_scat;
         int redist = 0;
         if constexpr (MODE == 0) {
+          if (fast) eps = (op == 0) ? 0 : a_opac / op;
           if (!(rng.next() > eps)) {
             const double z2 = rng.next();
             if ((z2 > eps_imc) || A.radiative_eq) redist = 1;
             else fate = ABSORBED;
           }
         }
-        if (fate == MOVING) isotropic_scatter<GRID, CT>(A, G, p, rng, redist);
+        if (fate == MOVING) {
+          if (fast) isotropic_scatter_fast<CT>(A, p, rng, redist);
+          else isotropic_scatter<GRID, CT>(A, G, p, rng, redist);
+        }
       } else {
         fate = STOPPED;
       }
@@ -782,12 +866,13 @@ __global__ void rescale_spectrum_batch_kernel(const StepArgs A, int64_t nspec)
   }
 }
 
-template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB, int MODE = 0>
+template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB, int MODE = 0,
+          bool FAST = (sizeof(OT) == sizeof(float2))>
 int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
                     cudaStream_t s)
 {
   const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
-  auto kern = propagate_kernel<GRID, OT, CT, BATCH, MODE, THREADS, MINB>;
+  auto kern = propagate_kernel<GRID, OT, CT, BATCH, MODE, FAST, THREADS, MINB>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
@@ -804,7 +889,12 @@ int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int 
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
-  return launch_kernel_t<GRID, OT, CT, 0, SED_PROP_THREADS, SED_PROP_MINB>(a, g, 0, num_sms, a.n_packets, s);
+  constexpr int T = SED_PROP_THREADS, B = SED_PROP_MINB;
+  // mixed tables on a grid with a tabulated velocity field: the reference's
+  // expressions (the division-free transforms assume v = x / t)
+  if (sizeof(OT) == sizeof(float2) && !g.homologous)
+    return launch_kernel_t<GRID, OT, CT, 0, T, B, 0, false>(a, g, 0, num_sms, a.n_packets, s);
+  return launch_kernel_t<GRID, OT, CT, 0, T, B>(a, g, 0, num_sms, a.n_packets, s);
 }
 
 // batched kernel shapes {threads, min blocks per SM}: 32 or 24 warps per SM
@@ -850,7 +940,7 @@ int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_
 int launch_propagate_diff(const StepArgs& a, const GridDev& g, int mode, int num_sms, cudaStream_t s)
 {
   constexpr int T = SED_PROP_THREADS, B = SED_PROP_MINB;
-  if (g.type != 0 || (mode != 1 && mode != 2)) return -1;
+  if (g.type != 0 || !g.homologous || (mode != 1 && mode != 2)) return -1;
   StepArgs b = a;
   if (mode == 2) b.smem_zones = 0;  // the replay tallies nothing per zone
   if (a.precision == 0)
