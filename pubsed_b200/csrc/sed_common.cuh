@@ -55,6 +55,9 @@ __host__ __device__ inline double u01(uint32_t a, uint32_t b)
   return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
 }
 
+// one 32-bit word as a deviate in [0, 1)
+__host__ __device__ inline double w01(uint32_t a) { return (double)a * (1.0 / 4294967296.0); }
+
 // Per-packet stream.  Each draw evaluates its Philox block: lanes of a warp
 // sit at different draw parities, so keeping the odd half of a block for the
 // next draw would only make half the lanes compute while the others wait.
@@ -77,6 +80,14 @@ struct PacketRng {
 #if SED_RNG_CACHE
     have = false;
 #endif
+  }
+  // Word layout of the mixed form: one Philox block per call, four 32-bit
+  // words each used as one deviate, counter {k, pid.lo, pid.hi, step}, key
+  // {seed, 1} (streams independent of the per-draw layout's key {seed, 0}).
+  __device__ uint4 block()
+  {
+    const PhiloxOut o = philox4x32_10(n++, (uint32_t)pid, (uint32_t)(pid >> 32), step, seed, 1u);
+    return make_uint4(o.w[0], o.w[1], o.w[2], o.w[3]);
   }
   __device__ double next()
   {

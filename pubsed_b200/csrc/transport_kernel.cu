@@ -305,8 +305,10 @@ __device__ __forceinline__ double dshift_fast(const StepArgs& A, double rsq, dou
 }
 
 // transport::isotropic_scatter (scatter.cpp:303-351), homologous flow
+// Its deviates are the four words of one Philox block: mu, phi, the
+// emissivity-CDF deviate and the position within the bin.
 template <typename CT>
-__device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p, PacketRng& rng, int redist)
+__device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p, const uint4 w, int redist)
 {
   const double b0 = p.x[0] * A.inv_ct, b1 = p.x[1] * A.inv_ct, b2 = p.x[2] * A.inv_ct;  // v / c
   const double bdotD = fma(b0, p.D[0], fma(b1, p.D[1], b2 * p.D[2]));
@@ -314,8 +316,8 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
   const double dshift_in = gamma * (1 - bdotD);
   p.e = p.e * dshift_in;
   p.nu = p.nu * dshift_in;
-  const double mu = 1 - 2.0 * rng.next();
-  const double phi = 2.0 * PI * rng.next();
+  const double mu = 1 - 2.0 * w01(w.x);
+  const double phi = 2.0 * PI * w01(w.y);
   const double smu = sqrt(1 - mu * mu);
   double s, c;
   sincos(phi, &s, &c);
@@ -324,9 +326,9 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
     const int nn = A.nu.n;
     const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
     const CT* crow = reinterpret_cast<const CT*>(A.cdf_coarse) + (size_t)p.ind * A.n_coarse;
-    const double u = rng.next();
+    const double u = w01(w.z);
     const int inu = (nn == 1) ? 0 : upper_bound_2level<CT>(row, crow, nn, A.n_coarse, u);
-    p.nu = loc_sample(A.nu, inu, rng.next());
+    p.nu = loc_sample(A.nu, inu, w01(w.w));
   }
   // comoving -> lab with the velocity reversed: beta' = -beta
   const double bdp = -fma(b0, Dn[0], fma(b1, Dn[1], b2 * Dn[2]));
@@ -348,14 +350,33 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
 // transport::emit_inner_source for one packet (emission.cpp:395-480).  The
 // source (core radius, packet energy, core CDF) and the zone lookup are
 // arguments so one model of a batch can supply its own.
-template <int GRID, class ZoneOf>
-__device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng, double rc,
+// Deviates of the emission: one per draw (the reference's layout), or the
+// 32-bit words of consecutive Philox blocks (the mixed form's layout).
+struct DrawNext {
+  PacketRng& r;
+  __device__ double operator()() { return r.next(); }
+};
+struct DrawWords {
+  PacketRng& r;
+  uint4 b;
+  int used = 4;
+  __device__ double operator()()
+  {
+    if (used == 4) { b = r.block(); used = 0; }
+    const uint32_t w = (used == 0) ? b.x : (used == 1) ? b.y : (used == 2) ? b.z : b.w;
+    ++used;
+    return w01(w);
+  }
+};
+
+template <int GRID, class ZoneOf, class Draw>
+__device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, Pkt& p, Draw& rng, double rc,
                                           double Ep, const double* core_cdf, const ZoneOf& zone_of)
 {
   if (rc == 0) {
     p.x[0] = p.x[1] = p.x[2] = 0;
-    const double mu = 1 - 2.0 * rng.next();
-    const double phi = 2.0 * PI * rng.next();
+    const double mu = 1 - 2.0 * rng();
+    const double phi = 2.0 * PI * rng();
     const double smu = sqrt(1 - mu * mu);
     double s, c;
     sincos(phi, &s, &c);
@@ -363,17 +384,17 @@ __device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, P
     p.D[1] = smu * s;
     p.D[2] = mu;
   } else {
-    const double phi_core = 2 * PI * rng.next();
+    const double phi_core = 2 * PI * rng();
     double sinp, cosp;
     sincos(phi_core, &sinp, &cosp);
-    const double cost = 1 - 2.0 * rng.next();
+    const double cost = 1 - 2.0 * rng();
     const double sint = sqrt(1 - cost * cost);
     const double a_phot = rc + rc * 1e-10;
     p.x[0] = a_phot * sint * cosp;
     p.x[1] = a_phot * sint * sinp;
     p.x[2] = a_phot * cost;
-    const double phi_loc = 2 * PI * rng.next();
-    const double cost_loc = sqrt(rng.next());
+    const double phi_loc = 2 * PI * rng();
+    const double cost_loc = sqrt(rng());
     const double sint_loc = sqrt(1 - cost_loc * cost_loc);
     double sl, cl;
     sincos(phi_loc, &sl, &cl);
@@ -385,15 +406,15 @@ __device__ __forceinline__ void emit_core(const StepArgs& A, const GridDev& G, P
   p.e = Ep;
   if (A.core_freq > 0) p.nu = A.core_freq;
   else {
-    const int inu = cdf_sample<double>(core_cdf, A.nu.n, rng.next());
-    p.nu = loc_sample(A.nu, inu, rng.next());
+    const int inu = cdf_sample<double>(core_cdf, A.nu.n, rng());
+    p.nu = loc_sample(A.nu, inu, rng());
     p.e /= 1.0;  // emissivity_weight_ is 1 (transport_init.cpp:322-332)
   }
   p.ind = zone_of(p.x);
   // the reference asserts p.ind >= 0 here (relativity.cpp:86); homologous
   // velocities do not depend on the zone, other velocity fields need one
   if (G.homologous || p.ind >= 0) comoving_to_lab<GRID>(G, p);
-  p.t = A.t_now + rng.next() * A.dt;
+  p.t = A.t_now + rng() * A.dt;
 }
 
 // spectrum_array::count (src/transport/spectrum_array.cpp:215-246)
@@ -472,7 +493,9 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   // the FP64 form keeps the reference's expressions
   constexpr bool fast = FAST;
   const int64_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
+  // deviates (per-draw layout) or Philox blocks (word layout) the emission uses
   uint32_t K = (A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u;
+  if (FAST) K = (K + 3u) / 4u;
   uint32_t step = A.step;
   if constexpr (BATCH) step = *A.step_dev;
   // batch: claimed queue entries [q_next, q_end), the current packet's model,
@@ -568,7 +591,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         pid = (unsigned long long)q_next++;
         m = find_model(A.models, A.n_models, (int64_t)pid);
         const BatchModel& M = A.models[m];
-        K = M.emit_draws;
+        K = FAST ? (M.emit_draws + 3u) / 4u : M.emit_draws;
         rng.init(M.seed, (uint64_t)(M.first_pid + ((int64_t)pid - M.pkt_off)), step, 0);
         BatchZoneOf zf;
         zf.slice = G.r_out;
@@ -576,7 +599,13 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         zf.slice.min = M.r_min;
         zf.slice.right = G.r_out.right + M.zone_off;
         zf.zone_off = M.zone_off;
-        emit_core<GRID>(A, G, p, rng, M.core_radius, M.Ep, M.core_cdf, zf);
+        if constexpr (FAST) {
+          DrawWords d{rng};
+          emit_core<GRID>(A, G, p, d, M.core_radius, M.Ep, M.core_cdf, zf);
+        } else {
+          DrawNext d{rng};
+          emit_core<GRID>(A, G, p, d, M.core_radius, M.Ep, M.core_cdf, zf);
+        }
       } else {
         pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
         if (pid >= (unsigned long long)A.n_packets) break;
@@ -591,7 +620,13 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
           acc_g = 0;
         }
         rng.init(A.seed, (uint64_t)A.first_pid + pid, step, 0);
-        emit_core<GRID>(A, G, p, rng, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<GRID>{G});
+        if constexpr (FAST) {
+          DrawWords d{rng};
+          emit_core<GRID>(A, G, p, d, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<GRID>{G});
+        } else {
+          DrawNext d{rng};
+          emit_core<GRID>(A, G, p, d, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<GRID>{G});
+        }
       }
       // transport::propagate (transport.cpp:202-254): its get_zone of the
       // emitted position is the p.ind emit_core set (x has not moved since)
@@ -663,7 +698,16 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       if (d_nu < 0) d_nu = -1 * d_nu;
       if (d_nu < d_bn) { d_bn = d_nu; new_ind = p.ind; }
       const double tot_lab = (MODE == 0 ? op : s_opac) * dshift;
-      const double tau_r = -1.0 * log(1 - rng.next());
+      // mixed form: the segment's Philox block gives tau (53 bits) and the
+      // two interaction tests
+      uint4 blk = make_uint4(0u, 0u, 0u, 0u);
+      double tau_r;
+      if constexpr (FAST) {
+        blk = rng.block();
+        tau_r = -1.0 * log(1 - u01(blk.x, blk.y));
+      } else {
+        tau_r = -1.0 * log(1 - rng.next());
+      }
       double d_sc = tau_r / tot_lab;
       if (tot_lab == 0) d_sc = INFINITY;
       double d_tm = (A.tstop - p.t) * C_LIGHT;
@@ -734,14 +778,14 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         int redist = 0;
         if constexpr (MODE == 0) {
           if (fast) eps = (op == 0) ? 0 : a_opac / op;
-          if (!(rng.next() > eps)) {
-            const double z2 = rng.next();
+          if (!((FAST ? w01(blk.z) : rng.next()) > eps)) {
+            const double z2 = FAST ? w01(blk.w) : rng.next();
             if ((z2 > eps_imc) || A.radiative_eq) redist = 1;
             else fate = ABSORBED;
           }
         }
         if (fate == MOVING) {
-          if (fast) isotropic_scatter_fast<CT>(A, p, rng, redist);
+          if (fast) isotropic_scatter_fast<CT>(A, p, rng.block(), redist);
           else isotropic_scatter<GRID, CT>(A, G, p, rng, redist);
         }
       } else {

@@ -3,7 +3,8 @@
 The fixtures free_*.npz are the reference's own transport::step run with its
 own OpenMP packet loop and random streams (tests/golden/make_golden.py).  The
 GPU runs the same workload with a different seed and more packets, in both
-forms (FP64 opacity tables, and FP32 tables with FP64 transport); each
+forms (the FP64 form, and the mixed form: FP32 tables, FP64 transport
+without divisions, Philox words as deviates); each
 spectrum must agree with the reference's per bin within Monte Carlo noise:
 chi^2 = sum (F_a - F_b)^2 / (F_a^2/N_a + F_b^2/N_b) over bins with at least
 10 packets in both runs (adjacent bins are merged first), p-value > 0.01.
@@ -64,11 +65,13 @@ def test_free_running_spectrum_matches_reference(sed_lib, case, n_packets, seed,
     assert abs(results[abi.PREC_FP64][0] - results[abi.PREC_MIXED][0]) < 0.5, results
 
 
-def test_mixed_and_fp64_forms_draw_the_same_packets(sed_lib):
-    """Same seed: the FP32 tables move few packet decisions, so the two
-    spectra agree far inside the Monte Carlo noise."""
-    w = workloads.type_ia(n_packets=200_000, n_zones=64, n_lines=50000, n_bins=1024, seed=77)
+def test_mixed_and_fp64_forms_agree_within_noise(sed_lib):
+    """The mixed form draws its deviates as the 32-bit words of one Philox
+    block per segment (and one per interaction), on streams independent of
+    the FP64 form's per-draw layout: the two spectra of the same workload
+    agree within Monte Carlo noise."""
+    w = workloads.type_ia(n_packets=400_000, n_zones=64, n_lines=50000, n_bins=1024, seed=77)
     f64, c64, _ = _gpu_spectrum(sed_lib, w, abi.PREC_FP64)
     f32, c32, _ = _gpu_spectrum(sed_lib, w, abi.PREC_MIXED)
     chi2, dof, p = chi2_spectra(f32, c32, f64, c64, merge=4)
-    assert dof >= 20 and chi2 / dof < 0.5, (chi2, dof)
+    assert dof >= 20 and p > P_MIN, (chi2, dof, p)
