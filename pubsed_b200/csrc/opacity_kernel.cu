@@ -639,6 +639,7 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
     }
   }
   const double N = em[nn - 1];
+  __syncthreads();  // every thread has N before em[] is overwritten below
   // normalised CDF, packed tables and the coarse CDF index for the packet kernel
   for (int j = tid; j < nn; j += bd) {
     const size_t k = (size_t)z * nn + j;
@@ -654,6 +655,23 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
       const size_t kc = (size_t)z * A.n_coarse + j / CDF_STRIDE;
       if constexpr (MIXED) reinterpret_cast<float*>(A.cdf_coarse_out)[kc] = (float)c;
       else reinterpret_cast<double*>(A.cdf_coarse_out)[kc] = c;
+    }
+    // the value the packet kernel compares against, as a double
+    em[j] = MIXED ? (double)(float)c : c;
+  }
+  // guide table of the stored row: guide[k] = upper_bound(row, k / G)
+  if (A.cdf_guide_out) {
+    __syncthreads();
+    const int G = A.guide_n;
+    uint16_t* gz = A.cdf_guide_out + (size_t)z * (G + 1);
+    for (int k = tid; k <= G; k += bd) {
+      const double t = (double)k / (double)G;
+      int lo = 0, hi = nn;
+      while (lo < hi) {
+        const int m = (lo + hi) >> 1;
+        if (em[m] <= t) lo = m + 1; else hi = m;
+      }
+      gz[k] = (uint16_t)lo;
     }
   }
 }

@@ -33,6 +33,13 @@ int alloc_tallies(sed_ctx* c)
   CK(c->d_cdf.resize(nz * nn * esz));
   c->n_coarse = (int)((nn + CDF_STRIDE - 1) / CDF_STRIDE);
   CK(c->d_cdf_coarse.resize(nz * (size_t)c->n_coarse * esz));
+  // guide tables: G = the power of two >= n_nu (uint16 bin indices)
+  c->guide_n = 0;
+  if (nn > 1 && nn <= 65535) {
+    c->guide_n = 1;
+    while ((size_t)c->guide_n < nn) c->guide_n <<= 1;
+    CK(c->d_cdf_guide.resize(nz * (size_t)(c->guide_n + 1)));
+  }
   CK(c->d_eps_imc.resize(nz)); CK(c->d_planck.resize(nz)); CK(c->d_ross.resize(nz)); CK(c->d_L.resize(nz));
   CK(c->d_n_elec.resize(nz)); CK(c->d_temp_c.resize(nz)); CK(c->d_solve_err.resize(nz));
   CK(cudaMemsetAsync(c->d_n_elec.p, 0, nz * sizeof(double), c->stream));
@@ -125,6 +132,7 @@ StepArgs sed::make_step_args(sed_ctx* c, double dt, int64_t n_emit)
   A.a3 = c->sp.n(); A.a2 = (int64_t)c->sm.n() * A.a3; A.a1 = (int64_t)c->sn.n() * A.a2;
   A.opac = c->d_opac.p; A.cdf = c->d_cdf.p; A.eps_imc = c->d_eps_imc.p;
   A.cdf_coarse = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
+  A.cdf_guide = c->guide_n ? c->d_cdf_guide.p : nullptr; A.guide_n = c->guide_n;
   A.rescale_lum = c->tp.core_fix_luminosity;
   A.J = c->d_J.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
   A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;
@@ -469,6 +477,7 @@ int sed::enqueue_opacity(sed_ctx* c, double dt)
   A.abs64 = c->d_abs64.p; A.scat64 = c->d_scat64.p; A.emis64 = c->d_emis64.p;
   A.opac_out = c->d_opac.p; A.cdf_out = c->d_cdf.p;
   A.cdf_coarse_out = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
+  A.cdf_guide_out = c->guide_n ? c->d_cdf_guide.p : nullptr; A.guide_n = c->guide_n;
   A.eps_imc = c->d_eps_imc.p; A.planck = c->d_planck.p; A.ross = c->d_ross.p; A.L_th = c->d_L.p;
   // passes over chunks of zones: per-zone inputs and outputs are offset to
   // the chunk, the scratch is reused with the chunk's zone count as stride
@@ -485,6 +494,7 @@ int sed::enqueue_opacity(sed_ctx* c, double dt)
     B.opac_out = static_cast<unsigned char*>(A.opac_out) + o * nn * 2 * esz;
     B.cdf_out = static_cast<unsigned char*>(A.cdf_out) + o * nn * esz;
     B.cdf_coarse_out = static_cast<unsigned char*>(A.cdf_coarse_out) + o * (size_t)c->n_coarse * esz;
+    if (A.cdf_guide_out) B.cdf_guide_out = A.cdf_guide_out + o * (size_t)(c->guide_n + 1);
     const int nl = launch_opacity(B, c->num_sms, c->stream);
     CK(cudaGetLastError());
     if (nl < 0) return set_err(c, SED_ERR_CUDA, "sed_set_opacity: opacity kernel configuration rejected");
@@ -511,6 +521,26 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
   if (!c || !abs || !emis_cdf || !eps_imc) return SED_ERR_ARG;
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_load_opacity: no grid");
   const size_t n = (size_t)c->nz * c->nu.n();
+  // guide tables of the stored rows (value(i) = stored CDF entry i as a double)
+  auto upload_guide = [&](auto value) -> int {
+    if (!c->guide_n) return SED_OK;
+    const int G = c->guide_n, nn = c->nu.n();
+    std::vector<uint16_t> g((size_t)c->nz * (G + 1));
+    for (int z = 0; z < c->nz; ++z)
+      for (int k = 0; k <= G; ++k) {
+        const double t = (double)k / (double)G;
+        int lo = 0, hi = nn;
+        while (lo < hi) {
+          const int m = (lo + hi) >> 1;
+          if (value((size_t)z * nn + m) <= t) lo = m + 1; else hi = m;
+        }
+        g[(size_t)z * (G + 1) + k] = (uint16_t)lo;
+      }
+    CK(cudaMemcpyAsync(c->d_cdf_guide.p, g.data(), g.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SED_OK;
+  };
+  int rc = SED_OK;
   if (c->tp.precision) {
     std::vector<float> o(2 * n), cd(n);
     for (size_t i = 0; i < n; ++i) { o[2 * i] = (float)abs[i]; o[2 * i + 1] = scat ? (float)scat[i] : 0.f; cd[i] = (float)emis_cdf[i]; }
@@ -522,6 +552,7 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
         co[(size_t)z * c->n_coarse + k] = cd[(size_t)z * c->nu.n() + std::min((k + 1) * CDF_STRIDE - 1, c->nu.n() - 1)];
     CK(cudaMemcpyAsync(c->d_cdf_coarse.p, co.data(), co.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    rc = upload_guide([&](size_t i) { return (double)cd[i]; });
   } else {
     std::vector<double> o(2 * n);
     for (size_t i = 0; i < n; ++i) { o[2 * i] = abs[i]; o[2 * i + 1] = scat ? scat[i] : 0.0; }
@@ -533,7 +564,9 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
         co[(size_t)z * c->n_coarse + k] = emis_cdf[(size_t)z * c->nu.n() + std::min((k + 1) * CDF_STRIDE - 1, c->nu.n() - 1)];
     CK(cudaMemcpyAsync(c->d_cdf_coarse.p, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    rc = upload_guide([&](size_t i) { return emis_cdf[i]; });
   }
+  if (rc) return rc;
   CK(cudaMemcpyAsync(c->d_eps_imc.p, eps_imc, (size_t)c->nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_opacity = true;
@@ -733,6 +766,7 @@ void sed_ctx_destroy(sed_ctx* c)
   c->d_ln_lv.release(); c->d_ln_c.release(); c->d_ln_c32.release(); c->d_fz_ia.release(); c->d_fz_c.release();
   c->d_fz_c32.release();
   c->d_opac.release(); c->d_cdf.release(); c->d_cdf_coarse.release(); c->d_counters.release();
+  c->d_cdf_guide.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -139,6 +139,7 @@ StepArgs step_args(sed_batch* b, double dt, const BatchModel* models, int64_t to
   A.a3 = c->sp.n(); A.a2 = (int64_t)c->sm.n() * A.a3; A.a1 = (int64_t)c->sn.n() * A.a2;
   A.opac = c->d_opac.p; A.cdf = c->d_cdf.p; A.eps_imc = c->d_eps_imc.p;
   A.cdf_coarse = c->d_cdf_coarse.p; A.n_coarse = c->n_coarse;
+  A.cdf_guide = c->guide_n ? c->d_cdf_guide.p : nullptr; A.guide_n = c->guide_n;
   A.rescale_lum = c->tp.core_fix_luminosity;
   A.J = c->d_J.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
   A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;

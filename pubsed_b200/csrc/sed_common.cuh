@@ -152,6 +152,24 @@ __device__ __forceinline__ int upper_bound_2level(const T* __restrict__ row, con
   return lo + upper_bound_t<T>(row + lo, hi - lo, v);
 }
 
+// upper_bound over a CDF row through its guide table: with guide[k] =
+// upper_bound(row, k / G) for a power of two G, the answer for u lies in
+// [guide[k], guide[k+1]] where k = floor(u G) (exact: u G is a scaling by a
+// power of two), so a binary search over that short range returns exactly
+// upper_bound(row, row + n, u).
+template <typename T>
+__device__ __forceinline__ int upper_bound_guided(const T* __restrict__ row, const uint16_t* __restrict__ guide, int G,
+                                                  double u)
+{
+  const int k = (int)(u * (double)G);
+  int lo = __ldg(guide + k), hi = __ldg(guide + k + 1);
+  while (lo < hi) {
+    const int m = (lo + hi) >> 1;
+    if ((double)__ldg(row + m) <= u) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
 // locate_array::locate (src/utils/locate_array.cpp:191-218): fast lin/log
 // index corrected by a binary search unless it is 0 or n
 __device__ __forceinline__ int loc_locate(const DevLoc& g, double x)

@@ -121,6 +121,8 @@ struct sed_ctx {
   bool have_opacity = false;
   DevBuf<unsigned char> d_opac, d_cdf, d_cdf_coarse;
   int n_coarse = 0;
+  DevBuf<uint16_t> d_cdf_guide;  // CDF guide tables, guide_n + 1 entries per zone
+  int guide_n = 0;
   int chunk_zones = 0;  // zones per opacity-build pass (bounds the FP64/LTE scratch)
   int opacity_launches = 0;
   DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_epsl64, d_epsf64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,

@@ -42,6 +42,8 @@ struct StepArgs {
   const void* cdf;            // [nz*n_nu] double or float emissivity CDF
   const void* cdf_coarse;     // [nz*n_coarse] every CDF_STRIDE-th CDF value (last of each block)
   int32_t n_coarse;           // blocks per zone row = ceil(n_nu / CDF_STRIDE)
+  const uint16_t* cdf_guide;  // [nz*(guide_n+1)] guide[k] = upper_bound(CDF row, k / guide_n), or null
+  int32_t guide_n;            // power of two >= n_nu (0: no guide table, n_nu > 65535)
   const double* eps_imc;      // [nz]
   int32_t rescale_lum;        // core_fix_luminosity (steady-state rescale)
   int32_t pad_;
@@ -148,6 +150,8 @@ struct OpacityArgs {
   void* cdf_out;                         // double / float [nz*n_nu]
   void* cdf_coarse_out;                  // double / float [nz*n_coarse]
   int32_t n_coarse;
+  uint16_t* cdf_guide_out;               // [nz*(guide_n+1)] or null
+  int32_t guide_n;
   double *eps_imc, *planck, *ross, *L_th;
 };
 

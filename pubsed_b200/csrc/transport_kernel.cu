@@ -240,6 +240,18 @@ struct GridZoneOf {
   __device__ int operator()(const double* x) const { return get_zone<GRID>(G, x); }
 };
 
+// upper_bound(CDF row of zone iz, u): through the guide table when there is
+// one, else the two-level search over the coarse table
+template <typename CT>
+__device__ __forceinline__ int cdf_row_sample(const StepArgs& A, int iz, double u)
+{
+  const int nn = A.nu.n;
+  const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)iz * nn;
+  if (A.cdf_guide) return upper_bound_guided<CT>(row, A.cdf_guide + (size_t)iz * (A.guide_n + 1), A.guide_n, u);
+  const CT* crow = reinterpret_cast<const CT*>(A.cdf_coarse) + (size_t)iz * A.n_coarse;
+  return upper_bound_2level<CT>(row, crow, nn, A.n_coarse, u);
+}
+
 template <typename CT>
 __device__ __forceinline__ int cdf_sample(const CT* __restrict__ y, int n, double u)
 {
@@ -268,11 +280,9 @@ __device__ __forceinline__ void isotropic_scatter(const StepArgs& A, const GridD
   const double Dn[3] = {smu * c, smu * s, mu};
   if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
     const int nn = A.nu.n;
-    const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
-    const CT* crow = reinterpret_cast<const CT*>(A.cdf_coarse) + (size_t)p.ind * A.n_coarse;
     const double u = rng.next();
     // cdf_array::sample (src/transport/cdf_array.h:84-89): upper_bound
-    const int inu = (nn == 1) ? 0 : upper_bound_2level<CT>(row, crow, nn, A.n_coarse, u);
+    const int inu = (nn == 1) ? 0 : cdf_row_sample<CT>(A, p.ind, u);
     p.nu = loc_sample(A.nu, inu, rng.next());
   }
   V[0] = -1 * V[0]; V[1] = -1 * V[1]; V[2] = -1 * V[2];
@@ -324,10 +334,8 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
   const double Dn[3] = {smu * c, smu * s, mu};
   if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
     const int nn = A.nu.n;
-    const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
-    const CT* crow = reinterpret_cast<const CT*>(A.cdf_coarse) + (size_t)p.ind * A.n_coarse;
     const double u = w01(w.z);
-    const int inu = (nn == 1) ? 0 : upper_bound_2level<CT>(row, crow, nn, A.n_coarse, u);
+    const int inu = (nn == 1) ? 0 : cdf_row_sample<CT>(A, p.ind, u);
     p.nu = loc_sample(A.nu, inu, w01(w.w));
   }
   // comoving -> lab with the velocity reversed: beta' = -beta

@@ -76,3 +76,32 @@ def test_grey_opacity_tables_match(sed_lib):
     # sequential sum (1024 bins)
     for k in ("emis_cdf", "L_thermal", "planck_mean", "rosseland_mean"):
         assert _rel(Og[k], Oo[k]) <= 1e-13, k
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_loaded_tables_replay(sed_lib, precision):
+    """sed_load_opacity: tables computed elsewhere (here the oracle's) drive the
+    packet kernel; the coarse and guide tables of the emissivity CDF are built
+    from them on the host.  FP64: every packet as in the oracle; mixed: the
+    same tables in FP32, spectrum within Monte Carlo noise of the FP64 run
+    (the mixed form draws its own deviates)."""
+    n = 4000
+    w = workloads.type_ia(n_packets=n, n_zones=32, n_lines=5000, n_bins=512, spectrum_bins=64, seed=23)
+    o = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    o.set_opacity(1.0)
+    T = o.opacity()
+    g = oracle_lib.Engine(sed_lib, "sed_", w, precision=precision)
+    g.load_opacity(T["abs"], T["scat"], T["emis_cdf"], T["eps_imc"])
+    g.record(True)
+    o.record(True)
+    so = o.transport(1.0)
+    sg = g.transport(1.0)
+    if precision == abi.PREC_FP64:
+        ro, rg = o.records(n), g.records(n)
+        assert np.array_equal(ro["fate"], rg["fate"])
+        assert np.array_equal(ro["draws"], rg["draws"])
+        oracle_lib.check_states(rg["state"], ro["state"])
+    else:
+        assert abs(sg["n_escaped"] - so["n_escaped"]) <= 5 * np.sqrt(so["n_escaped"]) + 5
+    o.close()
+    g.close()
