@@ -327,11 +327,13 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
   p.e = p.e * dshift_in;
   p.nu = p.nu * dshift_in;
   const double mu = 1 - 2.0 * w01(w.x);
-  const double phi = 2.0 * PI * w01(w.y);
+  // the azimuth's sine and cosine in FP32 (a direction sample, not a frame
+  // transform; the transforms below and the normalisation are FP64)
+  const float phi = (float)(2.0 * PI * w01(w.y));
   const double smu = sqrt(1 - mu * mu);
-  double s, c;
-  sincos(phi, &s, &c);
-  const double Dn[3] = {smu * c, smu * s, mu};
+  float sf, cf;
+  sincosf(phi, &sf, &cf);
+  const double Dn[3] = {smu * (double)cf, smu * (double)sf, mu};
   if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
     const int nn = A.nu.n;
     const double u = w01(w.z);
@@ -454,10 +456,11 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
   return v;
 }
 
-// Block size and minimum resident blocks per SM of the packet kernel.  The
-// kernel is latency bound (dependent FP64 chains, L2 table loads): 8 blocks
-// of 128 threads (32 warps/SM, 64 registers) run the Type Ia step 19% faster
-// than 2 blocks of 256 at 120 registers, despite a small register spill.
+// Block size and minimum resident blocks per SM of the differentiable-
+// transport kernels.  The packet kernel is latency bound (dependent FP64
+// chains, L2 table loads): 24-32 warps per SM at 64-80 registers beat fewer
+// warps with more registers (2 blocks of 256 at 120 registers ran the Type
+// Ia step 19% slower), despite a small register spill.
 #ifndef SED_PROP_THREADS
 #define SED_PROP_THREADS 128
 #endif
@@ -712,7 +715,10 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       double tau_r;
       if constexpr (FAST) {
         blk = rng.block();
-        tau_r = -1.0 * log(1 - u01(blk.x, blk.y));
+        // -log(1 - u) in FP32: log1pf for u < 1/2, logf of the exact FP64
+        // 1 - u above, so the relative error stays ~1e-7 over the whole range
+        const double u = u01(blk.x, blk.y);
+        tau_r = (double)((u < 0.5) ? -log1pf(-(float)u) : -logf((float)(1.0 - u)));
       } else {
         tau_r = -1.0 * log(1 - rng.next());
       }
@@ -938,15 +944,19 @@ int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int 
   return 1;
 }
 
+// Single-context shapes, measured on the Type Ia step (1e7 packets): the
+// mixed form runs best with 256 x 3 (80 registers, 976 ms vs 1019 ms at
+// 128 x 8), the FP64 form with 256 x 4 (64 registers, 1753 ms vs 1788 ms).
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
-  constexpr int T = SED_PROP_THREADS, B = SED_PROP_MINB;
   // mixed tables on a grid with a tabulated velocity field: the reference's
   // expressions (the division-free transforms assume v = x / t)
   if (sizeof(OT) == sizeof(float2) && !g.homologous)
-    return launch_kernel_t<GRID, OT, CT, 0, T, B, 0, false>(a, g, 0, num_sms, a.n_packets, s);
-  return launch_kernel_t<GRID, OT, CT, 0, T, B>(a, g, 0, num_sms, a.n_packets, s);
+    return launch_kernel_t<GRID, OT, CT, 0, 256, 4, 0, false>(a, g, 0, num_sms, a.n_packets, s);
+  if (sizeof(OT) == sizeof(float2))
+    return launch_kernel_t<GRID, OT, CT, 0, 256, 3>(a, g, 0, num_sms, a.n_packets, s);
+  return launch_kernel_t<GRID, OT, CT, 0, 256, 4>(a, g, 0, num_sms, a.n_packets, s);
 }
 
 // batched kernel shapes {threads, min blocks per SM}: 32 or 24 warps per SM
