@@ -35,6 +35,8 @@ struct sed_batch {
   DevBuf<double> d_rin, d_core_cdf, d_flux, d_click;
   DevBuf<unsigned long long> d_model_esc;
   DevBuf<uint32_t> d_step;
+  DevBuf<double> d_zone_rep;            // copies of the zone-scalar tallies (many zones)
+  int n_rep = 0;
   double models_dt = -1;                // dt the device model table was written for
   // launch shape
   int variant = 0, blocks_per_sm = 0, queue_chunk = 1;
@@ -147,6 +149,8 @@ StepArgs step_args(sed_batch* b, double dt, const BatchModel* models, int64_t to
   A.models = models; A.n_models = b->n_models; A.queue_chunk = std::max(1, b->queue_chunk);
   A.zone_nbr = b->d_nbr.p; A.zone_rin = b->d_rin.p;
   A.model_escaped = b->d_model_esc.p; A.step_dev = b->d_step.p;
+  A.n_rep = A.smem_zones ? 0 : b->n_rep;
+  A.zone_rep = b->d_zone_rep.p;
   return A;
 }
 
@@ -173,6 +177,7 @@ int wipe(sed_batch* b)
   BCK(cudaMemsetAsync(b->d_click.p, 0, b->d_click.n * sizeof(double), s));
   BCK(cudaMemsetAsync(c->d_counters.p, 0, (C_COUNT + 1) * sizeof(unsigned long long), s));
   BCK(cudaMemsetAsync(b->d_model_esc.p, 0, b->d_model_esc.n * sizeof(unsigned long long), s));
+  if (b->n_rep) BCK(cudaMemsetAsync(b->d_zone_rep.p, 0, b->d_zone_rep.n * sizeof(double), s));
   return SED_OK;
 }
 
@@ -324,6 +329,12 @@ int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n
   if ((e = b->d_click.resize((size_t)n_models * nspec)) != cudaSuccess) return fail(e);
   if ((e = b->d_model_esc.resize(n_models)) != cudaSuccess) return fail(e);
   if ((e = b->d_step.resize(1)) != cudaSuccess) return fail(e);
+  // zones beyond the per-block shared-memory tallies: 32 copies of the
+  // zone-scalar tallies (fewer if that would pass 256 MiB)
+  if ((size_t)5 * nz_tot * sizeof(double) > 64 * 1024) {
+    b->n_rep = (int)std::min<size_t>(32, std::max<size_t>(1, (size_t(256) << 20) / (5 * sizeof(double) * nz_tot)));
+    if ((e = b->d_zone_rep.resize((size_t)b->n_rep * 5 * nz_tot)) != cudaSuccess) return fail(e);
+  }
   if ((e = cudaMemsetAsync(b->d_step.p, 0, sizeof(uint32_t), c->stream)) != cudaSuccess) return fail(e);
   if ((e = cudaMemsetAsync(b->d_flux.p, 0, b->d_flux.n * sizeof(double), c->stream)) != cudaSuccess) return fail(e);
   if ((e = cudaMemsetAsync(b->d_click.p, 0, b->d_click.n * sizeof(double), c->stream)) != cudaSuccess) return fail(e);
@@ -627,6 +638,7 @@ void sed_batch_destroy(sed_batch* b)
   for (auto& ev : b->ev) if (ev) cudaEventDestroy(ev);
   b->d_models.release(); b->d_sample_models.release(); b->d_nbr.release(); b->d_rin.release();
   b->d_core_cdf.release(); b->d_flux.release(); b->d_click.release(); b->d_model_esc.release(); b->d_step.release();
+  b->d_zone_rep.release();
   b->d_rec_fate.release(); b->d_rec_ind.release(); b->d_rec_draws.release(); b->d_rec_state.release();
   if (b->inner) sed_ctx_destroy(b->inner);
   delete b;

@@ -36,6 +36,8 @@ struct StepArgs {
   const double* core_cdf;     // [n_nu] normalised core emission CDF
   int32_t max_segments;
   int32_t smem_zones;         // 1: per-block shared-memory zone tallies
+  int32_t n_rep;              // >0 (and smem_zones 0): zone-scalar tallies in n_rep global copies
+  double* zone_rep;           // [n_rep][5][nz] e_abs, fx, fy, fz, fr copies, summed by the finish kernel
   DevLoc nu, st, sn, sm, sp;  // frequency grid and spectrum grids
   int64_t a1, a2, a3;         // spectrum strides
   const void* opac;           // [nz*n_nu] double2 {abs, scat} or float2

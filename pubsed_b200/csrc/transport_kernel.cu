@@ -499,6 +499,12 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   double* t_fy = A.smem_zones ? s_tal + 2 * nz : A.fy;
   double* t_fz = A.smem_zones ? s_tal + 3 * nz : A.fz;
   double* t_fr = A.smem_zones ? s_tal + 4 * nz : A.fr;
+  if (!A.smem_zones && A.n_rep > 0) {
+    // the zones of the one or two models in flight take the atomics of
+    // every block: blocks spread them over n_rep copies
+    double* base = A.zone_rep + (size_t)(blockIdx.x % A.n_rep) * 5 * nz;
+    t_eabs = base; t_fx = base + nz; t_fy = base + 2 * nz; t_fz = base + 3 * nz; t_fr = base + 4 * nz;
+  }
   const OT* __restrict__ opac = reinterpret_cast<const OT*>(A.opac);
   // the mixed form takes the division-free transforms on homologous grids;
   // the FP64 form keeps the reference's expressions
@@ -904,6 +910,15 @@ __global__ void finish_zones_batch_kernel(const StepArgs A, const double* __rest
 {
   const int iz = blockIdx.x;
   if (iz >= nz) return;
+  if (!A.smem_zones && A.n_rep > 0) {  // sum the zone-scalar tally copies
+    if (threadIdx.x < 5) {
+      double sum = 0;
+      for (int r = 0; r < A.n_rep; ++r) sum += A.zone_rep[((size_t)r * 5 + threadIdx.x) * nz + iz];
+      double* dst[5] = {A.e_abs, A.fx, A.fy, A.fz, A.fr};
+      dst[threadIdx.x][iz] = sum;
+    }
+    __syncthreads();
+  }
   double fac = 1.0;
   if (do_rescale) {
     const int m = __ldg(A.zone_nbr + iz).w;

@@ -127,3 +127,25 @@ def test_autotuned_shapes_keep_every_packet(sed_lib):
             r1 = other.records(m, w.n_packets)
             for k in ("fate", "ind", "draws", "state"):
                 assert np.array_equal(r0[k], r1[k]), (m, k)
+
+
+def test_many_zone_batch_matches_separate_contexts(sed_lib):
+    """More zones than the per-block shared-memory tallies hold (24 models,
+    ~2600 zones): the zone-scalar tallies go to global copies that the finish
+    kernel sums; every model still matches its own context."""
+    bw = small_batch(n_models=24, zones=(90, 130), packets=(300, 800), seed=17)
+    assert bw.n_zones * 5 * 8 > 64 * 1024
+    be = BatchEngine(bw, precision=abi.PREC_FP64, graph=True)
+    be.record(True)
+    be.step(1.0)
+    for m, w in enumerate(bw.models):
+        g = oracle_lib.Engine(sed_lib, "sed_", w)
+        g.set_opacity(1.0)
+        g.record(True)
+        g.transport(1.0)
+        _same_packets(be.records(m, w.n_packets), g.records(w.n_packets))
+        _same_tallies(be.tallies(m), g.tallies())
+        fs, cs = g.spectrum()
+        fb, cb = be.spectrum(m)
+        assert np.array_equal(cb, cs)
+        g.close()
