@@ -575,10 +575,12 @@ def main():
     if os.path.exists(tfile):
         with open(tfile) as f:
             tr = json.load(f)
-        # DRAM bytes of one launch captured with ncu on this workload; the
-        # tables stay L2-resident, so traffic does not grow with the packet
-        # count and is only reported for the captured packet count
-        if int(tr.get("packets", -1)) == args.packets and tr.get("workload") == w.name:
+        # DRAM bytes of one launch of this workload's packet kernel captured
+        # with ncu (after the same L2 flush); the tables stay L2-resident, so
+        # the traffic is their first touch and does not grow with the packet
+        # count when the capture says so
+        same_n = int(tr.get("packets", -1)) == args.packets or tr.get("scales_with_packets") is False
+        if same_n and tr.get("workload") == w.name:
             traffic = float(tr["dram_bytes"])
 
     line = {
