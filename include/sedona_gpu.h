@@ -240,6 +240,18 @@ void sed_ctx_destroy(sed_ctx* ctx);
 /* Library version / build string (never NULL). */
 const char* sed_version(void);
 
+/* Radiative-equilibrium gas temperature of every zone after a transport step:
+ * transport::solve_eq_temperature (src/transport/solve_equilibrium.cpp:66-96)
+ * for LTE, i.e. per zone Brent's method (temp_brent_method, :227-320) on
+ * sum_i 4 pi kappa_abs B_nu(T) dnu - e_abs over [limits_temp_min,
+ * limits_temp_max] with the absorption opacities of the last opacity build;
+ * with set_Tgas_to_Trad, T = (e_rad / a)^(1/4).  The new temperatures replace
+ * the context's zone temperatures (the next sed_set_opacity uses them) and are
+ * copied to T_gas when it is not NULL.  A zone where Brent exhausts its 100
+ * iterations gets T = 0 as in the reference; their number goes to
+ * *n_unsolved (may be NULL). */
+int sed_solve_temperature(sed_ctx* ctx, int32_t set_Tgas_to_Trad, double* T_gas, int32_t* n_unsolved);
+
 /* Sets the Philox step number the next transport (or weighted forward) of
  * the context draws with; each step advances it by one.  Runs given the same
  * step number consume the same deviates (common random numbers), as

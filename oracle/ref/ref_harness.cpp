@@ -227,6 +227,10 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
     }
   }
   t.reduce_radiation(dt);
+  // the temperature solve transport::step runs next (transport.cpp:126-132);
+  // dump_tables then records the solved T_gas
+  if (t.radiative_eq == 1 && t.fix_Tgas_during_transport_ == 0 && t.solve_Tgas_with_updated_opacities_ == 0)
+    t.solve_eq_temperature();
   o.i32("pkt_fate", fate); o.i32("pkt_ind", ind); o.i32("pkt_draws", draws); o.f64("pkt_state", st);
   o.scalar("n_packets", (double)n); o.scalar("n_escaped", n_escaped); o.scalar("propagate_seconds", T1 - T0);
   o.scalar("draws_per_emitted_packet", K);

@@ -1448,6 +1448,93 @@ int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* st)
   return SED_OK;
 }
 
+/* ---------------------------------------------------------------- temperature
+ * transport::solve_eq_temperature (src/transport/solve_equilibrium.cpp:66-96)
+ * for LTE: per zone temp_brent_method (:227-320) on rad_eq_function_LTE with
+ * solve_flag 0 (:113-170): the emission sum_i 4 pi kappa_abs B_nu(T) dnu with
+ * the tables of the last set_opacity, minus the zone's normalised e_abs.
+ * set_Tgas_to_Trad: T = (e_rad / a)^(1/4) (:72-74). */
+static double blackbody_nu(double T, double nu)  /* transport_opacity.cpp:322-326 */
+{
+  double zeta = PC_H * nu / PC_K / T;
+  return 2.0 * nu * nu * nu * PC_H / PC_C / PC_C / (exp(zeta) - 1);
+}
+
+static double rad_eq_lte(const oracle_ctx* o, int c, double T)
+{
+  int nn = o->nu.n;
+  double E_emitted = 0.;
+  double E_absorbed = o->e_abs[c];
+  if (nn == 1) {
+    E_emitted = 4.0 * PC_PI * o->abs[c] * PC_SB / PC_PI * pow(T, 4);
+  } else {
+    for (int i = 0; i < nn; i++) {
+      double dnu = lg_delta(&o->nu, i);
+      double nu = lg_center(&o->nu, i);
+      double B_nu = blackbody_nu(T, nu);
+      double kappa_abs = o->abs[(size_t)c * nn + i];
+      E_emitted += 4.0 * PC_PI * kappa_abs * B_nu * dnu;
+    }
+  }
+  return (E_emitted - E_absorbed);
+}
+
+#define ORACLE_SIGN(a, b) ((b) >= 0.0 ? fabs(a) : -fabs(a))
+static double temp_brent(const oracle_ctx* o, int cell, int* failed)
+{
+  double brent_solve_tolerance = 1.0e-2;
+  int ITMAX = 100;
+  double EPS = 3.0e-8;
+  double a = o->op.temp_min, b = o->op.temp_max, c = b, d = 0, e = 0, min1, min2;
+  double fa = rad_eq_lte(o, cell, a), fb = rad_eq_lte(o, cell, b);
+  double fc, p, q, r, s, tol1, xm;
+  fc = fb;
+  for (int iter = 1; iter <= ITMAX; iter++) {
+    if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) { c = a; fc = fa; e = d = b - a; }
+    if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+    tol1 = 2.0 * EPS * fabs(b) + 0.5 * brent_solve_tolerance;
+    xm = 0.5 * (c - b);
+    if (fabs(xm) <= tol1 || fb == 0.0) return b;
+    if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+      s = fb / fa;
+      if (a == c) { p = 2.0 * xm * s; q = 1.0 - s; }
+      else {
+        q = fa / fc;
+        r = fb / fc;
+        p = s * (2.0 * xm * q * (q - r) - (b - a) * (r - 1.0));
+        q = (q - 1.0) * (r - 1.0) * (s - 1.0);
+      }
+      if (p > 0.0) q = -q;
+      p = fabs(p);
+      min1 = 3.0 * xm * q - fabs(tol1 * q);
+      min2 = fabs(e * q);
+      if (2.0 * p < (min1 < min2 ? min1 : min2)) { e = d; d = p / q; }
+      else { d = xm; e = d; }
+    } else { d = xm; e = d; }
+    a = b;
+    fa = fb;
+    if (fabs(d) > tol1) b += d;
+    else b += ORACLE_SIGN(tol1, xm);
+    fb = rad_eq_lte(o, cell, b);
+  }
+  (*failed)++;
+  return 0.0;  /* "Maximum number of iterations exceeded in zbrent" */
+}
+
+int oracle_solve_temperature(oracle_ctx* o, int32_t set_Tgas_to_Trad, double* T_gas, int32_t* n_unsolved)
+{
+  if (!o || !o->have_grid) return SED_ERR_STATE;
+  if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
+  int failed = 0;
+  for (int i = 0; i < o->nzones; i++) {
+    if (set_Tgas_to_Trad) o->T[i] = pow(o->e_rad[i] / PC_A, 0.25);
+    else o->T[i] = temp_brent(o, i, &failed);
+  }
+  if (T_gas) memcpy(T_gas, o->T, (size_t)o->nzones * sizeof(double));
+  if (n_unsolved) *n_unsolved = failed;
+  return SED_OK;
+}
+
 int oracle_get_spectrum(oracle_ctx* o, double* flux, double* click)
 {
   if (!o) return SED_ERR_ARG;

@@ -47,6 +47,8 @@ int oracle_set_rng_step(oracle_ctx* o, uint32_t step);
 int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* stats);
 int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
 int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
+/* radiative-equilibrium temperature solve after a transport step */
+int oracle_solve_temperature(oracle_ctx* o, int32_t set_Tgas_to_Trad, double* T_gas, int32_t* n_unsolved);
 const char* oracle_last_error(oracle_ctx* o);
 /* Philox4x32-10 block and the packet-stream uniform (oracle/philox.h) */
 void oracle_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

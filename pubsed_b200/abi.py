@@ -177,6 +177,7 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         "diff_forward": ([vp, C.c_double, _dp, C.c_int32, C.POINTER(StepStats)], C.c_int),
         "diff_vjp": ([vp, _dp, _dp, C.POINTER(StepStats)], C.c_int),
         "diff_jacobian": ([vp, _dp, C.POINTER(StepStats)], C.c_int),
+        "solve_temperature": ([vp, C.c_int32, _dp, _ip], C.c_int),
     })
     if prefix == "sed_":
         i64p = C.POINTER(C.c_int64)

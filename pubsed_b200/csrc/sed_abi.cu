@@ -658,6 +658,30 @@ int sed_step(sed_ctx* c, double dt, sed_step_stats* stats)
   return rc;
 }
 
+int sed_solve_temperature(sed_ctx* c, int32_t set_Tgas_to_Trad, double* T_gas, int32_t* n_unsolved)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_solve_temperature: no grid");
+  if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "sed_solve_temperature: no opacity tables");
+  TemperatureArgs A{};
+  A.nz = c->nz; A.precision = c->tp.precision; A.set_Tgas_to_Trad = set_Tgas_to_Trad ? 1 : 0;
+  A.nu = dev_loc(c->nu, c->d_nu);
+  A.opac = c->d_opac.p; A.e_abs = c->d_e_abs.p; A.e_rad = c->d_e_rad.p;
+  A.temp_min = c->op.temp_min; A.temp_max = c->op.temp_max;
+  A.T = c->d_T.p;
+  CK(c->d_temp_bad.resize(1));
+  A.n_unsolved = c->d_temp_bad.p;
+  CK(cudaMemsetAsync(c->d_temp_bad.p, 0, sizeof(int32_t), c->stream));
+  launch_temperature(A, c->stream);
+  CK(cudaGetLastError());
+  int32_t bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->d_temp_bad.p, sizeof bad, cudaMemcpyDeviceToHost, c->stream));
+  if (T_gas) CK(cudaMemcpyAsync(T_gas, c->d_T.p, (size_t)c->nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (n_unsolved) *n_unsolved = bad;
+  return SED_OK;
+}
+
 int sed_get_spectrum(sed_ctx* c, double* flux, double* click)
 {
   if (!c) return SED_ERR_ARG;
@@ -767,6 +791,7 @@ void sed_ctx_destroy(sed_ctx* c)
   c->d_fz_c32.release();
   c->d_opac.release(); c->d_cdf.release(); c->d_cdf_coarse.release(); c->d_counters.release();
   c->d_cdf_guide.release();
+  c->d_temp_bad.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -128,6 +128,7 @@ struct sed_ctx {
   DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_epsl64, d_epsf64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
       d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
   DevBuf<int32_t> d_solve_err;
+  DevBuf<int32_t> d_temp_bad;     // zones the temperature solve left unsolved
 
   // tallies
   DevBuf<double> d_J, d_e_abs, d_e_rad, d_fx, d_fy, d_fz, d_fr, d_flux, d_click;

@@ -105,6 +105,19 @@ int launch_propagate_batch(const StepArgs& a, const GridDev& g, int variant, int
 // the zone's model factor, then the device step counter advances
 int launch_finish_batch(const StepArgs& a, const double* vol, int nz_total, int64_t nspec, cudaStream_t s);
 
+// ---------------------------------------------------------------- temperature
+struct TemperatureArgs {
+  int32_t nz, precision, set_Tgas_to_Trad, pad_;
+  DevLoc nu;
+  const void* opac;            // {abs, scat} pairs, double2 or float2 [nz * n_nu]
+  const double *e_abs, *e_rad; // normalised zone tallies of the last step
+  double temp_min, temp_max;   // limits_temp_min / limits_temp_max
+  double* T;                   // [nz] zone temperature, replaced
+  int32_t* n_unsolved;         // zones where Brent hit its iteration limit
+};
+// radiative-equilibrium temperature of every zone (one thread per zone)
+int launch_temperature(const TemperatureArgs& a, cudaStream_t s);
+
 // ---------------------------------------------------------------- opacity
 struct OpacityArgs {
   int32_t nzones, n_nu, nelem;

@@ -8,7 +8,8 @@ inputs, plus the reference's outputs:
 
   replay_*.npz   one transport step in replay mode (per-packet fate, final
                  zone, number of deviates drawn, final state; J_nu, e_abs,
-                 e_rad, forces, spectrum; opacity tables)
+                 e_rad, forces, spectrum; opacity tables; the zone
+                 temperatures after the step's radiative-equilibrium solve)
   locate_kat.json  value/index pairs printed by the reference's own
                  src/utils/locate_array_test.cpp
 
@@ -51,7 +52,7 @@ FREE_CASES = {
 
 KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "J_nu", "e_abs", "e_rad", "fx_rad", "fy_rad", "fz_rad",
         "fr_rad", "spec_flux", "spec_click", "abs", "scat", "emis_cdf", "n_elec", "eps_imc", "planck_mean",
-        "rosseland_mean", "L_thermal", "nu_right", "nu_left"]
+        "rosseland_mean", "L_thermal", "nu_right", "nu_left", "T_gas"]
 
 
 def make_workload(gen: str, kw: dict):
@@ -68,6 +69,10 @@ def main():
         w = make_workload(gen, kw)
         out = run_ref.run(w, "replay", threads=1, seed=kw.get("seed", 0))
         arrays = {k: out[k] for k in KEYS}
+        # with grey opacity the reference never sets zone n_elec: its dump is
+        # whatever the memory held; the restatement has zeros there
+        if float(w.params.get("opacity_grey_opacity", 0)) != 0:
+            arrays["n_elec"] = np.zeros_like(arrays["n_elec"])
         np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
                             n_escaped=out["n_escaped"], **arrays)
         print(name, "packets", int(out["n_packets"]), "escaped", int(out["n_escaped"]))

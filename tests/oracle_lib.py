@@ -238,3 +238,13 @@ def spectrum_second_moment(eng: Engine, w, n: int) -> tuple:
         s1[b] += e
         s2[b] += e * e
     return s1, s2
+
+
+def solve_temperature(eng: Engine, set_Tgas_to_Trad: int = 0):
+    """Radiative-equilibrium temperature solve (sed_/oracle_solve_temperature);
+    returns the new zone temperatures and the number of zones Brent left unsolved."""
+    T = np.zeros(eng.nz)
+    bad = C.c_int32(0)
+    eng.check(eng.fn("solve_temperature")(eng.ctx, set_Tgas_to_Trad, T.ctypes.data_as(abi._dp), C.byref(bad)),
+              "solve_temperature")
+    return T, int(bad.value)

@@ -105,3 +105,36 @@ def test_loaded_tables_replay(sed_lib, precision):
         assert abs(sg["n_escaped"] - so["n_escaped"]) <= 5 * np.sqrt(so["n_escaped"]) + 5
     o.close()
     g.close()
+
+
+@pytest.mark.parametrize("case", ["grey", "ia"])
+def test_temperature_solve_matches_oracle(sed_lib, case):
+    """sed_solve_temperature after a replayed step: Brent on the same emission
+    sums gives the oracle's temperatures (the oracle's are the reference's,
+    tests/test_oracle_golden.py); the next opacity build runs at them; and
+    set_Tgas_to_Trad gives (e_rad / a)^(1/4)."""
+    if case == "grey":
+        w = workloads.lightbulb_grey(n_packets=20000, n_zones=64, n_bins=256, radiative_eq=1, seed=4)
+    else:
+        w = workloads.type_ia(n_packets=4000, n_zones=32, n_lines=5000, n_bins=512, spectrum_bins=64, seed=24)
+    o = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    g = oracle_lib.Engine(sed_lib, "sed_", w)
+    for e in (o, g):
+        e.set_opacity(1.0)
+        e.transport(1.0)
+    To, bo = oracle_lib.solve_temperature(o)
+    Tg, bg = oracle_lib.solve_temperature(g)
+    assert bo == bg == 0
+    # e_abs agrees to the summation order (1e-12); the root to far below
+    # Brent's 1e-2 K tolerance
+    assert np.max(np.abs(Tg - To) / To) <= 1e-9, np.max(np.abs(Tg - To) / To)
+    for e in (o, g):
+        e.set_opacity(1.0)
+    Oo, Og = o.opacity(), g.opacity()
+    for k in ("abs", "scat", "eps_imc"):
+        assert _rel(Og[k], Oo[k]) <= 1e-8, k
+    Ro, _ = oracle_lib.solve_temperature(o, set_Tgas_to_Trad=1)
+    Rg, _ = oracle_lib.solve_temperature(g, set_Tgas_to_Trad=1)
+    assert _rel(Rg, Ro) <= 1e-10
+    o.close()
+    g.close()

@@ -59,6 +59,13 @@ def test_oracle_matches_reference_replay(name):
     f, c = e.spectrum()
     assert np.array_equal(c, ref["spec_click"])
     assert _rel(f, ref["spec_flux"]) <= 1e-12
+    # the radiative-equilibrium temperature solve that ends transport::step
+    if int(w.params.get("transport_radiative_equilibrium", 0)):
+        Tg, nbad = oracle_lib.solve_temperature(e)
+        assert nbad == 0
+        # Brent on the same emission sums: the same iterates up to the last
+        # bit of e_abs (a tally, within 1e-12 above)
+        assert _rel(Tg, ref["T_gas"]) <= 1e-10
 
 
 @pytest.mark.parametrize("name", CASES)
