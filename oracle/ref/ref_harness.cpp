@@ -295,6 +295,13 @@ int main(int argc, char** argv)
   } else if (mode == "replay") {
     replay_step(t, dt, seed, step, o, threads);
     dump_tables(t, o);
+    // the reference's own text outputs of this step: spectrum_array::print
+    // (<prefix>_spectrum.dat) and, for 1D spheres, grid_1D_sphere::
+    // write_plotfile (plt_00001.dat in the working directory); their HDF5
+    // halves go to the stand-in, which writes nothing
+    t.optical_spectrum.set_name(o.prefix + "_spectrum");
+    t.optical_spectrum.print(0);
+    if (grid_type == "grid_1D_sphere") grid->write_plotfile(1, t.t_now_, 0);
   } else if (mode == "free") {
     oracle_rng_free_running();
     std::vector<double> times, opac_times;

@@ -59,6 +59,16 @@ class Engine:
         self._check(self.L.sed_step(self.ctx, dt, C.byref(st)), "sed_step")
         return st.as_dict()
 
+    def solve_temperature(self, set_Tgas_to_Trad: int = 0):
+        """sed_solve_temperature: new zone temperatures (also kept on the
+        device for the next opacity build) and the number of zones Brent left
+        unsolved."""
+        T = np.zeros(self.nz)
+        bad = C.c_int32(0)
+        self._check(self.L.sed_solve_temperature(self.ctx, int(set_Tgas_to_Trad), T.ctypes.data_as(abi._dp),
+                                                 C.byref(bad)), "sed_solve_temperature")
+        return T, int(bad.value)
+
     def spectrum(self):
         flux = np.zeros(self.nspec)
         click = np.zeros(self.nspec)

@@ -37,6 +37,14 @@ class LocGrid:
     def center(self) -> np.ndarray:
         return 0.5 * (self.left() + self.right)
 
+    def delta_at(self, i: int) -> float:
+        """locate_array::delta (locate_array.h:69-72)"""
+        return float(self.right[0] - self.min) if i == 0 else float(self.right[i] - self.right[i - 1])
+
+    def center_at(self, i: int) -> float:
+        """locate_array::center (locate_array.h:54-57)"""
+        return float(0.5 * (self.min + self.right[0])) if i == 0 else float(0.5 * (self.right[i - 1] + self.right[i]))
+
     def scaled(self, e: float) -> "LocGrid":
         """locate_array::scale (locate_array.cpp:540-548)"""
         d = self.delta * e if self.type == LOC_LIN else self.delta

@@ -480,3 +480,80 @@ def batch64(n_models: int = 64, zones: tuple = (64, 512), packets: tuple = (1e5,
     return BatchWorkload("batch64_1d", models,
                          notes={"n_models": n_models, "n_lines": n_lines, "n_bins": n_bins,
                                 "packet_scale": packet_scale})
+
+
+# ---------------------------------------------------------------- model files
+def read_mod_1d(path: str, grey_opacity: float = 0.0) -> ZoneModel:
+    """A 1D_sphere ASCII model file (".mod"), as grid_1D_sphere::read_ascii_file
+    reads it (src/grid/grid_1D_sphere.cpp:241-332): "1D_sphere <standard|SNR>",
+    n_zones, r_min, t_exp, n_elems, the Z.A species, then per zone r_out (not
+    in SNR files, where r_out = v t), v, rho, T_gas and the mass fractions,
+    normalised per zone.  The zone velocities are kept for non-homologous
+    runs (hydro_module "none")."""
+    with open(path) as f:
+        tok = f.read().split()
+    if tok[0] != "1D_sphere":
+        raise ValueError("grid type given in model file is not 1D_sphere")
+    system = tok[1]
+    if system not in ("standard", "SNR"):
+        raise ValueError("don't recognize model type " + system)
+    snr = system == "SNR"
+    n = int(tok[2])
+    r_min = float(tok[3])
+    t = float(tok[4])
+    ne = int(tok[5])
+    species = tok[6:6 + ne]
+    Z = [int(s.split(".")[0]) for s in species]
+    A = [int(s.split(".")[1]) for s in species]
+    p = 6 + ne
+    cols = (3 if snr else 4) + ne
+    vals = [float(x) for x in tok[p:p + n * cols]]
+    if len(vals) != n * cols:
+        raise ValueError("model file ends early")
+    r_out, v, rho, T, X = [], [], [], [], []
+    for i in range(n):
+        row = vals[i * cols:(i + 1) * cols]
+        if snr:
+            v_i, rho_i, T_i = row[0], row[1], row[2]
+            r_i = v_i * t
+            xs = row[3:]
+        else:
+            r_i, v_i, rho_i, T_i = row[0], row[1], row[2], row[3]
+            xs = row[4:]
+        norm = 0.0
+        for x in xs:
+            norm += x
+        r_out.append(r_i); v.append(v_i); rho.append(rho_i); T.append(T_i)
+        X.append([x / norm for x in xs])
+    r_out = np.array(r_out)
+    return ZoneModel(type=abi.GRID_1D_SPHERE, t_now=t, rho=np.array(rho), T=np.array(T), X=np.array(X),
+                     elem_Z=np.asarray(Z, np.int32), elem_A=np.asarray(A, np.int32),
+                     vol=shell_volumes(r_min, r_out), homologous=1, r_min=r_min, r_out=r_out, v=np.array(v))
+
+
+def lightbulb_vacuum(n_packets: int = 200_000, seed: int = 0) -> Workload:
+    """The reference's spherical-lightbulb test (tests/spherical_lightbulb/1D):
+    a static vacuum 1D sphere (100 zones, r_out = (i+1) 1.728e13 cm to five
+    significant digits, v = 0,
+    rho = 1e-20 g/cm^3, T = 2e5 K, one species 1.1, t = 20 d, hydro "none"),
+    grey opacity 1e-10 cm^2/g, a 1e4 K lightbulb of radius 5e14 cm and
+    L = 1e43 erg/s, log nu grid {0.2e14, 5e15, 0.01}, radiative equilibrium,
+    one steady-state iteration.  Its analytic checks: T_gas and T_rad within
+    1% of the dilution-factor temperature beyond 5e14 cm, the spectrum within
+    10% (mean) of the core blackbody."""
+    n = 100
+    # the model file holds the radii to five significant digits
+    r_out = np.array([float("%.4e" % ((i + 1) * 1.728e13)) for i in range(n)])
+    z = ZoneModel(type=abi.GRID_1D_SPHERE, t_now=1728000.0, rho=np.full(n, 1e-20), T=np.full(n, 2e5),
+                  X=np.ones((n, 1)), elem_Z=np.array([1], np.int32), elem_A=np.array([1], np.int32),
+                  vol=shell_volumes(0.0, r_out), homologous=0, r_min=0.0, r_out=r_out, v=np.zeros(n))
+    grid = [0.2e14, 5.0e15, 0.01, 1]
+    params = {
+        "grid_type": "grid_1D_sphere", "hydro_module": "none",
+        "transport_nu_grid": grid, "spectrum_nu_grid": grid,
+        "transport_radiative_equilibrium": 1, "transport_steady_iterate": 1,
+        "core_n_emit": int(n_packets), "core_radius": 5.0e14, "core_luminosity": 1.0e43,
+        "core_temperature": 1.0e4, "opacity_grey_opacity": 1e-10,
+        "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
+    }
+    return Workload("lightbulb_vacuum_1d", params, z, notes={"r0": 5.0e14, "T": 1e4, "L": 1e43})

@@ -9,7 +9,8 @@ inputs, plus the reference's outputs:
   replay_*.npz   one transport step in replay mode (per-packet fate, final
                  zone, number of deviates drawn, final state; J_nu, e_abs,
                  e_rad, forces, spectrum; opacity tables; the zone
-                 temperatures after the step's radiative-equilibrium solve)
+                 temperatures after the step's radiative-equilibrium solve;
+                 the reference's own spectrum .dat and, for 1D, plt .dat text)
   locate_kat.json  value/index pairs printed by the reference's own
                  src/utils/locate_array_test.cpp
 
@@ -73,6 +74,13 @@ def main():
         # whatever the memory held; the restatement has zeros there
         if float(w.params.get("opacity_grey_opacity", 0)) != 0:
             arrays["n_elec"] = np.zeros_like(arrays["n_elec"])
+        # the reference's own text outputs of the step
+        with open(os.path.join(out["_dir"], "out_spectrum.dat")) as f:
+            arrays["spectrum_dat"] = np.array(f.read())
+        plt = os.path.join(out["_dir"], "plt_00001.dat")
+        if os.path.exists(plt):
+            with open(plt) as f:
+                arrays["plt_dat"] = np.array(f.read())
         np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
                             n_escaped=out["n_escaped"], **arrays)
         print(name, "packets", int(out["n_packets"]), "escaped", int(out["n_escaped"]))
