@@ -68,6 +68,9 @@ __device__ __forceinline__ int get_next_zone(const GridDev& G, const double* x, 
     if (r_core >= r_in) { r_in = r_core; ind_in = -1; }
     double l_in;
     if ((i == 0) && (r_in == 0)) l_in = -1;
+    // moving outward the reference's -x.D - sqrt(rad) is negative, and only
+    // its sign is used below: the square root is skipped, the branch is the same
+    else if (xdotD > 0) l_in = -1;
     else {
       const double rad = xdotD * xdotD + r_in * r_in - rsq;
       l_in = (rad < 0) ? -1 : -1 * xdotD - sqrt(rad);
@@ -192,6 +195,7 @@ __device__ __forceinline__ int get_next_zone_batch(const StepArgs& A, const Grid
   const double r_in = __ldg(A.zone_rin + i);
   double l_in;
   if (nb.z) l_in = -1;
+  else if (xdotD > 0) l_in = -1;  // outward: negative in the reference too, only its sign is used
   else {
     const double rad = xdotD * xdotD + r_in * r_in - rsq;
     l_in = (rad < 0) ? -1 : -1 * xdotD - sqrt(rad);
