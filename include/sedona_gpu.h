@@ -81,6 +81,15 @@ typedef struct sed_transport_params {
   sed_locate_grid spec_nu;       /* spectrum_nu_grid */
   sed_locate_grid spec_mu;       /* mu grid: init(-1, 1, spectrum_n_mu) */
   sed_locate_grid spec_phi;      /* phi grid: init(0, 2*pi, spectrum_n_phi) */
+  /* radioactive source (transport::emit_radioactive, src/transport/emission.cpp:163-243);
+   * zero-initialised fields leave it off */
+  int64_t n_emit_radioactive;    /* particles_n_emit_radioactive */
+  int32_t force_rprocess_heating;/* force_rprocess_heating */
+  int32_t reserved3;
+  sed_locate_grid gamma_nu;      /* frequency grid of the gamma-ray spectrum (which shares
+                                    spec_time, spec_mu, spec_phi); n = 0: one catch-all bin.
+                                    The reference passes spectrum_nu_grid here
+                                    (transport_init.cpp:170-173), not gamma_nu_grid */
 } sed_transport_params;
 
 /* Zone geometry and gas state (grid_general + zone, src/grid/grid_general.h:34-147,
@@ -239,6 +248,14 @@ void sed_ctx_destroy(sed_ctx* ctx);
 
 /* Library version / build string (never NULL). */
 const char* sed_version(void);
+
+/* Radioactive source results of the last step (n_emit_radioactive > 0): the
+ * escaping gamma-ray spectrum (gamma_spectrum, n_t*n_gamma_nu*n_mu*n_phi) and
+ * per zone the decay luminosity per volume L_radio_emit and the deposited
+ * luminosity per volume L_radio_dep (zone.h:41-42, normalised as
+ * transport_mpi.cpp:419-420).  NULL pointers are skipped. */
+int sed_get_gamma_spectrum(sed_ctx* ctx, double* flux, double* click);
+int sed_get_radioactive_tallies(sed_ctx* ctx, double* L_radio_emit, double* L_radio_dep);
 
 /* Radiative-equilibrium gas temperature of every zone after a transport step:
  * transport::solve_eq_temperature (src/transport/solve_equilibrium.cpp:66-96)

@@ -45,6 +45,7 @@
 #define private public
 #define protected public
 #include "transport.h"
+#include "radioactive.h"
 #include "grid_1D_sphere.h"
 #include "grid_3D_cart.h"
 #include "ParameterReader.h"
@@ -172,6 +173,30 @@ void dump_tables(transport& t, Out& o)
   o.scalar("spec_n_phi", t.optical_spectrum.phi_grid.size());
 }
 
+// Per-packet deviate counts of an emission that starts with the radioactive
+// packets (transport::emit_radioactive, src/transport/emission.cpp:165-243):
+// zone, time, gamma-ray or positron, three for the position, two for the
+// direction, and two more for an optical photon's frequency; each core
+// packet then takes K.  The gamma-ray fraction of the sampled zone comes
+// from the reference's own radioactive::decay and zone_emission_cdf_.
+struct RadioWalk {
+  transport* t;
+  int64_t n_radio;
+  uint32_t K;
+  std::vector<double> gfrac;
+  std::vector<uint32_t> counts;
+};
+
+uint32_t radio_walk_count(void* user, uint64_t k, const double* u, uint32_t n)
+{
+  RadioWalk* w = static_cast<RadioWalk*>(user);
+  uint32_t total = 0;
+  if ((int64_t)k >= w->n_radio) total = w->K;
+  else if (n >= 3) total = (u[2] < w->gfrac[w->t->zone_emission_cdf_.sample(u[0])]) ? 8u : 10u;
+  if (total != 0 && n == total && (int64_t)k < w->n_radio) w->counts.push_back(total);
+  return total;
+}
+
 // transport::step (src/transport/transport.cpp:26-140) with per-packet
 // stream selection; returns the number of escaped packets
 int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, int threads)
@@ -186,10 +211,40 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
   const size_t n_before = t.particles.size();
   if (n_before != 0) { std::fprintf(stderr, "replay: expected an empty packet list\n"); std::exit(3); }
   const uint32_t K = core_draws_per_packet(t);
-  oracle_rng_emission(seed, 0, step, K);
+  const int64_t n_radio_req = t.params_->getScalar<int>("particles_n_emit_radioactive");
+  RadioWalk walk;
+  walk.t = &t;
+  walk.n_radio = 0;
+  walk.K = K;
+  if (n_radio_req > 0) {
+    // emit_radioactive's first deviate (the remainder test, emission.cpp:
+    // 187-189) comes from a stream no packet uses
+    radioactive radio;
+    const int force = t.params_->getScalar<int>("force_rprocess_heating");
+    for (int i = 0; i < t.grid->n_zones; ++i) {
+      double gf = 0;
+      radio.decay(t.grid->elems_Z, t.grid->elems_A, t.grid->z[i].X_gas, t.t_now_, &gf, force);
+      walk.gfrac.push_back(gf);
+    }
+    walk.n_radio = n_radio_req;
+    oracle_rng_walk(seed, 0, step, 1, radio_walk_count, &walk);
+  } else {
+    oracle_rng_emission(seed, 0, step, K);
+  }
   t.emit_particles(dt);
   const size_t n = t.particles.size();
-  if (oracle_rng_emission_draws() != (uint64_t)K * n) {
+  uint64_t radio_draws = 0;
+  if (n_radio_req > 0) {
+    if ((int64_t)walk.counts.size() != n_radio_req) {
+      std::fprintf(stderr, "replay: %zu radioactive packets emitted, %lld requested\n", walk.counts.size(),
+                   (long long)n_radio_req);
+      std::exit(3);
+    }
+    radio_draws = 1;
+    for (uint32_t c : walk.counts) radio_draws += c;
+  }
+  const size_t n_core = n - walk.counts.size();
+  if (oracle_rng_emission_draws() != radio_draws + (uint64_t)K * n_core) {
     std::fprintf(stderr, "replay: emission drew %llu deviates for %zu packets (expected %u each); only core emission is replayable\n",
                  (unsigned long long)oracle_rng_emission_draws(), n, K);
     std::exit(3);
@@ -201,16 +256,23 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
 #pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
   for (long i = 0; i < (long)n; ++i) {
     particle& p = t.particles[i];
-    oracle_rng_packet(seed, (uint64_t)i, step, K);
+    // radioactive packets keep drawing from where their emission stopped
+    // and record all their deviates; core packets record the ones after
+    // emission.  Records list the core packets first.
+    const bool radio = i < (long)walk.counts.size();
+    const uint32_t n0 = radio ? walk.counts[i] : K;
+    oracle_rng_packet(seed, (uint64_t)i, step, n0);
     p.fate = t.propagate(p, dt);
-    draws[i] = (int32_t)(oracle_rng_packet_draws() - K);
+    const long r = radio ? (long)n_core + i : i - (long)walk.counts.size();
+    draws[r] = (int32_t)(oracle_rng_packet_draws() - (radio ? 0 : K));
     if (p.fate == escaped) {
       double t_obs = p.t - p.x_dot_d() / pc::c;
       if (p.type == photon) t.optical_spectrum.count(t_obs, p.nu, p.e, p.D);
+      if (p.type == gammaray) t.gamma_spectrum.count(t_obs, p.nu, p.e, p.D);
       p.t = t_obs;
     }
-    fate[i] = (int32_t)p.fate; ind[i] = p.ind;
-    double* s = &st[(size_t)i * 9];
+    fate[r] = (int32_t)p.fate; ind[r] = p.ind;
+    double* s = &st[(size_t)r * 9];
     s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2]; s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
     s[6] = p.t; s[7] = p.e; s[8] = p.nu;
   }
@@ -234,6 +296,13 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
   o.i32("pkt_fate", fate); o.i32("pkt_ind", ind); o.i32("pkt_draws", draws); o.f64("pkt_state", st);
   o.scalar("n_packets", (double)n); o.scalar("n_escaped", n_escaped); o.scalar("propagate_seconds", T1 - T0);
   o.scalar("draws_per_emitted_packet", K);
+  if (n_radio_req > 0) {
+    std::vector<double> le(t.grid->n_zones), ld(t.grid->n_zones);
+    for (int i = 0; i < t.grid->n_zones; ++i) { le[i] = t.grid->z[i].L_radio_emit; ld[i] = t.grid->z[i].L_radio_dep; }
+    o.f64("L_radio_emit", le); o.f64("L_radio_dep", ld);
+    o.f64("gamma_flux", t.gamma_spectrum.flux); o.f64("gamma_click", t.gamma_spectrum.click);
+    o.scalar("n_radioactive", (double)walk.counts.size());
+  }
   return n_escaped;
 }
 

@@ -70,7 +70,7 @@ double MPI_Wtime(void)
 
 // ------------------------------------------------------------------ RNG
 namespace {
-enum RngMode { FREE = 0, PACKET = 1, EMIT = 2 };
+enum RngMode { FREE = 0, PACKET = 1, EMIT = 2, WALK = 3 };
 struct RngThreadState {
   int mode = FREE;
   uint32_t seed = 0;
@@ -80,6 +80,12 @@ struct RngThreadState {
   uint64_t emit_base = 0;  // first packet id of an emission batch
   uint32_t emit_k = 1;     // draws per emitted packet
   uint64_t emit_g = 0;     // draws taken in the current emission batch
+  // WALK: per-packet draw counts decided by the harness as the draws come
+  uint32_t walk_prefix = 0;  // draws served before the first packet
+  uint64_t walk_pkt = 0;     // current packet, relative to emit_base
+  double walk_u[32];         // the current packet's draws so far
+  oracle_rng_count_fn walk_fn = nullptr;
+  void* walk_user = nullptr;
 };
 thread_local RngThreadState g_rng;
 const gsl_rng_type g_type = {"philox4x32_10"};
@@ -124,6 +130,19 @@ double gsl_rng_uniform(const gsl_rng* rc)
   if (s.mode == EMIT) {
     uint64_t g = s.emit_g++;
     return oracle_packet_uniform(s.seed, s.emit_base + g / s.emit_k, s.step, (uint32_t)(g % s.emit_k));
+  }
+  if (s.mode == WALK) {
+    s.emit_g++;
+    if (s.walk_prefix > 0) {  // a stream no packet uses
+      --s.walk_prefix;
+      return oracle_packet_uniform(s.seed, ~0ull, s.step, s.walk_prefix);
+    }
+    const double u = oracle_packet_uniform(s.seed, s.emit_base + s.walk_pkt, s.step, s.n);
+    if (s.n < 32) s.walk_u[s.n] = u;
+    ++s.n;
+    const uint32_t total = s.walk_fn(s.walk_user, s.walk_pkt, s.walk_u, s.n);
+    if (total != 0 && s.n >= total) { ++s.walk_pkt; s.n = 0; }
+    return u;
   }
   return free_uniform(const_cast<gsl_rng*>(rc));
 }
@@ -170,6 +189,20 @@ void oracle_rng_emission(uint32_t seed, uint64_t pid_base, uint32_t step, uint32
   g_rng.emit_g = 0;
 }
 uint64_t oracle_rng_emission_draws() { return g_rng.emit_g; }
+void oracle_rng_walk(uint32_t seed, uint64_t pid_base, uint32_t step, uint32_t n_prefix, oracle_rng_count_fn fn,
+                     void* user)
+{
+  g_rng.mode = WALK;
+  g_rng.seed = seed;
+  g_rng.step = step;
+  g_rng.emit_base = pid_base;
+  g_rng.emit_g = 0;
+  g_rng.n = 0;
+  g_rng.walk_prefix = n_prefix;
+  g_rng.walk_pkt = 0;
+  g_rng.walk_fn = fn;
+  g_rng.walk_user = user;
+}
 
 // ------------------------------------------------------------------ HDF5
 namespace {

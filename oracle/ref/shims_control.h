@@ -13,5 +13,12 @@ uint32_t oracle_rng_packet_draws();
 // `draws_per_packet` draws (counter 0 .. k-1) from each
 void oracle_rng_emission(uint32_t seed, uint64_t pid_base, uint32_t step, uint32_t draws_per_packet);
 uint64_t oracle_rng_emission_draws();
+// calls on this thread first serve `n_prefix` draws from a stream no packet
+// uses, then walk packets pid_base, pid_base+1, ...; after each draw `fn`
+// gets the packet (relative to pid_base) and its draws so far and returns
+// the packet's number of draws once it is known (0 while it is not)
+typedef uint32_t (*oracle_rng_count_fn)(void* user, uint64_t packet, const double* u, uint32_t n_drawn);
+void oracle_rng_walk(uint32_t seed, uint64_t pid_base, uint32_t step, uint32_t n_prefix, oracle_rng_count_fn fn,
+                     void* user);
 
 #endif

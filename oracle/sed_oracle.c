@@ -88,6 +88,11 @@ struct oracle_ctx {
   int32_t *r_fate, *r_ind, *r_draws;
   double* r_state;
   uint32_t step;
+  /* radioactive source: gamma-ray spectrum and per-zone decay quantities */
+  lgrid gn;
+  int64_t nspec_g;
+  double *gflux, *gclick;
+  double *L_emit, *L_dep, *radio_cdf, *gamma_frac, *compton, *photoion;
   /* differentiable transport: exact Jacobian of the last weighted forward,
    * accumulated forward-mode per packet ([nspec][nzones][bands]) */
   double* jac;
@@ -202,6 +207,16 @@ int oracle_ctx_create(const sed_transport_params* p, oracle_ctx** out)
     o->core_cdf[j] = (j == 0) ? w : o->core_cdf[j - 1] + w;
   }
   cdf_normalize(o->core_cdf, nn);
+  if (p->n_emit_radioactive > 0) {
+    if (p->gamma_nu.n > 0 && p->gamma_nu.right) lgrid_copy(&o->gn, &p->gamma_nu);
+    else {  /* one catch-all bin */
+      o->gn.n = 1; o->gn.type = SED_LOC_NONE; o->gn.min = -INFINITY; o->gn.del = 0;
+      o->gn.x = (double*)malloc(sizeof(double)); o->gn.x[0] = INFINITY;
+    }
+    o->nspec_g = (int64_t)o->st.n * o->gn.n * o->sm.n * o->sp.n;
+    o->gflux = (double*)calloc((size_t)o->nspec_g, sizeof(double));
+    o->gclick = (double*)calloc((size_t)o->nspec_g, sizeof(double));
+  }
   *out = o;
   return SED_OK;
 }
@@ -1009,36 +1024,52 @@ static void emit_core_packet(const oracle_ctx* o, packet* p, double Ep, double t
   p->t = t_now + draw(o, p) * dt;
 }
 
-/* spectrum_array::count, src/transport/spectrum_array.cpp:215-246; returns
- * the index counted into, -1 when the packet is dropped */
+/* spectrum_array::count, src/transport/spectrum_array.cpp:215-246, on the
+ * frequency grid `sn` into flux/click; returns the index, -1 when dropped */
+static int64_t spectrum_count_on(oracle_ctx* o, const lgrid* sn, double* flux, double* click, double t, double w,
+                                 double E, const double* D);
 static int64_t spectrum_count(oracle_ctx* o, double t, double w, double E, const double* D)
+{
+  return spectrum_count_on(o, &o->sn, o->flux, o->click, t, w, E, D);
+}
+static int64_t spectrum_count_on(oracle_ctx* o, const lgrid* sn, double* flux, double* click, double t, double w,
+                                 double E, const double* D)
 {
   double mu = D[2];
   double phi = atan2(D[1], D[0]);
   if (phi < 0) phi += 2. * PC_PI;
   int t_bin = lg_locate(&o->st, t);
-  int l_bin = lg_locate(&o->sn, w);
+  int l_bin = lg_locate(sn, w);
   int m_bin = lg_locate(&o->sm, mu);
   int p_bin = lg_locate(&o->sp, phi);
   if (l_bin < 0) l_bin = 0;
-  if (l_bin >= o->sn.n) l_bin = 0;
+  if (l_bin >= sn->n) l_bin = 0;
   if ((t_bin < 0) || (l_bin < 0) || (m_bin < 0) || (p_bin < 0)) return -1;
   if (t_bin >= o->st.n) return -1;
   if (m_bin >= o->sm.n) return -1;
   if (p_bin >= o->sp.n) return -1;
-  int64_t a3 = o->sp.n, a2 = (int64_t)o->sm.n * a3, a1 = (int64_t)o->sn.n * a2;
+  int64_t a3 = o->sp.n, a2 = (int64_t)o->sm.n * a3, a1 = (int64_t)sn->n * a2;
   int64_t ind = t_bin * a1 + l_bin * a2 + m_bin * a3 + p_bin;
-  o->flux[ind] += E;
-  o->click[ind] += 1;
+  flux[ind] += E;
+  click[ind] += 1;
   return ind;
 }
 
-/* transport::propagate + propagate_monte_carlo, src/transport/transport.cpp:202-484 */
+/* transport::propagate + propagate_monte_carlo, src/transport/transport.cpp:202-484;
+ * relocate = 0 continues a packet whose zone is current (a gamma-ray that
+ * became an optical photon inside propagate_monte_carlo) */
+static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int64_t* nseg, int64_t* nscat,
+                          int relocate);
 static int propagate(oracle_ctx* o, packet* p, double t_now, double dt, int64_t* nseg, int64_t* nscat)
+{
+  return propagate_from(o, p, t_now, dt, nseg, nscat, 1);
+}
+static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int64_t* nseg, int64_t* nscat,
+                          int relocate)
 {
   int nn = o->nu.n;
   int nj = o->tp.store_Jnu ? nn : 1;
-  p->ind = get_zone(o, p->x);
+  if (relocate) p->ind = get_zone(o, p->x);
   if (p->ind == -1) return F_ABSORBED;
   if (p->ind == -2) return F_ESCAPED;
   double tstop = t_now + dt;
@@ -1233,9 +1264,452 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
   return SED_OK;
 }
 
+/* ---------------------------------------------------------------- radioactive source
+ * transport::emit_radioactive (src/transport/emission.cpp:163-243) with
+ * radioactive::decay (src/transport/radioactive.cpp:144-275), and gamma-ray
+ * transport: opacity (transport_opacity.cpp:187-203, 290-313), do_scatter
+ * and compton_scatter (scatter.cpp:45-133).  Radioactive packets take the
+ * stream ids before the core packets (the reference emits them first);
+ * each draws from its own stream in the reference's order. */
+#define TAU_56NI 757241.8
+#define TAU_56CO 9627379.
+#define AVERAGE_56NI_ENERGY 1.725
+#define AVERAGE_56CO_ENERGY 3.730
+#define CO_POSITRON_FRACTION 0.0324
+#define TAU_48CR 111976.
+#define TAU_48V 1.99107843e6
+#define AVERAGE_48CR_ENERGY 0.442
+#define AVERAGE_48V_ENERGY 3.066
+#define PC_M_E_MEV 0.510998910511
+#define PC_MEV_TO_ERGS 1.60217646e-6
+#define PC_ALPHA_FS 0.007
+static const double R_PROC_FIT[11] = {17.608179, -2.0442059, -0.42565322, 0.39830095, -0.0059089906,
+                                      -0.054805836, 0.014068697, -0.00086706160, -5.7056758e-05, 2.6401842e-06,
+                                      3.7186979e-07};
+
+static double rprocess_heating_rate(double t, double* gfrac)  /* radioactive.cpp:118-142 */
+{
+  double td = t / 3600.0 / 24.0;
+  double A1 = 8.4939E+09, alpha = 1.3642E+00, B1 = 8.3425E+09, beta1 = 3.6280E+00;
+  double B2 = 8.8616E+08, beta2 = 1.0847E+01;
+  double eps = A1 * pow(td, -1.0 * alpha) + B1 * exp(-1.0 * td / beta1) + B2 * exp(-1.0 * td / beta2);
+  double af = 0.56, bf = 0.17, df = 0.74;
+  double x = 2 * bf * pow(td, df);
+  double f = 0.36 * (exp(-af * td) + log(1 + x) / x);
+  *gfrac = 0;
+  return eps * f;
+}
+
+static double decay_energy_rate(int Z, int A, double t, double* gfrac)  /* radioactive.cpp:178-275 */
+{
+  double total = 0, gtotal = 0;
+  if ((Z == 28) && (A == 56)) {
+    double e_ni = exp(-t / TAU_56NI), e_co = exp(-t / TAU_56CO);
+    double ni56 = (e_ni / TAU_56NI);
+    double co56 = 1.0 / (TAU_56NI - TAU_56CO) * (e_ni - e_co);
+    double ni_E = ni56 * (AVERAGE_56NI_ENERGY * PC_MEV_TO_ERGS);
+    double co_E = co56 * (AVERAGE_56CO_ENERGY * PC_MEV_TO_ERGS);
+    gtotal = ni_E + (1 - CO_POSITRON_FRACTION) * co_E;
+    total = ni_E + co_E;
+  }
+  if ((Z == 27) && (A == 56)) {
+    double e_co = exp(-t / TAU_56CO);
+    double co56 = 1.0 / (TAU_56CO)*e_co;
+    double co_E = co56 * (AVERAGE_56CO_ENERGY * PC_MEV_TO_ERGS);
+    gtotal = (1 - CO_POSITRON_FRACTION) * co_E;
+    total = co_E;
+  }
+  if ((Z == 24) && (A == 48)) {
+    double e_cr = exp(-t / TAU_48CR), e_vn = exp(-t / TAU_48V);
+    double cr48 = (e_cr / TAU_48CR);
+    double vn48 = 1.0 / (TAU_48CR - TAU_48V) * (e_cr - e_vn);
+    double cr_E = cr48 * (AVERAGE_48CR_ENERGY * PC_MEV_TO_ERGS);
+    double vn_E = vn48 * (AVERAGE_48V_ENERGY * PC_MEV_TO_ERGS);
+    gtotal += cr_E + vn_E;
+    total += cr_E + vn_E;
+  }
+  if ((Z >= 58)) {
+    double at = log10(t);
+    double rproc = 0;
+    for (int j = 0; j < 11; j++) rproc += R_PROC_FIT[j] * pow(at, j);
+    rproc = pow(10.0, rproc) * (A * PC_M_P);
+    double fission_E = 0.1 * rproc;
+    double beta_E = 0.9 * rproc;
+    beta_E = 0.75 * beta_E;
+    total += (fission_E + beta_E);
+    gtotal += 0.5 * beta_E;
+  }
+  *gfrac = gtotal / total;
+  if (total == 0) *gfrac = 0;
+  return total;
+}
+
+/* per-zone decay luminosity (emission.cpp:189-205), gamma opacity
+ * coefficients, zone emission CDF; returns the grid total */
+static double radio_zones(oracle_ctx* o, double t)
+{
+  int nz = o->nzones, ne = o->nelem;
+  double L_tot = 0;
+  for (int i = 0; i < nz; i++) {
+    const double* X = o->X + (size_t)i * ne;
+    int rprocess_heat = 0;
+    for (int k = 0; k < ne; k++)
+      if (((o->eZ[k] > 57) && (o->eA[k] > 0)) || o->tp.force_rprocess_heating) rprocess_heat = 1;
+    double L_decay, gfrac;
+    if (rprocess_heat) L_decay = rprocess_heating_rate(t, &gfrac);
+    else {
+      double total = 0, gtotal = 0, gf;
+      for (int k = 0; k < ne; k++) {
+        double val = decay_energy_rate(o->eZ[k], o->eA[k], t, &gf);
+        val = val * X[k] / (o->eA[k] * PC_M_P);
+        total += val;
+        gtotal += val * gf;
+      }
+      gfrac = gtotal / total;
+      if (total == 0) gfrac = 0;
+      L_decay = total;
+    }
+    L_decay = o->rho[i] * L_decay * o->vol[i];
+    o->L_emit[i] = L_decay;
+    o->gamma_frac[i] = gfrac;
+    L_tot += L_decay;
+    o->radio_cdf[i] = (i == 0) ? L_decay : o->radio_cdf[i - 1] + L_decay;  /* cdf_array::set_value */
+    double comp = 0, phot = 0;
+    for (int k = 0; k < ne; k++) {
+      double dens = X[k] * o->rho[i];
+      double ndens = dens / (PC_M_P * o->eA[k]);
+      comp += ndens * PC_THOMSON * o->eZ[k];
+      double photo = pow(PC_ALPHA_FS, 4.0) * 4.0 * sqrt(2.0);
+      photo *= pow(1.0 * o->eZ[k], 5.0);
+      photo *= pow(PC_M_E_MEV, 3.5);
+      phot += ndens * 2.0 * PC_THOMSON * photo;
+    }
+    o->compton[i] = comp;
+    o->photoion[i] = phot;
+  }
+  cdf_normalize(o->radio_cdf, nz);
+  return L_tot;
+}
+
+static double klein_nishina(double x)  /* transport_opacity.cpp:302-313 */
+{
+  x = x / PC_M_E_MEV;
+  double logfac = log(1 + 2 * x);
+  double term1 = (1 + x) / x / x / x * (2 * x * (1 + x) / (1 + 2 * x) - logfac);
+  double term2 = 1.0 / 2.0 / x * logfac;
+  double term3 = -1.0 * (1 + 3 * x) / (1 + 2 * x) / (1 + 2 * x);
+  return .75 * (term1 + term2 + term3);
+}
+
+/* transport::lorentz_transform (relativity.cpp:84-127), either direction */
+static void lorentz(const oracle_ctx* o, packet* p, int tolab)
+{
+  double v[3], dvds;
+  get_velocity(o, p->ind, p->x, p->D, v, &dvds);
+  if (tolab) { v[0] *= -1; v[1] *= -1; v[2] *= -1; }
+  double beta2 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / PC_C / PC_C;
+  double vdd = v[0] * p->D[0] + v[1] * p->D[1] + v[2] * p->D[2];
+  double gamma = 1.0 / sqrt(1 - beta2);
+  double dshift = gamma * (1 - vdd / PC_C);
+  p->dvds = dvds;
+  p->e *= dshift;
+  p->nu *= dshift;
+  double f = (1 - gamma * vdd / PC_C / (gamma + 1));
+  p->D[0] = 1.0 / dshift * (p->D[0] - gamma * v[0] / PC_C * f);
+  p->D[1] = 1.0 / dshift * (p->D[1] - gamma * v[1] / PC_C * f);
+  p->D[2] = 1.0 / dshift * (p->D[2] - gamma * v[2] / PC_C * f);
+  double norm = p->D[0] * p->D[0] + p->D[1] * p->D[1] + p->D[2] * p->D[2];
+  p->D[0] /= norm;
+  p->D[1] /= norm;
+  p->D[2] /= norm;
+}
+
+/* grid::sample_in_zone (grid_1D_sphere.cpp:681-700, grid_3D_cart.cpp:484-494) */
+static void sample_in_zone(const oracle_ctx* o, int i, double u0, double u1, double u2, double* r)
+{
+  if (o->gtype == SED_GRID_1D_SPHERE) {
+    double r_0 = (i == 0) ? o->r_out.min : o->r_out.x[i - 1];
+    double ro = o->r_out.x[i];
+    double r_samp = pow(r_0 * r_0 * r_0 + u0 * (ro * ro * ro - r_0 * r_0 * r_0), 1.0 / 3.0);
+    double mu = 1 - 2.0 * u1;
+    double phi = 2.0 * PC_PI * u2;
+    double sin_theta = sqrt(1 - mu * mu);
+    r[0] = r_samp * sin_theta * cos(phi);
+    r[1] = r_samp * sin_theta * sin(phi);
+    r[2] = r_samp * mu;
+  } else {
+    int nyz = o->ny * o->nz;
+    int idx[3] = {i / nyz, (i / o->nz) % o->ny, i % o->nz};
+    double u[3] = {u0, u1, u2};
+    for (int a = 0; a < 3; a++) r[a] = lg_left(&o->ax[a], idx[a]) + u[a] * lg_delta(&o->ax[a], idx[a]);
+  }
+}
+
+static void iso_dir(const oracle_ctx* o, packet* p, double* D)
+{
+  double mu = 1 - 2.0 * draw(o, p);
+  double phi = 2.0 * PC_PI * draw(o, p);
+  double smu = sqrt(1 - mu * mu);
+  D[0] = smu * cos(phi);
+  D[1] = smu * sin(phi);
+  D[2] = mu;
+}
+
+static void sample_optical_nu(const oracle_ctx* o, packet* p)  /* sample_photon_frequency, emission.cpp:27-46 */
+{
+  int nn = o->nu.n;
+  int inu = cdf_sample(o->cdf + (size_t)p->ind * nn, nn, draw(o, p));
+  p->nu = lg_sample(&o->nu, inu, draw(o, p));
+}
+
+#define COMPTON_TRIES (1 << 16)
+/* propagate + propagate_monte_carlo for a gamma-ray; *photon is set when it
+ * becomes an optical photon (its state is then the photon's) */
+static int propagate_gamma(oracle_ctx* o, packet* p, double t_now, double dt, int* photon, int64_t* nseg,
+                           int64_t* nscat)
+{
+  *photon = 0;
+  p->ind = get_zone(o, p->x);
+  if (p->ind == -1) return F_ABSORBED;
+  if (p->ind == -2) return F_ESCAPED;
+  double tstop = t_now + dt;
+  int fate = F_MOVING;
+  int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
+  int64_t seg = 0;
+  while (fate == F_MOVING && !*photon) {
+    if (seg++ >= limit) { fate = F_STOPPED; break; }
+    int iz = p->ind;
+    double d_bn = 0;
+    int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);
+    double dshift = dshift_lab_to_comoving(o, p);
+    double c_opac = o->compton[iz] * klein_nishina(p->nu);
+    double p_opac = o->photoion[iz] * pow(p->nu, -3.5);
+    double opac = c_opac + p_opac;
+    double eps = p_opac / (c_opac + p_opac);
+    double d_nu = lg_delta(&o->nu, 0) / p->nu * PC_C / p->dvds;
+    if (p->dvds == 0) d_nu = INFINITY;
+    if (d_nu < 0) d_nu = -1 * d_nu;
+    if (d_nu < d_bn) { d_bn = d_nu; new_ind = p->ind; }
+    double tot_lab = opac * dshift;
+    double tau_r = -1.0 * log(1 - draw(o, p));
+    double d_sc = tau_r / tot_lab;
+    if (tot_lab == 0) d_sc = INFINITY;
+    double d_tm = (tstop - p->t) * PC_C;
+    if (o->tp.steady_state) d_tm = INFINITY;
+    int event;
+    double this_d;
+    if ((d_sc < d_bn) && (d_sc < d_tm)) { event = 0; this_d = d_sc; }
+    else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
+    else { event = 2; this_d = d_tm; }
+    double this_E = p->e * this_d;
+    if (o->tp.tally_forces) {
+      o->fx[iz] += this_E * dshift * opac * p->D[0] * dshift;
+      o->fy[iz] += this_E * dshift * opac * p->D[1] * dshift;
+      o->fz[iz] += this_E * dshift * opac * p->D[2] * dshift;
+      double rr = sqrt(p->x[0] * p->x[0] + p->x[1] * p->x[1] + p->x[2] * p->x[2]);
+      double xdotD = p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2];
+      o->fr[iz] += this_E * dshift * opac * xdotD / rr * dshift;
+    }
+    p->x[0] += this_d * p->D[0];
+    p->x[1] += this_d * p->D[1];
+    p->x[2] += this_d * p->D[2];
+    p->t = p->t + this_d / PC_C;
+    if (event == 1) {
+      if (new_ind == -1) {
+        if (o->tp.boundary_in_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
+        else { p->ind = new_ind; fate = F_ABSORBED; }
+      } else if (new_ind == -2) {
+        if (o->tp.boundary_out_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
+        else { p->ind = new_ind; fate = F_ESCAPED; }
+      } else {
+        p->ind = new_ind;
+      }
+    } else if (event == 0) {
+      (*nscat)++;
+      if (draw(o, p) > eps) {
+        lorentz(o, p, 0);
+        double E_ratio = 1, Dn[3];
+        for (int tries = 0;; ++tries) {
+          iso_dir(o, p, Dn);
+          double cost = p->D[0] * Dn[0] + p->D[1] * Dn[1] + p->D[2] * Dn[2];
+          E_ratio = 1 / (1 + p->nu / PC_M_E_MEV * (1 - cost));
+          double diff_cs = 0.5 * (E_ratio * E_ratio * (1 / E_ratio + E_ratio - 1 + cost * cost));
+          if (draw(o, p) < diff_cs) break;
+          if (tries + 1 >= COMPTON_TRIES) break;
+        }
+        p->nu = p->nu * E_ratio;
+        if (draw(o, p) > E_ratio) {
+          o->L_dep[p->ind] += p->e;
+          *photon = 1;
+          iso_dir(o, p, Dn);
+          sample_optical_nu(o, p);
+        }
+        p->D[0] = Dn[0]; p->D[1] = Dn[1]; p->D[2] = Dn[2];
+        lorentz(o, p, 1);
+      } else {
+        o->L_dep[p->ind] += p->e;
+        *photon = 1;
+        iso_dir(o, p, p->D);
+        sample_optical_nu(o, p);
+        lorentz(o, p, 1);
+      }
+    } else {
+      fate = F_STOPPED;
+    }
+  }
+  *nseg += seg;
+  return fate;
+}
+
+/* a radioactive packet's record: its end state and every deviate its
+ * stream gave, emission included */
+static void record_radio(oracle_ctx* o, int64_t r, int fate, const packet* p)
+{
+  o->r_fate[r] = fate; o->r_ind[r] = p->ind; o->r_draws[r] = (int32_t)p->n;
+  double* sv = o->r_state + (size_t)r * 9;
+  sv[0] = p->x[0]; sv[1] = p->x[1]; sv[2] = p->x[2]; sv[3] = p->D[0]; sv[4] = p->D[1]; sv[5] = p->D[2];
+  sv[6] = p->t; sv[7] = p->e; sv[8] = p->nu;
+}
+
+/* a transport step with the radioactive source: radioactive packets first,
+ * then the core packets; records hold the core packets, then the
+ * radioactive ones (as gamma-rays, or as the optical photons they became) */
+static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
+{
+  if (o->tp.steady_state) dt = 1;
+  double t_now = o->t_grid;
+  int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
+  int64_t n_radio = o->tp.n_emit_radioactive;
+  if (n_radio > o->tp.max_particles) n_radio = 0;
+  if (n_emit + n_radio > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
+  int64_t n_all = n_emit + n_radio;
+  int nz = o->nzones;
+  wipe_tallies(o);
+  memset(o->flux, 0, (size_t)o->nspec * sizeof(double));
+  memset(o->click, 0, (size_t)o->nspec * sizeof(double));
+  memset(o->gflux, 0, (size_t)o->nspec_g * sizeof(double));
+  memset(o->gclick, 0, (size_t)o->nspec_g * sizeof(double));
+  double** zarr[6] = {&o->L_emit, &o->L_dep, &o->radio_cdf, &o->gamma_frac, &o->compton, &o->photoion};
+  for (int q = 0; q < 6; q++) { free(*zarr[q]); *zarr[q] = (double*)calloc((size_t)nz, sizeof(double)); }
+  double L_tot = radio_zones(o, t_now);
+  double Ep_r = L_tot * dt / (1.0 * n_radio);
+  if (o->record) {
+    free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state);
+    o->nrec = n_all;
+    o->r_fate = (int32_t*)calloc((size_t)n_all + 1, 4);
+    o->r_ind = (int32_t*)calloc((size_t)n_all + 1, 4);
+    o->r_draws = (int32_t*)calloc((size_t)n_all + 1, 4);
+    o->r_state = (double*)calloc((size_t)n_all * 9 + 1, 8);
+    for (int64_t k = n_emit; k < n_all; ++k) o->r_fate[k] = -1;  /* stays when nothing is emitted */
+  }
+  int64_t nseg = 0, nscat = 0, nesc = 0, nabs = 0, nstop = 0;
+  for (int64_t k = 0; k < n_radio && L_tot != 0; ++k) {
+    packet p;
+    memset(&p, 0, sizeof p);
+    p.pid = (uint64_t)(o->tp.first_packet_id + k);
+    p.n = 0;
+    int i = cdf_sample(o->radio_cdf, nz, draw(o, &p));
+    double t = t_now + dt * draw(o, &p);
+    int is_gamma = draw(o, &p) < o->gamma_frac[i];
+    if (!is_gamma) o->L_dep[i] += Ep_r;
+    double u0 = draw(o, &p), u1 = draw(o, &p), u2 = draw(o, &p);
+    sample_in_zone(o, i, u0, u1, u2, p.x);
+    iso_dir(o, &p, p.D);
+    p.ind = i;
+    if (is_gamma) p.nu = 1;
+    else sample_optical_nu(o, &p);
+    p.e = Ep_r;
+    lorentz(o, &p, 1);
+    p.t = t;
+    int fate, relocate = 1;
+    if (is_gamma) {
+      int photon = 0;
+      fate = propagate_gamma(o, &p, t_now, dt, &photon, &nseg, &nscat);
+      if (!photon) {
+        if (fate == F_ESCAPED) {
+          double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / PC_C;
+          spectrum_count_on(o, &o->gn, o->gflux, o->gclick, t_obs, p.nu, p.e, p.D);
+          p.t = t_obs;
+          nesc++;
+        } else if (fate == F_ABSORBED) nabs++;
+        else nstop++;
+        if (o->record) record_radio(o, n_emit + k, fate, &p);
+        continue;
+      }
+      relocate = 0;
+    }
+    fate = propagate_from(o, &p, t_now, dt, &nseg, &nscat, relocate);
+    if (fate == F_ESCAPED) {
+      double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / PC_C;
+      spectrum_count(o, t_obs, p.nu, p.e, p.D);
+      p.t = t_obs;
+      nesc++;
+    } else if (fate == F_ABSORBED) nabs++;
+    else nstop++;
+    if (o->record) record_radio(o, n_emit + k, fate, &p);
+  }
+  double Ep = o->tp.core_luminosity * dt / n_emit;
+  uint32_t K = draws_per_emission(o);
+  for (int64_t j = 0; j < n_emit; ++j) {
+    packet p;
+    memset(&p, 0, sizeof p);
+    p.pid = (uint64_t)(o->tp.first_packet_id + n_radio + j);
+    p.n = 0;
+    emit_core_packet(o, &p, Ep, t_now, dt);
+    p.n = K;
+    int fate = propagate(o, &p, t_now, dt, &nseg, &nscat);
+    if (fate == F_ESCAPED) {
+      double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / PC_C;
+      spectrum_count(o, t_obs, p.nu, p.e, p.D);
+      p.t = t_obs;
+      nesc++;
+    } else if (fate == F_ABSORBED) nabs++;
+    else nstop++;
+    if (o->record) {
+      o->r_fate[j] = fate; o->r_ind[j] = p.ind; o->r_draws[j] = (int32_t)(p.n - K);
+      double* sv = o->r_state + (size_t)j * 9;
+      sv[0] = p.x[0]; sv[1] = p.x[1]; sv[2] = p.x[2]; sv[3] = p.D[0]; sv[4] = p.D[1]; sv[5] = p.D[2];
+      sv[6] = p.t; sv[7] = p.e; sv[8] = p.nu;
+    }
+  }
+  finish_step(o, dt, n_all, nesc);
+  for (int i = 0; i < nz; i++) {  /* transport_mpi.cpp:419-420 */
+    o->L_dep[i] /= o->vol[i] * dt;
+    o->L_emit[i] /= o->vol[i];
+  }
+  o->step++;
+  if (st) {
+    memset(st, 0, sizeof *st);
+    st->n_packets = n_all; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
+    st->n_segments = nseg; st->n_scatters = nscat;
+  }
+  return SED_OK;
+}
+
+int oracle_get_gamma_spectrum(oracle_ctx* o, double* flux, double* click)
+{
+  if (!o || !o->gflux) return SED_ERR_STATE;
+  if (flux) memcpy(flux, o->gflux, (size_t)o->nspec_g * sizeof(double));
+  if (click) memcpy(click, o->gclick, (size_t)o->nspec_g * sizeof(double));
+  return SED_OK;
+}
+
+int oracle_get_radioactive_tallies(oracle_ctx* o, double* L_emit, double* L_dep)
+{
+  if (!o || !o->L_dep) return SED_ERR_STATE;
+  if (L_emit) memcpy(L_emit, o->L_emit, (size_t)o->nzones * sizeof(double));
+  if (L_dep) memcpy(L_dep, o->L_dep, (size_t)o->nzones * sizeof(double));
+  return SED_OK;
+}
+
 int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
 {
   if (!o) return SED_ERR_ARG;
+  if (o->tp.n_emit_radioactive > 0) {
+    if (!o->have_grid) return SED_ERR_STATE;
+    if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
+    return transport_radio(o, dt, st);
+  }
   return oracle_transport_range(o, dt, 0, (int64_t)(o->tp.core_n_emit / 1.0), 1, st);
 }
 
@@ -1610,5 +2084,7 @@ void oracle_ctx_destroy(oracle_ctx* o)
   }
   free(o->zero_eps);
   free(o->jac);
+  free(o->gflux); free(o->gclick); free(o->L_emit); free(o->L_dep); free(o->radio_cdf); free(o->gamma_frac);
+  free(o->compton); free(o->photoion); free(o->gn.x);
   free(o);
 }

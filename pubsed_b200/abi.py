@@ -50,6 +50,8 @@ class TransportParams(C.Structure):
         ("first_packet_id", C.c_int64),
         ("nu_grid", LocateGrid), ("spec_time", LocateGrid), ("spec_nu", LocateGrid),
         ("spec_mu", LocateGrid), ("spec_phi", LocateGrid),
+        ("n_emit_radioactive", C.c_int64), ("force_rprocess_heating", C.c_int32), ("reserved3", C.c_int32),
+        ("gamma_nu", LocateGrid),
     ]
 
 
@@ -178,6 +180,8 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         "diff_vjp": ([vp, _dp, _dp, C.POINTER(StepStats)], C.c_int),
         "diff_jacobian": ([vp, _dp, C.POINTER(StepStats)], C.c_int),
         "solve_temperature": ([vp, C.c_int32, _dp, _ip], C.c_int),
+        "get_gamma_spectrum": ([vp, _dp, _dp], C.c_int),
+        "get_radioactive_tallies": ([vp, _dp, _dp], C.c_int),
     })
     if prefix == "sed_":
         i64p = C.POINTER(C.c_int64)

@@ -203,8 +203,13 @@ int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
   c->sn = host_loc(p->spec_nu);
   c->sm = host_loc(p->spec_mu);
   c->sp = host_loc(p->spec_phi);
+  if (valid_grid(p->gamma_nu)) c->gn = host_loc(p->gamma_nu);
+  else {  // one catch-all bin, as locate_array builds for an empty range
+    c->gn.type = LOC_NONE; c->gn.min = -INFINITY; c->gn.del = 0; c->gn.x.assign(1, INFINITY);
+  }
   // grid pointers in the copy are not retained
   c->tp.nu_grid.right = c->tp.spec_time.right = c->tp.spec_nu.right = c->tp.spec_mu.right = c->tp.spec_phi.right = nullptr;
+  c->tp.gamma_nu.right = nullptr;
   CK(upload(c, c->d_nu, c->nu.x.data(), c->nu.x.size()));
   CK(upload(c, c->d_st, c->st.x.data(), c->st.x.size()));
   CK(upload(c, c->d_sn, c->sn.x.data(), c->sn.x.size()));
@@ -218,6 +223,16 @@ int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
   CK(c->d_counters.resize(C_COUNT + 1));
   CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
+  if (p->n_emit_radioactive > 0) {
+    CK(upload(c, c->d_gn, c->gn.x.data(), c->gn.x.size()));
+    c->nspec_g = (int64_t)c->st.n() * c->gn.n() * c->sm.n() * c->sp.n();
+    CK(c->d_gflux.resize(c->nspec_g));
+    CK(c->d_gclick.resize(c->nspec_g));
+    CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
+    CK(c->d_L_tot.resize(1));
+    CK(c->d_reject.resize(1));
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->op.epsilon = 1.0;
   c->op.maximum_opacity = 1e40;
@@ -581,19 +596,39 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   if (c->tp.steady_state) dt = 1;
   // emit_inner_source packet count and energy (src/transport/emission.cpp:383-392)
   const int64_t n_emit = (int64_t)(c->tp.core_n_emit / 1.0);
-  if (n_emit > c->tp.max_particles)
+  // emit_radioactive runs first (emission.cpp:163-186, one rank): it adds
+  // nothing when its packets would not fit; the core packets then must fit
+  // next to them
+  int64_t n_radio = c->tp.n_emit_radioactive > 0 ? c->tp.n_emit_radioactive : 0;
+  if (n_radio > c->tp.max_particles) n_radio = 0;
+  if (n_emit + n_radio > c->tp.max_particles)
     return set_err(c, SED_ERR_CAPACITY, "Not enough particle space: %lld packets > particles_max_total %lld",
-                   (long long)n_emit, (long long)c->tp.max_particles);
+                   (long long)(n_emit + n_radio), (long long)c->tp.max_particles);
+  const int64_t n_all = n_emit + n_radio;
   const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
   const size_t nj = c->tp.store_Jnu ? nn : 1;
   if (c->record) {
-    CK(c->d_rec_fate.resize(std::max<int64_t>(n_emit, 1)));
-    CK(c->d_rec_ind.resize(std::max<int64_t>(n_emit, 1)));
-    CK(c->d_rec_draws.resize(std::max<int64_t>(n_emit, 1)));
-    CK(c->d_rec_state.resize(std::max<int64_t>(n_emit, 1) * 9));
-    c->n_rec = n_emit;
+    CK(c->d_rec_fate.resize(std::max<int64_t>(n_all, 1)));
+    CK(c->d_rec_ind.resize(std::max<int64_t>(n_all, 1)));
+    CK(c->d_rec_draws.resize(std::max<int64_t>(n_all, 1)));
+    CK(c->d_rec_state.resize(std::max<int64_t>(n_all, 1) * 9));
+    c->n_rec = n_all;
+  }
+  if (c->tp.n_emit_radioactive > 0) {
+    CK(c->d_radio_cdf.resize(nz)); CK(c->d_gamma_frac.resize(nz)); CK(c->d_compton.resize(nz));
+    CK(c->d_photoion.resize(nz)); CK(c->d_L_emit.resize(nz)); CK(c->d_L_dep.resize(nz));
+    CK(c->d_q_state.resize((size_t)std::max<int64_t>(n_radio, 1) * 9));
+    CK(c->d_q_ind.resize((size_t)std::max<int64_t>(n_radio, 1)));
+    CK(c->d_q_n.resize((size_t)std::max<int64_t>(n_radio, 1)));
   }
   CK(cudaEventRecord(c->ev[2], c->stream));
+  if (c->tp.n_emit_radioactive > 0) {
+    CK(cudaMemsetAsync(c->d_L_dep.p, 0, nz * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_L_emit.p, 0, nz * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_reject.p, 0, sizeof(int32_t), c->stream));
+  }
   // wipe_radiation (src/transport/transport_mpi.cpp:18-34) and the spectrum
   CK(cudaMemsetAsync(c->d_J.p, 0, nz * nj * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_e_abs.p, 0, nz * sizeof(double), c->stream));
@@ -612,8 +647,35 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   }
   const GridDev G = make_grid_dev(c);
   int launches = 0;
+  if (c->tp.n_emit_radioactive > 0) {
+    // decay luminosity and gamma-ray opacity per zone, then the radioactive
+    // packets (emitted before the core packets, so they take the first
+    // stream ids); their optical photons join the packet kernel's queue.
+    // Packet records: the core packets, then the radioactive ones.
+    A.n_core = n_emit;
+    RadioArgs R{};
+    R.nz = c->nz; R.n_elems = c->nelem; R.force_rproc = c->tp.force_rprocess_heating;
+    R.n_radio = n_radio; R.first_pid = c->tp.first_packet_id;
+    R.t_now = c->t_grid; R.dt = dt;
+    R.rho = c->d_rho.p; R.vol = c->d_vol.p; R.X = c->d_X.p; R.eZ = c->d_eZ.p; R.eA = c->d_eA.p;
+    R.L_emit = c->d_L_emit.p; R.gamma_frac = c->d_gamma_frac.p; R.compton = c->d_compton.p;
+    R.photoion = c->d_photoion.p; R.cdf = c->d_radio_cdf.p; R.L_tot = c->d_L_tot.p; R.L_dep = c->d_L_dep.p;
+    R.q_state = c->d_q_state.p; R.q_ind = c->d_q_ind.p; R.q_n = c->d_q_n.p; R.n_reject_cap = c->d_reject.p;
+    StepArgs AG = A;  // the gamma-ray spectrum
+    AG.sn = dev_loc(c->gn, c->d_gn);
+    AG.a3 = c->sp.n(); AG.a2 = (int64_t)c->sm.n() * AG.a3; AG.a1 = (int64_t)c->gn.n() * AG.a2;
+    AG.flux = c->d_gflux.p; AG.click = c->d_gclick.p;
+    launches += launch_radio_zones(R, c->stream);
+    launches += launch_gamma(A, AG, R, G, c->num_sms, c->stream);
+    CK(cudaGetLastError());
+    A.n_packets = n_all;
+    A.first_pid = c->tp.first_packet_id + n_radio;
+    A.radio_first_pid = c->tp.first_packet_id;
+    A.q_state = c->d_q_state.p; A.q_ind = c->d_q_ind.p; A.q_n = c->d_q_n.p;
+    A.L_dep = c->d_L_dep.p; A.L_emit = c->d_L_emit.p;
+  }
   CK(cudaEventRecord(c->ev[3], c->stream));
-  if (n_emit > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
+  if (A.n_packets > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[4], c->stream));
   launches += launch_finish(A, G, c->d_vol.p, c->nspec, c->stream);
@@ -625,7 +687,7 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   c->step++;
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
-    stats->n_packets = n_emit;
+    stats->n_packets = n_all;
     stats->n_escaped = (int64_t)cnt[C_ESCAPED];
     stats->n_absorbed = (int64_t)cnt[C_ABSORBED];
     stats->n_stopped = (int64_t)cnt[C_STOPPED];
@@ -656,6 +718,27 @@ int sed_step(sed_ctx* c, double dt, sed_step_stats* stats)
   rc = transport_impl(c, dt, stats, ms);
   if (stats && rc == SED_OK) stats->kernel_launches += c->opacity_launches;
   return rc;
+}
+
+int sed_get_gamma_spectrum(sed_ctx* c, double* flux, double* click)
+{
+  if (!c) return SED_ERR_ARG;
+  if (c->nspec_g == 0) return set_err(c, SED_ERR_STATE, "no radioactive source in this context");
+  if (flux) CK(cudaMemcpyAsync(flux, c->d_gflux.p, c->nspec_g * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (click) CK(cudaMemcpyAsync(click, c->d_gclick.p, c->nspec_g * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_get_radioactive_tallies(sed_ctx* c, double* L_radio_emit, double* L_radio_dep)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->d_L_dep.p) return set_err(c, SED_ERR_STATE, "no radioactive step yet");
+  const size_t nz = (size_t)c->nz;
+  if (L_radio_emit) CK(cudaMemcpyAsync(L_radio_emit, c->d_L_emit.p, nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (L_radio_dep) CK(cudaMemcpyAsync(L_radio_dep, c->d_L_dep.p, nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
 }
 
 int sed_solve_temperature(sed_ctx* c, int32_t set_Tgas_to_Trad, double* T_gas, int32_t* n_unsolved)
@@ -792,6 +875,10 @@ void sed_ctx_destroy(sed_ctx* c)
   c->d_opac.release(); c->d_cdf.release(); c->d_cdf_coarse.release(); c->d_counters.release();
   c->d_cdf_guide.release();
   c->d_temp_bad.release();
+  DevBuf<double>* rad[] = {&c->d_gn, &c->d_gflux, &c->d_gclick, &c->d_radio_cdf, &c->d_gamma_frac, &c->d_compton,
+                           &c->d_photoion, &c->d_L_emit, &c->d_L_dep, &c->d_L_tot, &c->d_q_state};
+  for (auto* b : rad) b->release();
+  c->d_q_ind.release(); c->d_reject.release(); c->d_q_n.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

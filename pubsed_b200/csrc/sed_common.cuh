@@ -20,6 +20,9 @@ constexpr double A_RAD = 7.5657e-15;
 constexpr double THOMSON = 0.66523e-24;
 constexpr double SIGMA_TOT = 0.0265400193567;
 constexpr double ERGS_TO_EV = 624150975230.2815;
+constexpr double M_E_MEV = 0.510998910511;  // electron rest energy (MeV)
+constexpr double MEV_TO_ERGS = 1.60217646e-6;
+constexpr double ALPHA_FS = 0.007;          // fine-structure constant as the reference has it
 
 enum Fate : int32_t { MOVING = 0, STOPPED = 1, ESCAPED = 2, ABSORBED = 3 };
 enum LocType : int32_t { LOC_FLEX = 0, LOC_LIN = 1, LOC_LOG = 2, LOC_NONE = 3 };

@@ -132,6 +132,15 @@ struct sed_ctx {
 
   // tallies
   DevBuf<double> d_J, d_e_abs, d_e_rad, d_fx, d_fy, d_fz, d_fr, d_flux, d_click;
+
+  // radioactive source: gamma-ray spectrum grid and tallies, per-zone decay
+  // quantities, and the queue of optical photons it hands to the packet kernel
+  HostLoc gn;
+  int64_t nspec_g = 0;
+  DevBuf<double> d_gn, d_gflux, d_gclick, d_radio_cdf, d_gamma_frac, d_compton, d_photoion, d_L_emit, d_L_dep,
+      d_L_tot, d_q_state;
+  DevBuf<int32_t> d_q_ind, d_reject;
+  DevBuf<uint32_t> d_q_n;
   DevBuf<unsigned long long> d_counters;
   int64_t nspec = 0;
 

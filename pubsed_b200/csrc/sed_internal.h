@@ -63,6 +63,13 @@ struct StepArgs {
   const double* zone_rin;            // [zones] inner wall after the core substitution
   unsigned long long* model_escaped; // [n_models] escaped packets per model
   uint32_t* step_dev;                // step counter on the device (advanced by the finish kernel)
+  // ---- radioactive source: queued optical photons (single-context kernels) ----
+  int64_t n_core;                    // queue entries [0, n_core) are core packets
+  int64_t radio_first_pid;           // Philox stream id of radioactive packet 0
+  const double* q_state;             // [n_radio * 9] {x, D, t, e, nu} of queued photons
+  const int32_t* q_ind;              // [n_radio] their zone (or -1 / -2)
+  const uint32_t* q_n;               // [n_radio] next deviate index; RADIO_NO_PHOTON: none
+  double *L_dep, *L_emit;            // [nz] radioactive tallies normalised by the finish kernel, or null
   // ---- differentiable transport (weighted forward and adjoint replay kernels only) ----
   const double* abs_scale;           // [nz * n_bands] factor on the absorption opacity, or null
   int32_t n_bands;                   // band of bin i = i * n_bands / n_nu
@@ -72,6 +79,35 @@ struct StepArgs {
   const double* adj_g;               // [nspec] d(loss)/d(flux) for the vector-Jacobian product
   double* adj_out;                   // VJP [nz * n_bands]; Jacobian [nspec * nz * n_bands]
 };
+
+constexpr uint32_t RADIO_NO_PHOTON = 0xFFFFFFFFu;
+
+// Radioactive gamma-ray source (transport::emit_radioactive, src/transport/
+// emission.cpp:163-243) and gamma-ray transport (Compton scattering and
+// photo-absorption, scatter.cpp:45-133, transport_opacity.cpp:290-313).
+struct RadioArgs {
+  int32_t nz, n_elems, force_rproc, pad_;
+  int64_t n_radio;                 // radioactive packets of the step
+  int64_t first_pid;               // Philox stream id of radioactive packet 0
+  double t_now, dt;
+  const double *rho, *vol, *X;     // zone state; X the zone's composition (not decayed)
+  const int32_t *eZ, *eA;
+  double *L_emit, *gamma_frac, *compton, *photoion;  // [nz] per-zone results
+  double* cdf;                     // [nz] zone emission CDF
+  double* L_tot;                   // device scalar: decay luminosity of the grid
+  double* L_dep;                   // [nz] deposition tally
+  double* q_state;                 // [n_radio * 9] {x, D, t, e, nu} of queued optical photons
+  int32_t* q_ind;                  // [n_radio] their zone
+  uint32_t* q_n;                   // [n_radio] their next deviate index, RADIO_NO_PHOTON if none
+  int32_t* n_reject_cap;           // Compton rejection loops that hit their cap
+};
+// per-zone decay luminosity, gamma fraction and gamma opacities, then the
+// zone emission CDF and the grid total (two launches)
+int launch_radio_zones(const RadioArgs& a, cudaStream_t s);
+// emission of the radioactive packets and transport of the gamma-rays; the
+// optical photons they become are queued for the packet kernel
+int launch_gamma(const StepArgs& a, const StepArgs& ag, const RadioArgs& r, const GridDev& g, int num_sms,
+                 cudaStream_t s);
 
 // One model of a batch: its packets are global queue entries
 // [pkt_off, pkt_off + n_packets), its zones [zone_off, zone_off + n_zones)

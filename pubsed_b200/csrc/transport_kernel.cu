@@ -630,6 +630,29 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       } else {
         pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
         if (pid >= (unsigned long long)A.n_packets) break;
+        if (!BATCH && MODE == 0 && A.q_n != nullptr && (int64_t)pid >= A.n_core) {
+          // an optical photon of the radioactive source, handed over by the
+          // gamma-ray kernel with its position in its Philox stream
+          const int64_t k = (int64_t)pid - A.n_core;
+          const uint32_t qn = A.q_n[k];
+          if (qn == RADIO_NO_PHOTON) continue;  // escaped or absorbed as a gamma-ray
+          const double* q = A.q_state + (size_t)k * 9;
+          p.x[0] = q[0]; p.x[1] = q[1]; p.x[2] = q[2];
+          p.D[0] = q[3]; p.D[1] = q[4]; p.D[2] = q[5];
+          p.t = q[6]; p.e = q[7]; p.nu = q[8];
+          p.ind = A.q_ind[k];
+          rng.init(A.seed, (uint64_t)(A.radio_first_pid + k), step, qn);
+          K = 0;  // a radioactive packet records every deviate of its stream
+          fate = MOVING;
+          if (p.ind == -1) fate = ABSORBED;
+          else if (p.ind == -2) fate = ESCAPED;
+          seg = 0;
+          acc_zone = -1;
+          acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
+          have = true;
+          if (fate != MOVING) continue;
+          goto segment;
+        }
         if constexpr (MODE == 2) {
           // only packets that reached the spectrum carry a gradient
           const int32_t sb = A.esc_bin[pid];
@@ -660,6 +683,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       have = true;
       if (fate != MOVING) continue;
     }
+  segment:
     {
       if (seg >= limit) { fate = STOPPED; ++n_lim; continue; }
       ++seg;
@@ -872,6 +896,10 @@ __device__ __forceinline__ void finish_zone(const StepArgs& A, const double* __r
   if (threadIdx.x == 0) {
     A.e_abs[iz] /= v * dt;
     A.fr[iz] /= v * C_LIGHT * dt;
+    if (A.L_dep) {  // transport_mpi.cpp:419-420
+      A.L_dep[iz] /= v * dt;
+      A.L_emit[iz] /= v;
+    }
     if ((nn == 1) || (!A.store_Jnu)) {
       double j0 = A.J[(size_t)iz * (A.store_Jnu ? nn : 1)];
       if (do_rescale && A.store_Jnu) { j0 *= fac; A.J[(size_t)iz * nn] = j0; }
@@ -940,6 +968,272 @@ __global__ void rescale_spectrum_batch_kernel(const StepArgs A, int64_t nspec)
     const int m = (int)(i / nspec);
     const int64_t n = A.models[m].n_packets;
     if (n > 0) A.flux[i] *= rescale_factor(A.model_escaped[m], n);
+  }
+}
+
+// ------------------------------------------------------------ gamma-rays
+// transport::lorentz_transform (relativity.cpp:84-127) in either direction:
+// tolab = 1 flips the velocity (comoving -> lab), tolab = 0 does not
+template <int GRID>
+__device__ __forceinline__ void lorentz_transform(const GridDev& G, Pkt& p, int tolab)
+{
+  double v[3], dvds;
+  get_velocity<GRID>(G, p.ind, p.x, p.D, v, &dvds);
+  if (tolab) { v[0] *= -1; v[1] *= -1; v[2] *= -1; }
+  const double beta2 = (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) / C_LIGHT / C_LIGHT;
+  const double vdd = v[0] * p.D[0] + v[1] * p.D[1] + v[2] * p.D[2];
+  const double gamma = 1.0 / sqrt(1 - beta2);
+  const double dshift = gamma * (1 - vdd / C_LIGHT);
+  p.dvds = dvds;
+  p.e *= dshift;
+  p.nu *= dshift;
+  const double f = (1 - gamma * vdd / C_LIGHT / (gamma + 1));
+  p.D[0] = 1.0 / dshift * (p.D[0] - gamma * v[0] / C_LIGHT * f);
+  p.D[1] = 1.0 / dshift * (p.D[1] - gamma * v[1] / C_LIGHT * f);
+  p.D[2] = 1.0 / dshift * (p.D[2] - gamma * v[2] / C_LIGHT * f);
+  const double norm = p.D[0] * p.D[0] + p.D[1] * p.D[1] + p.D[2] * p.D[2];
+  p.D[0] /= norm;
+  p.D[1] /= norm;
+  p.D[2] /= norm;
+}
+
+// transport::klein_nishina (transport_opacity.cpp:302-313), x in MeV
+__device__ __forceinline__ double klein_nishina(double x)
+{
+  x = x / M_E_MEV;
+  const double logfac = log(1 + 2 * x);
+  const double term1 = (1 + x) / x / x / x * (2 * x * (1 + x) / (1 + 2 * x) - logfac);
+  const double term2 = 1.0 / 2.0 / x * logfac;
+  const double term3 = -1.0 * (1 + 3 * x) / (1 + 2 * x) / (1 + 2 * x);
+  return .75 * (term1 + term2 + term3);
+}
+
+// grid::sample_in_zone: uniform in the shell volume (grid_1D_sphere.cpp:
+// 681-700) or in the Cartesian cell (grid_3D_cart.cpp:484-494)
+template <int GRID>
+__device__ __forceinline__ void sample_in_zone(const GridDev& G, int i, double u0, double u1, double u2, double* r)
+{
+  if constexpr (GRID == 0) {
+    const double r_0 = (i == 0) ? G.r_out.min : __ldg(G.r_out.right + i - 1);
+    const double ro = __ldg(G.r_out.right + i);
+    const double r_samp = pow(r_0 * r_0 * r_0 + u0 * (ro * ro * ro - r_0 * r_0 * r_0), 1.0 / 3.0);
+    const double mu = 1 - 2.0 * u1;
+    const double phi = 2.0 * PI * u2;
+    const double sin_theta = sqrt(1 - mu * mu);
+    r[0] = r_samp * sin_theta * cos(phi);
+    r[1] = r_samp * sin_theta * sin(phi);
+    r[2] = r_samp * mu;
+  } else {
+    const int nyz = G.ny * G.nz;
+    const int idx[3] = {i / nyz, (i / G.nz) % G.ny, i % G.nz};
+    const double u[3] = {u0, u1, u2};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) r[a] = loc_left(G.ax[a], idx[a]) + u[a] * loc_delta(G.ax[a], idx[a]);
+  }
+}
+
+// isotropic direction in the comoving frame (mu, phi: two deviates)
+__device__ __forceinline__ void isotropic_direction(PacketRng& rng, double* D)
+{
+  const double mu = 1 - 2.0 * rng.next();
+  const double phi = 2.0 * PI * rng.next();
+  const double smu = sqrt(1 - mu * mu);
+  D[0] = smu * cos(phi);
+  D[1] = smu * sin(phi);
+  D[2] = mu;
+}
+
+// transport::sample_photon_frequency for an optical photon (emission.cpp:27-46)
+template <typename CT>
+__device__ __forceinline__ void sample_optical_nu(const StepArgs& A, Pkt& p, PacketRng& rng)
+{
+  const int inu = (A.nu.n == 1) ? 0 : cdf_row_sample<CT>(A, p.ind, rng.next());
+  p.nu = loc_sample(A.nu, inu, rng.next());
+}
+
+// Radioactive packets: emission (transport::emit_radioactive, emission.cpp:
+// 212-236, and create_isotropic_particle, :57-107) and, for the gamma-rays,
+// the segment loop of propagate_monte_carlo with the gamma-ray opacity
+// (transport_opacity.cpp:290-296) and do_scatter / compton_scatter
+// (scatter.cpp:45-133).  Deviates come from the packet's own stream in the
+// reference's order.  A packet that is or becomes an optical photon is
+// queued, with its stream position, for the packet kernel.
+template <int GRID, typename CT>
+__global__ void __launch_bounds__(128, 8) gamma_kernel(const StepArgs A, const StepArgs AG, const RadioArgs R,
+                                                       const GridDev G)
+{
+  unsigned long long n_esc = 0, n_abs = 0, n_stop = 0, n_seg = 0, n_scat = 0, n_lim = 0;
+  const int64_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
+  constexpr int COMPTON_TRIES = 1 << 16;
+  const double L_tot = *R.L_tot;
+  const double Ep = L_tot * R.dt / (1.0 * R.n_radio);
+  for (;;) {
+    const int64_t k = (int64_t)atomicAdd(A.counters + C_COUNT, 1ULL);
+    if (k >= R.n_radio) break;
+    R.q_n[k] = RADIO_NO_PHOTON;
+    if (L_tot == 0) {  // the reference emits nothing then
+      if (A.rec_fate) {
+        const int64_t r = A.n_core + k;
+        A.rec_fate[r] = -1; A.rec_ind[r] = 0; A.rec_draws[r] = 0;
+        for (int j = 0; j < 9; ++j) A.rec_state[r * 9 + j] = 0;
+      }
+      continue;
+    }
+    PacketRng rng;
+    rng.init(A.seed, (uint64_t)(R.first_pid + k), A.step, 0);
+    Pkt p;
+    // zone_emission_cdf_.sample: upper_bound over the zones
+    const int i = (R.nz == 1) ? 0 : upper_bound_dev(R.cdf, R.nz, rng.next());
+    const double t = R.t_now + R.dt * rng.next();
+    const bool is_gamma = rng.next() < __ldg(R.gamma_frac + i);
+    if (!is_gamma) atomicAdd(R.L_dep + i, Ep);  // positrons deposit and become photons
+    const double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+    sample_in_zone<GRID>(G, i, u0, u1, u2, p.x);
+    isotropic_direction(rng, p.D);
+    p.ind = i;
+    if (is_gamma) p.nu = 1;  // sample_photon_frequency for gamma-rays (emission.cpp:35-38)
+    else sample_optical_nu<CT>(A, p, rng);
+    p.e = Ep;
+    lorentz_transform<GRID>(G, p, 1);
+    p.t = t;
+    // transport::propagate: the zone of the emitted position
+    p.ind = get_zone<GRID>(G, p.x);
+    bool photon = !is_gamma;
+    int fate = MOVING;
+    if (!photon) {
+      if (p.ind == -1) fate = ABSORBED;
+      else if (p.ind == -2) fate = ESCAPED;
+    }
+    int64_t seg = 0;
+    while (!photon && fate == MOVING) {
+      if (seg >= limit) { fate = STOPPED; ++n_lim; break; }
+      ++seg;
+      const int iz = p.ind;
+      double d_bn = 0;
+      const double rsq = (p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+      const double xdotD = (p.D[0] * p.x[0] + p.D[1] * p.x[1] + p.D[2] * p.x[2]);
+      int new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, rsq, xdotD, &d_bn);
+      const double dshift = dshift_lab_to_comoving<GRID>(G, p);
+      const double c_opac = __ldg(R.compton + iz) * klein_nishina(p.nu);
+      const double p_opac = __ldg(R.photoion + iz) * pow(p.nu, -3.5);
+      const double op = c_opac + p_opac;
+      const double eps = p_opac / (c_opac + p_opac);
+      double d_nu = loc_delta(A.nu, 0) / p.nu * C_LIGHT / p.dvds;  // i_nu = 0 for gamma-rays
+      if (p.dvds == 0) d_nu = INFINITY;
+      if (d_nu < 0) d_nu = -1 * d_nu;
+      if (d_nu < d_bn) { d_bn = d_nu; new_ind = p.ind; }
+      const double tot_lab = op * dshift;
+      const double tau_r = -1.0 * log(1 - rng.next());
+      double d_sc = tau_r / tot_lab;
+      if (tot_lab == 0) d_sc = INFINITY;
+      double d_tm = (A.tstop - p.t) * C_LIGHT;
+      if (A.steady) d_tm = INFINITY;
+      int event;
+      double this_d;
+      if ((d_sc < d_bn) && (d_sc < d_tm)) { event = 0; this_d = d_sc; }
+      else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
+      else { event = 2; this_d = d_tm; }
+      // radiation force tallies (gamma-rays add nothing to e_abs and J)
+      const double this_E = p.e * this_d;
+      if (A.tally_forces) {
+        atomicAdd(A.fx + iz, this_E * dshift * op * p.D[0] * dshift);
+        atomicAdd(A.fy + iz, this_E * dshift * op * p.D[1] * dshift);
+        atomicAdd(A.fz + iz, this_E * dshift * op * p.D[2] * dshift);
+        const double rr = sqrt(p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+        const double xd = p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2];
+        atomicAdd(A.fr + iz, this_E * dshift * op * xd / rr * dshift);
+      }
+      p.x[0] += this_d * p.D[0];
+      p.x[1] += this_d * p.D[1];
+      p.x[2] += this_d * p.D[2];
+      p.t = p.t + this_d / C_LIGHT;
+      if (event == 1) {
+        if (new_ind == -1) {
+          if (A.bound_in_reflect) { p.D[0] *= -1; p.D[1] *= -1; p.D[2] *= -1; }
+          else { p.ind = new_ind; fate = ABSORBED; }
+        } else if (new_ind == -2) {
+          if (A.bound_out_reflect) { p.D[0] *= -1; p.D[1] *= -1; p.D[2] *= -1; }
+          else { p.ind = new_ind; fate = ESCAPED; }
+        } else {
+          p.ind = new_ind;
+        }
+      } else if (event == 0) {
+        ++n_scat;
+        if (rng.next() > eps) {
+          // transport::compton_scatter (scatter.cpp:76-133)
+          lorentz_transform<GRID>(G, p, 0);
+          double E_ratio = 1, Dn[3];
+          for (int tries = 0;; ++tries) {
+            isotropic_direction(rng, Dn);
+            const double cost = p.D[0] * Dn[0] + p.D[1] * Dn[1] + p.D[2] * Dn[2];
+            E_ratio = 1 / (1 + p.nu / M_E_MEV * (1 - cost));
+            const double diff_cs = 0.5 * (E_ratio * E_ratio * (1 / E_ratio + E_ratio - 1 + cost * cost));
+            if (rng.next() < diff_cs) break;
+            if (tries + 1 >= COMPTON_TRIES) { atomicAdd(R.n_reject_cap, 1); break; }
+          }
+          p.nu = p.nu * E_ratio;
+          if (rng.next() > E_ratio) {
+            atomicAdd(R.L_dep + p.ind, p.e);
+            photon = true;
+            isotropic_direction(rng, Dn);
+            sample_optical_nu<CT>(A, p, rng);
+          }
+          p.D[0] = Dn[0];
+          p.D[1] = Dn[1];
+          p.D[2] = Dn[2];
+          lorentz_transform<GRID>(G, p, 1);
+        } else {
+          // photo-absorbed: deposited, re-emitted as an optical photon
+          atomicAdd(R.L_dep + p.ind, p.e);
+          photon = true;
+          isotropic_direction(rng, p.D);
+          sample_optical_nu<CT>(A, p, rng);
+          lorentz_transform<GRID>(G, p, 1);
+        }
+      } else {
+        fate = STOPPED;
+      }
+    }
+    n_seg += seg;
+    if (photon) {
+      double* q = R.q_state + (size_t)k * 9;
+      q[0] = p.x[0]; q[1] = p.x[1]; q[2] = p.x[2];
+      q[3] = p.D[0]; q[4] = p.D[1]; q[5] = p.D[2];
+      q[6] = p.t; q[7] = p.e; q[8] = p.nu;
+      R.q_ind[k] = p.ind;
+      R.q_n[k] = rng.n;
+      continue;
+    }
+    if (fate == ESCAPED) {
+      const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
+      spectrum_count(AG, AG.flux, AG.click, t_obs, p.nu, p.e, p.D);
+      p.t = t_obs;
+      ++n_esc;
+    } else if (fate == ABSORBED) {
+      ++n_abs;
+    } else {
+      ++n_stop;
+    }
+    if (A.rec_fate) {  // slots after the core packets'
+      const int64_t r = A.n_core + k;
+      A.rec_fate[r] = fate;
+      A.rec_ind[r] = p.ind;
+      A.rec_draws[r] = (int32_t)rng.n;
+      double* s = A.rec_state + r * 9;
+      s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
+      s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+      s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+    }
+  }
+  n_esc = warp_sum(n_esc); n_abs = warp_sum(n_abs); n_stop = warp_sum(n_stop);
+  n_seg = warp_sum(n_seg); n_scat = warp_sum(n_scat); n_lim = warp_sum(n_lim);
+  if ((threadIdx.x & 31) == 0) {
+    if (n_esc) atomicAdd(A.counters + C_ESCAPED, n_esc);
+    if (n_abs) atomicAdd(A.counters + C_ABSORBED, n_abs);
+    if (n_stop) atomicAdd(A.counters + C_STOPPED, n_stop);
+    if (n_seg) atomicAdd(A.counters + C_SEGMENTS, n_seg);
+    if (n_scat) atomicAdd(A.counters + C_SCATTERS, n_scat);
+    if (n_lim) atomicAdd(A.counters + C_LIMIT, n_lim);
   }
 }
 
@@ -1029,6 +1323,23 @@ int launch_propagate_diff(const StepArgs& a, const GridDev& g, int mode, int num
                      : launch_kernel_t<0, double2, double, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
   return mode == 1 ? launch_kernel_t<0, float2, float, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
                    : launch_kernel_t<0, float2, float, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
+}
+
+int launch_gamma(const StepArgs& a, const StepArgs& ag, const RadioArgs& r, const GridDev& g, int num_sms,
+                 cudaStream_t s)
+{
+  if (r.n_radio <= 0) return 0;
+  int64_t blocks = (int64_t)num_sms * 8;
+  const int64_t need = (r.n_radio + 127) / 128;
+  if (blocks > need) blocks = need;
+  if (g.type == 0) {
+    if (a.precision == 0) gamma_kernel<0, double><<<(unsigned)blocks, 128, 0, s>>>(a, ag, r, g);
+    else gamma_kernel<0, float><<<(unsigned)blocks, 128, 0, s>>>(a, ag, r, g);
+  } else {
+    if (a.precision == 0) gamma_kernel<1, double><<<(unsigned)blocks, 128, 0, s>>>(a, ag, r, g);
+    else gamma_kernel<1, float><<<(unsigned)blocks, 128, 0, s>>>(a, ag, r, g);
+  }
+  return 1;
 }
 
 void batch_variant_shape(int variant, int* threads, int* min_blocks)

@@ -113,6 +113,14 @@ class Workload:
         tp.spec_nu = abi.locate_grid(keep, ng)
         tp.spec_mu = abi.locate_grid(keep, mg)
         tp.spec_phi = abi.locate_grid(keep, pg)
+        # radioactive source (emit_radioactive).  The reference reads
+        # gamma_nu_grid but builds the gamma-ray spectrum on spectrum_nu_grid
+        # (transport_init.cpp:170-173), so MeV energies land in the first bin
+        # (spectrum_array::count keeps off-grid energies there); the same grid
+        # is passed here
+        tp.n_emit_radioactive = int(P.scalar("particles_n_emit_radioactive", int))
+        tp.force_rprocess_heating = int(P.scalar("force_rprocess_heating", int))
+        tp.gamma_nu = abi.locate_grid(keep, ng)
         return tp
 
     def grid_struct(self, keep: abi.Keep) -> abi.Grid:
@@ -225,7 +233,8 @@ IA_LAYERS = [  # (v_upper cm/s, mass fractions in IA_ELEMENTS order)
 def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_000, n_bins: int = 4096,
             n_levels_per_ion: int = 20, v_max: float = 3e9, epsilon: float = 1.0, seed: int = 0, data_seed: int = 0,
             bound_free: int = 0, free_free: int = 1, spectrum_bins: int = 1024,
-            v_core: float = 1e9, radiative_eq: int = 1) -> Workload:
+            v_core: float = 1e9, radiative_eq: int = 1, n_radioactive: int = 0,
+            t_days: float = 20.0) -> Workload:
     """Precision configuration: 1D Type Ia-like ejecta, 256 zones, 1.4 Msun,
     rho ~ exp(-v / 2.7e8 cm/s), t = 20 d, layered 56Ni / Si-S-Ca / C-O
     composition, T falling linearly from 1.2e4 K (inner) to 5e3 K (outer),
@@ -234,6 +243,9 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
     binned into 4096 log frequency bins, electron scattering and free-free,
     a central 1.2e4 K lightbulb, radiative equilibrium (absorbed packets are
     re-emitted from the zone emissivity), steady-state iteration.
+    n_radioactive > 0 adds that many 56Ni/56Co decay packets
+    (particles_n_emit_radioactive) with gamma-ray transport; t_days moves
+    the epoch (the ejecta thin out as t^-3, so gamma-rays escape late).
 
     Choices the configuration leaves open, fixed here: v_max = 3e9 cm/s;
     Si/S/Ca = 0.6/0.3/0.1 and C/O = 0.5/0.5 by mass; five ion stages per
@@ -248,7 +260,7 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
     radiative_eq = 0 makes absorption final (the form the differentiable
     transport needs)."""
     rng = np.random.default_rng(data_seed)  # synthetic atoms and lines; `seed` keys the packets
-    t = 20 * 86400.0
+    t = t_days * 86400.0
     v = np.array([(i + 1) * v_max / n_zones for i in range(n_zones)])
     vc = np.concatenate([[0.0], v[:-1]]) * 0.5 + v * 0.5
     Z = [e[0] for e in IA_ELEMENTS]
@@ -279,10 +291,12 @@ def type_ia(n_packets: int = 10_000_000, n_zones: int = 256, n_lines: int = 500_
         "core_n_emit": int(n_packets), "core_radius": float(v_core * t), "core_temperature": 1.2e4,
         "core_luminosity": 1e43,
         "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
-        "particles_max_total": max(int(1e7), int(n_packets)),
+        "particles_max_total": max(int(1e7), int(n_packets) + int(n_radioactive)),
     }
+    if n_radioactive > 0:
+        params["particles_n_emit_radioactive"] = int(n_radioactive)
     return Workload("type_ia_1d", params, z, atoms,
-                    notes={"v_max": v_max, "t_days": 20.0, "rho0": rho0, "log_del": d,
+                    notes={"v_max": v_max, "t_days": t_days, "rho0": rho0, "log_del": d,
                            "n_lines": n_lines, "n_levels_per_ion": n_levels_per_ion})
 
 

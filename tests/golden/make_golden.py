@@ -8,7 +8,9 @@ inputs, plus the reference's outputs:
 
   replay_*.npz   one transport step in replay mode (per-packet fate, final
                  zone, number of deviates drawn, final state; J_nu, e_abs,
-                 e_rad, forces, spectrum; opacity tables; the zone
+                 e_rad, forces, spectrum; with a radioactive source the
+                 gamma-ray spectrum and L_radio_emit / L_radio_dep; opacity
+                 tables; the zone
                  temperatures after the step's radiative-equilibrium solve;
                  the reference's own spectrum .dat and, for 1D, plt .dat text)
   locate_kat.json  value/index pairs printed by the reference's own
@@ -36,6 +38,14 @@ CASES = {
     "replay_grey_radeq": ("lightbulb_grey", dict(n_packets=600, n_zones=32, n_bins=128, radiative_eq=1, seed=5)),
     "replay_ia_lte": ("type_ia", dict(n_packets=300, n_zones=16, n_lines=5000, n_bins=256, n_levels_per_ion=6,
                                       bound_free=1, free_free=1, seed=7)),
+    # 56Ni/56Co decay packets (gamma-rays and positrons) next to the core
+    # packets; a small core so that most of the 56Ni sits outside it
+    "replay_ia_radio": ("type_ia", dict(n_packets=200, n_zones=16, n_lines=5000, n_bins=256, n_levels_per_ion=6,
+                                        v_core=1e8, n_radioactive=600, seed=19)),
+    # the same ejecta at 150 days: thin enough that gamma-rays escape
+    "replay_ia_radio_late": ("type_ia", dict(n_packets=100, n_zones=16, n_lines=5000, n_bins=256,
+                                             n_levels_per_ion=6, v_core=1e8, n_radioactive=800, t_days=150.0,
+                                             seed=23)),
     "replay_cart3d": ("cart3d", dict(n_packets=300, n_cells=6, n_lines=1500, n_bins=128, spectrum_bins=64, n_mu=4,
                                      seed=13)),
 }
@@ -70,6 +80,9 @@ def main():
         w = make_workload(gen, kw)
         out = run_ref.run(w, "replay", threads=1, seed=kw.get("seed", 0))
         arrays = {k: out[k] for k in KEYS}
+        for k in ("L_radio_emit", "L_radio_dep", "gamma_flux", "gamma_click"):
+            if k in out:
+                arrays[k] = out[k]
         # with grey opacity the reference never sets zone n_elec: its dump is
         # whatever the memory held; the restatement has zeros there
         if float(w.params.get("opacity_grey_opacity", 0)) != 0:

@@ -111,6 +111,17 @@ class Engine:
                                           P(out["L_thermal"])), "get_opacity")
         return out
 
+    def radioactive(self) -> dict:
+        """L_radio_emit / L_radio_dep per zone and the gamma-ray spectrum of
+        the last step (a radioactive source must be on)."""
+        le = np.zeros(self.nz); ld = np.zeros(self.nz)
+        ng = self.tp.spec_time.n * max(self.tp.gamma_nu.n, 1) * self.tp.spec_mu.n * self.tp.spec_phi.n
+        gf = np.zeros(ng); gc = np.zeros(ng)
+        P = lambda a: a.ctypes.data_as(abi._dp)
+        self.check(self.fn("get_radioactive_tallies")(self.ctx, P(le), P(ld)), "get_radioactive_tallies")
+        self.check(self.fn("get_gamma_spectrum")(self.ctx, P(gf), P(gc)), "get_gamma_spectrum")
+        return {"L_radio_emit": le, "L_radio_dep": ld, "gamma_flux": gf, "gamma_click": gc}
+
     def records(self, n: int) -> dict:
         fate = np.zeros(n, np.int32); ind = np.zeros(n, np.int32); draws = np.zeros(n, np.int32)
         st = np.zeros(n * 9)

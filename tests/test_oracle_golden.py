@@ -17,7 +17,8 @@ from pubsed_b200 import abi, grids, workloads
 import oracle_lib
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte", "replay_cart3d"]
+CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte", "replay_cart3d", "replay_ia_radio",
+         "replay_ia_radio_late"]
 
 
 def _load(name):
@@ -59,6 +60,14 @@ def test_oracle_matches_reference_replay(name):
     f, c = e.spectrum()
     assert np.array_equal(c, ref["spec_click"])
     assert _rel(f, ref["spec_flux"]) <= 1e-12
+    if "L_radio_dep" in ref:
+        # radioactive source: decay luminosity per zone is the same
+        # expression; deposition and the gamma-ray spectrum are tallies
+        R = e.radioactive()
+        assert _rel(R["L_radio_emit"], ref["L_radio_emit"]) <= 1e-14
+        assert _rel(R["L_radio_dep"], ref["L_radio_dep"]) <= 1e-12
+        assert np.array_equal(R["gamma_click"], ref["gamma_click"])
+        assert _rel(R["gamma_flux"], ref["gamma_flux"]) <= 1e-12
     # the radiative-equilibrium temperature solve that ends transport::step
     if int(w.params.get("transport_radiative_equilibrium", 0)):
         Tg, nbad = oracle_lib.solve_temperature(e)

@@ -1,0 +1,94 @@
+"""The oracle's radioactive source on the CPU: the edge cases and the
+energy bookkeeping that the reference's emission rules give
+(transport::emit_radioactive, src/transport/emission.cpp:165-243)."""
+import numpy as np
+import pytest
+
+from pubsed_b200 import workloads
+import oracle_lib
+
+
+def _step(w):
+    e = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    e.set_opacity(1.0)
+    e.record(True)
+    return e, e.transport(1.0)
+
+
+def _small(**over):
+    kw = dict(n_packets=200, n_zones=16, n_lines=2000, n_bins=128, n_levels_per_ion=6, v_core=1e8,
+              n_radioactive=400, seed=51)
+    kw.update(over)
+    return workloads.type_ia(**kw)
+
+
+def test_every_emitted_packet_ends_once():
+    w = _small(t_days=60.0)
+    e, st = _step(w)
+    assert st["n_packets"] == 600
+    assert st["n_escaped"] + st["n_absorbed"] + st["n_stopped"] == 600
+    rec = e.records(600)
+    assert np.all(rec["fate"] >= 1)
+    # radioactive packets record every deviate of their stream: at least the
+    # eight of a gamma-ray's emission
+    assert np.all(rec["draws"][200:] >= 8)
+    e.close()
+
+
+def test_no_radioactive_material():
+    w = _small()
+    w.zones.X[:, 2] += w.zones.X[:, -1]
+    w.zones.X[:, -1] = 0.0
+    e, st = _step(w)
+    assert st["n_packets"] == 600
+    assert st["n_escaped"] + st["n_absorbed"] + st["n_stopped"] == 200
+    rec = e.records(600)
+    assert np.all(rec["fate"][200:] == -1)
+    R = e.radioactive()
+    assert np.all(R["L_radio_emit"] == 0) and np.all(R["L_radio_dep"] == 0)
+    e.close()
+
+
+def test_forced_rprocess_deposits_everything():
+    w = _small()
+    w.params["force_rprocess_heating"] = 1
+    e, st = _step(w)
+    R = e.radioactive()
+    vol = w.zones.vol
+    assert abs(np.sum(R["L_radio_dep"] * vol) / np.sum(R["L_radio_emit"] * vol) - 1) < 1e-12
+    assert np.all(R["gamma_click"] == 0)
+    e.close()
+
+
+def test_capacity():
+    w = _small()
+    w.params["particles_max_total"] = 500
+    e = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    e.set_opacity(1.0)
+    with pytest.raises(RuntimeError, match=r"\(3\)"):
+        e.transport(1.0)
+    e.close()
+    w.params["particles_max_total"] = 300  # the 400 decay packets alone do not fit
+    e, st = _step(w)
+    assert st["n_packets"] == 200
+    e.close()
+
+
+def test_decay_luminosity_follows_the_56ni_chain():
+    """L_radio_emit per unit mass of 56Ni at two epochs against the two-step
+    decay chain written out here (tau_Ni = 8.8 d, tau_Co = 111.4 d, 1.725 and
+    3.730 MeV per decay)."""
+    for t_days in (5.0, 80.0):
+        w = _small(t_days=t_days)
+        e, _ = _step(w)
+        R = e.radioactive()
+        z = w.zones
+        ni = z.X[:, -1] > 0
+        t = t_days * 86400.0
+        tn, tc = 757241.8, 9627379.0
+        mev = 1.60217646e-6
+        rate = (np.exp(-t / tn) / tn * 1.725 + (np.exp(-t / tn) - np.exp(-t / tc)) / (tn - tc) * 3.730) * mev
+        expect = z.rho[ni] * z.X[ni, -1] / (56 * 1.67262158e-24) * rate
+        assert np.allclose(R["L_radio_emit"][ni], expect, rtol=1e-12)
+        assert np.all(R["L_radio_emit"][~ni] == 0)
+        e.close()
