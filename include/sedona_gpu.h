@@ -249,6 +249,13 @@ void sed_ctx_destroy(sed_ctx* ctx);
 /* Library version / build string (never NULL). */
 const char* sed_version(void);
 
+/* Packet counts of the following steps: core_n_emit (emit_inner_source) and
+ * particles_n_emit_radioactive (emit_radioactive), as the host's time loop
+ * changes them (particles_last_iter_pump on the last iteration,
+ * emission.cpp:180-184 and 377-382; multiply_particles_n_emit_by_dt_over_dtmax,
+ * :170-173).  SED_ERR_ARG for a negative count. */
+int sed_set_emission(sed_ctx* ctx, double core_n_emit, int64_t n_emit_radioactive);
+
 /* Radioactive source results of the last step (n_emit_radioactive > 0): the
  * escaping gamma-ray spectrum (gamma_spectrum, n_t*n_gamma_nu*n_mu*n_phi) and
  * per zone the decay luminosity per volume L_radio_emit and the deposited

@@ -370,6 +370,10 @@ int main(int argc, char** argv)
     // halves go to the stand-in, which writes nothing
     t.optical_spectrum.set_name(o.prefix + "_spectrum");
     t.optical_spectrum.print(0);
+    if (params.getScalar<int>("particles_n_emit_radioactive") > 0) {
+      t.gamma_spectrum.set_name(o.prefix + "_gamma");
+      t.gamma_spectrum.print(0);
+    }
     if (grid_type == "grid_1D_sphere") grid->write_plotfile(1, t.t_now_, 0);
   } else if (mode == "free") {
     oracle_rng_free_running();

@@ -92,6 +92,7 @@ struct oracle_ctx {
   lgrid gn;
   int64_t nspec_g;
   double *gflux, *gclick;
+  int64_t n_reject_cap;  /* Compton scatters that hit the rejection bound */
   double *L_emit, *L_dep, *radio_cdf, *gamma_frac, *compton, *photoion;
   /* differentiable transport: exact Jacobian of the last weighted forward,
    * accumulated forward-mode per packet ([nspec][nzones][bands]) */
@@ -178,6 +179,14 @@ static void cdf_normalize(double* y, int n)
 }
 
 /* ---------------------------------------------------------------- context */
+static void alloc_gamma_spectrum(oracle_ctx* o)
+{
+  if (o->gflux) return;
+  o->nspec_g = (int64_t)o->st.n * o->gn.n * o->sm.n * o->sp.n;
+  o->gflux = (double*)calloc((size_t)o->nspec_g, sizeof(double));
+  o->gclick = (double*)calloc((size_t)o->nspec_g, sizeof(double));
+}
+
 int oracle_ctx_create(const sed_transport_params* p, oracle_ctx** out)
 {
   if (!p || !out) return SED_ERR_ARG;
@@ -207,16 +216,13 @@ int oracle_ctx_create(const sed_transport_params* p, oracle_ctx** out)
     o->core_cdf[j] = (j == 0) ? w : o->core_cdf[j - 1] + w;
   }
   cdf_normalize(o->core_cdf, nn);
-  if (p->n_emit_radioactive > 0) {
-    if (p->gamma_nu.n > 0 && p->gamma_nu.right) lgrid_copy(&o->gn, &p->gamma_nu);
-    else {  /* one catch-all bin */
-      o->gn.n = 1; o->gn.type = SED_LOC_NONE; o->gn.min = -INFINITY; o->gn.del = 0;
-      o->gn.x = (double*)malloc(sizeof(double)); o->gn.x[0] = INFINITY;
-    }
-    o->nspec_g = (int64_t)o->st.n * o->gn.n * o->sm.n * o->sp.n;
-    o->gflux = (double*)calloc((size_t)o->nspec_g, sizeof(double));
-    o->gclick = (double*)calloc((size_t)o->nspec_g, sizeof(double));
+  /* the gamma-ray spectrum (used once a step emits radioactive packets) */
+  if (p->gamma_nu.n > 0 && p->gamma_nu.right) lgrid_copy(&o->gn, &p->gamma_nu);
+  else {  /* one catch-all bin */
+    o->gn.n = 1; o->gn.type = SED_LOC_NONE; o->gn.min = -INFINITY; o->gn.del = 0;
+    o->gn.x = (double*)malloc(sizeof(double)); o->gn.x[0] = INFINITY;
   }
+  if (p->n_emit_radioactive > 0) alloc_gamma_spectrum(o);
   *out = o;
   return SED_OK;
 }
@@ -1535,7 +1541,7 @@ static int propagate_gamma(oracle_ctx* o, packet* p, double t_now, double dt, in
           E_ratio = 1 / (1 + p->nu / PC_M_E_MEV * (1 - cost));
           double diff_cs = 0.5 * (E_ratio * E_ratio * (1 / E_ratio + E_ratio - 1 + cost * cost));
           if (draw(o, p) < diff_cs) break;
-          if (tries + 1 >= COMPTON_TRIES) break;
+          if (tries + 1 >= COMPTON_TRIES) { o->n_reject_cap++; break; }
         }
         p->nu = p->nu * E_ratio;
         if (draw(o, p) > E_ratio) {
@@ -1592,6 +1598,7 @@ static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
   double** zarr[6] = {&o->L_emit, &o->L_dep, &o->radio_cdf, &o->gamma_frac, &o->compton, &o->photoion};
   for (int q = 0; q < 6; q++) { free(*zarr[q]); *zarr[q] = (double*)calloc((size_t)nz, sizeof(double)); }
   double L_tot = radio_zones(o, t_now);
+  o->n_reject_cap = 0;
   double Ep_r = L_tot * dt / (1.0 * n_radio);
   if (o->record) {
     free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state);
@@ -1683,6 +1690,7 @@ static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
     st->n_packets = n_all; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
     st->n_segments = nseg; st->n_scatters = nscat;
   }
+  if (o->n_reject_cap > 0) return fail(o, SED_ERR_LIMIT, "Compton scatters hit the rejection-sampling bound");
   return SED_OK;
 }
 
@@ -1814,6 +1822,16 @@ static int propagate_weighted(oracle_ctx* o, packet* p, double t_now, double dt,
   }
   *nseg += seg;
   return fate;
+}
+
+int oracle_set_emission(oracle_ctx* o, double core_n_emit, int64_t n_emit_radioactive)
+{
+  if (!o) return SED_ERR_ARG;
+  if (!(core_n_emit >= 0) || n_emit_radioactive < 0) return fail(o, SED_ERR_ARG, "negative packet count");
+  o->tp.core_n_emit = core_n_emit;
+  o->tp.n_emit_radioactive = n_emit_radioactive;
+  if (n_emit_radioactive > 0) alloc_gamma_spectrum(o);
+  return SED_OK;
 }
 
 int oracle_set_rng_step(oracle_ctx* o, uint32_t step)

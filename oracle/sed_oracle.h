@@ -47,6 +47,8 @@ int oracle_set_rng_step(oracle_ctx* o, uint32_t step);
 int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* stats);
 int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
 int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
+/* packet counts of the next steps */
+int oracle_set_emission(oracle_ctx* o, double core_n_emit, int64_t n_emit_radioactive);
 /* radioactive source results of the last step */
 int oracle_get_gamma_spectrum(oracle_ctx* o, double* flux, double* click);
 int oracle_get_radioactive_tallies(oracle_ctx* o, double* L_radio_emit, double* L_radio_dep);

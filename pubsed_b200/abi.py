@@ -182,6 +182,7 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         "solve_temperature": ([vp, C.c_int32, _dp, _ip], C.c_int),
         "get_gamma_spectrum": ([vp, _dp, _dp], C.c_int),
         "get_radioactive_tallies": ([vp, _dp, _dp], C.c_int),
+        "set_emission": ([vp, C.c_double, C.c_int64], C.c_int),
     })
     if prefix == "sed_":
         i64p = C.POINTER(C.c_int64)

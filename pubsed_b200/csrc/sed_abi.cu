@@ -181,6 +181,21 @@ extern "C" {
 
 const char* sed_version(void) { return "sedona-b200 transport 0.1 (sm_100a)"; }
 
+// gamma-ray spectrum and the radioactive scalars, once per context
+static int alloc_gamma_spectrum(sed_ctx* c)
+{
+  if (c->nspec_g > 0) return SED_OK;
+  CK(upload(c, c->d_gn, c->gn.x.data(), c->gn.x.size()));
+  c->nspec_g = (int64_t)c->st.n() * c->gn.n() * c->sm.n() * c->sp.n();
+  CK(c->d_gflux.resize(c->nspec_g));
+  CK(c->d_gclick.resize(c->nspec_g));
+  CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
+  CK(c->d_L_tot.resize(1));
+  CK(c->d_reject.resize(1));
+  return SED_OK;
+}
+
 int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
 {
   if (!p || !out) return SED_ERR_ARG;
@@ -224,14 +239,8 @@ int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
   CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
   if (p->n_emit_radioactive > 0) {
-    CK(upload(c, c->d_gn, c->gn.x.data(), c->gn.x.size()));
-    c->nspec_g = (int64_t)c->st.n() * c->gn.n() * c->sm.n() * c->sp.n();
-    CK(c->d_gflux.resize(c->nspec_g));
-    CK(c->d_gclick.resize(c->nspec_g));
-    CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
-    CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
-    CK(c->d_L_tot.resize(1));
-    CK(c->d_reject.resize(1));
+    const int rc = alloc_gamma_spectrum(c);
+    if (rc) return rc;
   }
   CK(cudaStreamSynchronize(c->stream));
   c->op.epsilon = 1.0;
@@ -683,6 +692,9 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   CK(cudaEventRecord(c->ev[5], c->stream));
   unsigned long long cnt[C_COUNT + 1];
   CK(cudaMemcpyAsync(cnt, c->d_counters.p, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+  int32_t n_reject_cap = 0;
+  if (c->tp.n_emit_radioactive > 0)
+    CK(cudaMemcpyAsync(&n_reject_cap, c->d_reject.p, sizeof n_reject_cap, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->step++;
   if (stats) {
@@ -704,10 +716,27 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     stats->ms_total = ms + ms_opacity;
   }
   if (cnt[C_LIMIT] > 0) return set_err(c, SED_ERR_LIMIT, "%llu packets hit the segment limit", cnt[C_LIMIT]);
+  if (n_reject_cap > 0)
+    return set_err(c, SED_ERR_LIMIT, "%d Compton scatters hit the rejection-sampling bound", (int)n_reject_cap);
   return SED_OK;
 }
 
 int sed_transport(sed_ctx* c, double dt, sed_step_stats* stats) { return transport_impl(c, dt, stats, 0.f); }
+
+int sed_set_emission(sed_ctx* c, double core_n_emit, int64_t n_emit_radioactive)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!(core_n_emit >= 0) || n_emit_radioactive < 0)
+    return set_err(c, SED_ERR_ARG, "sed_set_emission: negative packet count");
+  c->tp.core_n_emit = core_n_emit;
+  c->tp.n_emit_radioactive = n_emit_radioactive;
+  if (n_emit_radioactive > 0) {
+    const int rc = alloc_gamma_spectrum(c);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
 
 int sed_step(sed_ctx* c, double dt, sed_step_stats* stats)
 {

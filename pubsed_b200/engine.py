@@ -87,6 +87,23 @@ class Engine:
                     "sed_get_zone_tallies")
         return out
 
+    def set_emission(self, core_n_emit: float, n_emit_radioactive: int):
+        """sed_set_emission: packet counts of the following steps."""
+        self._check(self.L.sed_set_emission(self.ctx, float(core_n_emit), int(n_emit_radioactive)), "sed_set_emission")
+        self.tp.core_n_emit = float(core_n_emit)
+        self.tp.n_emit_radioactive = int(n_emit_radioactive)
+
+    def radioactive(self) -> dict:
+        """Radioactive source results of the last step: L_radio_emit and
+        L_radio_dep per zone (per volume) and the gamma-ray spectrum."""
+        le, ld = np.zeros(self.nz), np.zeros(self.nz)
+        ng = self.tp.spec_time.n * max(self.tp.gamma_nu.n, 1) * self.tp.spec_mu.n * self.tp.spec_phi.n
+        gf, gc = np.zeros(ng), np.zeros(ng)
+        P = lambda a: a.ctypes.data_as(abi._dp)
+        self._check(self.L.sed_get_radioactive_tallies(self.ctx, P(le), P(ld)), "sed_get_radioactive_tallies")
+        self._check(self.L.sed_get_gamma_spectrum(self.ctx, P(gf), P(gc)), "sed_get_gamma_spectrum")
+        return {"L_radio_emit": le, "L_radio_dep": ld, "gamma_flux": gf, "gamma_click": gc}
+
     def opacity(self) -> dict:
         n = self.nz * self.nn
         out = {k: np.zeros(n) for k in ("abs", "scat", "emis_cdf")}

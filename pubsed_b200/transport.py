@@ -3,8 +3,10 @@
 context of the CUDA library and runs `step(dt)` as transport::step does
 (src/transport/transport.cpp:26-140): opacity build, emission, propagation,
 tally normalisation, then the radiative-equilibrium temperature solve when
-the parameters ask for it.  `output_spectrum(it)` and `write_plotfile(iw)`
-write the reference's text outputs; `run_steady` iterates like the
+the parameters ask for it.  With particles_n_emit_radioactive > 0 the step
+also emits and transports the decay packets and keeps L_radio_emit /
+L_radio_dep and the gamma-ray spectrum.  `output_spectrum(it)` and
+`write_plotfile(iw)` write the reference's text outputs; `run_steady` iterates like the
 reference's driver does for steady-state runs
 (src/main/SedonaClass.cpp:349-390).
 """
@@ -29,22 +31,45 @@ class Transport:
         self.fix_Tgas = self.P.scalar("transport_fix_Tgas_during_transport", int)
         self.solve_Tgas_updated = self.P.scalar("transport_solve_Tgas_with_updated_opacities", int)
         self.set_Tgas_to_Trad = self.P.scalar("transport_set_Tgas_to_Trad", int)
+        self.n_radio = self.P.scalar("particles_n_emit_radioactive", int)
         self.tallies = None
+        self.radio = None
         self.n_unsolved = 0
         self.last_stats = None
 
-    def step(self, dt: float = 1.0) -> dict:
+    def emission_counts(self, dt: float, last_iteration: bool) -> tuple:
+        """Packet counts of a step: emit_radioactive scales its count by
+        dt / tstep_max_dt when multiply_particles_n_emit_by_dt_over_dtmax is
+        set (an int times a double, truncated: emission.cpp:170-173), and on
+        the last iteration both it and emit_inner_source multiply theirs by
+        particles_last_iter_pump when that is not 0 (:180-184, :377-382)."""
+        n_core = int(self.P.scalar("core_n_emit", int))
+        n_radio = int(self.n_radio)
+        if n_radio and self.P.scalar("multiply_particles_n_emit_by_dt_over_dtmax", int):
+            n_radio = int(n_radio * (dt / self.P.scalar("tstep_max_dt")))
+        if last_iteration:
+            pump = self.P.scalar("particles_last_iter_pump", int)
+            if pump != 0:
+                n_core *= pump
+                n_radio *= pump
+        return n_core, n_radio
+
+    def step(self, dt: float = 1.0, last_iteration: bool = False) -> dict:
         """transport::step: the zone state of the workload is copied in, the
         step runs on the device, tallies come back, and with radiative
         equilibrium the new gas temperatures replace the workload's."""
         if self.steady_state:
             dt = 1.0
+        n_core, n_radio = self.emission_counts(dt, last_iteration)
+        if (n_core, n_radio) != (int(self.eng.tp.core_n_emit), int(self.eng.tp.n_emit_radioactive)):
+            self.eng.set_emission(n_core, n_radio)
         self.eng.upload_grid()
         st = self.eng.step(dt)
         if self.radiative_eq and not self.fix_Tgas and not self.solve_Tgas_updated:
             T, self.n_unsolved = self.eng.solve_temperature(self.set_Tgas_to_Trad)
             self.w.zones.T = T
         self.tallies = self.eng.tallies()
+        self.radio = self.eng.radioactive() if n_radio > 0 else None
         self.last_stats = st
         return st
 
@@ -53,13 +78,21 @@ class Transport:
 
     def output_spectrum(self, it: int, outdir: str = ".") -> Optional[str]:
         """transport::output_spectrum(it) (src/transport/transport_output.cpp:
-        17-60): spectrum_name + "_" + it (or "_final" for it < 0), text part."""
-        name = self.P.get("spectrum_name")
-        if not name or self.P.scalar("spectrum_suppress_txt", int):
+        17-60): spectrum_name + "_" + it (or "_final" for it < 0), text part;
+        with gamma_name set, the gamma-ray spectrum too (on the same grids,
+        as the reference builds it).  Returns the optical spectrum's path."""
+        if self.P.scalar("spectrum_suppress_txt", int):
             return None
         base = "_final" if it < 0 else "_%d" % it
-        flux, click = self.eng.spectrum()
         tg, ng, mg, pg = self.w.spectrum_grids()
+        gname = self.P.get("gamma_name")
+        if gname and self.radio is not None:
+            output.write_spectrum_dat(os.path.join(outdir, gname + base), self.radio["gamma_flux"],
+                                      self.radio["gamma_click"], tg, ng, mg, pg)
+        name = self.P.get("spectrum_name")
+        if not name:
+            return None
+        flux, click = self.eng.spectrum()
         return output.write_spectrum_dat(os.path.join(outdir, name + base), flux, click, tg, ng, mg, pg)
 
     def write_plotfile(self, iw: int, t: float, outdir: str = ".") -> str:
@@ -72,8 +105,10 @@ class Transport:
         fr = bool(self.P.scalar("output_write_mass_fractions", int))
         elems = list(zip(z.elem_Z.tolist(), z.elem_A.tolist()))
         v = z.v if z.v is not None else np.zeros(z.n_zones)
+        R = self.radio or {}
         return output.write_plotfile_1d(os.path.join(outdir, output.plotfile_name(iw)), t, z.r_min, z.r_out, z.rho,
                                         v, z.T, self.tallies["e_rad"], n_elec,
+                                        L_dep=R.get("L_radio_dep"), L_emit=R.get("L_radio_emit"),
                                         X=z.X if fr else None, elems=elems if fr else None)
 
     def close(self):
@@ -84,11 +119,12 @@ def run_steady(workload, outdir: str = ".", precision: int = abi.PREC_FP64, devi
     """Steady-state iterations as the reference's driver runs them
     (SedonaClass::evolve_system with transport_steady_iterate = n): each
     iteration steps the transport and writes spectrum_<it>.dat and
-    plt_<it>.dat at the grid time."""
+    plt_<it>.dat at the grid time; the last iteration is flagged
+    (SedonaClass.cpp:333), which pumps its emission."""
     n_iter = max(1, workload.P.scalar("transport_steady_iterate", int))
     tr = Transport(workload, precision=precision, device=device)
     for it in range(1, n_iter + 1):
-        tr.step(1.0)
+        tr.step(1.0, last_iteration=(it == n_iter))
         tr.output_spectrum(it, outdir)
         tr.write_plotfile(it, workload.zones.t_now, outdir)
     return tr

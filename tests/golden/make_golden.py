@@ -90,6 +90,10 @@ def main():
         # the reference's own text outputs of the step
         with open(os.path.join(out["_dir"], "out_spectrum.dat")) as f:
             arrays["spectrum_dat"] = np.array(f.read())
+        gam = os.path.join(out["_dir"], "out_gamma.dat")
+        if os.path.exists(gam):
+            with open(gam) as f:
+                arrays["gamma_dat"] = np.array(f.read())
         plt = os.path.join(out["_dir"], "plt_00001.dat")
         if os.path.exists(plt):
             with open(plt) as f:

@@ -14,7 +14,8 @@ from pubsed_b200 import abi, output, workloads
 import oracle_lib
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte", "replay_cart3d"]
+CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte", "replay_cart3d", "replay_ia_radio",
+         "replay_ia_radio_late"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -31,12 +32,17 @@ def test_text_outputs_match_reference(name, tmp_path):
     tg, ng, mg, pg = w.spectrum_grids()
     path = output.write_spectrum_dat(str(tmp_path / "spec"), flux, click, tg, ng, mg, pg)
     assert open(path).read() == str(ref["spectrum_dat"])
+    R = {}
+    if "gamma_dat" in ref.files:  # binned on the optical spectrum's grids, as the reference does
+        R = e.radioactive()
+        path = output.write_spectrum_dat(str(tmp_path / "gamma"), R["gamma_flux"], R["gamma_click"], tg, ng, mg, pg)
+        assert open(path).read() == str(ref["gamma_dat"])
     if "plt_dat" in ref.files:
         z = w.zones
         tal = e.tallies()
         n_elec = e.opacity()["n_elec"]
         p = output.write_plotfile_1d(str(tmp_path / "plt_00001.dat"), z.t_now, z.r_min, z.r_out, z.rho, z.v, T,
-                                     tal["e_rad"], n_elec)
+                                     tal["e_rad"], n_elec, L_dep=R.get("L_radio_dep"), L_emit=R.get("L_radio_emit"))
         mine = open(p).read().splitlines()
         theirs = str(ref["plt_dat"]).splitlines()
         assert len(mine) == len(theirs)

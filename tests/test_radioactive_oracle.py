@@ -92,3 +92,37 @@ def test_decay_luminosity_follows_the_56ni_chain():
         assert np.allclose(R["L_radio_emit"][ni], expect, rtol=1e-12)
         assert np.all(R["L_radio_emit"][~ni] == 0)
         e.close()
+
+
+def test_set_emission_changes_the_next_step():
+    """sed_/oracle_set_emission: a context made without a radioactive source
+    can take one later (the gamma-ray spectrum is allocated then)."""
+    w = _small(n_radioactive=0)
+    e = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    e.set_opacity(1.0)
+    assert e.transport(1.0)["n_packets"] == 200
+    e.check(e.fn("set_emission")(e.ctx, 300.0, 500), "set_emission")
+    e.tp.n_emit_radioactive = 500
+    st = e.transport(1.0)
+    assert st["n_packets"] == 800
+    R = e.radioactive()
+    assert np.sum(R["L_radio_emit"]) > 0
+    with pytest.raises(RuntimeError, match=r"\(1\)"):
+        e.check(e.fn("set_emission")(e.ctx, -1.0, 0), "set_emission")
+    e.close()
+
+
+def test_emission_count_rules():
+    """Transport.emission_counts: dt scaling of the radioactive count
+    (truncated), then the last-iteration pump of both counts."""
+    from types import SimpleNamespace
+    from pubsed_b200.params import Params
+    from pubsed_b200.transport import Transport
+    P = Params({"core_n_emit": 1000, "multiply_particles_n_emit_by_dt_over_dtmax": 1, "tstep_max_dt": 3.0,
+                "particles_last_iter_pump": 10})
+    t = SimpleNamespace(P=P, n_radio=100)
+    assert Transport.emission_counts(t, 1.0, False) == (1000, 33)
+    assert Transport.emission_counts(t, 1.0, True) == (10000, 330)
+    P2 = Params({"core_n_emit": 1000, "particles_last_iter_pump": 0})
+    t2 = SimpleNamespace(P=P2, n_radio=100)
+    assert Transport.emission_counts(t2, 0.5, True) == (1000, 100)
