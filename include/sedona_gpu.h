@@ -241,8 +241,35 @@ int sed_record_packets(sed_ctx* ctx, int32_t enable);
 int sed_get_packet_records(sed_ctx* ctx, int64_t n, int32_t* fate, int32_t* ind,
                            int32_t* draws, double* state9);
 
-/* Number of packets carried to the next step (time-dependent runs). */
+/* Number of packets carried to the next step: transport::n_particles, the
+ * particle vector after clean_up_particle_vector (transport.cpp:91, 164-194).
+ * A time-dependent step keeps its stopped packets, in the reference's vector
+ * order, and propagates them first in the next step; a steady-state step
+ * keeps none. */
 int64_t sed_n_particles(sed_ctx* ctx);
+/* The carried packets: zone, type (enum PType: 0 photon, 1 gamma-ray) and
+ * {x, D, t, e, nu} of the first n (n <= sed_n_particles). */
+int sed_get_particles(sed_ctx* ctx, int64_t n, int32_t* ind, int32_t* type, double* state9);
+/* transport::wipe_spectra (src/transport/transport_output.cpp:63-67): empties
+ * the optical and gamma-ray spectra.  A steady-state step starts from empty
+ * spectra (the driver wipes them every iteration, SedonaClass.cpp:349); a
+ * time-dependent step adds to them. */
+int sed_wipe_spectra(sed_ctx* ctx);
+/* The transport clock (transport::t_now_): the first grid's t_now; a
+ * time-dependent step advances it by dt (transport.cpp:136) while the grid's
+ * time is the caller's (the hydro step moves it, hydro_homologous.cpp:27-45).
+ * Emission times, the end of the step, decay rates and the Sobolev time of
+ * the opacity build use it; velocities use the grid's time. */
+int sed_set_time(sed_ctx* ctx, double t_now);
+double sed_get_time(sed_ctx* ctx);
+/* transport::initialize_particles (src/transport/emission.cpp:112-159): n
+ * photons drawn in proportion to e_rad[zone] * vol (erg/cm^3, per zone), each
+ * with a blackbody spectrum at the zone's gas temperature, isotropic in the
+ * comoving frame, at the transport clock's time; they join the carried
+ * packets.  Packet k draws from Philox stream first_packet_id + (carried
+ * packets) + k at step number 0xFFFFFFFF.  SED_ERR_CAPACITY when n exceeds
+ * particles_max_total. */
+int sed_initialize_particles(sed_ctx* ctx, int64_t n, const double* e_rad);
 const char* sed_last_error(sed_ctx* ctx);
 void sed_ctx_destroy(sed_ctx* ctx);
 

@@ -46,6 +46,7 @@
 #define protected public
 #include "transport.h"
 #include "radioactive.h"
+#include "hydro_homologous.h"
 #include "grid_1D_sphere.h"
 #include "grid_3D_cart.h"
 #include "ParameterReader.h"
@@ -59,10 +60,12 @@ namespace {
 
 struct Out {
   std::string prefix;
+  std::string sfx;  // appended to array and scalar names (one set per replayed step)
   std::ostringstream meta;
   bool first = true;
-  void arr(const std::string& name, const void* p, size_t bytes, const char* ext, size_t count)
+  void arr(const std::string& name0, const void* p, size_t bytes, const char* ext, size_t count)
   {
+    const std::string name = name0 + sfx;
     std::string fn = prefix + "." + name + "." + ext;
     FILE* f = std::fopen(fn.c_str(), "wb");
     if (!f) { std::perror(fn.c_str()); std::exit(2); }
@@ -81,7 +84,7 @@ struct Out {
   {
     char buf[64];
     std::snprintf(buf, sizeof buf, "%.17g", v);
-    scalars << (sfirst ? "" : ", ") << "\"" << n << "\": " << buf;
+    scalars << (sfirst ? "" : ", ") << "\"" << n << sfx << "\": " << buf;
     sfirst = false;
   }
   void finish()
@@ -208,8 +211,9 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
   if (t.use_ddmc_) { std::fprintf(stderr, "replay: DDMC is not on the replayed path\n"); std::exit(3); }
   t.wipe_radiation();
 
+  // the packets the last step left (the census) keep the front of the
+  // vector; emission appends after them
   const size_t n_before = t.particles.size();
-  if (n_before != 0) { std::fprintf(stderr, "replay: expected an empty packet list\n"); std::exit(3); }
   const uint32_t K = core_draws_per_packet(t);
   const int64_t n_radio_req = t.params_->getScalar<int>("particles_n_emit_radioactive");
   RadioWalk walk;
@@ -227,9 +231,9 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
       walk.gfrac.push_back(gf);
     }
     walk.n_radio = n_radio_req;
-    oracle_rng_walk(seed, 0, step, 1, radio_walk_count, &walk);
+    oracle_rng_walk(seed, n_before, step, 1, radio_walk_count, &walk);
   } else {
-    oracle_rng_emission(seed, 0, step, K);
+    oracle_rng_emission(seed, n_before, step, K);
   }
   t.emit_particles(dt);
   const size_t n = t.particles.size();
@@ -243,35 +247,37 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
     radio_draws = 1;
     for (uint32_t c : walk.counts) radio_draws += c;
   }
-  const size_t n_core = n - walk.counts.size();
+  const size_t n_core = n - n_before - walk.counts.size();
+  const size_t n_q = n_before + walk.counts.size();  // census + radioactive: the queued packets
   if (oracle_rng_emission_draws() != radio_draws + (uint64_t)K * n_core) {
     std::fprintf(stderr, "replay: emission drew %llu deviates for %zu packets (expected %u each); only core emission is replayable\n",
                  (unsigned long long)oracle_rng_emission_draws(), n, K);
     std::exit(3);
   }
 
-  std::vector<int32_t> fate(n), ind(n), draws(n), spec_bin(n, -1);
+  std::vector<int32_t> fate(n), ind(n), draws(n), ptype(n), spec_bin(n, -1);
   std::vector<double> st((size_t)n * 9);
   const double T0 = now();
 #pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
   for (long i = 0; i < (long)n; ++i) {
     particle& p = t.particles[i];
-    // radioactive packets keep drawing from where their emission stopped
-    // and record all their deviates; core packets record the ones after
-    // emission.  Records list the core packets first.
-    const bool radio = i < (long)walk.counts.size();
-    const uint32_t n0 = radio ? walk.counts[i] : K;
+    // census packets draw this step's stream from its start; radioactive
+    // packets keep drawing from where their emission stopped; both record
+    // all their deviates, core packets the ones after emission.  Records
+    // list the core packets first, then the queued (census, radioactive) ones.
+    const bool queued = i < (long)n_q;
+    const uint32_t n0 = i < (long)n_before ? 0u : (queued ? walk.counts[i - n_before] : K);
     oracle_rng_packet(seed, (uint64_t)i, step, n0);
     p.fate = t.propagate(p, dt);
-    const long r = radio ? (long)n_core + i : i - (long)walk.counts.size();
-    draws[r] = (int32_t)(oracle_rng_packet_draws() - (radio ? 0 : K));
+    const long r = queued ? (long)n_core + i : i - (long)n_q;
+    draws[r] = (int32_t)(oracle_rng_packet_draws() - (queued ? 0 : K));
     if (p.fate == escaped) {
       double t_obs = p.t - p.x_dot_d() / pc::c;
       if (p.type == photon) t.optical_spectrum.count(t_obs, p.nu, p.e, p.D);
       if (p.type == gammaray) t.gamma_spectrum.count(t_obs, p.nu, p.e, p.D);
       p.t = t_obs;
     }
-    fate[r] = (int32_t)p.fate; ind[r] = p.ind;
+    fate[r] = (int32_t)p.fate; ind[r] = p.ind; ptype[r] = (int32_t)p.type;
     double* s = &st[(size_t)r * 9];
     s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2]; s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
     s[6] = p.t; s[7] = p.e; s[8] = p.nu;
@@ -293,7 +299,24 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
   // dump_tables then records the solved T_gas
   if (t.radiative_eq == 1 && t.fix_Tgas_during_transport_ == 0 && t.solve_Tgas_with_updated_opacities_ == 0)
     t.solve_eq_temperature();
+  // advance time step (transport.cpp:136) and record the packets carried on
+  if (!t.steady_state) t.t_now_ += dt;
+  if (!t.steady_state) {
+    const size_t nc = t.particles.size();
+    std::vector<int32_t> cind(nc), ctype(nc);
+    std::vector<double> cst(nc * 9);
+    for (size_t k = 0; k < nc; ++k) {
+      const particle& p = t.particles[k];
+      cind[k] = p.ind; ctype[k] = (int32_t)p.type;
+      double* s = &cst[k * 9];
+      s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2]; s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+      s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+    }
+    o.i32("census_ind", cind); o.i32("census_type", ctype); o.f64("census_state", cst);
+    o.scalar("n_census_before", (double)n_before);
+  }
   o.i32("pkt_fate", fate); o.i32("pkt_ind", ind); o.i32("pkt_draws", draws); o.f64("pkt_state", st);
+  if (!t.steady_state) o.i32("pkt_type", ptype);
   o.scalar("n_packets", (double)n); o.scalar("n_escaped", n_escaped); o.scalar("propagate_seconds", T1 - T0);
   o.scalar("draws_per_emitted_packet", K);
   if (n_radio_req > 0) {
@@ -347,9 +370,19 @@ int main(int argc, char** argv)
   grid->init(&params);
 
   transport t;
+  // initialize_particles (called by transport::init) draws 8 deviates per
+  // packet: packet k from stream k at step number 0xFFFFFFFF
+  const int n_init = params.getScalar<int>("particles_n_initialize");
+  if (n_init > 0) oracle_rng_emission(seed, 0, 0xFFFFFFFFu, 8);
   const double Ti0 = now();
   t.init(&params, grid);
   const double Ti1 = now();
+  if (n_init > 0 && oracle_rng_emission_draws() != 8ull * (uint64_t)t.particles.size()) {
+    std::fprintf(stderr, "replay: initialisation drew %llu deviates for %zu packets\n",
+                 (unsigned long long)oracle_rng_emission_draws(), t.particles.size());
+    return 3;
+  }
+  oracle_rng_free_running();
   o.scalar("init_seconds", Ti1 - Ti0);
   o.scalar("threads", threads);
 
@@ -362,7 +395,28 @@ int main(int argc, char** argv)
     o.scalar("set_opacity_seconds", T1 - T0);
     dump_tables(t, o);
   } else if (mode == "replay") {
-    replay_step(t, dt, seed, step, o, threads);
+    // time-dependent runs: the driver's homologous hydro step moves the grid
+    // to t + dt before each transport step (SedonaClass.cpp:346-358)
+    hydro_homologous hydro;
+    const bool use_hydro = !t.steady_state && params.getScalar<std::string>("hydro_module") == "homologous";
+    if (use_hydro) hydro.init(&params, grid);
+    if (n_init > 0) {
+      std::vector<int32_t> cind, ctype;
+      std::vector<double> cst;
+      for (const particle& p : t.particles) {
+        cind.push_back(p.ind); ctype.push_back((int32_t)p.type);
+        const double v[9] = {p.x[0], p.x[1], p.x[2], p.D[0], p.D[1], p.D[2], p.t, p.e, p.nu};
+        cst.insert(cst.end(), v, v + 9);
+      }
+      o.i32("init_ind", cind); o.i32("init_type", ctype); o.f64("init_state", cst);
+    }
+    for (int s = 0; s < steps; ++s) {
+      o.sfx = steps > 1 ? "_s" + std::to_string(s) : "";
+      if (use_hydro) hydro.step(dt);
+      replay_step(t, dt, seed, step + (uint32_t)s, o, threads);
+      if (steps > 1) dump_tables(t, o);
+    }
+    o.sfx = "";
     dump_tables(t, o);
     // the reference's own text outputs of this step: spectrum_array::print
     // (<prefix>_spectrum.dat) and, for 1D spheres, grid_1D_sphere::

@@ -163,14 +163,18 @@ def load_outputs(prefix: str) -> dict:
 
 
 def run(workload, mode: str, n_packets: Optional[int] = None, threads: Optional[int] = None,
-        seed: Optional[int] = None, steps: int = 1, timeout: float = 3600, keep_dir: Optional[str] = None) -> dict:
-    """mode: replay | free | opacity.  Returns the harness outputs."""
+        seed: Optional[int] = None, steps: int = 1, timeout: float = 3600, keep_dir: Optional[str] = None,
+        dt: Optional[float] = None) -> dict:
+    """mode: replay | free | opacity.  dt: the step of a time-dependent run.
+    Returns the harness outputs."""
     if not available():
         raise FileNotFoundError("reference harness not built: " + REF_BIN)
     d = keep_dir or tempfile.mkdtemp(prefix="sedref_")
     ppath, spath = render(workload, d, n_packets)
     prefix = os.path.join(d, "out")
     cmd = [REF_BIN, mode, ppath, prefix, "--store", spath, "--steps", str(steps)]
+    if dt is not None:
+        cmd += ["--dt", repr(float(dt))]
     if seed is not None:
         cmd += ["--seed", str(seed)]
     else:

@@ -93,6 +93,14 @@ struct oracle_ctx {
   int64_t nspec_g;
   double *gflux, *gclick;
   int64_t n_reject_cap;  /* Compton scatters that hit the rejection bound */
+  /* transport clock (transport::t_now_) and the packets carried to the next
+   * step, in the reference's vector order */
+  double t_now;
+  int have_t_now;
+  int64_t n_census;
+  double* c_state;
+  int32_t *c_ind, *c_type;
+  int32_t* r_type;
   double *L_emit, *L_dep, *radio_cdf, *gamma_frac, *compton, *photoion;
   /* differentiable transport: exact Jacobian of the last weighted forward,
    * accumulated forward-mode per packet ([nspec][nzones][bands]) */
@@ -261,6 +269,9 @@ int oracle_set_grid(oracle_ctx* o, const sed_grid* g)
   o->homologous = g->homologous;
   o->nelem = g->n_elems;
   o->t_grid = g->t_now;
+  /* transport::init takes the grid's time; a time-dependent run keeps its
+   * own clock afterwards */
+  if (!o->have_t_now || o->tp.steady_state) { o->t_now = g->t_now; o->have_t_now = 1; }
   size_t nz = (size_t)g->n_zones;
   if (g->type == SED_GRID_1D_SPHERE) {
     sed_locate_grid rg = {g->n_zones, SED_LOC_FLEX, g->r_min, 0.0, g->r_out};
@@ -778,7 +789,7 @@ int oracle_set_opacity(oracle_ctx* o, double dt)
   g.lev_n = (double*)calloc(nl ? nl : 1, sizeof(double));
   g.n_dens = (double*)calloc((size_t)(o->nelem > 0 ? o->nelem : 1), sizeof(double));
   g.mass_frac = (double*)calloc((size_t)(o->nelem > 0 ? o->nelem : 1), sizeof(double));
-  g.time = o->t_grid;
+  g.time = o->t_now;
   double* opac = (double*)calloc((size_t)nn, sizeof(double));
   double* aopac = (double*)calloc((size_t)nn, sizeof(double));
   double* emis = (double*)calloc((size_t)nn, sizeof(double));
@@ -1212,7 +1223,7 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
   if (!o || !o->have_grid) return SED_ERR_STATE;
   if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
   if (o->tp.steady_state) dt = 1;
-  double t_now = o->t_grid;
+  double t_now = o->t_now;
   int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
   if (n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
   if (first == 0) {
@@ -1567,68 +1578,130 @@ static int propagate_gamma(oracle_ctx* o, packet* p, double t_now, double dt, in
   return fate;
 }
 
-/* a radioactive packet's record: its end state and every deviate its
- * stream gave, emission included */
-static void record_radio(oracle_ctx* o, int64_t r, int fate, const packet* p)
+/* the record of a packet: fate, zone, deviates, end state and type */
+static void record_at(oracle_ctx* o, int64_t r, int fate, const packet* p, int32_t draws, int type)
 {
-  o->r_fate[r] = fate; o->r_ind[r] = p->ind; o->r_draws[r] = (int32_t)p->n;
+  o->r_fate[r] = fate; o->r_ind[r] = p->ind; o->r_draws[r] = draws; o->r_type[r] = type;
   double* sv = o->r_state + (size_t)r * 9;
   sv[0] = p->x[0]; sv[1] = p->x[1]; sv[2] = p->x[2]; sv[3] = p->D[0]; sv[4] = p->D[1]; sv[5] = p->D[2];
   sv[6] = p->t; sv[7] = p->e; sv[8] = p->nu;
 }
 
-/* a transport step with the radioactive source: radioactive packets first,
- * then the core packets; records hold the core packets, then the
- * radioactive ones (as gamma-rays, or as the optical photons they became) */
-static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
+#define T_PHOTON 0
+#define T_GAMMA 1
+
+/* transport::clean_up_particle_vector (transport.cpp:164-194), literally, on
+ * the step's packet vector (queued packets, then core packets; radioactive
+ * packets that were never emitted are not in it): the stopped packets that
+ * remain become the census */
+static void build_census(oracle_ctx* o, int64_t n_core, int64_t n_q)
+{
+  int64_t n_all = n_core + n_q, m = 0;
+  int64_t* v = (int64_t*)malloc((size_t)(n_all + 1) * sizeof(int64_t));
+  for (int64_t r = 0; r < n_all; ++r) {
+    int64_t slot = r < n_q ? n_core + r : r - n_q;
+    if (o->r_fate[slot] != -1) v[m++] = slot;
+  }
+#define DEAD(k) (o->r_fate[v[k]] == F_ESCAPED || o->r_fate[v[k]] == F_ABSORBED)
+  int64_t size = m, i = 0;
+  for (;;) {
+    while (size > 0 && DEAD(size - 1)) size--;
+    if (i >= size) break;
+    if (DEAD(i)) { v[i] = v[size - 1]; size--; }
+    i++;
+  }
+#undef DEAD
+  free(o->c_state); free(o->c_ind); free(o->c_type);
+  o->c_state = (double*)malloc((size_t)(size + 1) * 9 * sizeof(double));
+  o->c_ind = (int32_t*)malloc((size_t)(size + 1) * sizeof(int32_t));
+  o->c_type = (int32_t*)malloc((size_t)(size + 1) * sizeof(int32_t));
+  for (int64_t k = 0; k < size; ++k) {
+    memcpy(o->c_state + (size_t)k * 9, o->r_state + (size_t)v[k] * 9, 9 * sizeof(double));
+    o->c_ind[k] = o->r_ind[v[k]];
+    o->c_type[k] = o->r_type[v[k]];
+  }
+  o->n_census = size;
+  free(v);
+}
+
+/* transport::step with every source this restatement has (transport.cpp:
+ * 26-140): the census the last step left, then the radioactive packets,
+ * then the core packets, each on its own Philox stream (census and
+ * radioactive packets first).  Records list the core packets, then the
+ * queued ones (as gamma-rays, or as the optical photons they became). */
+int oracle_wipe_spectra(oracle_ctx* o);
+
+static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
 {
   if (o->tp.steady_state) dt = 1;
-  double t_now = o->t_grid;
+  int timedep = !o->tp.steady_state;
+  double t_now = o->t_now;
   int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
-  int64_t n_radio = o->tp.n_emit_radioactive;
-  if (n_radio > o->tp.max_particles) n_radio = 0;
-  if (n_emit + n_radio > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
-  int64_t n_all = n_emit + n_radio;
+  int64_t n_census = o->n_census;
+  int64_t n_radio = o->tp.n_emit_radioactive > 0 ? o->tp.n_emit_radioactive : 0;
+  if (n_census + n_radio > o->tp.max_particles) n_radio = 0;
+  if (n_census + n_radio + n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
+  int64_t n_q = n_census + n_radio, n_all = n_emit + n_q;
+  int census_gammas = 0;
+  for (int64_t k = 0; k < n_census; ++k) census_gammas += (o->c_type[k] == T_GAMMA);
+  int gamma_phase = n_radio > 0 || census_gammas > 0;
   int nz = o->nzones;
   wipe_tallies(o);
-  memset(o->flux, 0, (size_t)o->nspec * sizeof(double));
-  memset(o->click, 0, (size_t)o->nspec * sizeof(double));
-  memset(o->gflux, 0, (size_t)o->nspec_g * sizeof(double));
-  memset(o->gclick, 0, (size_t)o->nspec_g * sizeof(double));
-  double** zarr[6] = {&o->L_emit, &o->L_dep, &o->radio_cdf, &o->gamma_frac, &o->compton, &o->photoion};
-  for (int q = 0; q < 6; q++) { free(*zarr[q]); *zarr[q] = (double*)calloc((size_t)nz, sizeof(double)); }
-  double L_tot = radio_zones(o, t_now);
+  /* spectra accumulate over time-dependent steps; a steady-state iteration
+   * starts from empty ones (SedonaClass.cpp:349) */
+  if (gamma_phase) alloc_gamma_spectrum(o);
+  if (!timedep) oracle_wipe_spectra(o);
+  double L_tot = 0;
+  if (gamma_phase) {
+    double** zarr[6] = {&o->L_emit, &o->L_dep, &o->radio_cdf, &o->gamma_frac, &o->compton, &o->photoion};
+    for (int q = 0; q < 6; q++) { free(*zarr[q]); *zarr[q] = (double*)calloc((size_t)nz, sizeof(double)); }
+    L_tot = radio_zones(o, t_now);
+    /* emit_radioactive sets L_radio_emit only when it emits */
+    if (n_radio == 0) memset(o->L_emit, 0, (size_t)nz * sizeof(double));
+  }
   o->n_reject_cap = 0;
   double Ep_r = L_tot * dt / (1.0 * n_radio);
-  if (o->record) {
-    free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state);
+  if (o->record || timedep) {
+    free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state); free(o->r_type);
     o->nrec = n_all;
     o->r_fate = (int32_t*)calloc((size_t)n_all + 1, 4);
     o->r_ind = (int32_t*)calloc((size_t)n_all + 1, 4);
     o->r_draws = (int32_t*)calloc((size_t)n_all + 1, 4);
+    o->r_type = (int32_t*)calloc((size_t)n_all + 1, 4);
     o->r_state = (double*)calloc((size_t)n_all * 9 + 1, 8);
     for (int64_t k = n_emit; k < n_all; ++k) o->r_fate[k] = -1;  /* stays when nothing is emitted */
   }
+  int keep = o->record || timedep;
   int64_t nseg = 0, nscat = 0, nesc = 0, nabs = 0, nstop = 0;
-  for (int64_t k = 0; k < n_radio && L_tot != 0; ++k) {
+  for (int64_t k = 0; k < n_q; ++k) {
     packet p;
     memset(&p, 0, sizeof p);
     p.pid = (uint64_t)(o->tp.first_packet_id + k);
     p.n = 0;
-    int i = cdf_sample(o->radio_cdf, nz, draw(o, &p));
-    double t = t_now + dt * draw(o, &p);
-    int is_gamma = draw(o, &p) < o->gamma_frac[i];
-    if (!is_gamma) o->L_dep[i] += Ep_r;
-    double u0 = draw(o, &p), u1 = draw(o, &p), u2 = draw(o, &p);
-    sample_in_zone(o, i, u0, u1, u2, p.x);
-    iso_dir(o, &p, p.D);
-    p.ind = i;
-    if (is_gamma) p.nu = 1;
-    else sample_optical_nu(o, &p);
-    p.e = Ep_r;
-    lorentz(o, &p, 1);
-    p.t = t;
-    int fate, relocate = 1;
+    int is_gamma, relocate = 1;
+    if (k < n_census) {
+      const double* c = o->c_state + (size_t)k * 9;
+      p.x[0] = c[0]; p.x[1] = c[1]; p.x[2] = c[2]; p.D[0] = c[3]; p.D[1] = c[4]; p.D[2] = c[5];
+      p.t = c[6]; p.e = c[7]; p.nu = c[8];
+      p.ind = o->c_ind[k];
+      is_gamma = (o->c_type[k] == T_GAMMA);
+    } else {
+      if (L_tot == 0) continue;
+      int i = cdf_sample(o->radio_cdf, nz, draw(o, &p));
+      double t = t_now + dt * draw(o, &p);
+      is_gamma = draw(o, &p) < o->gamma_frac[i];
+      if (!is_gamma) o->L_dep[i] += Ep_r;
+      double u0 = draw(o, &p), u1 = draw(o, &p), u2 = draw(o, &p);
+      sample_in_zone(o, i, u0, u1, u2, p.x);
+      iso_dir(o, &p, p.D);
+      p.ind = i;
+      if (is_gamma) p.nu = 1;
+      else sample_optical_nu(o, &p);
+      p.e = Ep_r;
+      lorentz(o, &p, 1);
+      p.t = t;
+    }
+    int fate;
     if (is_gamma) {
       int photon = 0;
       fate = propagate_gamma(o, &p, t_now, dt, &photon, &nseg, &nscat);
@@ -1640,7 +1713,7 @@ static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
           nesc++;
         } else if (fate == F_ABSORBED) nabs++;
         else nstop++;
-        if (o->record) record_radio(o, n_emit + k, fate, &p);
+        if (keep) record_at(o, n_emit + k, fate, &p, (int32_t)p.n, T_GAMMA);
         continue;
       }
       relocate = 0;
@@ -1653,14 +1726,14 @@ static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
       nesc++;
     } else if (fate == F_ABSORBED) nabs++;
     else nstop++;
-    if (o->record) record_radio(o, n_emit + k, fate, &p);
+    if (keep) record_at(o, n_emit + k, fate, &p, (int32_t)p.n, T_PHOTON);
   }
   double Ep = o->tp.core_luminosity * dt / n_emit;
   uint32_t K = draws_per_emission(o);
   for (int64_t j = 0; j < n_emit; ++j) {
     packet p;
     memset(&p, 0, sizeof p);
-    p.pid = (uint64_t)(o->tp.first_packet_id + n_radio + j);
+    p.pid = (uint64_t)(o->tp.first_packet_id + n_q + j);
     p.n = 0;
     emit_core_packet(o, &p, Ep, t_now, dt);
     p.n = K;
@@ -1672,25 +1745,122 @@ static int transport_radio(oracle_ctx* o, double dt, sed_step_stats* st)
       nesc++;
     } else if (fate == F_ABSORBED) nabs++;
     else nstop++;
-    if (o->record) {
-      o->r_fate[j] = fate; o->r_ind[j] = p.ind; o->r_draws[j] = (int32_t)(p.n - K);
-      double* sv = o->r_state + (size_t)j * 9;
-      sv[0] = p.x[0]; sv[1] = p.x[1]; sv[2] = p.x[2]; sv[3] = p.D[0]; sv[4] = p.D[1]; sv[5] = p.D[2];
-      sv[6] = p.t; sv[7] = p.e; sv[8] = p.nu;
-    }
+    if (keep) record_at(o, j, fate, &p, (int32_t)(p.n - K), T_PHOTON);
   }
   finish_step(o, dt, n_all, nesc);
-  for (int i = 0; i < nz; i++) {  /* transport_mpi.cpp:419-420 */
-    o->L_dep[i] /= o->vol[i] * dt;
-    o->L_emit[i] /= o->vol[i];
-  }
+  if (gamma_phase)
+    for (int i = 0; i < nz; i++) {  /* transport_mpi.cpp:419-420 */
+      o->L_dep[i] /= o->vol[i] * dt;
+      o->L_emit[i] /= o->vol[i];
+    }
+  if (timedep) build_census(o, n_emit, n_q);
+  else o->n_census = 0;
   o->step++;
+  if (timedep) o->t_now += dt;
   if (st) {
     memset(st, 0, sizeof *st);
     st->n_packets = n_all; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
     st->n_segments = nseg; st->n_scatters = nscat;
   }
   if (o->n_reject_cap > 0) return fail(o, SED_ERR_LIMIT, "Compton scatters hit the rejection-sampling bound");
+  return SED_OK;
+}
+
+int64_t oracle_n_particles(oracle_ctx* o) { return o ? o->n_census : 0; }
+
+int oracle_wipe_spectra(oracle_ctx* o)  /* transport::wipe_spectra (transport_output.cpp:63-67) */
+{
+  if (!o) return SED_ERR_ARG;
+  memset(o->flux, 0, (size_t)o->nspec * sizeof(double));
+  memset(o->click, 0, (size_t)o->nspec * sizeof(double));
+  if (o->gflux) {
+    memset(o->gflux, 0, (size_t)o->nspec_g * sizeof(double));
+    memset(o->gclick, 0, (size_t)o->nspec_g * sizeof(double));
+  }
+  return SED_OK;
+}
+
+int oracle_get_particles(oracle_ctx* o, int64_t n, int32_t* ind, int32_t* type, double* state9)
+{
+  if (!o) return SED_ERR_ARG;
+  if (n < 0 || n > o->n_census) return fail(o, SED_ERR_ARG, "more packets than carried");
+  if (n == 0) return SED_OK;
+  if (ind) memcpy(ind, o->c_ind, (size_t)n * 4);
+  if (type) memcpy(type, o->c_type, (size_t)n * 4);
+  if (state9) memcpy(state9, o->c_state, (size_t)n * 72);
+  return SED_OK;
+}
+
+int oracle_set_time(oracle_ctx* o, double t_now)
+{
+  if (!o) return SED_ERR_ARG;
+  o->t_now = t_now;
+  o->have_t_now = 1;
+  return SED_OK;
+}
+
+double oracle_get_time(oracle_ctx* o) { return o ? o->t_now : 0.0; }
+
+static double blackbody_nu(double T, double nu);
+
+/* transport::initialize_particles (emission.cpp:112-159): zone from e_rad *
+ * vol, then create_isotropic_particle with a blackbody emissivity at the
+ * gas temperature, at the transport clock's time.  The deviates of packet k
+ * come from stream first_packet_id + (carried packets) + k at step number
+ * 0xFFFFFFFF. */
+int oracle_initialize_particles(oracle_ctx* o, int64_t n, const double* e_rad)
+{
+  if (!o) return SED_ERR_ARG;
+  if (!o->have_grid) return SED_ERR_STATE;
+  if (n < 0 || (n > 0 && !e_rad)) return fail(o, SED_ERR_ARG, "bad arguments");
+  if (n == 0) return SED_OK;
+  if (n > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space to initialize");
+  int nz = o->nzones, ng = o->nu.n;
+  double* zc = (double*)malloc((size_t)nz * sizeof(double));
+  double* bb = (double*)malloc((size_t)nz * ng * sizeof(double));
+  double E_sum = 0;
+  for (int i = 0; i < nz; ++i) {
+    double E_zone = e_rad[i] * o->vol[i];
+    zc[i] = (i == 0) ? E_zone : zc[i - 1] + E_zone;
+    E_sum += E_zone;
+    double* row = bb + (size_t)i * ng;
+    for (int j = 0; j < ng; ++j) {
+      double emis = blackbody_nu(o->T[i], lg_center(&o->nu, j)) * lg_delta(&o->nu, j);
+      row[j] = (j == 0) ? emis : row[j - 1] + emis;
+    }
+    cdf_normalize(row, ng);
+  }
+  cdf_normalize(zc, nz);
+  int64_t off = o->n_census;
+  o->c_state = (double*)realloc(o->c_state, (size_t)(off + n) * 9 * sizeof(double));
+  o->c_ind = (int32_t*)realloc(o->c_ind, (size_t)(off + n) * sizeof(int32_t));
+  o->c_type = (int32_t*)realloc(o->c_type, (size_t)(off + n) * sizeof(int32_t));
+  double Ep = E_sum / (1.0 * n);
+  uint32_t saved = o->step;
+  o->step = 0xFFFFFFFFu;
+  for (int64_t k = 0; k < n; ++k) {
+    packet p;
+    memset(&p, 0, sizeof p);
+    p.pid = (uint64_t)(o->tp.first_packet_id + off + k);
+    int i = cdf_sample(zc, nz, draw(o, &p));
+    p.ind = i;
+    double u0 = draw(o, &p), u1 = draw(o, &p), u2 = draw(o, &p);
+    sample_in_zone(o, i, u0, u1, u2, p.x);
+    iso_dir(o, &p, p.D);
+    int inu = cdf_sample(bb + (size_t)i * ng, ng, draw(o, &p));
+    p.nu = lg_sample(&o->nu, inu, draw(o, &p));
+    p.e = Ep;
+    lorentz(o, &p, 1);
+    p.t = o->t_now;
+    double* c = o->c_state + (size_t)(off + k) * 9;
+    c[0] = p.x[0]; c[1] = p.x[1]; c[2] = p.x[2]; c[3] = p.D[0]; c[4] = p.D[1]; c[5] = p.D[2];
+    c[6] = p.t; c[7] = p.e; c[8] = p.nu;
+    o->c_ind[off + k] = i;
+    o->c_type[off + k] = T_PHOTON;
+  }
+  o->step = saved;
+  o->n_census = off + n;
+  free(zc); free(bb);
   return SED_OK;
 }
 
@@ -1713,10 +1883,10 @@ int oracle_get_radioactive_tallies(oracle_ctx* o, double* L_emit, double* L_dep)
 int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
 {
   if (!o) return SED_ERR_ARG;
-  if (o->tp.n_emit_radioactive > 0) {
+  if (o->tp.n_emit_radioactive > 0 || o->n_census > 0 || !o->tp.steady_state) {
     if (!o->have_grid) return SED_ERR_STATE;
     if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
-    return transport_radio(o, dt, st);
+    return transport_general(o, dt, st);
   }
   return oracle_transport_range(o, dt, 0, (int64_t)(o->tp.core_n_emit / 1.0), 1, st);
 }
@@ -1850,7 +2020,7 @@ int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32
     return fail(o, SED_ERR_ARG, "differentiable transport: unsupported configuration");
   if (n_bands < 1 || n_bands > o->nu.n) return fail(o, SED_ERR_ARG, "bad band count");
   if (o->tp.steady_state) dt = 1;
-  double t_now = o->t_grid;
+  double t_now = o->t_now;
   int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
   if (n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
   wipe_tallies(o);
@@ -2104,5 +2274,6 @@ void oracle_ctx_destroy(oracle_ctx* o)
   free(o->jac);
   free(o->gflux); free(o->gclick); free(o->L_emit); free(o->L_dep); free(o->radio_cdf); free(o->gamma_frac);
   free(o->compton); free(o->photoion); free(o->gn.x);
+  free(o->c_state); free(o->c_ind); free(o->c_type); free(o->r_type);
   free(o);
 }

@@ -47,6 +47,14 @@ int oracle_set_rng_step(oracle_ctx* o, uint32_t step);
 int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* stats);
 int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
 int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
+/* packets carried between time-dependent steps, the transport clock, and
+ * the initial radiation field's packets */
+int64_t oracle_n_particles(oracle_ctx* o);
+int oracle_wipe_spectra(oracle_ctx* o);
+int oracle_get_particles(oracle_ctx* o, int64_t n, int32_t* ind, int32_t* type, double* state9);
+int oracle_set_time(oracle_ctx* o, double t_now);
+double oracle_get_time(oracle_ctx* o);
+int oracle_initialize_particles(oracle_ctx* o, int64_t n, const double* e_rad);
 /* packet counts of the next steps */
 int oracle_set_emission(oracle_ctx* o, double core_n_emit, int64_t n_emit_radioactive);
 /* radioactive source results of the last step */

@@ -167,7 +167,6 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
     }
     if prefix == "sed_":
         sig["step"] = ([vp, C.c_double, C.POINTER(StepStats)], C.c_int)
-        sig["n_particles"] = ([vp], C.c_int64)
         sig["version"] = ([], C.c_char_p)
     else:
         sig["ctx_create"] = ([C.POINTER(TransportParams), C.POINTER(vp)], C.c_int)
@@ -183,6 +182,12 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         "get_gamma_spectrum": ([vp, _dp, _dp], C.c_int),
         "get_radioactive_tallies": ([vp, _dp, _dp], C.c_int),
         "set_emission": ([vp, C.c_double, C.c_int64], C.c_int),
+        "get_particles": ([vp, C.c_int64, _ip, _ip, _dp], C.c_int),
+        "set_time": ([vp, C.c_double], C.c_int),
+        "get_time": ([vp], C.c_double),
+        "initialize_particles": ([vp, C.c_int64, _dp], C.c_int),
+        "n_particles": ([vp], C.c_int64),
+        "wipe_spectra": ([vp], C.c_int),
     })
     if prefix == "sed_":
         i64p = C.POINTER(C.c_int64)

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include <cub/cub.cuh>
 #include "sed_ctx.h"
 
 using namespace sed;
@@ -116,7 +117,7 @@ StepArgs sed::make_step_args(sed_ctx* c, double dt, int64_t n_emit)
   A.n_packets = n_emit;
   A.first_pid = c->tp.first_packet_id;
   A.Ep = n_emit > 0 ? c->tp.core_luminosity * dt / n_emit : 0.0;
-  A.t_now = c->t_grid; A.dt = dt; A.tstop = c->t_grid + dt;
+  A.t_now = c->t_now; A.dt = dt; A.tstop = c->t_now + dt;
   if (c->t_grid > 0) {
     A.inv_t = 1.0 / c->t_grid;
     A.ct = C_LIGHT * c->t_grid;
@@ -263,6 +264,10 @@ int sed_set_grid(sed_ctx* c, const sed_grid* g)
   c->nelem = g->n_elems;
   c->homologous = g->homologous;
   c->t_grid = g->t_now;
+  // transport::init takes the grid's time (transport_init.cpp:371); a
+  // time-dependent run then keeps its own clock, a steady-state run never
+  // advances either
+  if (!c->have_t_now || c->tp.steady_state) { c->t_now = g->t_now; c->have_t_now = true; }
   const size_t nz = (size_t)g->n_zones;
   if (g->type == SED_GRID_1D_SPHERE) {
     if (!g->r_out) return set_err(c, SED_ERR_ARG, "sed_set_grid: 1D sphere needs r_out");
@@ -465,7 +470,7 @@ int sed::enqueue_opacity(sed_ctx* c, double dt)
   A.use_line = c->op.use_line_expansion; A.use_fuzz = c->op.use_fuzz_expansion;
   A.radiative_eq = c->tp.radiative_eq; A.omit_scat = c->tp.omit_scattering; A.precision = c->tp.precision;
   A.epsilon = c->op.epsilon; A.max_opacity = c->op.maximum_opacity; A.temp_min = c->op.temp_min;
-  A.temp_max = c->op.temp_max; A.fleck_alpha = c->tp.fleck_alpha; A.dt = dt; A.time = c->t_grid;
+  A.temp_max = c->op.temp_max; A.fleck_alpha = c->tp.fleck_alpha; A.dt = dt; A.time = c->t_now;
   A.nu = dev_loc(c->nu, c->d_nu);
   A.rho = c->d_rho.p; A.T = c->d_T.p; A.e_gas = c->d_egas.p; A.grey = c->d_grey.p; A.X = c->d_X.p;
   A.eZ = c->d_eZ.p; A.eA = c->d_eA.p; A.zero_eps_atom = c->d_zero_eps_atom.p;
@@ -597,46 +602,103 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
   return SED_OK;
 }
 
+// The stopped packets of the step, in the reference's vector order, become
+// the census (clean_up_particle_vector, transport.cpp:164-194).
+static int build_census(sed_ctx* c, CensusArgs& C, int64_t n_all, int64_t* n_alive)
+{
+  const size_t m = (size_t)n_all + 1;
+  CK(c->d_cmp.resize(5 * m));
+  C.flag_e = c->d_cmp.p; C.flag_a = C.flag_e + m; C.scan_e = C.flag_a + m; C.scan_a = C.scan_e + m;
+  C.front_dead = C.scan_a + m;
+  CK(c->d_cmp_count.resize(1));
+  C.n_gamma = c->d_cmp_count.p;
+  CK(cudaMemsetAsync(C.n_gamma, 0, sizeof(unsigned long long), c->stream));
+  CK(c->d_census_state.resize(std::max<size_t>(m - 1, 1) * 9));
+  CK(c->d_census_ind.resize(std::max<size_t>(m - 1, 1)));
+  CK(c->d_census_type.resize(std::max<size_t>(m - 1, 1)));
+  C.census_state = c->d_census_state.p; C.census_ind = c->d_census_ind.p; C.census_type = c->d_census_type.p;
+  launch_census_flags(C, n_all, c->stream);
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, C.flag_e, C.scan_e, (int)m, c->stream));
+  CK(c->d_scan_tmp.resize(std::max<size_t>(tmp, 1)));
+  CK(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp, C.flag_e, C.scan_e, (int)m, c->stream));
+  CK(cub::DeviceScan::ExclusiveSum(c->d_scan_tmp.p, tmp, C.flag_a, C.scan_a, (int)m, c->stream));
+  launch_census_compact(C, n_all, c->stream);
+  CK(cudaGetLastError());
+  int32_t na = 0;
+  unsigned long long ng = 0;
+  CK(cudaMemcpyAsync(&na, C.scan_a + n_all, sizeof na, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&ng, C.n_gamma, sizeof ng, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *n_alive = na;
+  c->n_census_gamma = (int64_t)ng;
+  return SED_OK;
+}
+
 static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms_opacity)
 {
   if (!c) return SED_ERR_ARG;
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_transport: no grid");
   if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "sed_transport: opacity tables not set");
   if (c->tp.steady_state) dt = 1;
+  const bool timedep = !c->tp.steady_state;
   // emit_inner_source packet count and energy (src/transport/emission.cpp:383-392)
   const int64_t n_emit = (int64_t)(c->tp.core_n_emit / 1.0);
-  // emit_radioactive runs first (emission.cpp:163-186, one rank): it adds
-  // nothing when its packets would not fit; the core packets then must fit
-  // next to them
+  // The packet list of the step (transport.cpp:46-54): the census the last
+  // step left, then emit_radioactive (emission.cpp:163-243: it adds nothing
+  // when its packets would not fit next to the census), then the core
+  // packets, which must fit next to both.  Census and radioactive packets
+  // are the queue; their Philox streams come first, the core packets' after.
+  const int64_t n_census = c->n_census;
   int64_t n_radio = c->tp.n_emit_radioactive > 0 ? c->tp.n_emit_radioactive : 0;
-  if (n_radio > c->tp.max_particles) n_radio = 0;
-  if (n_emit + n_radio > c->tp.max_particles)
+  if (n_census + n_radio > c->tp.max_particles) n_radio = 0;
+  if (n_census + n_radio + n_emit > c->tp.max_particles)
     return set_err(c, SED_ERR_CAPACITY, "Not enough particle space: %lld packets > particles_max_total %lld",
-                   (long long)(n_emit + n_radio), (long long)c->tp.max_particles);
-  const int64_t n_all = n_emit + n_radio;
+                   (long long)(n_census + n_radio + n_emit), (long long)c->tp.max_particles);
+  const int64_t n_q = n_census + n_radio;
+  const int64_t n_all = n_emit + n_q;
+  const bool gamma_phase = n_radio > 0 || (n_census > 0 && c->n_census_gamma > 0);
+  const bool keep = c->record || timedep;  // end states: records, and the next census
   const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
   const size_t nj = c->tp.store_Jnu ? nn : 1;
-  if (c->record) {
+  if (keep) {
     CK(c->d_rec_fate.resize(std::max<int64_t>(n_all, 1)));
     CK(c->d_rec_ind.resize(std::max<int64_t>(n_all, 1)));
     CK(c->d_rec_draws.resize(std::max<int64_t>(n_all, 1)));
+    CK(c->d_rec_type.resize(std::max<int64_t>(n_all, 1)));
     CK(c->d_rec_state.resize(std::max<int64_t>(n_all, 1) * 9));
-    c->n_rec = n_all;
   }
-  if (c->tp.n_emit_radioactive > 0) {
+  if (c->record) c->n_rec = n_all;
+  if (n_q > 0) {
+    CK(c->d_q_state.resize((size_t)n_q * 9));
+    CK(c->d_q_ind.resize((size_t)n_q));
+    CK(c->d_q_n.resize((size_t)n_q));
+    CK(c->d_q_type.resize((size_t)n_q));
+  }
+  if (gamma_phase) {
+    if (c->nspec_g == 0) {
+      const int rc = alloc_gamma_spectrum(c);
+      if (rc) return rc;
+    }
     CK(c->d_radio_cdf.resize(nz)); CK(c->d_gamma_frac.resize(nz)); CK(c->d_compton.resize(nz));
     CK(c->d_photoion.resize(nz)); CK(c->d_L_emit.resize(nz)); CK(c->d_L_dep.resize(nz));
-    CK(c->d_q_state.resize((size_t)std::max<int64_t>(n_radio, 1) * 9));
-    CK(c->d_q_ind.resize((size_t)std::max<int64_t>(n_radio, 1)));
-    CK(c->d_q_n.resize((size_t)std::max<int64_t>(n_radio, 1)));
   }
   CK(cudaEventRecord(c->ev[2], c->stream));
-  if (c->tp.n_emit_radioactive > 0) {
+  if (gamma_phase) {
     CK(cudaMemsetAsync(c->d_L_dep.p, 0, nz * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_L_emit.p, 0, nz * sizeof(double), c->stream));
-    CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
-    CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
     CK(cudaMemsetAsync(c->d_reject.p, 0, sizeof(int32_t), c->stream));
+  }
+  // spectra: a steady-state iteration starts from empty ones (the driver's
+  // wipe_spectra, SedonaClass.cpp:349); a time-dependent run accumulates
+  // them over its steps
+  if (!timedep) {
+    CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
+    if (c->nspec_g > 0) {
+      CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
+      CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
+    }
   }
   // wipe_radiation (src/transport/transport_mpi.cpp:18-34) and the spectrum
   CK(cudaMemsetAsync(c->d_J.p, 0, nz * nj * sizeof(double), c->stream));
@@ -646,26 +708,34 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   CK(cudaMemsetAsync(c->d_fy.p, 0, nz * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_fz.p, 0, nz * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_fr.p, 0, nz * sizeof(double), c->stream));
-  CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
-  CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
   CK(cudaMemsetAsync(c->d_counters.p, 0, (C_COUNT + 1) * sizeof(unsigned long long), c->stream));
 
   StepArgs A = make_step_args(c, dt, n_emit);
-  if (c->record) {
-    A.rec_fate = c->d_rec_fate.p; A.rec_ind = c->d_rec_ind.p; A.rec_draws = c->d_rec_draws.p; A.rec_state = c->d_rec_state.p;
+  if (keep) {
+    A.rec_fate = c->d_rec_fate.p; A.rec_ind = c->d_rec_ind.p; A.rec_draws = c->d_rec_draws.p;
+    A.rec_state = c->d_rec_state.p; A.rec_type = c->d_rec_type.p;
   }
+  A.n_core = n_emit;
   const GridDev G = make_grid_dev(c);
   int launches = 0;
-  if (c->tp.n_emit_radioactive > 0) {
-    // decay luminosity and gamma-ray opacity per zone, then the radioactive
-    // packets (emitted before the core packets, so they take the first
-    // stream ids); their optical photons join the packet kernel's queue.
-    // Packet records: the core packets, then the radioactive ones.
-    A.n_core = n_emit;
+  CensusArgs C{};
+  C.n_census = n_census; C.n_core = n_emit; C.n_q = n_q;
+  if (n_q > 0) {
+    C.q_state = c->d_q_state.p; C.q_ind = c->d_q_ind.p; C.q_type = c->d_q_type.p; C.q_n = c->d_q_n.p;
+  }
+  if (n_census > 0) {
+    C.census_state = c->d_census_state.p; C.census_ind = c->d_census_ind.p; C.census_type = c->d_census_type.p;
+    launches += launch_census_load(C, G, c->stream);
+  }
+  if (gamma_phase) {
+    // decay luminosity and gamma-ray opacity per zone, then the census
+    // gamma-rays and the radioactive packets; the optical photons they
+    // become join the packet kernel's queue
     RadioArgs R{};
     R.nz = c->nz; R.n_elems = c->nelem; R.force_rproc = c->tp.force_rprocess_heating;
-    R.n_radio = n_radio; R.first_pid = c->tp.first_packet_id;
-    R.t_now = c->t_grid; R.dt = dt;
+    R.n_census = n_census; R.n_radio = n_radio; R.first_pid = c->tp.first_packet_id;
+    R.q_type = c->d_q_type.p;
+    R.t_now = c->t_now; R.dt = dt;
     R.rho = c->d_rho.p; R.vol = c->d_vol.p; R.X = c->d_X.p; R.eZ = c->d_eZ.p; R.eA = c->d_eA.p;
     R.L_emit = c->d_L_emit.p; R.gamma_frac = c->d_gamma_frac.p; R.compton = c->d_compton.p;
     R.photoion = c->d_photoion.p; R.cdf = c->d_radio_cdf.p; R.L_tot = c->d_L_tot.p; R.L_dep = c->d_L_dep.p;
@@ -675,13 +745,17 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     AG.a3 = c->sp.n(); AG.a2 = (int64_t)c->sm.n() * AG.a3; AG.a1 = (int64_t)c->gn.n() * AG.a2;
     AG.flux = c->d_gflux.p; AG.click = c->d_gclick.p;
     launches += launch_radio_zones(R, c->stream);
+    // emit_radioactive sets L_radio_emit only when it emits (emission.cpp:176, 205)
+    if (n_radio == 0) CK(cudaMemsetAsync(c->d_L_emit.p, 0, nz * sizeof(double), c->stream));
     launches += launch_gamma(A, AG, R, G, c->num_sms, c->stream);
     CK(cudaGetLastError());
+    A.L_dep = c->d_L_dep.p; A.L_emit = c->d_L_emit.p;
+  }
+  if (n_q > 0) {
     A.n_packets = n_all;
-    A.first_pid = c->tp.first_packet_id + n_radio;
+    A.first_pid = c->tp.first_packet_id + n_q;
     A.radio_first_pid = c->tp.first_packet_id;
     A.q_state = c->d_q_state.p; A.q_ind = c->d_q_ind.p; A.q_n = c->d_q_n.p;
-    A.L_dep = c->d_L_dep.p; A.L_emit = c->d_L_emit.p;
   }
   CK(cudaEventRecord(c->ev[3], c->stream));
   if (A.n_packets > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
@@ -693,10 +767,23 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   unsigned long long cnt[C_COUNT + 1];
   CK(cudaMemcpyAsync(cnt, c->d_counters.p, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
   int32_t n_reject_cap = 0;
-  if (c->tp.n_emit_radioactive > 0)
+  if (gamma_phase)
     CK(cudaMemcpyAsync(&n_reject_cap, c->d_reject.p, sizeof n_reject_cap, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  // the stopped packets stay for the next step; a steady-state step leaves
+  // none (its packets never reach the end of the step)
+  int64_t n_next = 0;
+  if (timedep && n_all > 0) {
+    C.rec_fate = c->d_rec_fate.p; C.rec_ind = c->d_rec_ind.p; C.rec_type = c->d_rec_type.p;
+    C.rec_state = c->d_rec_state.p;
+    const int rc = build_census(c, C, n_all, &n_next);
+    if (rc) return rc;
+    launches += 4;
+  }
+  c->n_census = n_next;
+  if (n_next == 0) c->n_census_gamma = 0;
   c->step++;
+  if (timedep) c->t_now += dt;
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
     stats->n_packets = n_all;
@@ -874,7 +961,82 @@ int sed_get_packet_records(sed_ctx* c, int64_t n, int32_t* fate, int32_t* ind, i
   return SED_OK;
 }
 
-int64_t sed_n_particles(sed_ctx* c) { (void)c; return 0; }
+int64_t sed_n_particles(sed_ctx* c) { return c ? c->n_census : 0; }
+
+int sed_wipe_spectra(sed_ctx* c)
+{
+  if (!c) return SED_ERR_ARG;
+  CK(cudaMemsetAsync(c->d_flux.p, 0, c->nspec * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_click.p, 0, c->nspec * sizeof(double), c->stream));
+  if (c->nspec_g > 0) {
+    CK(cudaMemsetAsync(c->d_gflux.p, 0, c->nspec_g * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->d_gclick.p, 0, c->nspec_g * sizeof(double), c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_set_time(sed_ctx* c, double t_now)
+{
+  if (!c) return SED_ERR_ARG;
+  c->t_now = t_now;
+  c->have_t_now = true;
+  return SED_OK;
+}
+
+double sed_get_time(sed_ctx* c) { return c ? c->t_now : 0.0; }
+
+int sed_get_particles(sed_ctx* c, int64_t n, int32_t* ind, int32_t* type, double* state9)
+{
+  if (!c) return SED_ERR_ARG;
+  if (n < 0 || n > c->n_census) return set_err(c, SED_ERR_ARG, "sed_get_particles: %lld of %lld packets",
+                                               (long long)n, (long long)c->n_census);
+  if (n == 0) return SED_OK;
+  if (ind) CK(cudaMemcpyAsync(ind, c->d_census_ind.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (type) CK(cudaMemcpyAsync(type, c->d_census_type.p, n * 4, cudaMemcpyDeviceToHost, c->stream));
+  if (state9) CK(cudaMemcpyAsync(state9, c->d_census_state.p, n * 72, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_initialize_particles(sed_ctx* c, int64_t n, const double* e_rad)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_initialize_particles: no grid");
+  if (n < 0 || (n > 0 && !e_rad)) return set_err(c, SED_ERR_ARG, "sed_initialize_particles: bad arguments");
+  if (n == 0) return SED_OK;
+  // emission.cpp:122-125: the packets must fit on their own
+  if (n > c->tp.max_particles)
+    return set_err(c, SED_ERR_CAPACITY, "Not enough particle space to initialize %lld packets", (long long)n);
+  const int64_t off = c->n_census;
+  const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
+  // the census grows to off + n packets; what it held is kept
+  DevBuf<double> st;
+  DevBuf<int32_t> ind, typ;
+  CK(st.resize((size_t)(off + n) * 9)); CK(ind.resize((size_t)(off + n))); CK(typ.resize((size_t)(off + n)));
+  if (off > 0) {
+    CK(cudaMemcpyAsync(st.p, c->d_census_state.p, (size_t)off * 72, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(ind.p, c->d_census_ind.p, (size_t)off * 4, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(typ.p, c->d_census_type.p, (size_t)off * 4, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  DevBuf<double> erad, zcdf, esum, bb;
+  CK(upload(c, erad, e_rad, nz));
+  CK(zcdf.resize(nz)); CK(esum.resize(1)); CK(bb.resize(nz * nn));
+  InitArgs I{};
+  I.n = n; I.census_off = off; I.seed = c->tp.rng_seed; I.first_pid = c->tp.first_packet_id + off;
+  I.t_now = c->t_now; I.nz = c->nz;
+  I.e_rad = erad.p; I.vol = c->d_vol.p; I.T = c->d_T.p;
+  I.zone_cdf = zcdf.p; I.E_sum = esum.p; I.bb_cdf = bb.p;
+  I.nu = dev_loc(c->nu, c->d_nu);
+  I.census_state = st.p; I.census_ind = ind.p; I.census_type = typ.p;
+  launch_init_particles(I, make_grid_dev(c), c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  std::swap(c->d_census_state, st); std::swap(c->d_census_ind, ind); std::swap(c->d_census_type, typ);
+  st.release(); ind.release(); typ.release(); erad.release(); zcdf.release(); esum.release(); bb.release();
+  c->n_census = off + n;
+  return SED_OK;
+}
 
 const char* sed_last_error(sed_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
@@ -908,6 +1070,8 @@ void sed_ctx_destroy(sed_ctx* c)
                            &c->d_photoion, &c->d_L_emit, &c->d_L_dep, &c->d_L_tot, &c->d_q_state};
   for (auto* b : rad) b->release();
   c->d_q_ind.release(); c->d_reject.release(); c->d_q_n.release();
+  c->d_rec_type.release(); c->d_census_state.release(); c->d_census_ind.release(); c->d_census_type.release();
+  c->d_q_type.release(); c->d_cmp.release(); c->d_scan_tmp.release(); c->d_cmp_count.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -155,11 +155,25 @@ struct sed_ctx {
   DevBuf<int32_t> d_esc_bin;
   DevBuf<double> d_esc_e, d_abs_scale, d_adj_g, d_adj_out;
 
-  // per-packet records
+  // per-packet records (also the end states a time-dependent step builds
+  // its census from)
   int record = 0;
   int64_t n_rec = 0;
-  DevBuf<int32_t> d_rec_fate, d_rec_ind, d_rec_draws;
+  DevBuf<int32_t> d_rec_fate, d_rec_ind, d_rec_draws, d_rec_type;
   DevBuf<double> d_rec_state;
+
+  // transport clock (transport::t_now_): the first grid's time, then
+  // advanced by dt after each time-dependent step (transport.cpp:136)
+  double t_now = 0;
+  bool have_t_now = false;
+  // packets carried to the next step, in the reference's vector order:
+  // {x, D, t, e, nu}, zone, type; and the queue entries they load into
+  int64_t n_census = 0, n_census_gamma = 0;
+  DevBuf<double> d_census_state;
+  DevBuf<int32_t> d_census_ind, d_census_type, d_q_type;
+  DevBuf<int32_t> d_cmp;                  // flags, sums and front list of the compaction
+  DevBuf<unsigned char> d_scan_tmp;       // scan scratch
+  DevBuf<unsigned long long> d_cmp_count;
 };
 
 namespace sed {

@@ -55,6 +55,7 @@ struct StepArgs {
   unsigned long long* counters;  // [C_COUNT]
   int32_t *rec_fate, *rec_ind, *rec_draws;  // optional per-packet records
   double* rec_state;
+  int32_t* rec_type;                         // PType of the record (with the records of a time-dependent step)
   // ---- batch of independent 1D models (batched kernels only) ----
   const BatchModel* models;         // [n_models], ordered by pkt_off
   int32_t n_models;
@@ -63,12 +64,12 @@ struct StepArgs {
   const double* zone_rin;            // [zones] inner wall after the core substitution
   unsigned long long* model_escaped; // [n_models] escaped packets per model
   uint32_t* step_dev;                // step counter on the device (advanced by the finish kernel)
-  // ---- radioactive source: queued optical photons (single-context kernels) ----
-  int64_t n_core;                    // queue entries [0, n_core) are core packets
-  int64_t radio_first_pid;           // Philox stream id of radioactive packet 0
-  const double* q_state;             // [n_radio * 9] {x, D, t, e, nu} of queued photons
-  const int32_t* q_ind;              // [n_radio] their zone (or -1 / -2)
-  const uint32_t* q_n;               // [n_radio] next deviate index; RADIO_NO_PHOTON: none
+  // ---- queued packets: the census, then the radioactive packets (single-context kernels) ----
+  int64_t n_core;                    // queue entries [0, n_core) are core packets, the rest queued packets
+  int64_t radio_first_pid;           // Philox stream id of queued packet 0
+  const double* q_state;             // [n_q * 9] {x, D, t, e, nu} of queued photons
+  const int32_t* q_ind;              // [n_q] their zone (or -1 / -2)
+  const uint32_t* q_n;               // [n_q] next deviate index; RADIO_NO_PHOTON: none
   double *L_dep, *L_emit;            // [nz] radioactive tallies normalised by the finish kernel, or null
   // ---- differentiable transport (weighted forward and adjoint replay kernels only) ----
   const double* abs_scale;           // [nz * n_bands] factor on the absorption opacity, or null
@@ -81,14 +82,20 @@ struct StepArgs {
 };
 
 constexpr uint32_t RADIO_NO_PHOTON = 0xFFFFFFFFu;
+// particle types (enum PType, src/transport/particle.h:8)
+constexpr int32_t TYPE_PHOTON = 0, TYPE_GAMMA = 1;
+// Philox step number of the deviates transport::initialize_particles draws
+constexpr uint32_t INIT_STEP = 0xFFFFFFFFu;
 
 // Radioactive gamma-ray source (transport::emit_radioactive, src/transport/
 // emission.cpp:163-243) and gamma-ray transport (Compton scattering and
 // photo-absorption, scatter.cpp:45-133, transport_opacity.cpp:290-313).
 struct RadioArgs {
   int32_t nz, n_elems, force_rproc, pad_;
-  int64_t n_radio;                 // radioactive packets of the step
-  int64_t first_pid;               // Philox stream id of radioactive packet 0
+  int64_t n_census;                // queued packets [0, n_census) come from the census
+  int64_t n_radio;                 // radioactive packets of the step: queued packets [n_census, n_census + n_radio)
+  int64_t first_pid;               // Philox stream id of queued packet 0
+  const int32_t* q_type;           // [n_census] census packet types
   double t_now, dt;
   const double *rho, *vol, *X;     // zone state; X the zone's composition (not decayed)
   const int32_t *eZ, *eA;
@@ -96,9 +103,9 @@ struct RadioArgs {
   double* cdf;                     // [nz] zone emission CDF
   double* L_tot;                   // device scalar: decay luminosity of the grid
   double* L_dep;                   // [nz] deposition tally
-  double* q_state;                 // [n_radio * 9] {x, D, t, e, nu} of queued optical photons
-  int32_t* q_ind;                  // [n_radio] their zone
-  uint32_t* q_n;                   // [n_radio] their next deviate index, RADIO_NO_PHOTON if none
+  double* q_state;                 // [n_q * 9] {x, D, t, e, nu} of queued optical photons
+  int32_t* q_ind;                  // [n_q] their zone
+  uint32_t* q_n;                   // [n_q] their next deviate index, RADIO_NO_PHOTON if none
   int32_t* n_reject_cap;           // Compton rejection loops that hit their cap
 };
 // per-zone decay luminosity, gamma fraction and gamma opacities, then the
@@ -108,6 +115,50 @@ int launch_radio_zones(const RadioArgs& a, cudaStream_t s);
 // optical photons they become are queued for the packet kernel
 int launch_gamma(const StepArgs& a, const StepArgs& ag, const RadioArgs& r, const GridDev& g, int num_sms,
                  cudaStream_t s);
+
+// Packets carried between time-dependent steps: transport::step leaves
+// the stopped packets in its particle vector (transport.cpp:91, 164-194).
+struct CensusArgs {
+  int64_t n_census;                // census packets loaded at the start of the step
+  int64_t n_core, n_q;             // record slots: [0, n_core) core packets, then the n_q queued packets
+  double* census_state;            // [n * 9] {x, D, t, e, nu}: read at the start, rewritten at the end
+  int32_t *census_ind, *census_type;
+  double* q_state;                 // queue of the step
+  int32_t *q_ind, *q_type;
+  uint32_t* q_n;
+  const int32_t *rec_fate, *rec_ind, *rec_type;  // end states of the step's packets
+  const double* rec_state;
+  int32_t *flag_e, *flag_a;        // [n + 1] packet exists / is stopped, in the reference's vector order
+  int32_t *scan_e, *scan_a;        // their exclusive sums
+  int32_t* front_dead;             // [n]
+  unsigned long long* n_gamma;     // gamma-rays in the new census
+};
+// loads the census into the front of the step's queue (2 launches at most)
+int launch_census_load(const CensusArgs& a, const GridDev& g, cudaStream_t s);
+// existence / stopped flags of the step's packets in vector order
+int launch_census_flags(const CensusArgs& a, int64_t n, cudaStream_t s);
+// the reference's swap-from-the-back compaction (clean_up_particle_vector)
+// of the stopped packets into the census, from the flags' exclusive sums
+int launch_census_compact(const CensusArgs& a, int64_t n, cudaStream_t s);
+
+// transport::initialize_particles (src/transport/emission.cpp:112-159):
+// photons emitted in proportion to e_rad * vol with a blackbody spectrum at
+// the gas temperature, appended to the census
+struct InitArgs {
+  int64_t n, census_off;           // packets; first census slot
+  uint32_t seed;
+  int64_t first_pid;
+  double t_now;
+  int32_t nz;
+  const double *e_rad, *vol, *T;   // [nz]
+  double* zone_cdf;                // [nz] scratch
+  double* E_sum;                   // device scalar
+  double* bb_cdf;                  // [nz * n_nu] scratch: blackbody emissivity CDF per zone
+  DevLoc nu;
+  double* census_state;
+  int32_t *census_ind, *census_type;
+};
+int launch_init_particles(const InitArgs& a, const GridDev& g, cudaStream_t s);
 
 // One model of a batch: its packets are global queue entries
 // [pkt_off, pkt_off + n_packets), its zones [zone_off, zone_off + n_zones)

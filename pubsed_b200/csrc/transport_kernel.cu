@@ -595,6 +595,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
           A.rec_fate[pid] = fate;
           A.rec_ind[pid] = p.ind;
           A.rec_draws[pid] = (int32_t)(rng.n - K);
+          if (A.rec_type) A.rec_type[pid] = TYPE_PHOTON;
           double* s = A.rec_state + pid * 9;
           s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
           s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
@@ -631,11 +632,12 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
         if (pid >= (unsigned long long)A.n_packets) break;
         if (!BATCH && MODE == 0 && A.q_n != nullptr && (int64_t)pid >= A.n_core) {
-          // an optical photon of the radioactive source, handed over by the
+          // a queued photon: a census photon (stream position 0), or an
+          // optical photon of the radioactive source handed over by the
           // gamma-ray kernel with its position in its Philox stream
           const int64_t k = (int64_t)pid - A.n_core;
           const uint32_t qn = A.q_n[k];
-          if (qn == RADIO_NO_PHOTON) continue;  // escaped or absorbed as a gamma-ray
+          if (qn == RADIO_NO_PHOTON) continue;  // ended as a gamma-ray
           const double* q = A.q_state + (size_t)k * 9;
           p.x[0] = q[0]; p.x[1] = q[1]; p.x[2] = q[2];
           p.D[0] = q[3]; p.D[1] = q[4]; p.D[2] = q[5];
@@ -1067,38 +1069,54 @@ __global__ void __launch_bounds__(128, 8) gamma_kernel(const StepArgs A, const S
   constexpr int COMPTON_TRIES = 1 << 16;
   const double L_tot = *R.L_tot;
   const double Ep = L_tot * R.dt / (1.0 * R.n_radio);
+  const int64_t n_q = R.n_census + R.n_radio;
   for (;;) {
     const int64_t k = (int64_t)atomicAdd(A.counters + C_COUNT, 1ULL);
-    if (k >= R.n_radio) break;
-    R.q_n[k] = RADIO_NO_PHOTON;
-    if (L_tot == 0) {  // the reference emits nothing then
-      if (A.rec_fate) {
-        const int64_t r = A.n_core + k;
-        A.rec_fate[r] = -1; A.rec_ind[r] = 0; A.rec_draws[r] = 0;
-        for (int j = 0; j < 9; ++j) A.rec_state[r * 9 + j] = 0;
-      }
-      continue;
-    }
+    if (k >= n_q) break;
     PacketRng rng;
-    rng.init(A.seed, (uint64_t)(R.first_pid + k), A.step, 0);
     Pkt p;
-    // zone_emission_cdf_.sample: upper_bound over the zones
-    const int i = (R.nz == 1) ? 0 : upper_bound_dev(R.cdf, R.nz, rng.next());
-    const double t = R.t_now + R.dt * rng.next();
-    const bool is_gamma = rng.next() < __ldg(R.gamma_frac + i);
-    if (!is_gamma) atomicAdd(R.L_dep + i, Ep);  // positrons deposit and become photons
-    const double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
-    sample_in_zone<GRID>(G, i, u0, u1, u2, p.x);
-    isotropic_direction(rng, p.D);
-    p.ind = i;
-    if (is_gamma) p.nu = 1;  // sample_photon_frequency for gamma-rays (emission.cpp:35-38)
-    else sample_optical_nu<CT>(A, p, rng);
-    p.e = Ep;
-    lorentz_transform<GRID>(G, p, 1);
-    p.t = t;
-    // transport::propagate: the zone of the emitted position
+    bool photon;
+    if (k < R.n_census) {
+      // a gamma-ray of the census continues on its stream of this step;
+      // census photons are the packet kernel's
+      if (R.q_type[k] != TYPE_GAMMA) continue;
+      R.q_n[k] = RADIO_NO_PHOTON;
+      rng.init(A.seed, (uint64_t)(R.first_pid + k), A.step, 0);
+      const double* q = R.q_state + (size_t)k * 9;
+      p.x[0] = q[0]; p.x[1] = q[1]; p.x[2] = q[2];
+      p.D[0] = q[3]; p.D[1] = q[4]; p.D[2] = q[5];
+      p.t = q[6]; p.e = q[7]; p.nu = q[8];
+      p.dvds = 0;
+      photon = false;
+    } else {
+      R.q_n[k] = RADIO_NO_PHOTON;
+      if (L_tot == 0) {  // the reference emits nothing then
+        if (A.rec_fate) {
+          const int64_t r = A.n_core + k;
+          A.rec_fate[r] = -1; A.rec_ind[r] = 0; A.rec_draws[r] = 0;
+          for (int j = 0; j < 9; ++j) A.rec_state[r * 9 + j] = 0;
+        }
+        continue;
+      }
+      rng.init(A.seed, (uint64_t)(R.first_pid + k), A.step, 0);
+      // zone_emission_cdf_.sample: upper_bound over the zones
+      const int i = (R.nz == 1) ? 0 : upper_bound_dev(R.cdf, R.nz, rng.next());
+      const double t = R.t_now + R.dt * rng.next();
+      const bool is_gamma = rng.next() < __ldg(R.gamma_frac + i);
+      if (!is_gamma) atomicAdd(R.L_dep + i, Ep);  // positrons deposit and become photons
+      const double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+      sample_in_zone<GRID>(G, i, u0, u1, u2, p.x);
+      isotropic_direction(rng, p.D);
+      p.ind = i;
+      if (is_gamma) p.nu = 1;  // sample_photon_frequency for gamma-rays (emission.cpp:35-38)
+      else sample_optical_nu<CT>(A, p, rng);
+      p.e = Ep;
+      lorentz_transform<GRID>(G, p, 1);
+      p.t = t;
+      photon = !is_gamma;
+    }
+    // transport::propagate: the zone of the packet's position
     p.ind = get_zone<GRID>(G, p.x);
-    bool photon = !is_gamma;
     int fate = MOVING;
     if (!photon) {
       if (p.ind == -1) fate = ABSORBED;
@@ -1219,6 +1237,7 @@ __global__ void __launch_bounds__(128, 8) gamma_kernel(const StepArgs A, const S
       A.rec_fate[r] = fate;
       A.rec_ind[r] = p.ind;
       A.rec_draws[r] = (int32_t)rng.n;
+      if (A.rec_type) A.rec_type[r] = TYPE_GAMMA;
       double* s = A.rec_state + r * 9;
       s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
       s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
@@ -1234,6 +1253,159 @@ __global__ void __launch_bounds__(128, 8) gamma_kernel(const StepArgs A, const S
     if (n_seg) atomicAdd(A.counters + C_SEGMENTS, n_seg);
     if (n_scat) atomicAdd(A.counters + C_SCATTERS, n_scat);
     if (n_lim) atomicAdd(A.counters + C_LIMIT, n_lim);
+  }
+}
+
+// ------------------------------------------------------------ census
+// The census opens the step's queue.  transport::propagate starts with
+// get_zone (transport.cpp:205-209), so each packet is located again on the
+// grid of this step.
+template <int GRID>
+__global__ void census_load_kernel(const CensusArgs C, const GridDev G)
+{
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < C.n_census; k += stride) {
+    const double* s = C.census_state + k * 9;
+    double* q = C.q_state + k * 9;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) q[j] = s[j];
+    C.q_type[k] = C.census_type[k];
+    C.q_ind[k] = get_zone<GRID>(G, s);
+    C.q_n[k] = 0;
+  }
+}
+
+// Record slot of the packet at position r of the reference's vector
+// (census, then radioactive, then core packets).
+__device__ __forceinline__ int64_t census_slot(const CensusArgs& C, int64_t r)
+{
+  return r < C.n_q ? C.n_core + r : r - C.n_q;
+}
+
+__global__ void census_flags_kernel(const CensusArgs C, int64_t n)
+{
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r <= n; r += stride) {
+    if (r == n) { C.flag_e[r] = 0; C.flag_a[r] = 0; continue; }
+    const int32_t f = C.rec_fate[census_slot(C, r)];
+    C.flag_e[r] = (f != -1);  // -1: a radioactive packet that was never emitted
+    C.flag_a[r] = (f == STOPPED);
+  }
+}
+
+// clean_up_particle_vector keeps the n_alive stopped packets: a stopped
+// packet at vector position s < n_alive stays there, and the j-th removed
+// position below n_alive (counted from the front) takes the j-th stopped
+// packet counted from the back.
+__global__ void census_front_kernel(const CensusArgs C, int64_t n)
+{
+  const int64_t n_alive = C.scan_a[n];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += stride) {
+    if (!C.flag_e[r] || C.flag_a[r]) continue;
+    const int64_t s = C.scan_e[r];
+    if (s < n_alive) C.front_dead[s - C.scan_a[r]] = (int32_t)s;
+  }
+}
+
+__global__ void census_scatter_kernel(const CensusArgs C, int64_t n)
+{
+  const int64_t n_alive = C.scan_a[n];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long ng = 0;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += stride) {
+    if (!C.flag_a[r]) continue;
+    const int64_t s = C.scan_e[r];
+    const int64_t dest = s < n_alive ? s : C.front_dead[n_alive - 1 - C.scan_a[r]];
+    const int64_t slot = census_slot(C, r);
+    const double* src = C.rec_state + slot * 9;
+    double* d = C.census_state + dest * 9;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) d[j] = src[j];
+    C.census_ind[dest] = C.rec_ind[slot];
+    C.census_type[dest] = C.rec_type[slot];
+    if (C.rec_type[slot] == TYPE_GAMMA) ++ng;
+  }
+  if (ng) atomicAdd(C.n_gamma, ng);
+}
+
+// ------------------------------------------------------------ initialisation
+// transport::blackbody_nu (transport_opacity.cpp:322-326)
+__device__ __forceinline__ double blackbody_nu(double T, double nu)
+{
+  const double zeta = H_PLANCK * nu / K_BOLTZ / T;
+  return 2.0 * nu * nu * nu * H_PLANCK / C_LIGHT / C_LIGHT / (exp(zeta) - 1);
+}
+
+// cdf_array::normalize (src/transport/cdf_array.h:62-74), in order
+__device__ void cdf_normalize_seq(double* y, int n)
+{
+  for (int i = 0; i < n; ++i) if (isnan(y[i])) y[i] = 0;
+  if (y[n - 1] == 0) for (int i = 0; i < n; ++i) y[i] = 1.0;
+  const double N = y[n - 1];
+  for (int i = 0; i < n; ++i) y[i] /= N;
+}
+
+// the zone CDF of e_rad * vol and its sum, in the reference's order
+// (emission.cpp:128-150); one thread
+__global__ void init_zone_cdf_kernel(const InitArgs I)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double E_sum = 0;
+  for (int i = 0; i < I.nz; ++i) {
+    const double E_zone = I.e_rad[i] * I.vol[i];
+    I.zone_cdf[i] = (i == 0) ? E_zone : I.zone_cdf[i - 1] + E_zone;
+    E_sum += E_zone;
+  }
+  cdf_normalize_seq(I.zone_cdf, I.nz);
+  *I.E_sum = E_sum;
+}
+
+// the blackbody emissivity CDF of each zone at its gas temperature
+// (emission.cpp:137-146); one thread per zone, bins in order
+__global__ void init_bb_cdf_kernel(const InitArgs I)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= I.nz) return;
+  const int ng = I.nu.n;
+  double* row = I.bb_cdf + (size_t)i * ng;
+  const double T = I.T[i];
+  for (int j = 0; j < ng; ++j) {
+    const double emis = blackbody_nu(T, loc_center(I.nu, j)) * loc_delta(I.nu, j);
+    row[j] = (j == 0) ? emis : row[j - 1] + emis;
+  }
+  cdf_normalize_seq(row, ng);
+}
+
+// the packets: zone, then create_isotropic_particle (emission.cpp:57-107)
+// with the blackbody emissivity, at time t_now
+template <int GRID>
+__global__ void init_particles_kernel(const InitArgs I, const GridDev G)
+{
+  const double Ep = *I.E_sum / (1.0 * I.n);
+  const int ng = I.nu.n;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < I.n; k += stride) {
+    PacketRng rng;
+    rng.init(I.seed, (uint64_t)(I.first_pid + k), INIT_STEP, 0);
+    Pkt p;
+    const int i = (I.nz == 1) ? 0 : upper_bound_dev(I.zone_cdf, I.nz, rng.next());
+    p.ind = i;
+    const double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+    sample_in_zone<GRID>(G, i, u0, u1, u2, p.x);
+    isotropic_direction(rng, p.D);
+    const int inu = (ng == 1) ? 0 : upper_bound_dev(I.bb_cdf + (size_t)i * ng, ng, rng.next());
+    p.nu = loc_sample(I.nu, inu, rng.next());
+    p.e = Ep;
+    lorentz_transform<GRID>(G, p, 1);
+    p.t = I.t_now;
+    const int64_t c = I.census_off + k;
+    double* d = I.census_state + c * 9;
+    d[0] = p.x[0]; d[1] = p.x[1]; d[2] = p.x[2];
+    d[3] = p.D[0]; d[4] = p.D[1]; d[5] = p.D[2];
+    d[6] = p.t; d[7] = p.e; d[8] = p.nu;
+    I.census_ind[c] = i;
+    I.census_type[c] = TYPE_PHOTON;
   }
 }
 
@@ -1340,6 +1512,48 @@ int launch_gamma(const StepArgs& a, const StepArgs& ag, const RadioArgs& r, cons
     else gamma_kernel<1, float><<<(unsigned)blocks, 128, 0, s>>>(a, ag, r, g);
   }
   return 1;
+}
+
+static unsigned grid_for(int64_t n, int threads, int num_blocks_max)
+{
+  int64_t b = (n + threads - 1) / threads;
+  if (b > num_blocks_max) b = num_blocks_max;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+int launch_census_load(const CensusArgs& a, const GridDev& g, cudaStream_t s)
+{
+  if (a.n_census <= 0) return 0;
+  const unsigned b = grid_for(a.n_census, 256, 148 * 16);
+  if (g.type == 0) census_load_kernel<0><<<b, 256, 0, s>>>(a, g);
+  else census_load_kernel<1><<<b, 256, 0, s>>>(a, g);
+  return 1;
+}
+
+int launch_census_flags(const CensusArgs& a, int64_t n, cudaStream_t s)
+{
+  census_flags_kernel<<<grid_for(n + 1, 256, 148 * 16), 256, 0, s>>>(a, n);
+  return 1;
+}
+
+int launch_census_compact(const CensusArgs& a, int64_t n, cudaStream_t s)
+{
+  if (n <= 0) return 0;
+  census_front_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(a, n);
+  census_scatter_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(a, n);
+  return 2;
+}
+
+int launch_init_particles(const InitArgs& a, const GridDev& g, cudaStream_t s)
+{
+  if (a.n <= 0) return 0;
+  init_zone_cdf_kernel<<<1, 32, 0, s>>>(a);
+  init_bb_cdf_kernel<<<(a.nz + 127) / 128, 128, 0, s>>>(a);
+  const unsigned b = grid_for(a.n, 128, 148 * 8);
+  if (g.type == 0) init_particles_kernel<0><<<b, 128, 0, s>>>(a, g);
+  else init_particles_kernel<1><<<b, 128, 0, s>>>(a, g);
+  return 3;
 }
 
 void batch_variant_shape(int variant, int* threads, int* min_blocks)

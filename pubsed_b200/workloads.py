@@ -221,6 +221,46 @@ def lightbulb_grey(n_packets: int = 1_000_000, n_zones: int = 128, n_bins: int =
                     notes={"log_del": d, "v_max": 1e9, "t_days": 10.0})
 
 
+def time_dependent(base: str, n_initialize: int = 0, dt_days: float = 0.1, **kw) -> Workload:
+    """The workload `base(**kw)` run time-dependently
+    (transport_steady_iterate = 0): packets that reach the end of a step are
+    carried to the next, the grid expands homologously between steps
+    (`homologous_step`), and particles_n_initialize packets of the initial
+    radiation field (e_rad = a T^4) start in the census.  notes["dt"] is the
+    step (dt_days)."""
+    w = globals()[base](**kw)
+    w.params["transport_steady_iterate"] = 0
+    w.params["particles_n_initialize"] = int(n_initialize)
+    w.params["particles_max_total"] = max(int(w.params.get("particles_max_total", 1e7)), 4 * int(n_initialize) + 1)
+    w.name = w.name + "_td"
+    w.notes["dt"] = dt_days * 86400.0
+    return w
+
+
+def initial_e_rad(zones: ZoneModel) -> np.ndarray:
+    """Zone radiation energy density of a model without an erad column:
+    a T_gas^4 (grid_1D_sphere.cpp:354, :130)."""
+    return A_RAD_CGS * np.power(zones.T, 4.0)
+
+
+def homologous_step(zones: ZoneModel, dt: float) -> None:
+    """hydro_homologous::step (src/hydro/hydro_homologous.cpp:27-45) on a 1D
+    sphere: e = (t + dt) / t, rho /= e^3, walls and r_min scaled by e
+    (locate_array::scale), shell volumes recomputed (grid_1D_sphere::expand,
+    :413-426), t += dt; the reference's operations in its order."""
+    if zones.type != abi.GRID_1D_SPHERE:
+        raise ValueError("homologous_step: 1D spheres only")
+    e = (zones.t_now + dt) / zones.t_now
+    zones.rho = zones.rho / e / e / e
+    zones.r_out = zones.r_out * e
+    zones.r_min = zones.r_min * e
+    zones.vol = shell_volumes(zones.r_min, zones.r_out)
+    zones.t_now = zones.t_now + dt
+
+
+A_RAD_CGS = 7.5657e-15  # physical_constants::a
+
+
 # Type Ia-like layered composition: (Z, A) and mass fractions per layer
 IA_ELEMENTS = [(6, 12), (8, 16), (14, 28), (16, 32), (20, 40), (28, 56)]
 IA_LAYERS = [  # (v_upper cm/s, mass fractions in IA_ELEMENTS order)

@@ -13,6 +13,9 @@ inputs, plus the reference's outputs:
                  tables; the zone
                  temperatures after the step's radiative-equilibrium solve;
                  the reference's own spectrum .dat and, for 1D, plt .dat text)
+  replay_td_*.npz  several time-dependent steps in replay mode: the initial
+                 packets, and per step (suffix _s<k>) the per-packet results,
+                 the census carried on, tallies and the accumulated spectrum
   locate_kat.json  value/index pairs printed by the reference's own
                  src/utils/locate_array_test.cpp
 
@@ -49,6 +52,21 @@ CASES = {
     "replay_cart3d": ("cart3d", dict(n_packets=300, n_cells=6, n_lines=1500, n_bins=128, spectrum_bins=64, n_mu=4,
                                      seed=13)),
 }
+
+# time-dependent replays: several steps with the census carried between them,
+# the grid expanding homologously before each step, initial packets from the
+# radiation field; every per-step array carries the suffix _s<step>
+TD_CASES = {
+    "replay_td_grey": ("time_dependent", dict(base="lightbulb_grey", n_initialize=300, dt_days=0.1, n_packets=200,
+                                              n_zones=32, n_bins=128, radiative_eq=0, seed=3), 3),
+    # gamma-rays and photons in flight at the end of each step
+    "replay_td_ia_radio": ("time_dependent", dict(base="type_ia", n_initialize=200, dt_days=0.5, n_packets=100,
+                                                  n_zones=16, n_lines=5000, n_bins=256, n_levels_per_ion=6,
+                                                  v_core=1e8, n_radioactive=300, t_days=60.0, seed=29), 3),
+}
+TD_KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "pkt_type", "census_ind", "census_type", "census_state",
+           "J_nu", "e_abs", "e_rad", "fr_rad", "spec_flux", "spec_click", "T_gas"]
+TD_RADIO_KEYS = ["L_radio_emit", "L_radio_dep", "gamma_flux", "gamma_click"]
 
 FREE_CASES = {
     "free_grey_radeq": ("lightbulb_grey", dict(n_packets=200000, n_zones=128, n_bins=256, radiative_eq=1, seed=101)),
@@ -101,6 +119,22 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw),
                             n_escaped=out["n_escaped"], **arrays)
         print(name, "packets", int(out["n_packets"]), "escaped", int(out["n_escaped"]))
+    for name, (gen, kw, steps) in TD_CASES.items():
+        if only and name not in only:
+            continue
+        w = make_workload(gen, kw)
+        out = run_ref.run(w, "replay", threads=1, seed=kw.get("seed", 0), steps=steps, dt=w.notes["dt"])
+        arrays = {}
+        for k in ("init_ind", "init_type", "init_state"):
+            if k in out:
+                arrays[k] = out[k]
+        for st in range(steps):
+            for k in TD_KEYS + (TD_RADIO_KEYS if kw.get("n_radioactive") else []):
+                arrays["%s_s%d" % (k, st)] = out["%s_s%d" % (k, st)]
+            arrays["n_escaped_s%d" % st] = out["n_escaped_s%d" % st]
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), generator=gen, kwargs=json.dumps(kw), steps=steps,
+                            **arrays)
+        print(name, "steps", steps, "census", [int(arrays["census_ind_s%d" % i].size) for i in range(steps)])
     # free-running reference steps (its own transport::step, OpenMP, streams
     # independent of the per-packet replay streams) for the chi-squared tests
     for name, (gen, kw) in FREE_CASES.items():

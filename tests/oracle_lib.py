@@ -122,6 +122,18 @@ class Engine:
         self.check(self.fn("get_gamma_spectrum")(self.ctx, P(gf), P(gc)), "get_gamma_spectrum")
         return {"L_radio_emit": le, "L_radio_dep": ld, "gamma_flux": gf, "gamma_click": gc}
 
+    def initialize_particles(self, n: int, e_rad) -> None:
+        k = abi.Keep()
+        self.check(self.fn("initialize_particles")(self.ctx, int(n), k.d(e_rad)), "initialize_particles")
+
+    def census(self) -> dict:
+        """The packets carried to the next step: zone, type, {x, D, t, e, nu}."""
+        n = int(self.fn("n_particles")(self.ctx))
+        ind = np.zeros(max(n, 1), np.int32); typ = np.zeros(max(n, 1), np.int32); st = np.zeros(max(n, 1) * 9)
+        self.check(self.fn("get_particles")(self.ctx, n, ind.ctypes.data_as(abi._ip), typ.ctypes.data_as(abi._ip),
+                                            st.ctypes.data_as(abi._dp)), "get_particles")
+        return {"ind": ind[:n], "type": typ[:n], "state": st[:n * 9].reshape(n, 9)}
+
     def records(self, n: int) -> dict:
         fate = np.zeros(n, np.int32); ind = np.zeros(n, np.int32); draws = np.zeros(n, np.int32)
         st = np.zeros(n * 9)
@@ -259,3 +271,32 @@ def solve_temperature(eng: Engine, set_Tgas_to_Trad: int = 0):
     eng.check(eng.fn("solve_temperature")(eng.ctx, set_Tgas_to_Trad, T.ctypes.data_as(abi._dp), C.byref(bad)),
               "solve_temperature")
     return T, int(bad.value)
+
+
+def td_steps(eng: Engine, w, steps: int, n_initialize: int = 0, radio: bool = False) -> list:
+    """Runs `steps` time-dependent steps as the reference's driver does: the
+    initial packets first, then per step the homologous hydro step, the grid
+    upload, the opacity build and the transport step, and with radiative
+    equilibrium the temperature solve feeding the next step.  Returns per
+    step the records, census, tallies, spectrum (and radioactive results)."""
+    from pubsed_b200 import workloads
+    dt = w.notes["dt"]
+    if n_initialize:
+        eng.initialize_particles(n_initialize, workloads.initial_e_rad(w.zones))
+    out = []
+    for _ in range(steps):
+        workloads.homologous_step(w.zones, dt)
+        eng.set_grid()
+        eng.set_opacity(dt)
+        eng.record(True)
+        st = eng.transport(dt)
+        r = {"stats": st, "records": eng.records(st["n_packets"]), "census": eng.census(),
+             "tallies": eng.tallies(), "spectrum": eng.spectrum()}
+        if radio:
+            r["radio"] = eng.radioactive()
+        if int(w.params.get("transport_radiative_equilibrium", 0)):
+            T, _ = solve_temperature(eng)
+            w.zones.T = T
+            r["T_gas"] = T
+        out.append(r)
+    return out

@@ -43,7 +43,7 @@ def test_oracle_mirrors_the_abi():
     import oracle_lib
     lib = oracle_lib.oracle_lib()
     for n in declared_functions():
-        if n in ("sed_step", "sed_n_particles", "sed_version", "sed_lte_electron_density_noalloc"):
+        if n in ("sed_step", "sed_version", "sed_lte_electron_density_noalloc"):
             continue
         # a batch is checked model by model against separate oracle contexts
         if n.startswith("sed_batch_"):

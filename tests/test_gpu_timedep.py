@@ -1,0 +1,128 @@
+"""Time-dependent steps on the GPU: the census (packets carried between
+steps in the reference's vector order, transport.cpp:164-194), the
+homologous grid between steps, the transport clock, accumulated spectra and
+the initial radiation field's packets (transport::initialize_particles).
+
+FP64 form against the reference's own replayed steps (golden fixtures) and,
+at larger sizes, against the oracle: fate, zone, deviate counts and the
+census order exactly, states within oracle_lib's criterion."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from pubsed_b200 import abi, workloads
+import oracle_lib
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _rel(a, b):
+    fin = np.isfinite(b)
+    assert np.array_equal(np.isfinite(a), fin)
+    s = np.maximum(np.abs(b[fin]), 1e-300)
+    return float(np.max(np.abs(a[fin] - b[fin]) / s)) if s.size else 0.0
+
+
+def _load(name):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    kw = json.loads(str(d["kwargs"]))
+    return d, kw
+
+
+@pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio"])
+def test_time_dependent_steps_match_reference_replay(sed_lib, name):
+    ref, kw = _load(name)
+    w = workloads.time_dependent(**kw)
+    g = oracle_lib.Engine(sed_lib, "sed_", w)
+    radio = bool(kw.get("n_radioactive"))
+    res = oracle_lib.td_steps(g, w, int(ref["steps"]), kw.get("n_initialize", 0), radio)
+    for s, r in enumerate(res):
+        sf = "_s%d" % s
+        rec = r["records"]
+        for k in ("fate", "ind", "draws"):
+            assert np.array_equal(rec[k], ref["pkt_" + k + sf]), (s, k)
+        oracle_lib.check_states(rec["state"], ref["pkt_state" + sf].reshape(-1, 9))
+        c = r["census"]
+        assert np.array_equal(c["ind"], ref["census_ind" + sf])
+        assert np.array_equal(c["type"], ref["census_type" + sf])
+        oracle_lib.check_states(c["state"], ref["census_state" + sf].reshape(-1, 9))
+        f, cl = r["spectrum"]
+        assert np.array_equal(cl, ref["spec_click" + sf])
+        assert _rel(f, ref["spec_flux" + sf]) <= oracle_lib.TALLY_RTOL
+        T = r["tallies"]
+        for k, rk in (("e_abs", "e_abs"), ("e_rad", "e_rad")):
+            oracle_lib.zone_tally_close(T[k], ref[rk + sf])
+        if radio:
+            R = r["radio"]
+            assert _rel(R["L_radio_emit"], ref["L_radio_emit" + sf]) <= 1e-12
+            oracle_lib.zone_tally_close(R["L_radio_dep"], ref["L_radio_dep" + sf])
+            assert np.array_equal(R["gamma_click"], ref["gamma_click" + sf])
+    g.close()
+
+
+@pytest.mark.parametrize("radio", [0, 1])
+def test_time_dependent_steps_match_oracle(sed_lib, radio):
+    """20 000 initial packets, 5000 core (and 20 000 decay) packets per step,
+    4 steps: the census grows to tens of thousands of packets."""
+    kw = dict(base="type_ia", n_initialize=20000, dt_days=0.5, n_packets=5000, n_zones=48, n_lines=20000,
+              n_bins=512, n_levels_per_ion=8, v_core=1e8, t_days=40.0, seed=61)
+    if radio:
+        kw["n_radioactive"] = 20000
+    wg, wo = workloads.time_dependent(**kw), workloads.time_dependent(**kw)
+    g = oracle_lib.Engine(sed_lib, "sed_", wg)
+    o = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", wo)
+    rg = oracle_lib.td_steps(g, wg, 4, kw["n_initialize"], bool(radio))
+    ro = oracle_lib.td_steps(o, wo, 4, kw["n_initialize"], bool(radio))
+    for s, (a, b) in enumerate(zip(rg, ro)):
+        for k in ("fate", "ind", "draws"):
+            assert np.array_equal(a["records"][k], b["records"][k]), (s, k)
+        oracle_lib.check_states(a["records"]["state"], b["records"]["state"])
+        assert np.array_equal(a["census"]["ind"], b["census"]["ind"]), s
+        assert np.array_equal(a["census"]["type"], b["census"]["type"]), s
+        oracle_lib.check_states(a["census"]["state"], b["census"]["state"])
+        assert np.array_equal(a["spectrum"][1], b["spectrum"][1])
+        for k in ("e_abs", "e_rad"):
+            oracle_lib.zone_tally_close(a["tallies"][k], b["tallies"][k])
+        if radio:
+            assert np.array_equal(a["radio"]["gamma_click"], b["radio"]["gamma_click"])
+    assert rg[-1]["census"]["ind"].size > 10000
+    if radio:
+        assert np.any(rg[-1]["census"]["type"] == 1)  # gamma-rays in flight are carried too
+    g.close()
+    o.close()
+
+
+def test_mixed_form_time_dependent(sed_lib):
+    """The mixed form carries its census the same way; its census and escape
+    counts agree with the FP64 form's within Monte Carlo noise."""
+    kw = dict(base="type_ia", n_initialize=40000, dt_days=0.5, n_packets=20000, n_zones=48, n_lines=20000,
+              n_bins=512, n_levels_per_ion=8, v_core=1e8, t_days=40.0, seed=67)
+    out = {}
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        w = workloads.time_dependent(**kw)
+        e = oracle_lib.Engine(sed_lib, "sed_", w, precision=prec)
+        res = oracle_lib.td_steps(e, w, 3, kw["n_initialize"])
+        out[prec] = [(r["census"]["ind"].size, r["stats"]["n_escaped"]) for r in res]
+        e.close()
+    for (c64, e64), (c32, e32) in zip(out[abi.PREC_FP64], out[abi.PREC_MIXED]):
+        assert abs(c32 - c64) <= 5 * np.sqrt(c64) + 10
+        assert abs(e32 - e64) <= 5 * np.sqrt(max(e64, 1)) + 10
+
+
+def test_census_capacity(sed_lib):
+    """The census counts against particles_max_total: new core packets that
+    do not fit next to it are an error."""
+    w = workloads.time_dependent("lightbulb_grey", n_initialize=3000, dt_days=0.1, n_packets=2000, n_zones=16,
+                                 n_bins=64, seed=71)
+    w.params["particles_max_total"] = 4000
+    g = oracle_lib.Engine(sed_lib, "sed_", w)
+    g.initialize_particles(3000, workloads.initial_e_rad(w.zones))
+    assert int(g.fn("n_particles")(g.ctx)) == 3000
+    g.set_opacity(w.notes["dt"])
+    with pytest.raises(RuntimeError, match=r"\(3\)"):
+        g.transport(w.notes["dt"])
+    g.close()
