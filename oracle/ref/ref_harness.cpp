@@ -208,7 +208,7 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
   t.set_opacity(dt);
   t.reduce_opacities();
   t.reduce_Lthermal();
-  if (t.use_ddmc_) { std::fprintf(stderr, "replay: DDMC is not on the replayed path\n"); std::exit(3); }
+  if (t.use_ddmc_) t.compute_diffusion_probabilities(dt);
   t.wipe_radiation();
 
   // the packets the last step left (the census) keep the front of the

@@ -1081,6 +1081,256 @@ static int propagate(oracle_ctx* o, packet* p, double t_now, double dt, int64_t*
 {
   return propagate_from(o, p, t_now, dt, nseg, nscat, 1);
 }
+/* ---------------------------------------------------------------- discrete diffusion
+ * transport_use_ddmc = 2 (src/transport/discrete_diffusion.cpp:114-510), 1D
+ * spheres.  A photon in a zone whose total opacity times the zone width
+ * exceeds transport_ddmc_tau_threshold makes discrete diffusion events
+ * (leakage to a neighbour, effective scattering, end of step) instead of
+ * Monte Carlo segments; it enters such a zone through
+ * move_across_DDMC_interface. */
+static void lorentz(const oracle_ctx* o, packet* p, int tolab);
+static void sample_in_zone(const oracle_ctx* o, int i, double u0, double u1, double u2, double* r);
+static double zone_size(const oracle_ctx* o, int i) { return lg_delta(&o->r_out, i); }  /* grid_1D_sphere.h:65-68 */
+
+static int opacity_of(const oracle_ctx* o, int iz, double nu_cmf, double* opac, double* eps)
+{
+  int nn = o->nu.n;
+  int i_nu = lg_locate_wb(&o->nu, nu_cmf);
+  double a_opac = o->abs[(size_t)iz * nn + i_nu];
+  double s_opac = o->tp.omit_scattering ? 0 : o->scat[(size_t)iz * nn + i_nu];
+  *opac = a_opac + s_opac;
+  *eps = (*opac == 0) ? 0 : a_opac / *opac;
+  return i_nu;
+}
+
+static double pr(const packet* p) { return sqrt(p->x[0] * p->x[0] + p->x[1] * p->x[1] + p->x[2] * p->x[2]); }
+
+/* the zone test of transport::propagate (transport.cpp:219-231) */
+static int in_ddmc_zone(const oracle_ctx* o, packet* p)
+{
+  double dshift = dshift_lab_to_comoving(o, p);
+  double sigma, eps;
+  opacity_of(o, p->ind, p->nu * dshift, &sigma, &eps);
+  return sigma * zone_size(o, p->ind) > o->tp.ddmc_tau;
+}
+
+/* transport::sample_dir_from_blackbody_surface (discrete_diffusion.cpp:753-794) */
+static void bb_surface_dir(const oracle_ctx* o, packet* p)
+{
+  double mu = sqrt(draw(o, p));
+  double phi = 2.0 * PC_PI * draw(o, p);
+  double smu = sqrt(1.0 - mu * mu);
+  double v1 = smu * cos(phi), v2 = smu * sin(phi), v3 = mu;
+  double r1 = p->x[0] / pr(p), r2 = p->x[1] / pr(p), r3 = p->x[2] / pr(p);
+  double costheta = r3, sintheta = sqrt(1 - costheta * costheta);
+  double v1p = v1 * costheta + r1 * v3 * sintheta - r2 * (1.0 - costheta) * (-r2 * v1 + r1 * v2);
+  double v2p = v2 * costheta + r2 * v3 * sintheta - r1 * (1.0 - costheta) * (-r2 * v1 + r1 * v2);
+  double v3p = v3 * costheta - (r1 * v1 + r2 * v2) * sintheta;
+  double norm = sqrt(v1p * v1p + v2p * v2p + v3p * v3p);
+  p->D[0] = v1p / norm; p->D[1] = v2p / norm; p->D[2] = v3p / norm;
+}
+
+/* transport::move_across_DDMC_interface (discrete_diffusion.cpp:413-510):
+ * returns 1 when the photon converts to the diffusive zone new_ind (left in
+ * the comoving frame, as the reference leaves it) */
+static int move_across(const oracle_ctx* o, packet* p, int new_ind, double sigma_i, double dr)
+{
+  int nz = o->nzones;
+  int ip = p->ind + 1, im = p->ind - 1;
+  if (ip == nz) ip = p->ind;
+  if (im < 0) im = 0;
+  double r_p = o->r_out.x[p->ind];
+  double r_m = o->r_out.x[im];
+  if (p->ind == 0) r_m = o->r_out.min;
+  double r_interface = 0, r_0 = 0;
+  if (new_ind == ip) { r_interface = r_p; r_0 = r_interface + 0.5 * dr; }
+  else if (new_ind == im) { r_interface = r_m; r_0 = r_interface - 0.5 * dr; }
+  (void)r_0;
+  lorentz(o, p, 0);
+  double rr = pr(p);
+  double mu = (p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2]) / rr;
+  mu = fabs(mu);
+  double p_convert = 4.0 * (1.0 + 1.5 * mu) / (3.0 * sigma_i * dr + 6.0 * 0.7104);
+  double xi = draw(o, p);
+  double u0 = draw(o, p), u1 = draw(o, p), u2 = draw(o, p);
+  double push = 1.0e-8;
+  if (xi <= p_convert) {
+    p->ind = new_ind;
+    sample_in_zone(o, p->ind, u0, u1, u2, p->x);
+    return 1;
+  }
+  sample_in_zone(o, p->ind, u0, u1, u2, p->x);
+  if (new_ind == ip) {
+    double d = r_interface - pr(p);
+    d *= (1.0 - push);
+    p->x[0] += p->x[0] / pr(p) * d;
+    p->x[1] += p->x[1] / pr(p) * d;
+    p->x[2] += p->x[2] / pr(p) * d;
+  } else if (new_ind == im) {
+    double d = pr(p) - r_interface;
+    d *= (1.0 - push);
+    p->x[0] -= p->x[0] / pr(p) * d;
+    p->x[1] -= p->x[1] / pr(p) * d;
+    p->x[2] -= p->x[2] / pr(p) * d;
+  }
+  bb_surface_dir(o, p);
+  double mu2 = (p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2]) / pr(p);
+  if (new_ind == ip) {
+    if (mu2 > 0.0) { p->D[0] = -p->D[0]; p->D[1] = -p->D[1]; p->D[2] = -p->D[2]; }
+  } else if (new_ind == im) {
+    if (mu2 < 0.0) { p->D[0] = -p->D[0]; p->D[1] = -p->D[1]; p->D[2] = -p->D[2]; }
+  }
+  lorentz(o, p, 1);
+  return 0;
+}
+
+#define DDMC_SCATTER_TRIES (1 << 16)
+/* one pass of the event loop of transport::discrete_diffuse_DDMC
+ * (discrete_diffusion.cpp:136-404); *dt_remaining carries over the passes of
+ * one call */
+static int ddmc_event(oracle_ctx* o, packet* p, double* dt_remaining, int64_t* nscat)
+{
+  int nz = o->nzones, nn = o->nu.n, nj = o->tp.store_Jnu ? nn : 1;
+  double lambda_ddmc = 0.7104, push = 1.0e-8;
+  int fate = F_MOVING;
+  int ii = p->ind, ip = ii + 1, im = ii - 1;
+  if (ip == nz) ip = ii;
+  if (im < 0) im = 0;
+  double dx = zone_size(o, ii), dxp1 = zone_size(o, ip), dxm1 = zone_size(o, im);
+  double sigma_i, sigma_im1, sigma_ip1, eps_i, eps_ip1, eps_im1;
+  double dshift = dshift_lab_to_comoving(o, p);
+  int i_nu = opacity_of(o, ii, p->nu * dshift, &sigma_i, &eps_i);
+  opacity_of(o, ip, p->nu * dshift, &sigma_ip1, &eps_ip1);
+  opacity_of(o, im, p->nu * dshift, &sigma_im1, &eps_im1);
+  double r_p = o->r_out.x[ii];
+  double r_m = o->r_out.x[im];
+  if (ii == 0) r_m = o->r_out.min;
+  double r_0 = 0.5 * (r_p + r_m);
+  double Xi = 1.0 + dx * dx / (12.0 * r_0 * r_0);
+  double geo_factor = r_m * r_m / r_0 / r_0 / Xi;
+  double tau_im1 = sigma_im1 * dxm1;
+  int ddmc_on_im1 = !(tau_im1 <= o->tp.ddmc_tau);
+  double sigma_leak_left;
+  if (ddmc_on_im1) sigma_leak_left = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + sigma_im1 * dxm1)) * geo_factor;
+  else sigma_leak_left = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + 2.0 * lambda_ddmc)) * geo_factor;
+  geo_factor = r_p * r_p / r_0 / r_0 / Xi;
+  double tau_ip1 = sigma_ip1 * dxp1;
+  int ddmc_on_ip1 = !(tau_ip1 <= o->tp.ddmc_tau);
+  double sigma_leak_right;
+  if (ddmc_on_ip1) sigma_leak_right = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + sigma_ip1 * dxp1)) * geo_factor;
+  else sigma_leak_right = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + 2.0 * lambda_ddmc)) * geo_factor;
+  if (ip == ii) sigma_leak_right = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + 2.0 * lambda_ddmc)) * geo_factor;
+  if (ii == 0) sigma_leak_left = 0.0;
+  double sigma_leak_tot = sigma_leak_left + sigma_leak_right;
+  double xi = draw(o, p);
+  int leaked2imc = 0;
+  double d_stay = PC_C * *dt_remaining;
+  double d_leak = -log(xi) / (sigma_leak_left + sigma_leak_right);
+  double d_sc;
+  if (nn == 1) d_sc = INFINITY;
+  else {
+    double tau_r = -1.0 * log(draw(o, p));
+    if (eps_i > 0.0) {
+      double k_es_inelastic = sigma_i * eps_i;
+      dshift = dshift_lab_to_comoving(o, p);
+      i_nu = opacity_of(o, p->ind, p->nu * dshift, &sigma_i, &eps_i);
+      const double* cdf = o->cdf + (size_t)p->ind * nn;
+      double elastic_frac = (i_nu == 0) ? cdf[0] : (cdf[i_nu] - cdf[i_nu - 1]);
+      k_es_inelastic *= 1.0 - elastic_frac;
+      d_sc = tau_r / k_es_inelastic;
+    } else d_sc = INFINITY;
+  }
+  int event;
+  double this_d;
+  if ((d_sc < d_leak) && (d_sc < d_stay)) { event = 0; this_d = d_sc; }
+  else if (d_leak < d_stay) { event = 1; this_d = d_leak; }
+  else { event = 2; this_d = d_stay; }
+  double this_dt = this_d / PC_C;
+  p->t += this_dt;
+  *dt_remaining -= this_dt;
+  o->J[(size_t)p->ind * nj] += p->e * this_d;
+  o->e_abs[p->ind] += (p->e * dshift) * this_d * sigma_i * eps_i;
+  if (event == 0) {
+    (*nscat)++;
+    int now_i_nu = i_nu;
+    for (int tries = 0; now_i_nu == i_nu; ++tries) {
+      if (tries >= DDMC_SCATTER_TRIES) { o->n_reject_cap++; break; }
+      /* do_scatter(p, 1.0) (scatter.cpp:12-41) */
+      fate = F_MOVING;
+      if (draw(o, p) > 1.0) isotropic_scatter(o, p, 0);
+      else {
+        double z2 = draw(o, p);
+        if ((z2 > o->eps_imc[p->ind]) || o->tp.radiative_eq) isotropic_scatter(o, p, 1);
+        else fate = F_ABSORBED;
+      }
+      dshift = dshift_lab_to_comoving(o, p);
+      double s2, e2;
+      now_i_nu = opacity_of(o, p->ind, p->nu * dshift, &s2, &e2);
+    }
+  } else if (event == 2) {
+    *dt_remaining = -1.0;
+    fate = F_STOPPED;
+  } else {
+    double P_leak_left = sigma_leak_left / sigma_leak_tot;
+    double xi2 = draw(o, p);
+    if (xi2 <= P_leak_left) {
+      p->ind--;
+      double rr = pr(p);
+      double dr = rr - r_m;
+      if (ddmc_on_im1) dr += draw(o, p) * dxm1;
+      else dr *= (1.0 + push);
+      p->x[0] -= p->x[0] / rr * dr;
+      p->x[1] -= p->x[1] / rr * dr;
+      p->x[2] -= p->x[2] / rr * dr;
+      if (!ddmc_on_im1) {
+        leaked2imc = 1;
+        lorentz(o, p, 0);
+        bb_surface_dir(o, p);
+        double mu = (p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2]) / pr(p);
+        if (mu > 0.0) { p->D[0] = -p->D[0]; p->D[1] = -p->D[1]; p->D[2] = -p->D[2]; }
+        lorentz(o, p, 1);
+      }
+    } else {
+      p->ind++;
+      double rr = pr(p);
+      double dr = r_p - rr;
+      if (ddmc_on_ip1) dr += draw(o, p) * dxp1;
+      else dr *= (1.0 + push);
+      p->x[0] += p->x[0] / rr * dr;
+      p->x[1] += p->x[1] / rr * dr;
+      p->x[2] += p->x[2] / rr * dr;
+      if (!ddmc_on_ip1) {
+        leaked2imc = 1;
+        lorentz(o, p, 0);
+        bb_surface_dir(o, p);
+        double mu = (p->x[0] * p->D[0] + p->x[1] * p->D[1] + p->x[2] * p->D[2]) / pr(p);
+        if (mu < 0.0) { p->D[0] = -p->D[0]; p->D[1] = -p->D[1]; p->D[2] = -p->D[2]; }
+        lorentz(o, p, 1);
+      }
+    }
+  }
+  /* advection and adiabatic loss (discrete_diffusion.cpp:371-397) */
+  double zone_vel[3], dvds;
+  get_velocity(o, p->ind, p->x, p->D, zone_vel, &dvds);
+  double vel = sqrt(zone_vel[0] * zone_vel[0] + zone_vel[1] * zone_vel[1] + zone_vel[2] * zone_vel[2]);
+  double v_over_r = vel / pr(p);
+  double dlnrhodt = dvds + 2.0 * v_over_r;
+  double doppler_shift_ddmc = (1.0 - dlnrhodt * this_dt / 3.0);
+  lorentz(o, p, 0);
+  p->e *= doppler_shift_ddmc;
+  p->nu *= doppler_shift_ddmc;
+  lorentz(o, p, 1);
+  if (!leaked2imc) {
+    p->x[0] += zone_vel[0] * this_dt;
+    p->x[1] += zone_vel[1] * this_dt;
+    p->x[2] += zone_vel[2] * this_dt;
+  }
+  p->ind = get_zone(o, p->x);
+  if (p->ind == -1) fate = F_ABSORBED;
+  if (p->ind == -2) fate = F_ESCAPED;
+  return fate;
+}
+
 static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int64_t* nseg, int64_t* nscat,
                           int relocate)
 {
@@ -1093,12 +1343,32 @@ static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int
   int fate = F_MOVING;
   int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
   int64_t seg = 0;
+  /* discrete diffusion: the zone test before every pass (transport.cpp:
+   * 216-246, 272-286); the remaining time of one diffusion call */
+  int dd = (o->tp.use_ddmc == 2) && (o->gtype == SED_GRID_1D_SPHERE);
+  int in_call = 0;
+  double dt_remaining = 0;
   while (fate == F_MOVING) {
     if (seg++ >= limit) { fate = F_STOPPED; break; }
+    if (dd && in_ddmc_zone(o, p)) {
+      if (!in_call) { dt_remaining = tstop - p->t; in_call = 1; }
+      fate = ddmc_event(o, p, &dt_remaining, nscat);
+      continue;
+    }
+    in_call = 0;
     int iz = p->ind;
     double d_bn = 0;
     int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);
     double dshift = dshift_lab_to_comoving(o, p);
+    /* a diffusive neighbour (transport.cpp:295-309) */
+    int new_cell_ddmc = 0;
+    double sigma_new = 0, dr_new = 0;
+    if (dd && new_ind >= 0) {
+      double e_new;
+      opacity_of(o, new_ind, p->nu * dshift, &sigma_new, &e_new);
+      dr_new = zone_size(o, new_ind);
+      new_cell_ddmc = sigma_new * dr_new > o->tp.ddmc_tau;
+    }
     /* transport::get_opacity, transport_opacity.cpp:268-299 */
     double nu_cmf = p->nu * dshift;
     int i_nu = lg_locate_wb(&o->nu, nu_cmf);
@@ -1145,6 +1415,8 @@ static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int
       } else if (new_ind == -2) {
         if (o->tp.boundary_out_reflect) { p->D[0] *= -1; p->D[1] *= -1; p->D[2] *= -1; }
         else { p->ind = new_ind; fate = F_ESCAPED; }
+      } else if (dd && new_cell_ddmc && (new_ind != p->ind)) {
+        move_across(o, p, new_ind, sigma_new, dr_new);
       } else {
         p->ind = new_ind;
       }

@@ -52,6 +52,7 @@ class TransportParams(C.Structure):
         ("spec_mu", LocateGrid), ("spec_phi", LocateGrid),
         ("n_emit_radioactive", C.c_int64), ("force_rprocess_heating", C.c_int32), ("reserved3", C.c_int32),
         ("gamma_nu", LocateGrid),
+        ("use_ddmc", C.c_int32), ("reserved4", C.c_int32), ("ddmc_tau", C.c_double),
     ]
 
 

@@ -121,6 +121,9 @@ class Workload:
         tp.n_emit_radioactive = int(P.scalar("particles_n_emit_radioactive", int))
         tp.force_rprocess_heating = int(P.scalar("force_rprocess_heating", int))
         tp.gamma_nu = abi.locate_grid(keep, ng)
+        # discrete diffusion (transport_init.cpp:336-341)
+        tp.use_ddmc = int(P.scalar("transport_use_ddmc", int))
+        tp.ddmc_tau = float(P.scalar("transport_ddmc_tau_threshold")) if tp.use_ddmc else 0.0
         return tp
 
     def grid_struct(self, keep: abi.Keep) -> abi.Grid:
@@ -221,14 +224,16 @@ def lightbulb_grey(n_packets: int = 1_000_000, n_zones: int = 128, n_bins: int =
                     notes={"log_del": d, "v_max": 1e9, "t_days": 10.0})
 
 
-def time_dependent(base: str, n_initialize: int = 0, dt_days: float = 0.1, **kw) -> Workload:
+def time_dependent(base: str, n_initialize: int = 0, dt_days: float = 0.1, params: Optional[dict] = None,
+                   **kw) -> Workload:
     """The workload `base(**kw)` run time-dependently
     (transport_steady_iterate = 0): packets that reach the end of a step are
     carried to the next, the grid expands homologously between steps
     (`homologous_step`), and particles_n_initialize packets of the initial
-    radiation field (e_rad = a T^4) start in the census.  notes["dt"] is the
-    step (dt_days)."""
+    radiation field (e_rad = a T^4) start in the census; `params` are set
+    over the base's parameters.  notes["dt"] is the step (dt_days)."""
     w = globals()[base](**kw)
+    w.params.update(params or {})
     w.params["transport_steady_iterate"] = 0
     w.params["particles_n_initialize"] = int(n_initialize)
     w.params["particles_max_total"] = max(int(w.params.get("particles_max_total", 1e7)), 4 * int(n_initialize) + 1)

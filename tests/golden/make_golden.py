@@ -63,6 +63,20 @@ TD_CASES = {
     "replay_td_ia_radio": ("time_dependent", dict(base="type_ia", n_initialize=200, dt_days=0.5, n_packets=100,
                                                   n_zones=16, n_lines=5000, n_bins=256, n_levels_per_ion=6,
                                                   v_core=1e8, n_radioactive=300, t_days=60.0, seed=29), 3),
+    # discrete diffusion (transport_use_ddmc = 2) in the optically thick
+    # zones and frequencies, Monte Carlo elsewhere, interfaces both ways
+    "replay_td_ddmc_ia": ("time_dependent", dict(base="type_ia", n_initialize=200, dt_days=0.5,
+                                                 params={"transport_use_ddmc": 2,
+                                                         "transport_ddmc_tau_threshold": 3.0},
+                                                 n_packets=100, n_zones=16, n_lines=5000, n_bins=256,
+                                                 n_levels_per_ion=6, v_core=1e8, t_days=40.0, seed=31), 3),
+    # grey, every zone diffusive; the initial radiation field only (a central
+    # point source would put photons at r = 0, where the reference's
+    # diffusion step divides by r)
+    "replay_td_ddmc_grey": ("time_dependent", dict(base="lightbulb_grey", n_initialize=400, dt_days=0.1,
+                                                   params={"transport_use_ddmc": 2,
+                                                           "transport_ddmc_tau_threshold": 0.1},
+                                                   n_packets=0, n_zones=32, n_bins=64, radiative_eq=1, seed=7), 3),
 }
 TD_KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "pkt_type", "census_ind", "census_type", "census_state",
            "J_nu", "e_abs", "e_rad", "fr_rad", "spec_flux", "spec_click", "T_gas"]

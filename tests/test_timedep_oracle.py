@@ -31,7 +31,7 @@ def _rel(a, b):
     return float(np.max(np.abs(a[fin] - b[fin]) / s)) if s.size else 0.0
 
 
-@pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio"])
+@pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio", "replay_td_ddmc_ia", "replay_td_ddmc_grey"])
 def test_oracle_matches_reference_time_dependent_replay(name):
     ref, w, kw = load_td(name)
     steps = int(ref["steps"])
