@@ -2155,6 +2155,8 @@ int oracle_get_radioactive_tallies(oracle_ctx* o, double* L_emit, double* L_dep)
 int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
 {
   if (!o) return SED_ERR_ARG;
+  if (o->tp.use_ddmc != 0 && (o->tp.use_ddmc != 2 || o->gtype != SED_GRID_1D_SPHERE || !o->homologous))
+    return fail(o, SED_ERR_ARG, "discrete diffusion is built for method 2 on 1D spheres with homologous velocities");
   if (o->tp.n_emit_radioactive > 0 || o->n_census > 0 || !o->tp.steady_state) {
     if (!o->have_grid) return SED_ERR_STATE;
     if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");

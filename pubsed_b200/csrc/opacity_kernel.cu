@@ -14,7 +14,7 @@
 //                       opacity per frequency bin in the reference's order
 //                       (GasState::computeOpacity, GasState_opacities.cpp:11-136),
 //                       then the opacity cap, Planck/Rosseland means,
-//                       emissivity CDF (blocked prefix sum in a fixed order,
+//                       emissivity CDF (the reference's sequential prefix sum,
 //                       cdf_array::set_value), L_thermal, Fleck factor and
 //                       the packed tables the packet kernel reads.  The
 //                       zone's level populations are staged in shared memory
@@ -571,11 +571,10 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
   __syncthreads();
 
   // emissivity CDF: cdf_array::set_value prefix sum of emis*dnu (cdf_array.h:
-  // 53-75) and L_thermal = 4 pi sum(emis*dnu).  Blocked scan in a fixed
-  // order: each thread sums a contiguous run of bins, thread 0 scans the run
-  // totals, each run then adds its offset.  Non-negative terms, so every
-  // prefix is within a few ulp of the sequential sum; a NaN term propagates
-  // to the end of the CDF exactly as in the sequential sum.
+  // 53-75) and L_thermal = 4 pi sum(emis*dnu), in the reference's order so
+  // the FP64 CDF is the reference's to the bit (a bin's share, the difference
+  // of two neighbouring values, then is too): the terms in parallel, the two
+  // running sums by one thread (a few microseconds per zone)
   double* em = R2;
   double Lth = 0;
   if (nn == 1) {
@@ -585,32 +584,19 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
       em[0] = 1;
     }
   } else {
-    const int per = (nn + bd - 1) / bd;
-    const int j0 = min(nn, tid * per), j1 = min(nn, j0 + per);
-    double run = 0, Lp = 0;
-    for (int j = j0; j < j1; ++j) {
-      const double ednu = em[j] * loc_delta(A.nu, j);
-      run = (j == j0) ? ednu : run + ednu;
-      em[j] = run;
-      Lp += 4 * PI * ednu;
-    }
-    red[0][tid] = run;
-    red[1][tid] = Lp;
+    for (int j = tid; j < nn; j += bd) em[j] = em[j] * loc_delta(A.nu, j);
     __syncthreads();
     if (tid == 0) {
-      double acc = 0, Lacc = 0;
-      for (int t = 0; t < bd; ++t) {
-        const double v = red[0][t];
-        red[0][t] = acc;
-        acc = (t == 0) ? v : acc + v;
-        Lacc += red[1][t];
+      double run = 0, L = 0;
+      for (int j = 0; j < nn; ++j) {
+        const double ednu = em[j];
+        run = (j == 0) ? ednu : run + ednu;
+        em[j] = run;
+        L += 4 * PI * ednu;
       }
-      red[2][0] = Lacc;
+      red[2][0] = L;
     }
     __syncthreads();
-    const double off = red[0][tid];
-    if (tid > 0)
-      for (int j = j0; j < j1; ++j) em[j] = off + em[j];
     Lth = red[2][0];
   }
   __syncthreads();

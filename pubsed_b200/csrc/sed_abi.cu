@@ -126,6 +126,7 @@ StepArgs sed::make_step_args(sed_ctx* c, double dt, int64_t n_emit)
   }
   A.core_radius = c->tp.core_radius; A.core_freq = c->tp.core_photon_frequency; A.core_cdf = c->d_core_cdf.p;
   A.max_segments = c->tp.max_segments;
+  A.use_ddmc = c->tp.use_ddmc; A.ddmc_tau = c->tp.ddmc_tau;
   const size_t zone_smem = (size_t)5 * nz * sizeof(double);
   A.smem_zones = (zone_smem <= 64 * 1024) ? 1 : 0;
   A.nu = dev_loc(c->nu, c->d_nu); A.st = dev_loc(c->st, c->d_st); A.sn = dev_loc(c->sn, c->d_sn);
@@ -655,6 +656,9 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   if (n_census + n_radio + n_emit > c->tp.max_particles)
     return set_err(c, SED_ERR_CAPACITY, "Not enough particle space: %lld packets > particles_max_total %lld",
                    (long long)(n_census + n_radio + n_emit), (long long)c->tp.max_particles);
+  if (c->tp.use_ddmc != 0 && (c->tp.use_ddmc != 2 || c->gtype != SED_GRID_1D_SPHERE || !c->homologous))
+    return set_err(c, SED_ERR_ARG, "transport_use_ddmc %d: discrete diffusion is built for method 2 on 1D spheres "
+                   "with homologous velocities", (int)c->tp.use_ddmc);
   const int64_t n_q = n_census + n_radio;
   const int64_t n_all = n_emit + n_q;
   const bool gamma_phase = n_radio > 0 || (n_census > 0 && c->n_census_gamma > 0);
@@ -803,6 +807,8 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     stats->ms_total = ms + ms_opacity;
   }
   if (cnt[C_LIMIT] > 0) return set_err(c, SED_ERR_LIMIT, "%llu packets hit the segment limit", cnt[C_LIMIT]);
+  if (cnt[C_DDMC_CAP] > 0)
+    return set_err(c, SED_ERR_LIMIT, "%llu diffusion scatters found no new frequency bin", cnt[C_DDMC_CAP]);
   if (n_reject_cap > 0)
     return set_err(c, SED_ERR_LIMIT, "%d Compton scatters hit the rejection-sampling bound", (int)n_reject_cap);
   return SED_OK;

@@ -22,7 +22,7 @@ struct GridDev {
 struct BatchModel;
 
 // counters[] slots written by the packet kernel
-enum Counter { C_QUEUE = 0, C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT, C_COUNT };
+enum Counter { C_QUEUE = 0, C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT, C_DDMC_CAP, C_COUNT };
 
 struct StepArgs {
   int32_t steady, radiative_eq, bound_in_reflect, bound_out_reflect;
@@ -35,6 +35,8 @@ struct StepArgs {
   double core_radius, core_freq;
   const double* core_cdf;     // [n_nu] normalised core emission CDF
   int32_t max_segments;
+  int32_t use_ddmc;           // 2: discrete diffusion in diffusive zones (1D)
+  double ddmc_tau;            // transport_ddmc_tau_threshold
   int32_t smem_zones;         // 1: per-block shared-memory zone tallies
   int32_t n_rep;              // >0 (and smem_zones 0): zone-scalar tallies in n_rep global copies
   double* zone_rep;           // [n_rep][5][nz] e_abs, fx, fy, fz, fr copies, summed by the finish kernel

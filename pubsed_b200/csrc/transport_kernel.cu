@@ -487,7 +487,22 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 // gradient with respect to the (zone, band) absorption factors, where w is
 // the packet's escaping energy times d(loss)/d(its spectrum bin).
 // FAST (mixed form on a homologous grid): the division-free transforms above.
-template <int GRID, typename OT, typename CT, int BATCH, int MODE, bool FAST, int THREADS, int MINB>
+// discrete diffusion (1D spheres, FP64 expressions), defined with the
+// gamma-ray helpers below
+template <typename OT>
+__device__ bool ddmc_zone(const StepArgs& A, const GridDev& G, const OT* __restrict__ opac, Pkt& p);
+template <typename OT, typename CT>
+__device__ int ddmc_event(const StepArgs& A, const GridDev& G, const OT* __restrict__ opac, Pkt& p, PacketRng& rng,
+                          double& dt_remaining, double& acc_eabs, unsigned long long& n_scat,
+                          unsigned long long& n_cap);
+__device__ void ddmc_move_across(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng, int new_ind,
+                                 double sigma_i, double dr);
+template <typename OT>
+__device__ __forceinline__ int ddmc_opacity(const StepArgs& A, const OT* __restrict__ opac, int iz, double nu_cmf,
+                                            double* op, double* eps);
+
+// DD: discrete diffusion on (transport_use_ddmc = 2; 1D, FP64 expressions)
+template <int GRID, typename OT, typename CT, int BATCH, int MODE, bool FAST, int THREADS, int MINB, bool DD = false>
 __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs A, const GridDev G)
 {
   extern __shared__ double s_tal[];  // [5][nz] when A.smem_zones
@@ -545,6 +560,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   // tally when it leaves (the same terms, summed per visit first)
   int acc_zone = -1;
   double acc_eabs = 0, acc_fx = 0, acc_fy = 0, acc_fz = 0, acc_fr = 0;
+  // discrete diffusion: whether the last pass was a diffusion event (one
+  // call of discrete_diffuse_DDMC) and the time that call has left
+  bool dd_call = false;
+  double dd_rem = 0;
+  unsigned long long n_ddcap = 0;
   for (;;) {
     if (fate != MOVING) {
       if (have && MODE == 2) {
@@ -649,6 +669,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
           if (p.ind == -1) fate = ABSORBED;
           else if (p.ind == -2) fate = ESCAPED;
           seg = 0;
+          dd_call = false;
           acc_zone = -1;
           acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
           have = true;
@@ -680,6 +701,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       if (p.ind == -1) fate = ABSORBED;
       else if (p.ind == -2) fate = ESCAPED;
       seg = 0;
+      dd_call = false;
       acc_zone = -1;
       acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
       have = true;
@@ -703,6 +725,16 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         acc_zone = iz;
         acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
       }
+      if constexpr (DD) {
+        // transport::propagate's zone test (transport.cpp:216-246): a photon
+        // in a diffusive zone takes a diffusion event instead of a segment
+        if (ddmc_zone<OT>(A, G, opac, p)) {
+          if (!dd_call) { dd_rem = A.tstop - p.t; dd_call = true; }
+          fate = ddmc_event<OT, CT>(A, G, opac, p, rng, dd_rem, acc_eabs, n_scat, n_ddcap);
+          continue;
+        }
+        dd_call = false;
+      }
       double d_bn = 0;
       double rsq, xdotD;
       if (fast) {
@@ -721,6 +753,17 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         p.dvds = A.inv_t;
       } else {
         dshift = dshift_lab_to_comoving<GRID>(G, p);
+      }
+      // a diffusive neighbour (transport.cpp:295-309)
+      bool new_cell_ddmc = false;
+      double sigma_new = 0, dr_new = 0;
+      if constexpr (DD) {
+        if (new_ind >= 0) {
+          double e_new;
+          ddmc_opacity<OT>(A, opac, new_ind, p.nu * dshift, &sigma_new, &e_new);
+          dr_new = loc_delta(G.r_out, new_ind);
+          new_cell_ddmc = sigma_new * dr_new > A.ddmc_tau;
+        }
       }
       // transport::get_opacity (transport_opacity.cpp:268-299)
       const double nu_cmf = p.nu * dshift;
@@ -817,6 +860,8 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         } else if (new_ind == -2) {
           if (A.bound_out_reflect) { p.D[0] *= -1; p.D[1] *= -1; p.D[2] *= -1; }
           else { p.ind = new_ind; fate = ESCAPED; }
+        } else if (DD && new_cell_ddmc && new_ind != p.ind) {
+          ddmc_move_across(A, G, p, rng, new_ind, sigma_new, dr_new);
         } else {
           p.ind = new_ind;
         }
@@ -849,6 +894,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   // counters: warp reduction, one atomic per warp
   n_esc = warp_sum(n_esc); n_abs = warp_sum(n_abs); n_stop = warp_sum(n_stop);
   n_seg = warp_sum(n_seg); n_scat = warp_sum(n_scat); n_lim = warp_sum(n_lim);
+  if constexpr (DD) n_ddcap = warp_sum(n_ddcap);
   if ((threadIdx.x & 31) == 0) {
     if (n_esc) atomicAdd(A.counters + C_ESCAPED, n_esc);
     if (n_abs) atomicAdd(A.counters + C_ABSORBED, n_abs);
@@ -856,6 +902,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
     if (n_seg) atomicAdd(A.counters + C_SEGMENTS, n_seg);
     if (n_scat) atomicAdd(A.counters + C_SCATTERS, n_scat);
     if (n_lim) atomicAdd(A.counters + C_LIMIT, n_lim);
+    if (n_ddcap) atomicAdd(A.counters + C_DDMC_CAP, n_ddcap);
   }
   if (MODE != 2 && A.smem_zones) {
     __syncthreads();
@@ -1051,6 +1098,269 @@ __device__ __forceinline__ void sample_optical_nu(const StepArgs& A, Pkt& p, Pac
 {
   const int inu = (A.nu.n == 1) ? 0 : cdf_row_sample<CT>(A, p.ind, rng.next());
   p.nu = loc_sample(A.nu, inu, rng.next());
+}
+
+// ------------------------------------------------------------ discrete diffusion
+// transport_use_ddmc = 2 (src/transport/discrete_diffusion.cpp:114-510), on
+// 1D spheres with the reference's FP64 expressions.
+
+// transport::get_opacity of zone iz at comoving frequency nu_cmf
+template <typename OT>
+__device__ __forceinline__ int ddmc_opacity(const StepArgs& A, const OT* __restrict__ opac, int iz, double nu_cmf,
+                                            double* op, double* eps)
+{
+  const int nn = A.nu.n;
+  const int i_nu = loc_within_fast<false>(A.nu, nu_cmf);
+  const OT ab = opac[(size_t)iz * nn + i_nu];
+  const double a_opac = (double)ab.x;
+  const double s_opac = A.omit_scat ? 0.0 : (double)ab.y;
+  *op = a_opac + s_opac;
+  *eps = (*op == 0) ? 0 : a_opac / *op;
+  return i_nu;
+}
+
+__device__ __forceinline__ double pkt_r(const Pkt& p)
+{
+  return sqrt(p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+}
+
+// the zone test of transport::propagate (transport.cpp:219-231)
+template <typename OT>
+__device__ bool ddmc_zone(const StepArgs& A, const GridDev& G, const OT* __restrict__ opac, Pkt& p)
+{
+  const double dshift = dshift_lab_to_comoving<0>(G, p);
+  double sigma, eps;
+  ddmc_opacity<OT>(A, opac, p.ind, p.nu * dshift, &sigma, &eps);
+  return sigma * loc_delta(G.r_out, p.ind) > A.ddmc_tau;
+}
+
+// transport::sample_dir_from_blackbody_surface (discrete_diffusion.cpp:753-794)
+__device__ void bb_surface_dir(PacketRng& rng, Pkt& p)
+{
+  const double mu = sqrt(rng.next());
+  const double phi = 2.0 * PI * rng.next();
+  const double smu = sqrt(1.0 - mu * mu);
+  const double v1 = smu * cos(phi), v2 = smu * sin(phi), v3 = mu;
+  const double r1 = p.x[0] / pkt_r(p), r2 = p.x[1] / pkt_r(p), r3 = p.x[2] / pkt_r(p);
+  const double costheta = r3, sintheta = sqrt(1 - costheta * costheta);
+  const double v1p = v1 * costheta + r1 * v3 * sintheta - r2 * (1.0 - costheta) * (-r2 * v1 + r1 * v2);
+  const double v2p = v2 * costheta + r2 * v3 * sintheta - r1 * (1.0 - costheta) * (-r2 * v1 + r1 * v2);
+  const double v3p = v3 * costheta - (r1 * v1 + r2 * v2) * sintheta;
+  const double norm = sqrt(v1p * v1p + v2p * v2p + v3p * v3p);
+  p.D[0] = v1p / norm;
+  p.D[1] = v2p / norm;
+  p.D[2] = v3p / norm;
+}
+
+// transport::move_across_DDMC_interface (discrete_diffusion.cpp:413-510):
+// the photon converts to the diffusive zone new_ind (and stays in the
+// comoving frame, as the reference leaves it) or is put back next to the
+// interface with a direction away from it
+__device__ void ddmc_move_across(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng, int new_ind,
+                                 double sigma_i, double dr)
+{
+  const int nz = G.nzones;
+  int ip = p.ind + 1, im = p.ind - 1;
+  if (ip == nz) ip = p.ind;
+  if (im < 0) im = 0;
+  const double r_p = __ldg(G.r_out.right + p.ind);
+  double r_m = __ldg(G.r_out.right + im);
+  if (p.ind == 0) r_m = G.r_out.min;
+  double r_interface = 0;
+  if (new_ind == ip) r_interface = r_p;
+  else if (new_ind == im) r_interface = r_m;
+  lorentz_transform<0>(G, p, 0);
+  const double rr = pkt_r(p);
+  double mu = (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / rr;
+  mu = fabs(mu);
+  const double p_convert = 4.0 * (1.0 + 1.5 * mu) / (3.0 * sigma_i * dr + 6.0 * 0.7104);
+  const double xi = rng.next();
+  const double u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+  const double push = 1.0e-8;
+  if (xi <= p_convert) {
+    p.ind = new_ind;
+    sample_in_zone<0>(G, p.ind, u0, u1, u2, p.x);
+    return;
+  }
+  sample_in_zone<0>(G, p.ind, u0, u1, u2, p.x);
+  if (new_ind == ip) {
+    double d = r_interface - pkt_r(p);
+    d *= (1.0 - push);
+    p.x[0] += p.x[0] / pkt_r(p) * d;  // the radius is taken again after each coordinate moves
+    p.x[1] += p.x[1] / pkt_r(p) * d;
+    p.x[2] += p.x[2] / pkt_r(p) * d;
+  } else if (new_ind == im) {
+    double d = pkt_r(p) - r_interface;
+    d *= (1.0 - push);
+    p.x[0] -= p.x[0] / pkt_r(p) * d;
+    p.x[1] -= p.x[1] / pkt_r(p) * d;
+    p.x[2] -= p.x[2] / pkt_r(p) * d;
+  }
+  bb_surface_dir(rng, p);
+  const double mu2 = (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / pkt_r(p);
+  if ((new_ind == ip && mu2 > 0.0) || (new_ind == im && mu2 < 0.0)) {
+    p.D[0] = -p.D[0]; p.D[1] = -p.D[1]; p.D[2] = -p.D[2];
+  }
+  lorentz_transform<0>(G, p, 1);
+}
+
+// One pass of the event loop of transport::discrete_diffuse_DDMC
+// (discrete_diffusion.cpp:136-404): leakage to a neighbour, effective
+// (inelastic) scattering, or the end of the step, then advection and the
+// adiabatic loss.  dt_remaining carries over the passes of one call; the
+// zone's J (bin 0, as the reference tallies it) and e_abs are tallied.  The
+// effective-scattering loop, unbounded in the reference, gives up after
+// 65536 re-emissions that stay in the same bin (counted).
+template <typename OT, typename CT>
+__device__ int ddmc_event(const StepArgs& A, const GridDev& G, const OT* __restrict__ opac, Pkt& p, PacketRng& rng,
+                          double& dt_remaining, double& acc_eabs, unsigned long long& n_scat,
+                          unsigned long long& n_cap)
+{
+  const int nz = G.nzones, nn = A.nu.n;
+  const int nj = A.store_Jnu ? nn : 1;
+  const double lambda_ddmc = 0.7104, push = 1.0e-8;
+  int fate = MOVING;
+  const int ii = p.ind;
+  int ip = ii + 1, im = ii - 1;
+  if (ip == nz) ip = ii;
+  if (im < 0) im = 0;
+  const double dx = loc_delta(G.r_out, ii), dxp1 = loc_delta(G.r_out, ip), dxm1 = loc_delta(G.r_out, im);
+  double dshift = dshift_lab_to_comoving<0>(G, p);
+  double sigma_i, eps_i, sigma_ip1, eps_ip1, sigma_im1, eps_im1;
+  int i_nu = ddmc_opacity<OT>(A, opac, ii, p.nu * dshift, &sigma_i, &eps_i);
+  ddmc_opacity<OT>(A, opac, ip, p.nu * dshift, &sigma_ip1, &eps_ip1);
+  ddmc_opacity<OT>(A, opac, im, p.nu * dshift, &sigma_im1, &eps_im1);
+  const double r_p = __ldg(G.r_out.right + ii);
+  double r_m = __ldg(G.r_out.right + im);
+  if (ii == 0) r_m = G.r_out.min;
+  const double r_0 = 0.5 * (r_p + r_m);
+  const double Xi = 1.0 + dx * dx / (12.0 * r_0 * r_0);
+  double geo_factor = r_m * r_m / r_0 / r_0 / Xi;
+  const double tau_im1 = sigma_im1 * dxm1;
+  const bool ddmc_on_im1 = !(tau_im1 <= A.ddmc_tau);
+  double sigma_leak_left;
+  if (ddmc_on_im1) sigma_leak_left = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + sigma_im1 * dxm1)) * geo_factor;
+  else sigma_leak_left = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + 2.0 * lambda_ddmc)) * geo_factor;
+  geo_factor = r_p * r_p / r_0 / r_0 / Xi;
+  const double tau_ip1 = sigma_ip1 * dxp1;
+  const bool ddmc_on_ip1 = !(tau_ip1 <= A.ddmc_tau);
+  double sigma_leak_right;
+  if (ddmc_on_ip1) sigma_leak_right = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + sigma_ip1 * dxp1)) * geo_factor;
+  else sigma_leak_right = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + 2.0 * lambda_ddmc)) * geo_factor;
+  if (ip == ii) sigma_leak_right = (2.0 / 3.0 / dx) * (1.0 / (sigma_i * dx + 2.0 * lambda_ddmc)) * geo_factor;
+  if (ii == 0) sigma_leak_left = 0.0;
+  const double sigma_leak_tot = sigma_leak_left + sigma_leak_right;
+  const double xi = rng.next();
+  bool leaked2imc = false;
+  const double d_stay = C_LIGHT * dt_remaining;
+  const double d_leak = -log(xi) / (sigma_leak_left + sigma_leak_right);
+  double d_sc;
+  if (nn == 1) d_sc = INFINITY;
+  else {
+    const double tau_r = -1.0 * log(rng.next());
+    if (eps_i > 0.0) {
+      double k_es_inelastic = sigma_i * eps_i;
+      dshift = dshift_lab_to_comoving<0>(G, p);
+      i_nu = ddmc_opacity<OT>(A, opac, p.ind, p.nu * dshift, &sigma_i, &eps_i);
+      // emissivity_[zone].get_value(i_nu): the bin's share of the CDF
+      const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
+      const double elastic_frac = (i_nu == 0) ? (double)row[0] : (double)(row[i_nu] - row[i_nu - 1]);
+      k_es_inelastic *= 1.0 - elastic_frac;
+      d_sc = tau_r / k_es_inelastic;
+    } else {
+      d_sc = INFINITY;
+    }
+  }
+  int event;
+  double this_d;
+  if ((d_sc < d_leak) && (d_sc < d_stay)) { event = 0; this_d = d_sc; }
+  else if (d_leak < d_stay) { event = 1; this_d = d_leak; }
+  else { event = 2; this_d = d_stay; }
+  const double this_dt = this_d / C_LIGHT;
+  p.t += this_dt;
+  dt_remaining -= this_dt;
+  atomicAdd(A.J + (size_t)p.ind * nj, p.e * this_d);
+  acc_eabs += (p.e * dshift) * this_d * sigma_i * eps_i;
+  if (event == 0) {
+    ++n_scat;
+    int now_i_nu = i_nu;
+    for (int tries = 0; now_i_nu == i_nu; ++tries) {
+      if (tries >= (1 << 16)) { ++n_cap; break; }
+      // do_scatter(p, 1.0) (scatter.cpp:12-41): never coherent
+      fate = MOVING;
+      if (rng.next() > 1.0) {
+        isotropic_scatter<0, CT>(A, G, p, rng, 0);
+      } else {
+        const double z2 = rng.next();
+        if ((z2 > __ldg(A.eps_imc + p.ind)) || A.radiative_eq) isotropic_scatter<0, CT>(A, G, p, rng, 1);
+        else fate = ABSORBED;
+      }
+      dshift = dshift_lab_to_comoving<0>(G, p);
+      double s2, e2;
+      now_i_nu = ddmc_opacity<OT>(A, opac, p.ind, p.nu * dshift, &s2, &e2);
+    }
+  } else if (event == 2) {
+    dt_remaining = -1.0;
+    fate = STOPPED;
+  } else {
+    const double P_leak_left = sigma_leak_left / sigma_leak_tot;
+    const double xi2 = rng.next();
+    if (xi2 <= P_leak_left) {
+      p.ind--;
+      const double rr = pkt_r(p);
+      double dr = rr - r_m;
+      if (ddmc_on_im1) dr += rng.next() * dxm1;
+      else dr *= (1.0 + push);
+      p.x[0] -= p.x[0] / rr * dr;
+      p.x[1] -= p.x[1] / rr * dr;
+      p.x[2] -= p.x[2] / rr * dr;
+      if (!ddmc_on_im1) {
+        leaked2imc = true;
+        lorentz_transform<0>(G, p, 0);
+        bb_surface_dir(rng, p);
+        const double mu = (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / pkt_r(p);
+        if (mu > 0.0) { p.D[0] = -p.D[0]; p.D[1] = -p.D[1]; p.D[2] = -p.D[2]; }
+        lorentz_transform<0>(G, p, 1);
+      }
+    } else {
+      p.ind++;
+      const double rr = pkt_r(p);
+      double dr = r_p - rr;
+      if (ddmc_on_ip1) dr += rng.next() * dxp1;
+      else dr *= (1.0 + push);
+      p.x[0] += p.x[0] / rr * dr;
+      p.x[1] += p.x[1] / rr * dr;
+      p.x[2] += p.x[2] / rr * dr;
+      if (!ddmc_on_ip1) {
+        leaked2imc = true;
+        lorentz_transform<0>(G, p, 0);
+        bb_surface_dir(rng, p);
+        const double mu = (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / pkt_r(p);
+        if (mu < 0.0) { p.D[0] = -p.D[0]; p.D[1] = -p.D[1]; p.D[2] = -p.D[2]; }
+        lorentz_transform<0>(G, p, 1);
+      }
+    }
+  }
+  // advection and the adiabatic loss (discrete_diffusion.cpp:371-397)
+  double zone_vel[3], dvds;
+  get_velocity<0>(G, p.ind, p.x, p.D, zone_vel, &dvds);
+  const double vel = sqrt(zone_vel[0] * zone_vel[0] + zone_vel[1] * zone_vel[1] + zone_vel[2] * zone_vel[2]);
+  const double v_over_r = vel / pkt_r(p);
+  const double dlnrhodt = dvds + 2.0 * v_over_r;
+  const double doppler_shift_ddmc = (1.0 - dlnrhodt * this_dt / 3.0);
+  lorentz_transform<0>(G, p, 0);
+  p.e *= doppler_shift_ddmc;
+  p.nu *= doppler_shift_ddmc;
+  lorentz_transform<0>(G, p, 1);
+  if (!leaked2imc) {
+    p.x[0] += zone_vel[0] * this_dt;
+    p.x[1] += zone_vel[1] * this_dt;
+    p.x[2] += zone_vel[2] * this_dt;
+  }
+  p.ind = get_zone<0>(G, p.x);
+  if (p.ind == -1) fate = ABSORBED;
+  if (p.ind == -2) fate = ESCAPED;
+  return fate;
 }
 
 // Radioactive packets: emission (transport::emit_radioactive, emission.cpp:
@@ -1410,12 +1720,12 @@ __global__ void init_particles_kernel(const InitArgs I, const GridDev G)
 }
 
 template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB, int MODE = 0,
-          bool FAST = (sizeof(OT) == sizeof(float2))>
+          bool FAST = (sizeof(OT) == sizeof(float2)), bool DD = false>
 int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
                     cudaStream_t s)
 {
   const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
-  auto kern = propagate_kernel<GRID, OT, CT, BATCH, MODE, FAST, THREADS, MINB>;
+  auto kern = propagate_kernel<GRID, OT, CT, BATCH, MODE, FAST, THREADS, MINB, DD>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
@@ -1435,6 +1745,10 @@ int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int 
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
+  // discrete diffusion (1D, homologous): the reference's expressions in both forms
+  if constexpr (GRID == 0) {
+    if (a.use_ddmc == 2) return launch_kernel_t<0, OT, CT, 0, 256, 4, 0, false, true>(a, g, 0, num_sms, a.n_packets, s);
+  }
   // mixed tables on a grid with a tabulated velocity field: the reference's
   // expressions (the division-free transforms assume v = x / t)
   if (sizeof(OT) == sizeof(float2) && !g.homologous)
