@@ -90,8 +90,8 @@ typedef struct sed_transport_params {
                                     spec_time, spec_mu, spec_phi); n = 0: one catch-all bin.
                                     The reference passes spectrum_nu_grid here
                                     (transport_init.cpp:170-173), not gamma_nu_grid */
-  /* discrete diffusion in optically thick zones (1D spheres, homologous
-   * velocities): transport_use_ddmc (0 off, 2 DDMC, Densmore et al. 2007,
+  /* discrete diffusion in optically thick zones (1D spheres):
+   * transport_use_ddmc (0 off, 2 DDMC, Densmore et al. 2007,
    * src/transport/discrete_diffusion.cpp:114-404) and
    * transport_ddmc_tau_threshold: a zone is diffusive for a photon when its
    * total opacity at the photon's comoving frequency times the zone width

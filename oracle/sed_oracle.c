@@ -904,6 +904,9 @@ static void get_velocity(const oracle_ctx* o, int i, const double* x, const doub
     return;
   }
   if (o->gtype == SED_GRID_1D_SPHERE) {
+    /* a diffusion leak past the outer wall leaves the index one past the
+     * grid; the last zone's velocity field is used there */
+    if (i >= o->nzones) i = o->nzones - 1;
     double rr = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
     double v_0, r_0;
     if (i == 0) { v_0 = 0; r_0 = o->r_out.min; }
@@ -2155,8 +2158,8 @@ int oracle_get_radioactive_tallies(oracle_ctx* o, double* L_emit, double* L_dep)
 int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
 {
   if (!o) return SED_ERR_ARG;
-  if (o->tp.use_ddmc != 0 && (o->tp.use_ddmc != 2 || o->gtype != SED_GRID_1D_SPHERE || !o->homologous))
-    return fail(o, SED_ERR_ARG, "discrete diffusion is built for method 2 on 1D spheres with homologous velocities");
+  if (o->tp.use_ddmc != 0 && (o->tp.use_ddmc != 2 || o->gtype != SED_GRID_1D_SPHERE))
+    return fail(o, SED_ERR_ARG, "discrete diffusion is built for method 2 on 1D spheres");
   if (o->tp.n_emit_radioactive > 0 || o->n_census > 0 || !o->tp.steady_state) {
     if (!o->have_grid) return SED_ERR_STATE;
     if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");

@@ -656,9 +656,9 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   if (n_census + n_radio + n_emit > c->tp.max_particles)
     return set_err(c, SED_ERR_CAPACITY, "Not enough particle space: %lld packets > particles_max_total %lld",
                    (long long)(n_census + n_radio + n_emit), (long long)c->tp.max_particles);
-  if (c->tp.use_ddmc != 0 && (c->tp.use_ddmc != 2 || c->gtype != SED_GRID_1D_SPHERE || !c->homologous))
-    return set_err(c, SED_ERR_ARG, "transport_use_ddmc %d: discrete diffusion is built for method 2 on 1D spheres "
-                   "with homologous velocities", (int)c->tp.use_ddmc);
+  if (c->tp.use_ddmc != 0 && (c->tp.use_ddmc != 2 || c->gtype != SED_GRID_1D_SPHERE))
+    return set_err(c, SED_ERR_ARG, "transport_use_ddmc %d: discrete diffusion is built for method 2 on 1D spheres",
+                   (int)c->tp.use_ddmc);
   const int64_t n_q = n_census + n_radio;
   const int64_t n_all = n_emit + n_q;
   const bool gamma_phase = n_radio > 0 || (n_census > 0 && c->n_census_gamma > 0);

@@ -122,6 +122,10 @@ __device__ __forceinline__ void get_velocity(const GridDev& G, int i, const doub
     return;
   }
   if constexpr (GRID == 0) {
+    // a diffusion leak past the outer wall leaves the zone index one past
+    // the grid (discrete_diffusion.cpp:324-328), where the reference reads
+    // past its zone array; the last zone's velocity field is used instead
+    if (i >= G.nzones) i = G.nzones - 1;
     const double rr = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
     double v_0, r_0;
     if (i == 0) { v_0 = 0; r_0 = G.r_out.min; }
@@ -1745,7 +1749,7 @@ int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int 
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
-  // discrete diffusion (1D, homologous): the reference's expressions in both forms
+  // discrete diffusion (1D): the reference's expressions in both forms
   if constexpr (GRID == 0) {
     if (a.use_ddmc == 2) return launch_kernel_t<0, OT, CT, 0, 256, 4, 0, false, true>(a, g, 0, num_sms, a.n_packets, s);
   }

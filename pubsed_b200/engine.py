@@ -87,6 +87,15 @@ class Engine:
                     "sed_get_zone_tallies")
         return out
 
+    def initialize_particles(self, n: int, e_rad) -> None:
+        """sed_initialize_particles: n packets of the radiation field e_rad."""
+        e = np.ascontiguousarray(e_rad, dtype=np.float64)
+        self._check(self.L.sed_initialize_particles(self.ctx, int(n), e.ctypes.data_as(abi._dp)),
+                    "sed_initialize_particles")
+
+    def n_particles(self) -> int:
+        return int(self.L.sed_n_particles(self.ctx))
+
     def set_emission(self, core_n_emit: float, n_emit_radioactive: int):
         """sed_set_emission: packet counts of the following steps."""
         self._check(self.L.sed_set_emission(self.ctx, float(core_n_emit), int(n_emit_radioactive)), "sed_set_emission")

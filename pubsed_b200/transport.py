@@ -36,6 +36,11 @@ class Transport:
         self.radio = None
         self.n_unsolved = 0
         self.last_stats = None
+        # transport::init ends with initialize_particles (transport_init.cpp:376-379)
+        n_init = int(self.P.scalar("particles_n_initialize", int))
+        if n_init > 0:
+            from .workloads import initial_e_rad
+            self.eng.initialize_particles(n_init, initial_e_rad(workload.zones))
 
     def emission_counts(self, dt: float, last_iteration: bool) -> tuple:
         """Packet counts of a step: emit_radioactive scales its count by
@@ -74,7 +79,8 @@ class Transport:
         return st
 
     def n_particles(self) -> int:
-        return 0  # every packet of a step finishes within the step (steady state or escape/absorption)
+        """transport::n_particles: packets carried to the next step."""
+        return self.eng.n_particles()
 
     def output_spectrum(self, it: int, outdir: str = ".") -> Optional[str]:
         """transport::output_spectrum(it) (src/transport/transport_output.cpp:
@@ -127,4 +133,51 @@ def run_steady(workload, outdir: str = ".", precision: int = abi.PREC_FP64, devi
         tr.step(1.0, last_iteration=(it == n_iter))
         tr.output_spectrum(it, outdir)
         tr.write_plotfile(it, workload.zones.t_now, outdir)
+    return tr
+
+
+def run_time_dependent(workload, outdir: Optional[str] = ".", precision: int = abi.PREC_FP64, device: int = 0,
+                       on_write=None) -> Transport:
+    """The reference driver's time loop (SedonaClass::evolve_system,
+    src/main/SedonaClass.cpp:300-414) for a time-dependent run: per step the
+    step size (tstep_max_dt, at most tstep_max_delta of the time once t > 0,
+    at least tstep_min_dt), the homologous hydro step when hydro_module is
+    "homologous", the transport step, and every output_write_plt_file_time a
+    plot file and spectrum (with outdir) at t + dt; the loop ends after the
+    step that starts beyond tstep_time_stop or after tstep_max_steps steps.
+    on_write(i_write, t_write, transport) is called at each write."""
+    from . import workloads as wl
+    P = workload.P
+    n_steps = int(P.scalar("tstep_max_steps", int))
+    t_stop = P.scalar("tstep_time_stop")
+    dt_max, dt_min, dt_del = P.scalar("tstep_max_dt"), P.scalar("tstep_min_dt"), P.scalar("tstep_max_delta")
+    write_step = P.scalar("output_write_plt_file_time")
+    write_log = P.scalar("output_write_plt_log_space")
+    hydro = P.get("hydro_module") == "homologous"
+    tr = Transport(workload, precision=precision, device=device)
+    t = workload.zones.t_now
+    next_write = t
+    i_write = 0
+    for _ in range(n_steps):
+        dt = dt_max
+        if dt_del > 0 and t > 0 and dt > t * dt_del:
+            dt = t * dt_del
+        if dt < dt_min:
+            dt = dt_min
+        if hydro:
+            wl.homologous_step(workload.zones, dt)
+        tr.step(dt)
+        if t >= next_write:
+            t_write = t + dt
+            if outdir is not None:
+                if workload.zones.type == abi.GRID_1D_SPHERE:
+                    tr.write_plotfile(i_write + 1, t_write, outdir)
+                tr.output_spectrum(i_write + 1, outdir)
+            if on_write is not None:
+                on_write(i_write + 1, t_write, tr)
+            next_write = next_write * (1.0 + write_log) if (write_log > 0 and i_write > 0) else next_write + write_step
+            i_write += 1
+        if t > t_stop:
+            break
+        t += dt
     return tr

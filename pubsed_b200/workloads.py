@@ -242,6 +242,38 @@ def time_dependent(base: str, n_initialize: int = 0, dt_days: float = 0.1, param
     return w
 
 
+def diffusing_pulse(n_initialize: int = 100_000, seed: int = 0, method: int = 2) -> Workload:
+    """The reference's diffusing-pulse test (tests/diffusing_pulse/1D_ddmc;
+    model from tests/diffusing_pulse/models/make_mod.py): a static 1D sphere
+    ("standard" model, v = 0, hydro "none"), 200 zones of 0.5 cm out to
+    100 cm, rho = 1 g/cm^3, T = 1e4 K inside r < 5 cm and 0 outside, one
+    species 1.1, grey opacity 1 cm^2/g with epsilon = 0 (pure scattering),
+    one frequency bin, 1e5 packets of the initial radiation field and no
+    other source; discrete diffusion (method 2) above zone optical depth
+    0.1; steps of at most 5e-10 s growing by at most 10% of the time (the
+    default tstep_max_delta: the test's own "tstel_max_delta" is a typo the
+    defaults shadow) to 1e-8 s, plot files every 5e-10 s.  Its check: at the
+    6th, 12th and 18th plot file T_rad within 10% (mean) of the diffusion
+    solution of a pulse at r0 = 2.5 cm with D = c / (3 rho kappa)."""
+    n, dr = 200, 1.0e2 / 200
+    r_out = np.array([(i + 1) * dr for i in range(n)])
+    T = np.array([1e4 if (i + 1) * dr < 5.0 else 0.0 for i in range(n)])
+    z = ZoneModel(type=abi.GRID_1D_SPHERE, t_now=0.0, rho=np.ones(n), T=T, X=np.ones((n, 1)),
+                  elem_Z=np.array([1], np.int32), elem_A=np.array([1], np.int32), vol=shell_volumes(0.0, r_out),
+                  homologous=0, r_min=0.0, r_out=r_out, v=np.zeros(n))
+    params = {
+        "grid_type": "grid_1D_sphere", "hydro_module": "none",
+        "tstep_max_steps": 1000, "tstep_time_stop": 1e-8, "tstep_max_dt": 5e-10, "tstep_min_dt": 0.0,
+        "particles_n_initialize": int(n_initialize), "transport_use_ddmc": int(method),
+        "transport_ddmc_tau_threshold": 0.1, "transport_steady_iterate": 0,
+        "opacity_grey_opacity": 1.0, "opacity_epsilon": 0.0,
+        "output_write_plt_file_time": 5e-10, "spectrum_time_grid": [0, 1e-9, 1e-7],
+        "transport_fix_rng_seed": 1, "transport_rng_seed": int(seed),
+        "particles_max_total": 4 * int(n_initialize),
+    }
+    return Workload("diffusing_pulse_1d", params, z, notes={"r0": 2.5, "rho": 1.0, "kappa": 1.0})
+
+
 def initial_e_rad(zones: ZoneModel) -> np.ndarray:
     """Zone radiation energy density of a model without an erad column:
     a T_gas^4 (grid_1D_sphere.cpp:354, :130)."""
