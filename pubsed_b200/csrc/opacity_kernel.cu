@@ -14,8 +14,9 @@
 //                       opacity per frequency bin in the reference's order
 //                       (GasState::computeOpacity, GasState_opacities.cpp:11-136),
 //                       then the opacity cap, Planck/Rosseland means,
-//                       emissivity CDF (the reference's sequential prefix sum,
-//                       cdf_array::set_value), L_thermal, Fleck factor and
+//                       emissivity CDF (cdf_array::set_value prefix sum, in
+//                       the reference's order for FP64 grids up to 65536
+//                       zones), L_thermal, Fleck factor and
 //                       the packed tables the packet kernel reads.  The
 //                       zone's level populations are staged in shared memory
 //                       with their reciprocals, so a line costs two
@@ -571,10 +572,16 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
   __syncthreads();
 
   // emissivity CDF: cdf_array::set_value prefix sum of emis*dnu (cdf_array.h:
-  // 53-75) and L_thermal = 4 pi sum(emis*dnu), in the reference's order so
-  // the FP64 CDF is the reference's to the bit (a bin's share, the difference
-  // of two neighbouring values, then is too): the terms in parallel, the two
-  // running sums by one thread (a few microseconds per zone)
+  // 53-75) and L_thermal = 4 pi sum(emis*dnu).  FP64 tables of grids up to
+  // 65536 zones: in the reference's order, so the CDF is the reference's sum
+  // to the bit (and a bin's share of it, the difference of two neighbouring
+  // values, too): the terms in parallel, the running sums by one thread, a
+  // few microseconds per zone.  Otherwise (FP32 tables, or millions of zones
+  // where a serial row per CTA would dominate the build) a blocked scan in a
+  // fixed order: each thread sums a contiguous run of bins, thread 0 scans
+  // the run totals, each run adds its offset; non-negative terms, so every
+  // prefix is within a few ulp of the sequential sum, and a NaN term
+  // propagates to the end as in the sequential sum.
   double* em = R2;
   double Lth = 0;
   if (nn == 1) {
@@ -583,7 +590,7 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
       Lth += 4 * PI * ab_r[0] * bb_int;
       em[0] = 1;
     }
-  } else {
+  } else if (!MIXED && A.seq_cdf) {
     for (int j = tid; j < nn; j += bd) em[j] = em[j] * loc_delta(A.nu, j);
     __syncthreads();
     if (tid == 0) {
@@ -597,6 +604,34 @@ __global__ void __launch_bounds__(256) zone_opacity_kernel(const OpacityArgs A)
       red[2][0] = L;
     }
     __syncthreads();
+    Lth = red[2][0];
+  } else {
+    const int per = (nn + bd - 1) / bd;
+    const int j0 = min(nn, tid * per), j1 = min(nn, j0 + per);
+    double run = 0, Lp = 0;
+    for (int j = j0; j < j1; ++j) {
+      const double ednu = em[j] * loc_delta(A.nu, j);
+      run = (j == j0) ? ednu : run + ednu;
+      em[j] = run;
+      Lp += 4 * PI * ednu;
+    }
+    red[0][tid] = run;
+    red[1][tid] = Lp;
+    __syncthreads();
+    if (tid == 0) {
+      double acc = 0, Lacc = 0;
+      for (int t = 0; t < bd; ++t) {
+        const double v = red[0][t];
+        red[0][t] = acc;
+        acc = (t == 0) ? v : acc + v;
+        Lacc += red[1][t];
+      }
+      red[2][0] = Lacc;
+    }
+    __syncthreads();
+    const double off = red[0][tid];
+    if (tid > 0)
+      for (int j = j0; j < j1; ++j) em[j] = off + em[j];
     Lth = red[2][0];
   }
   __syncthreads();

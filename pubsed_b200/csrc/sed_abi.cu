@@ -467,6 +467,7 @@ int sed::enqueue_opacity(sed_ctx* c, double dt)
   if (c->tp.steady_state) dt = 1;
   OpacityArgs A{};
   A.nzones = c->nz; A.n_nu = c->nu.n(); A.nelem = c->nelem;
+  A.seq_cdf = (c->nz <= 65536) ? 1 : 0;
   A.use_es = c->op.use_electron_scattering; A.use_ff = c->op.use_free_free; A.use_bf = c->op.use_bound_free;
   A.use_line = c->op.use_line_expansion; A.use_fuzz = c->op.use_fuzz_expansion;
   A.radiative_eq = c->tp.radiative_eq; A.omit_scat = c->tp.omit_scattering; A.precision = c->tp.precision;

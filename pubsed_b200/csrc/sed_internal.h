@@ -210,6 +210,7 @@ int launch_temperature(const TemperatureArgs& a, cudaStream_t s);
 // ---------------------------------------------------------------- opacity
 struct OpacityArgs {
   int32_t nzones, n_nu, nelem;
+  int32_t seq_cdf;   // FP64 emissivity CDF summed in the reference's order (grids up to 65536 zones)
   int32_t use_es, use_ff, use_bf, use_line, use_fuzz;
   int32_t radiative_eq, omit_scat, precision;
   double epsilon, max_opacity, temp_min, temp_max, fleck_alpha, dt, time;
