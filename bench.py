@@ -124,8 +124,11 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
     t_opac = float(out["set_opacity_seconds"][0])
     # the opacity build is per step, propagation per packet: the reference's
     # time for the full step is t_opac + (t_sample - t_opac) * N / n_sample
-    n_full = args.packets
-    t = t_opac * zone_scale + max(t_sample - t_opac, 0.0) * n_full / n_sample
+    # packets of a step: core packets, and decay packets when the workload has them
+    frac = w.params.get("particles_n_emit_radioactive", 0) / max(int(w.params.get("core_n_emit", 1)), 1)
+    n_full = int(args.packets * (1 + frac))
+    n_sample_all = int(n_sample * (1 + frac))
+    t = t_opac * zone_scale + max(t_sample - t_opac, 0.0) * n_full / n_sample_all
     value = n_full / t
     grid_note = "" if zone_scale == 1 else (
         " on a reduced %d-zone grid of the same model: set_opacity scaled by the zone count (x%g), "
@@ -141,9 +144,9 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
                                        "packets per step (%.2f s, of which set_opacity %.2f s); full-step time "
                                        "= set_opacity + propagation scaled to %d packets%s" %
                                        (w.name, "full zone/line/bin" if zone_scale == 1 else "full line/bin",
-                                        n_sample, t_sample, t_opac, n_full, grid_note)},
+                                        n_sample_all, t_sample, t_opac, n_full, grid_note)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "sample_packets_per_s": n_sample / t_sample, "set_opacity_seconds": t_opac}
+            "sample_packets_per_s": n_sample_all / t_sample, "set_opacity_seconds": t_opac}
 
 
 # ------------------------------------------------------------------ batches
@@ -430,13 +433,111 @@ def main_adjoint(args, rank: int, world: int, local: int):
 
 
 # ------------------------------------------------------------------ GPU arm
+def main_ddmc(args, rank: int, world: int, local: int):
+    """Time-dependent discrete diffusion: the reference's diffusing-pulse
+    configuration (tests/diffusing_pulse/1D_ddmc) with 1e7 packets of the
+    initial radiation field, every zone diffusive.  A step is one transport
+    step of dt = 5e-10 s over the packets carried from the step before (the
+    run advances through the warm-up steps too); value = packets carried
+    through the timed steps / their device time."""
+    from pubsed_b200 import workloads
+    n = args.packets or 10_000_000
+    n_ref = args.ref_packets or 20_000
+    dt = 5e-10
+    cores = os.cpu_count() or 1
+
+    def reference_arm(n_sample, steps, warmup):
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+        import run_ref
+        if not run_ref.available():
+            return None, "reference harness oracle/_ref/sedona_ref is not built"
+        w = workloads.diffusing_pulse(n_initialize=n_sample, seed=rank)
+        out = run_ref.run(w, "free", threads=cores, steps=warmup + steps, dt=dt, timeout=3600)
+        times = list(out["step_seconds"])[warmup:]
+        t = sum(times) / len(times)
+        return n_sample / t, "transport::step of the diffusing pulse (200 zones, DDMC) with %d packets " \
+            "carried per step, %d threads, %.3f s per step" % (n_sample, cores, t)
+
+    if args.impl == "reference":
+        if world > 1 and rank != 0:
+            return
+        v, note = reference_arm(n_ref, args.steps, args.warmup)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": note}), flush=True)
+            return
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": "diffusing_pulse_1d_ddmc",
+                                                          "packets_per_step": n_ref, "threads": cores},
+                          "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                                           "sample": note},
+                          "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+
+    import torch
+    from pubsed_b200 import abi, engine
+    torch.cuda.set_device(local)
+    out = {}
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        w = workloads.diffusing_pulse(n_initialize=n, seed=rank)
+        eng = engine.Engine(w, precision=prec, device=local, seed_offset=rank)
+        eng.initialize_particles(n, workloads.initial_e_rad(w.zones))
+        for _ in range(args.warmup):
+            eng.step(dt)
+        torch.cuda.synchronize()
+        clk = ClockSampler(local)
+        stats = []
+        with clk:
+            for _ in range(args.steps):
+                stats.append(eng.step(dt))
+        torch.cuda.synchronize()
+        pk = sum(int(s["n_packets"]) for s in stats)
+        ms = sum(s["ms_total"] for s in stats)
+        out[prec] = {"value": pk / (ms * 1e-3), "ms_per_step": ms / len(stats), "stats": stats, "clk": clk,
+                     "census": eng.n_particles()}
+        if prec == abi.PREC_MIXED:
+            # end to end through the C ABI: zone state up, step, spectrum and
+            # zone tallies down, wall clock
+            e2e_pk, t0 = 0, time.perf_counter()
+            h2d = d2h = 0
+            for _ in range(2):
+                h2d = eng.upload_grid()
+                st = eng.step(dt)
+                f, c = eng.spectrum()
+                tal = eng.tallies()
+                d2h = f.nbytes + c.nbytes + sum(v.nbytes for v in tal.values())
+                e2e_pk += int(st["n_packets"])
+            t_e2e = time.perf_counter() - t0
+            out[prec]["e2e"] = {"value": world * e2e_pk / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                                "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / 2 * 1e3}
+        eng.close()
+    m = out[abi.PREC_MIXED]
+    last = m["stats"][-1]
+    line = {"metric": METRIC, "value": world * m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 transport / f32 opacity tables", "data": "synthetic",
+            "config": {"workload": "diffusing_pulse_1d_ddmc", "n_zones": 200, "packets_per_step": int(last["n_packets"]),
+                       "segments_per_step": int(last["n_segments"]), "dt": dt, "precision": "mixed",
+                       "l2": "tables L2-resident (200 zones x 1 bin)", "parallelism": "single"},
+            "plain_fp64": {"value": out[abi.PREC_FP64]["value"], "ms_per_step": out[abi.PREC_FP64]["ms_per_step"]},
+            "gpu_launches": int(sum(s["kernel_launches"] for s in m["stats"])),
+            "e2e": m["e2e"], "clocks": m["clk"].summary()}
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        v, note = reference_arm(n_ref, 1, 1)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": note}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d", "batch64", "adjoint"])
+    ap.add_argument("--workload", default="type_ia", choices=["type_ia", "cart3d", "batch64", "adjoint", "radio", "ddmc"])
     ap.add_argument("--fd-entries", type=int, default=32, help="adjoint: (zone, band) entries checked by central FD")
     ap.add_argument("--packet-scale", type=float, default=1.0, help="batch64: scales every model's packet count")
     ap.add_argument("--cells", type=int, default=128, help="cells per axis of the cart3d workload")
@@ -450,11 +551,23 @@ def main():
         return main_batch(args, rank, world, local)
     if args.workload == "adjoint":
         return main_adjoint(args, rank, world, local)
+    if args.workload == "ddmc":
+        return main_ddmc(args, rank, world, local)
 
     from pubsed_b200 import workloads
 
     sample_fn = None
-    if args.workload == "cart3d":
+    radio_frac = 0.0  # radioactive packets per core packet
+    if args.workload == "radio":
+        # the Type Ia step with its 56Ni/56Co decay packets: one per ten core
+        # packets, the reference's Type Ia spectrum example's ratio
+        # (examples/supernova/TypeIa/spectrum/param.lua: 1e5 core, 1e4 decay)
+        radio_frac = 0.1
+
+        def wl(n):
+            return workloads.type_ia(n_packets=n, n_radioactive=int(n * radio_frac))
+        default_packets, default_ref = 10_000_000, 20_000
+    elif args.workload == "cart3d":
         def wl(n):
             return workloads.cart3d(n_packets=n, n_cells=args.cells)
 
@@ -517,7 +630,7 @@ def main():
     if not args.skip_fp64:
         e64, st64, wall64, _ = run_mode(abi.PREC_FP64, args.steps, min(args.warmup, 3))
         ms64 = sum(s["ms_total"] for s in st64) / len(st64)
-        fp64 = {"value": args.packets / (ms64 * 1e-3), "ms_per_step": ms64}
+        fp64 = {"value": int(st64[-1]["n_packets"]) / (ms64 * 1e-3), "ms_per_step": ms64}
         spec64 = e64.spectrum()
         e64.close()
 
@@ -529,7 +642,8 @@ def main():
     if world > 1:
         dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
     ms_max = float(t_local.item())
-    value = world * args.packets / (ms_max * 1e-3)
+    n_step = int(stats[-1]["n_packets"])  # core packets (and decay packets)
+    value = world * n_step / (ms_max * 1e-3)
     last = stats[-1]
     kern_ms = sum(s["ms_propagate_kernel"] for s in stats) / len(stats)
 
@@ -553,7 +667,7 @@ def main():
     t_e2e = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.packets / float(t_e2e.item())
+    e2e_value = world * n_step / float(t_e2e.item())
 
     # roofline of the packet kernel: algorithmic bytes per segment and per
     # packet (zone geometry 16 B in 1D / 24 B in 3D, {abs,scat} 8 B (FP32),
@@ -588,7 +702,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 transport / f32 opacity tables", "data": "synthetic",
         "config": {"workload": w.name, "n_zones": w.zones.n_zones, "n_lines": w.notes["n_lines"],
-                   "n_bins": w.nu_grid().n, "packets_per_step": args.packets, "precision": "mixed",
+                   "n_bins": w.nu_grid().n, "packets_per_step": n_step, "precision": "mixed",
+                   "radioactive_packets_per_step": int(w.params.get("particles_n_emit_radioactive", 0)),
                    "segments_per_step": last["n_segments"], "l2": "flushed between steps (256 MiB write)",
                    "parallelism": "replicas" if world > 1 else "single"},
         "ms_opacity": last["ms_opacity"], "ms_transport": last["ms_transport"],

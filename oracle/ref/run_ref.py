@@ -84,14 +84,18 @@ def atoms_to_store(store: Store, atom_file: str, fuzz_file: str, model):
 
 
 def write_mod_file(path: str, zones):
-    """1D_sphere "SNR" ASCII model (grid_1D_sphere.cpp:241-332); numbers are
-    written with 17 significant digits so they parse back exactly."""
+    """1D_sphere ASCII model (grid_1D_sphere.cpp:241-332): "SNR" (r_out = v t)
+    for homologous models, "standard" (explicit r_out column) otherwise;
+    numbers are written with 17 significant digits so they parse back
+    exactly."""
+    snr = bool(zones.homologous)
     with open(path, "w") as f:
-        f.write("1D_sphere SNR\n")
+        f.write("1D_sphere %s\n" % ("SNR" if snr else "standard"))
         f.write("%d %r %r %d\n" % (zones.n_zones, float(zones.r_min), float(zones.t_now), zones.n_elems))
         f.write(" ".join("%d.%d" % (z, a) for z, a in zip(zones.elem_Z, zones.elem_A)) + "\n")
         for i in range(zones.n_zones):
-            row = [repr(float(zones.v[i])), repr(float(zones.rho[i])), repr(float(zones.T[i]))]
+            row = [] if snr else [repr(float(zones.r_out[i]))]
+            row += [repr(float(zones.v[i])), repr(float(zones.rho[i])), repr(float(zones.T[i]))]
             row += [repr(float(x)) for x in zones.X[i]]
             f.write(" ".join(row) + "\n")
 
