@@ -341,6 +341,15 @@ int sed_diff_forward(sed_ctx* ctx, double dt, const double* abs_scale, int32_t n
  * + k] = sum_s grad_flux[s] d flux[s] / d abs_scale[z, k].  Replays every
  * escaped packet from its Philox stream (nothing of its path was stored). */
 int sed_diff_vjp(sed_ctx* ctx, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
+/* Vector-Jacobian product with respect to the density of each zone, the
+ * opacity per unit mass held (absorption and scattering extinction of the
+ * zone scale together): grad_rho[z] = sum_s grad_flux[s] d E[flux[s]] /
+ * d ln rho_z.  Per escaped packet of weight w: the absorption weight's
+ * pathwise derivative -w sum (a dshift l), and, because the scattering
+ * opacity decides where the path goes, the score of the sampled path
+ * w (n_scatterings - sum s dshift l) over the packet's segments in zone z
+ * (a likelihood-ratio estimator: unbiased, noisier than the pathwise one). */
+int sed_diff_vjp_density(sed_ctx* ctx, const double* grad_flux, double* grad_rho, sed_step_stats* stats);
 /* Full Jacobian of the last weighted forward: jac[(s * n_zones + z) * n_bands
  * + k] = d flux[s] / d abs_scale[z, k], s over the n_spec spectrum bins. */
 int sed_diff_jacobian(sed_ctx* ctx, double* jac, sed_step_stats* stats);

@@ -105,6 +105,7 @@ struct oracle_ctx {
   /* differentiable transport: exact Jacobian of the last weighted forward,
    * accumulated forward-mode per packet ([nspec][nzones][bands]) */
   double* jac;
+  double* jac_rho;  /* [nspec][nzones] d flux / d ln rho of the last weighted forward */
   int64_t jac_n;
   int diff_bands;
   char err[256];
@@ -2181,6 +2182,10 @@ typedef struct {
   double* acc;     /* [nzones * bands] sum of a0 dshift l of the current packet */
   int64_t* touched;
   int64_t n_touched;
+  double* rho;     /* [nzones] sum of (a + s) dshift l minus the scatters, per zone */
+  unsigned char* rmark;  /* [nzones] zone touched by the current packet */
+  int64_t* rtouched;
+  int64_t n_rtouched;
 } diff_acc;
 
 static int propagate_weighted(oracle_ctx* o, packet* p, double t_now, double dt, const double* abs_scale,
@@ -2233,6 +2238,12 @@ static int propagate_weighted(oracle_ctx* o, packet* p, double t_now, double dt,
       int64_t key = (int64_t)iz * n_bands + band;
       if (da->acc[key] == 0) da->touched[da->n_touched++] = key;
       da->acc[key] += a0 * dshift * this_d;
+      /* density of zone iz scales a and s alike: the weight's log falls by
+       * (a dshift l), the path's log-likelihood by (s dshift l) per segment
+       * and rises by one per scattering (score of the sampled path) */
+      if (!da->rmark[iz]) { da->rmark[iz] = 1; da->rtouched[da->n_rtouched++] = iz; }
+      da->rho[iz] += (a_opac + s_opac) * dshift * this_d;
+      if (event == 0) da->rho[iz] -= 1.0;
     }
     o->e_abs[iz] += this_E * dshift * a_opac * dshift * o->eps_imc[iz];
     if (o->tp.store_Jnu) o->J[(size_t)iz * nj + i_nu] += this_E;
@@ -2308,10 +2319,18 @@ int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32
   o->jac_n = o->nspec * (int64_t)nzb;
   o->jac = (double*)calloc((size_t)o->jac_n, sizeof(double));
   o->diff_bands = n_bands;
+  free(o->jac_rho);
+  o->jac_rho = (double*)calloc((size_t)o->nspec * (size_t)o->nzones, sizeof(double));
   diff_acc da;
   da.acc = (double*)calloc(nzb, sizeof(double));
   da.touched = (int64_t*)malloc(nzb * sizeof(int64_t));
-  if (!o->jac || !da.acc || !da.touched) { free(da.acc); free(da.touched); return fail(o, SED_ERR_NOMEM, "out of memory"); }
+  da.rho = (double*)calloc((size_t)o->nzones, sizeof(double));
+  da.rmark = (unsigned char*)calloc((size_t)o->nzones, 1);
+  da.rtouched = (int64_t*)malloc((size_t)o->nzones * sizeof(int64_t));
+  if (!o->jac || !o->jac_rho || !da.acc || !da.touched || !da.rho || !da.rmark || !da.rtouched) {
+    free(da.acc); free(da.touched); free(da.rho); free(da.rmark); free(da.rtouched);
+    return fail(o, SED_ERR_NOMEM, "out of memory");
+  }
   double Ep = o->tp.core_luminosity * dt / n_emit;
   uint32_t K = draws_per_emission(o);
   if (o->record) {
@@ -2331,20 +2350,27 @@ int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32
     emit_core_packet(o, &p, Ep, t_now, dt);
     p.n = K;
     da.n_touched = 0;
+    da.n_rtouched = 0;
     int fate = propagate_weighted(o, &p, t_now, dt, abs_scale, n_bands, &da, &nseg, &nscat);
     if (fate == F_ESCAPED) {
       double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / PC_C;
       int64_t s = spectrum_count(o, t_obs, p.nu, p.e, p.D);
-      if (s >= 0)
+      if (s >= 0) {
         for (int64_t q = 0; q < da.n_touched; ++q) {
           int64_t key = da.touched[q];
           o->jac[s * (int64_t)nzb + key] -= p.e * da.acc[key];
         }
+        for (int64_t q = 0; q < da.n_rtouched; ++q) {
+          int64_t z = da.rtouched[q];
+          o->jac_rho[s * (int64_t)o->nzones + z] -= p.e * da.rho[z];
+        }
+      }
       p.t = t_obs;
       nesc++;
     } else if (fate == F_ABSORBED) nabs++;
     else nstop++;
     for (int64_t q = 0; q < da.n_touched; ++q) da.acc[da.touched[q]] = 0;
+    for (int64_t q = 0; q < da.n_rtouched; ++q) { da.rho[da.rtouched[q]] = 0; da.rmark[da.rtouched[q]] = 0; }
     if (o->record) {
       o->r_fate[k] = fate; o->r_ind[k] = p.ind; o->r_draws[k] = (int32_t)(p.n - K);
       double* sv = o->r_state + (size_t)k * 9;
@@ -2352,8 +2378,7 @@ int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32
       sv[6] = p.t; sv[7] = p.e; sv[8] = p.nu;
     }
   }
-  free(da.acc);
-  free(da.touched);
+  free(da.acc); free(da.touched); free(da.rho); free(da.rmark); free(da.rtouched);
   finish_step(o, dt, n_emit, nesc);
   o->step++;
   if (st) {
@@ -2373,6 +2398,23 @@ int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, 
   for (int64_t s = 0; s < o->nspec; ++s) {
     if (grad_flux[s] == 0) continue;
     for (size_t q = 0; q < nzb; ++q) grad_scale[q] += grad_flux[s] * o->jac[(size_t)s * nzb + q];
+  }
+  if (st) memset(st, 0, sizeof *st);
+  return SED_OK;
+}
+
+/* d flux / d ln(rho) of each zone, the opacity per unit mass held: both
+ * extinctions of the zone scale with its density; the estimator is the
+ * pathwise derivative of the absorption weight plus the score of the
+ * scattering path (likelihood ratio), per escaped packet */
+int oracle_diff_vjp_density(oracle_ctx* o, const double* grad_flux, double* grad_rho, sed_step_stats* st)
+{
+  if (!o || !grad_flux || !grad_rho) return SED_ERR_ARG;
+  if (!o->jac_rho) return fail(o, SED_ERR_STATE, "no weighted forward");
+  for (int z = 0; z < o->nzones; ++z) grad_rho[z] = 0;
+  for (int64_t s = 0; s < o->nspec; ++s) {
+    if (grad_flux[s] == 0) continue;
+    for (int z = 0; z < o->nzones; ++z) grad_rho[z] += grad_flux[s] * o->jac_rho[(size_t)s * o->nzones + z];
   }
   if (st) memset(st, 0, sizeof *st);
   return SED_OK;
@@ -2552,5 +2594,6 @@ void oracle_ctx_destroy(oracle_ctx* o)
   free(o->gflux); free(o->gclick); free(o->L_emit); free(o->L_dep); free(o->radio_cdf); free(o->gamma_frac);
   free(o->compton); free(o->photoion); free(o->gn.x);
   free(o->c_state); free(o->c_ind); free(o->c_type); free(o->r_type);
+  free(o->jac_rho);
   free(o);
 }

@@ -46,6 +46,7 @@ int oracle_locate(const sed_locate_grid* g, double x);
 int oracle_set_rng_step(oracle_ctx* o, uint32_t step);
 int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* stats);
 int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
+int oracle_diff_vjp_density(oracle_ctx* o, const double* grad_flux, double* grad_rho, sed_step_stats* st);
 int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
 /* packets carried between time-dependent steps, the transport clock, and
  * the initial radiation field's packets */

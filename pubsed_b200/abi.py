@@ -179,6 +179,7 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         "diff_forward": ([vp, C.c_double, _dp, C.c_int32, C.POINTER(StepStats)], C.c_int),
         "diff_vjp": ([vp, _dp, _dp, C.POINTER(StepStats)], C.c_int),
         "diff_jacobian": ([vp, _dp, C.POINTER(StepStats)], C.c_int),
+        "diff_vjp_density": ([vp, _dp, _dp, C.POINTER(StepStats)], C.c_int),
         "solve_temperature": ([vp, C.c_int32, _dp, _ip], C.c_int),
         "get_gamma_spectrum": ([vp, _dp, _dp], C.c_int),
         "get_radioactive_tallies": ([vp, _dp, _dp], C.c_int),

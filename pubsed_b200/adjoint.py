@@ -12,6 +12,16 @@ its backward is the path-replay vector-Jacobian product.  `step` fixes the
 Philox step number, so every evaluation with the same step uses the same
 deviates (common random numbers) and the spectrum is a smooth function of
 theta.
+
+`vjp_density(g)` is the gradient with respect to each zone's density (both
+extinctions of the zone scale with it; opacity per unit mass held), and
+`spectrum_from_density(r, engine, step)` the torch Function of the per-zone
+density factors r: its forward scales the tables of the last opacity build,
+its backward is that replay.  The scattering part of the density derivative
+is a likelihood-ratio (score) term, since the scattering opacity decides
+where a path goes: unbiased, but not a smooth function of r for fixed
+deviates, so it is checked against finite differences of the expected
+spectrum, not of one set of deviates.
 """
 from __future__ import annotations
 
@@ -69,6 +79,37 @@ class DiffEngine(Engine):
         self.last_replay = st.as_dict()
         return out.reshape(self.nz, self.n_bands)
 
+    def vjp_density(self, grad_flux: np.ndarray) -> np.ndarray:
+        """sum_s grad_flux[s] d E[flux[s]] / d ln rho_z of the last forward."""
+        g = np.ascontiguousarray(grad_flux, dtype=np.float64).reshape(-1)
+        if g.size != self.nspec:
+            raise ValueError("grad_flux has %d entries, expected %d" % (g.size, self.nspec))
+        out = np.zeros(self.nz)
+        st = abi.StepStats()
+        self._check(self.L.sed_diff_vjp_density(self.ctx, g.ctypes.data_as(abi._dp), out.ctypes.data_as(abi._dp),
+                                                C.byref(st)), "sed_diff_vjp_density")
+        self.last_replay = st.as_dict()
+        return out
+
+    def forward_density(self, r: np.ndarray, step: Optional[int] = None, dt: float = 1.0):
+        """Weighted forward with the extinction of zone z scaled by r[z]
+        (the tables of the last opacity build, both absorption and
+        scattering); returns (flux, click, stats)."""
+        if not self._have_tables:
+            self.tables(dt)
+        if not hasattr(self, "_base"):
+            self._base = self.opacity()
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
+        if r.size != self.nz:
+            raise ValueError("r has %d entries, expected %d" % (r.size, self.nz))
+        b = self._base
+        ab = (b["abs"].reshape(self.nz, -1) * r[:, None]).ravel()
+        sc = (b["scat"].reshape(self.nz, -1) * r[:, None]).ravel()
+        k = abi.Keep()
+        self._check(self.L.sed_load_opacity(self.ctx, k.d(ab), k.d(sc), k.d(b["emis_cdf"]), k.d(b["eps_imc"])),
+                    "sed_load_opacity")
+        return self.forward(None, step=step, dt=dt)
+
     def jacobian(self) -> np.ndarray:
         out = np.zeros(self.nspec * self.nz * self.n_bands)
         st = abi.StepStats()
@@ -116,7 +157,49 @@ def _make_function():
     return SpectrumFromAbsorption
 
 
+def _make_density_function():
+    torch = _torch()
+
+    class SpectrumFromDensity(torch.autograd.Function):
+        """flux = F(r): the weighted transport's binned emergent spectrum as a
+        function of per-zone density factors r ([n_zones], float64) applied
+        to both extinctions of the last opacity build.  Backward:
+        d/d r_z = (d/d ln rho_z) / r_z from the density replay."""
+
+        @staticmethod
+        def forward(ctx, r, engine: DiffEngine, step: int):
+            rr = r.detach().to("cpu", torch.float64).numpy()
+            flux, _, _ = engine.forward_density(rr, step=step)
+            ctx.engine = engine
+            ctx.step = step
+            ctx.fid = engine.forward_id
+            ctx.save_for_backward(r)
+            return torch.from_numpy(flux).to(r.device)
+
+        @staticmethod
+        def backward(ctx, grad_flux):
+            (r,) = ctx.saved_tensors
+            eng = ctx.engine
+            rr = r.detach().to("cpu", torch.float64).numpy()
+            if eng.forward_id != ctx.fid:
+                eng.forward_density(rr, step=ctx.step)
+            g = grad_flux.detach().to("cpu", torch.float64).numpy()
+            grad = eng.vjp_density(g) / rr
+            return torch.from_numpy(grad).to(r.device, r.dtype), None, None
+
+    return SpectrumFromDensity
+
+
 _FN = None
+_FN_RHO = None
+
+
+def spectrum_from_density(r, engine: DiffEngine, step: int = 0):
+    """torch entry point: the spectrum as a function of per-zone density factors."""
+    global _FN_RHO
+    if _FN_RHO is None:
+        _FN_RHO = _make_density_function()
+    return _FN_RHO.apply(r, engine, step)
 
 
 def spectrum_from_absorption(theta, engine: DiffEngine, step: int = 0):

@@ -5,8 +5,11 @@
 // sed_diff_vjp / sed_diff_jacobian then launch the adjoint replay kernel:
 // each escaped packet is emitted and walked again from its Philox stream
 // (same step number, same deviates, same path) and every segment adds
-// -w a0 dshift l to the (zone, band) entry it crossed.  Nothing of a path is
-// stored between the two launches.
+// -w a0 dshift l to the (zone, band) entry it crossed.  sed_diff_vjp_density
+// replays the same way into one entry per zone: -w ((a + s) dshift l) per
+// segment and +w per scattering (the score of the scattering path, a
+// likelihood-ratio term, since the scattering opacity decides where the
+// path goes).  Nothing of a path is stored between the two launches.
 #include <cstring>
 #include <vector>
 
@@ -51,7 +54,7 @@ void fill_stats(sed_step_stats* st, const unsigned long long* cnt, int64_t n, fl
 }
 
 // the adjoint replay of the last weighted forward into c->d_adj_out
-int replay(sed_ctx* c, bool jacobian, sed_step_stats* st)
+int replay(sed_ctx* c, bool jacobian, sed_step_stats* st, bool density = false)
 {
   if (!c->have_diff) return set_err(c, SED_ERR_STATE, "sed_diff_vjp/jacobian: no weighted forward to replay");
   StepArgs A = make_step_args(c, c->diff_dt, c->diff_n);
@@ -63,6 +66,7 @@ int replay(sed_ctx* c, bool jacobian, sed_step_stats* st)
   A.adj_g = c->d_adj_g.p;
   A.adj_out = c->d_adj_out.p;
   A.adj_jacobian = jacobian ? 1 : 0;
+  A.adj_density = density ? 1 : 0;
   CK(cudaMemsetAsync(c->d_counters.p, 0, (C_COUNT + 1) * sizeof(unsigned long long), c->stream));
   CK(cudaEventRecord(c->ev[3], c->stream));
   if (c->diff_n > 0 && launch_propagate_diff(A, make_grid_dev(c), 2, c->num_sms, c->stream) < 0)
@@ -168,6 +172,20 @@ int sed_diff_vjp(sed_ctx* c, const double* grad_flux, double* grad_scale, sed_st
   int rc = replay(c, false, st);
   if (rc) return rc;
   CK(cudaMemcpyAsync(grad_scale, c->d_adj_out.p, n_out * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return SED_OK;
+}
+
+int sed_diff_vjp_density(sed_ctx* c, const double* grad_flux, double* grad_rho, sed_step_stats* st)
+{
+  if (!c || !grad_flux || !grad_rho) return SED_ERR_ARG;
+  const size_t n_out = (size_t)c->nz;
+  CK(upload(c, c->d_adj_g, grad_flux, (size_t)c->nspec));
+  CK(c->d_adj_out.resize(n_out));
+  CK(cudaMemsetAsync(c->d_adj_out.p, 0, n_out * sizeof(double), c->stream));
+  int rc = replay(c, false, st, true);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(grad_rho, c->d_adj_out.p, n_out * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return SED_OK;
 }

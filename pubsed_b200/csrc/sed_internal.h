@@ -77,6 +77,7 @@ struct StepArgs {
   const double* abs_scale;           // [nz * n_bands] factor on the absorption opacity, or null
   int32_t n_bands;                   // band of bin i = i * n_bands / n_nu
   int32_t adj_jacobian;              // adjoint: 1 = full Jacobian rows, 0 = vector-Jacobian product
+  int32_t adj_density;               // adjoint: 1 = d / d ln rho per zone (likelihood-ratio score + absorption)
   int32_t* esc_bin;                  // [n_packets] spectrum index of an escaped, counted packet; -1 otherwise
   double* esc_e;                     // [n_packets] its energy at escape
   const double* adj_g;               // [nspec] d(loss)/d(flux) for the vector-Jacobian product

@@ -826,13 +826,27 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         this_E = (tau_a > 0 ? p.e * (-em1 / tau_a) : p.e) * this_d;
       }
       if constexpr (MODE == 2) {
-        const int64_t key = adj_row + (int64_t)iz * A.n_bands + band;
-        if (key != acc_key) {
-          if (acc_key >= 0) atomicAdd(A.adj_out + acc_key, -adj_w * acc_g);
-          acc_key = key;
-          acc_g = 0;
+        if (A.adj_density) {
+          // d / d ln rho of zone iz, opacity per mass held: the weight's log
+          // falls by a dshift l, the sampled path's log-likelihood by
+          // s dshift l per segment and rises by one per scattering
+          const int64_t key = iz;
+          if (key != acc_key) {
+            if (acc_key >= 0) atomicAdd(A.adj_out + acc_key, -adj_w * acc_g);
+            acc_key = key;
+            acc_g = 0;
+          }
+          acc_g += (a_opac + s_opac) * dshift * this_d;
+          if (event == 0) acc_g -= 1.0;
+        } else {
+          const int64_t key = adj_row + (int64_t)iz * A.n_bands + band;
+          if (key != acc_key) {
+            if (acc_key >= 0) atomicAdd(A.adj_out + acc_key, -adj_w * acc_g);
+            acc_key = key;
+            acc_g = 0;
+          }
+          acc_g += (double)ab.x * dshift * this_d;  // d(theta a0 dshift l) / d theta
         }
-        acc_g += (double)ab.x * dshift * this_d;  // d(theta a0 dshift l) / d theta
       }
       const double eps_imc = __ldg(A.eps_imc + iz);
       if constexpr (MODE == 0) {

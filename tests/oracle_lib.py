@@ -333,3 +333,13 @@ def compare_td(rg: list, ro: list, max_frac: float = 1e-4) -> int:
             zone_tally_close(a["tallies"][k], b["tallies"][k])
         full += 1
     return full
+
+
+def diff_vjp_density(eng: Engine, g: np.ndarray) -> np.ndarray:
+    """d(g . flux)/d ln(rho_z) of the last weighted forward (sed_/oracle_diff_vjp_density)."""
+    out = np.zeros(eng.nz)
+    st = abi.StepStats()
+    gg = np.ascontiguousarray(g, dtype=np.float64)
+    eng.check(eng.fn("diff_vjp_density")(eng.ctx, gg.ctypes.data_as(abi._dp), out.ctypes.data_as(abi._dp),
+                                         C.byref(st)), "diff_vjp_density")
+    return out
