@@ -136,6 +136,18 @@ def run_steady(workload, outdir: str = ".", precision: int = abi.PREC_FP64, devi
     return tr
 
 
+def step_size(t: float, dt_max: float, dt_min: float, dt_del: float) -> float:
+    """The driver's time step (SedonaClass.cpp:318-328, no hydro limit):
+    tstep_max_dt, at most tstep_max_delta of the time once t > 0, at least
+    tstep_min_dt."""
+    dt = dt_max
+    if dt_del > 0 and t > 0 and dt > t * dt_del:
+        dt = t * dt_del
+    if dt < dt_min:
+        dt = dt_min
+    return dt
+
+
 def run_time_dependent(workload, outdir: Optional[str] = ".", precision: int = abi.PREC_FP64, device: int = 0,
                        on_write=None) -> Transport:
     """The reference driver's time loop (SedonaClass::evolve_system,
@@ -159,11 +171,7 @@ def run_time_dependent(workload, outdir: Optional[str] = ".", precision: int = a
     next_write = t
     i_write = 0
     for _ in range(n_steps):
-        dt = dt_max
-        if dt_del > 0 and t > 0 and dt > t * dt_del:
-            dt = t * dt_del
-        if dt < dt_min:
-            dt = dt_min
+        dt = step_size(t, dt_max, dt_min, dt_del)
         if hydro:
             wl.homologous_step(workload.zones, dt)
         tr.step(dt)

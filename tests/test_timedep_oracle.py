@@ -91,3 +91,19 @@ def test_clock_and_spectrum_accumulate():
     e.check(e.fn("wipe_spectra")(e.ctx), "wipe_spectra")
     assert e.spectrum()[1].sum() == 0
     e.close()
+
+
+def test_driver_step_sizes():
+    """The driver's step rule on the diffusing pulse's settings: the first
+    step is tstep_max_dt (t = 0), then at most 10% of the time until that
+    exceeds tstep_max_dt; tstep_min_dt is a floor."""
+    from pubsed_b200.transport import step_size
+    t, seq = 0.0, []
+    for _ in range(40):
+        dt = step_size(t, 5e-10, 0.0, 0.1)
+        seq.append(dt)
+        t += dt
+    assert seq[0] == 5e-10 and seq[1] == 5e-10 * 0.1
+    assert all(b >= a for a, b in zip(seq[1:], seq[2:]))
+    assert seq[-1] == 5e-10
+    assert step_size(1.0, 5e-10, 1e-9, 0.1) == 1e-9
