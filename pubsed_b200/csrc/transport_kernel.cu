@@ -784,7 +784,9 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       double eps = 0;
       if (!(fast)) eps = (op == 0) ? 0 : a_opac / op;
       double d_nu;
-      if (fast) d_nu = loc_delta(A.nu, i_nu) * A.ct / p.nu;
+      // distance to the bin's edge: only where the segment stops to look up
+      // the next bin, so FP32 in the mixed form
+      if (fast) d_nu = (double)((float)(loc_delta(A.nu, i_nu) * A.ct) / (float)p.nu);
       else {
         d_nu = loc_delta(A.nu, i_nu) / p.nu * C_LIGHT / p.dvds;
         if (p.dvds == 0) d_nu = INFINITY;
@@ -805,7 +807,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       } else {
         tau_r = -1.0 * log(1 - rng.next());
       }
-      double d_sc = tau_r / tot_lab;
+      // mixed form: tau is an FP32 deviate, so its distance is formed in FP32
+      // (an IEEE division, off the FP64 pipe); position and time stay FP64
+      double d_sc;
+      if constexpr (FAST) d_sc = (double)((float)tau_r / (float)tot_lab);
+      else d_sc = tau_r / tot_lab;
       if (tot_lab == 0) d_sc = INFINITY;
       double d_tm = (A.tstop - p.t) * C_LIGHT;
       if (A.steady) d_tm = INFINITY;
