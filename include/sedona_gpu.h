@@ -259,6 +259,15 @@ int64_t sed_n_particles(sed_ctx* ctx);
 /* The carried packets: zone, type (enum PType: 0 photon, 1 gamma-ray) and
  * {x, D, t, e, nu} of the first n (n <= sed_n_particles). */
 int sed_get_particles(sed_ctx* ctx, int64_t n, int32_t* ind, int32_t* type, double* state9);
+/* The inner source's luminosity and, when weights is not NULL, its spectrum:
+ * weights[i] = L_nu dnu of frequency bin i (core_spectrum_file, read by
+ * transport::setup_core_emission, src/transport/transport_init.cpp:486-537),
+ * summed in bin order into the emission CDF and normalised as cdf_array
+ * does.  The luminosity is what emit_inner_source divides among the packets
+ * (emission.cpp:386-389); the host sets it each step from core_luminosity at
+ * the transport clock when that is a function of time.  At context creation
+ * the spectrum is a blackbody at core_temperature. */
+int sed_set_core_source(sed_ctx* ctx, double luminosity, const double* weights);
 /* transport::wipe_spectra (src/transport/transport_output.cpp:63-67): empties
  * the optical and gamma-ray spectra.  A steady-state step starts from empty
  * spectra (the driver wipes them every iteration, SedonaClass.cpp:349); a

@@ -2044,6 +2044,19 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
 
 int64_t oracle_n_particles(oracle_ctx* o) { return o ? o->n_census : 0; }
 
+int oracle_set_core_source(oracle_ctx* o, double luminosity, const double* weights)
+{
+  if (!o) return SED_ERR_ARG;
+  if (!(luminosity >= 0)) return fail(o, SED_ERR_ARG, "negative luminosity");
+  o->tp.core_luminosity = luminosity;
+  if (weights) {  /* transport_init.cpp:509-537: set_value per bin, then normalize */
+    int nn = o->nu.n;
+    for (int j = 0; j < nn; ++j) o->core_cdf[j] = (j == 0) ? weights[0] : o->core_cdf[j - 1] + weights[j];
+    cdf_normalize(o->core_cdf, nn);
+  }
+  return SED_OK;
+}
+
 int oracle_wipe_spectra(oracle_ctx* o)  /* transport::wipe_spectra (transport_output.cpp:63-67) */
 {
   if (!o) return SED_ERR_ARG;

@@ -52,6 +52,7 @@ int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
  * the initial radiation field's packets */
 int64_t oracle_n_particles(oracle_ctx* o);
 int oracle_wipe_spectra(oracle_ctx* o);
+int oracle_set_core_source(oracle_ctx* o, double luminosity, const double* weights);
 int oracle_get_particles(oracle_ctx* o, int64_t n, int32_t* ind, int32_t* type, double* state9);
 int oracle_set_time(oracle_ctx* o, double t_now);
 double oracle_get_time(oracle_ctx* o);

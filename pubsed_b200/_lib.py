@@ -43,7 +43,7 @@ EXPORTED = [
     "sed_n_particles", "sed_last_error", "sed_ctx_destroy", "sed_version",
     "sed_set_rng_step", "sed_diff_forward", "sed_diff_vjp", "sed_diff_vjp_density", "sed_diff_jacobian", "sed_solve_temperature",
     "sed_get_gamma_spectrum", "sed_get_radioactive_tallies", "sed_set_emission",
-    "sed_get_particles", "sed_set_time", "sed_get_time", "sed_initialize_particles", "sed_wipe_spectra",
+    "sed_get_particles", "sed_set_time", "sed_get_time", "sed_initialize_particles", "sed_wipe_spectra", "sed_set_core_source",
     "sed_batch_create", "sed_batch_set_opacity_params", "sed_batch_set_atomic_data", "sed_batch_autotune",
     "sed_batch_set_tuning", "sed_batch_use_graph", "sed_batch_step", "sed_batch_set_zone_state", "sed_batch_get_escaped",
     "sed_batch_get_spectrum", "sed_batch_get_zone_tallies", "sed_batch_get_opacity", "sed_batch_record_packets",

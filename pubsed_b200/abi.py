@@ -190,6 +190,7 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
         "initialize_particles": ([vp, C.c_int64, _dp], C.c_int),
         "n_particles": ([vp], C.c_int64),
         "wipe_spectra": ([vp], C.c_int),
+        "set_core_source": ([vp, C.c_double, _dp], C.c_int),
     })
     if prefix == "sed_":
         i64p = C.POINTER(C.c_int64)

@@ -970,6 +970,26 @@ int sed_get_packet_records(sed_ctx* c, int64_t n, int32_t* fate, int32_t* ind, i
 
 int64_t sed_n_particles(sed_ctx* c) { return c ? c->n_census : 0; }
 
+int sed_set_core_source(sed_ctx* c, double luminosity, const double* weights)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!(luminosity >= 0)) return set_err(c, SED_ERR_ARG, "sed_set_core_source: luminosity %g", luminosity);
+  c->tp.core_luminosity = luminosity;
+  if (weights) {
+    // core_emission_spectrum_: cdf_array::set_value in bin order, then normalize
+    const int nn = c->nu.n();
+    std::vector<double> cdf(nn);
+    for (int j = 0; j < nn; ++j) cdf[j] = (j == 0) ? weights[0] : cdf[j - 1] + weights[j];
+    for (int j = 0; j < nn; ++j) if (std::isnan(cdf[j])) cdf[j] = 0;
+    if (cdf[nn - 1] == 0) for (int j = 0; j < nn; ++j) cdf[j] = 1.0;
+    const double N = cdf[nn - 1];
+    for (int j = 0; j < nn; ++j) cdf[j] /= N;
+    CK(upload(c, c->d_core_cdf, cdf.data(), cdf.size()));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return SED_OK;
+}
+
 int sed_wipe_spectra(sed_ctx* c)
 {
   if (!c) return SED_ERR_ARG;

@@ -24,6 +24,10 @@ class Engine:
         self.tp.rng_seed = (self.tp.rng_seed + seed_offset) & 0xFFFFFFFF
         self.ctx = C.c_void_p()
         self._check(self.L.sed_ctx_create(C.byref(self.tp), device, C.byref(self.ctx)), "sed_ctx_create")
+        _, L_core, weights = workload.core_source()
+        if weights is not None:  # core_spectrum_file in place of the blackbody
+            w = np.ascontiguousarray(weights, dtype=np.float64)
+            self._check(self.L.sed_set_core_source(self.ctx, L_core, w.ctypes.data_as(abi._dp)), "sed_set_core_source")
         self.nz = workload.zones.n_zones
         self.nn = self.tp.nu_grid.n
         self.nspec = self.tp.spec_time.n * self.tp.spec_nu.n * self.tp.spec_mu.n * self.tp.spec_phi.n
@@ -86,6 +90,14 @@ class Engine:
                                                 P(out["fx"]), P(out["fy"]), P(out["fz"]), P(out["fr"])),
                     "sed_get_zone_tallies")
         return out
+
+    def set_core_luminosity(self, L: float) -> None:
+        """sed_set_core_source with the spectrum kept."""
+        self._check(self.L.sed_set_core_source(self.ctx, float(L), None), "sed_set_core_source")
+        self.tp.core_luminosity = float(L)
+
+    def time(self) -> float:
+        return float(self.L.sed_get_time(self.ctx))
 
     def initialize_particles(self, n: int, e_rad) -> None:
         """sed_initialize_particles: n packets of the radiation field e_rad."""

@@ -68,6 +68,11 @@ class Transport:
         n_core, n_radio = self.emission_counts(dt, last_iteration)
         if (n_core, n_radio) != (int(self.eng.tp.core_n_emit), int(self.eng.tp.n_emit_radioactive)):
             self.eng.set_emission(n_core, n_radio)
+        # emit_inner_source takes core_luminosity at the transport clock when
+        # it is not 0 (emission.cpp:386-388)
+        L_now = self.P.function("core_luminosity", self.eng.time())
+        if L_now != 0 and L_now != self.eng.tp.core_luminosity:
+            self.eng.set_core_luminosity(L_now)
         self.eng.upload_grid()
         st = self.eng.step(dt)
         if self.radiative_eq and not self.fix_Tgas and not self.solve_Tgas_updated:

@@ -10,6 +10,7 @@ and the reference harness all see identical inputs.
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 from typing import Any, Optional
 
@@ -103,8 +104,9 @@ class Workload:
         tp.max_particles = P.scalar("particles_max_total", int)
         tp.core_n_emit = self.n_packets if n_packets is None else int(n_packets)
         tp.core_radius = P.scalar("core_radius")
-        tp.core_luminosity = P.function("core_luminosity", self.zones.t_now)
-        tp.core_temperature = P.scalar("core_temperature")
+        T_core, L_core, _ = self.core_source()
+        tp.core_luminosity = L_core
+        tp.core_temperature = T_core
         tp.core_photon_frequency = P.scalar("core_photon_frequency")
         tp.fleck_alpha = P.scalar("transport_fleck_alpha")
         tp.max_segments = 0
@@ -125,6 +127,46 @@ class Workload:
         tp.use_ddmc = int(P.scalar("transport_use_ddmc", int))
         tp.ddmc_tau = float(P.scalar("transport_ddmc_tau_threshold")) if tp.use_ddmc else 0.0
         return tp
+
+    def core_source(self):
+        """transport::setup_core_emission (src/transport/transport_init.cpp:
+        465-547) and the luminosity emit_inner_source takes (emission.cpp:
+        386-388): T_core from L and r_core when it is 0; the per-bin emission
+        weights (a blackbody at T_core, or L_nu read from core_spectrum_file),
+        and L = core_luminosity at the grid time, or, when that is 0, the
+        spectrum's luminosity (sum over bins of 4 pi r_core^2 pi B_nu dnu, or
+        of L_nu dnu).  Returns (T_core, L, weights) with weights None for the
+        blackbody, which the library forms itself."""
+        P = self.P
+        r_core = P.scalar("core_radius")
+        T_core = P.scalar("core_temperature")
+        L0 = P.function("core_luminosity", 0.0)
+        if L0 != 0 and r_core != 0 and T_core == 0:
+            T_core = (L0 / (4.0 * PI * r_core * r_core * SB_CGS)) ** 0.25
+        g = self.nu_grid()
+        path = P.get("core_spectrum_file")
+        weights, L_sum = None, 0.0
+        cspec = read_core_spectrum(path) if path else None
+        if cspec is not None:
+            weights = np.zeros(g.n)
+            for j in range(g.n):
+                nu, dnu = g.center_at(j), g.delta_at(j)
+                ind = _lower_bound(cspec[0], nu) - 1
+                Lnu = 0.0 if (ind < 0 or ind >= len(cspec[0]) - 1) else cspec[1][ind]
+                weights[j] = Lnu * dnu * 1.0
+                L_sum += Lnu * dnu
+        else:
+            for j in range(g.n):
+                nu, dnu = g.center_at(j), g.delta_at(j)
+                if T_core <= 0:
+                    bb = 1.0
+                else:
+                    bb = 2.0 * nu * nu * nu * H_CGS / C_CGS / C_CGS / (math.exp(H_CGS * nu / K_CGS / T_core) - 1)
+                L_sum += 4.0 * PI * r_core * r_core * PI * bb * dnu
+        L = P.function("core_luminosity", self.zones.t_now)
+        if L == 0:
+            L = L0 if L0 != 0 else L_sum
+        return T_core, L, weights
 
     def grid_struct(self, keep: abi.Keep) -> abi.Grid:
         z = self.zones
@@ -222,6 +264,75 @@ def lightbulb_grey(n_packets: int = 1_000_000, n_zones: int = 128, n_bins: int =
     }
     return Workload("lightbulb_grey_1d", params, z,
                     notes={"log_del": d, "v_max": 1e9, "t_days": 10.0})
+
+
+H_CGS, K_CGS, C_CGS, SB_CGS = 6.6260755e-27, 1.380658e-16, 2.99792458e10, 5.6704e-5  # physical_constants.h
+
+
+def _lower_bound(a, v) -> int:
+    """std::lower_bound's binary search, step for step (the result on an
+    unsorted list is the reference's too)."""
+    first, n = 0, len(a)
+    while n > 0:
+        half = n >> 1
+        if a[first + half] < v:
+            first += half + 1
+            n -= half + 1
+        else:
+            n = half
+    return first
+
+
+def read_core_spectrum(path: str):
+    """The (nu, L_nu) pairs setup_core_emission reads from core_spectrum_file
+    (transport_init.cpp:488-501), as its stream loop reads them: pairs while
+    the stream is not at its end, where a read that finds the end leaves its
+    variable as it was.  So a file that ends in whitespace yields the last
+    pair twice, and an odd token count repeats the previous L_nu.  An
+    unreadable file reads as no file (None)."""
+    try:
+        with open(path) as f:
+            data = f.read()
+    except OSError:
+        return None
+    toks = data.split()
+    n = len(toks)
+    trailing = n > 0 and data[-1].isspace()
+    nus, Ls = [], []
+    i, eof = 0, False
+    x1 = x2 = None
+    while not eof:
+        failed = False
+        if i < n:
+            x1 = float(toks[i]); i += 1
+            if i == n and not trailing:
+                eof = True
+        else:
+            eof = failed = True
+        if not (failed or eof):
+            if i < n:
+                x2 = float(toks[i]); i += 1
+                if i == n and not trailing:
+                    eof = True
+            else:
+                eof = True
+        if x1 is None or x2 is None:
+            raise ValueError("core_spectrum_file %s holds no (nu, L_nu) pair" % path)
+        nus.append(x1)
+        Ls.append(x2)
+    return nus, Ls
+
+
+def with_params(base: str, params: dict, **kw) -> Workload:
+    """The workload `base(**kw)` with `params` set over its parameters; a
+    relative core_spectrum_file is taken from the repository root."""
+    w = globals()[base](**kw)
+    p = dict(params)
+    f = p.get("core_spectrum_file")
+    if f and not os.path.isabs(f):
+        p["core_spectrum_file"] = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), f)
+    w.params.update(p)
+    return w
 
 
 def time_dependent(base: str, n_initialize: int = 0, dt_days: float = 0.1, params: Optional[dict] = None,

@@ -49,6 +49,17 @@ CASES = {
     "replay_ia_radio_late": ("type_ia", dict(n_packets=100, n_zones=16, n_lines=5000, n_bins=256,
                                              n_levels_per_ion=6, v_core=1e8, n_radioactive=800, t_days=150.0,
                                              seed=23)),
+    # the inner source's spectrum read from core_spectrum_file, its
+    # luminosity the file's integral (core_luminosity = 0)
+    "replay_core_file": ("with_params", dict(base="lightbulb_grey",
+                                             params={"core_spectrum_file": "tests/golden/core_spectrum.txt",
+                                                     "core_luminosity": 0.0},
+                                             n_packets=800, n_zones=32, n_bins=128, seed=9)),
+    # a core of radius 1e14 cm with core_temperature 0: T from L and r
+    "replay_core_derived": ("with_params", dict(base="lightbulb_grey",
+                                                params={"core_radius": 1e14, "core_temperature": 0.0,
+                                                        "core_luminosity": 1e42},
+                                                n_packets=800, n_zones=32, n_bins=128, seed=10)),
     "replay_cart3d": ("cart3d", dict(n_packets=300, n_cells=6, n_lines=1500, n_bins=128, spectrum_bins=64, n_mu=4,
                                      seed=13)),
 }
@@ -102,10 +113,24 @@ def make_workload(gen: str, kw: dict):
     return getattr(workloads, gen)(**kw)
 
 
+def write_core_spectrum():
+    """A synthetic inner-source spectrum for replay_core_file: L_nu of a
+    broken power law on 60 log-spaced frequencies inside the grid, one pair
+    per line, the file ending in a newline (the reference then reads the last
+    pair twice)."""
+    nu = np.logspace(14.05, 15.9, 60)
+    L = np.where(nu < 6e14, 1e28 * (nu / 6e14) ** 2, 1e28 * (nu / 6e14) ** -3)
+    with open(os.path.join(HERE, "core_spectrum.txt"), "w") as f:
+        for a, b in zip(nu, L):
+            f.write("%.6e %.6e\n" % (a, b))
+
+
 def main():
     if not run_ref.available():
         raise SystemExit("build the reference harness first: oracle/ref/build_ref.sh")
     only = set(sys.argv[1:])
+    if not only or "replay_core_file" in only:
+        write_core_spectrum()
     for name, (gen, kw) in CASES.items():
         if only and name not in only:
             continue

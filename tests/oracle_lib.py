@@ -43,6 +43,9 @@ class Engine:
         f = getattr(lib, prefix + "ctx_create")
         rc = f(C.byref(self.tp), device, C.byref(self.ctx)) if prefix == "sed_" else f(C.byref(self.tp), C.byref(self.ctx))
         self.check(rc, "ctx_create")
+        _, L_core, weights = workload.core_source()
+        if weights is not None:  # core_spectrum_file in place of the blackbody
+            self.check(self.fn("set_core_source")(self.ctx, L_core, abi.Keep().d(weights)), "set_core_source")
         self.nz = workload.zones.n_zones
         self.nn = self.tp.nu_grid.n
         self.nspec = self.tp.spec_time.n * self.tp.spec_nu.n * self.tp.spec_mu.n * self.tp.spec_phi.n

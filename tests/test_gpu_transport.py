@@ -138,3 +138,29 @@ def test_temperature_solve_matches_oracle(sed_lib, case):
     assert _rel(Rg, Ro) <= 1e-10
     o.close()
     g.close()
+
+
+@pytest.mark.parametrize("name", ["replay_core_file", "replay_core_derived"])
+def test_core_source_rules_match_reference_replay(sed_lib, name):
+    """The inner source as transport::setup_core_emission sets it up: a
+    spectrum read from core_spectrum_file with its luminosity the file's
+    integral, and a core temperature derived from L and r_core; every packet
+    against the reference's replayed step."""
+    import json
+    import os
+    from pubsed_b200 import workloads
+    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+    w = getattr(workloads, str(ref["generator"]))(**json.loads(str(ref["kwargs"])))
+    g = oracle_lib.Engine(sed_lib, "sed_", w)
+    g.set_opacity(1.0)
+    g.record(True)
+    st = g.transport(1.0)
+    n = int(ref["pkt_fate"].size)
+    rec = g.records(n)
+    for k in ("fate", "ind", "draws"):
+        assert np.array_equal(rec[k], ref["pkt_" + k]), k
+    oracle_lib.check_states(rec["state"], ref["pkt_state"].reshape(-1, 9))
+    assert st["n_escaped"] == int(ref["n_escaped"])
+    f, c = g.spectrum()
+    assert np.array_equal(c, ref["spec_click"])
+    g.close()

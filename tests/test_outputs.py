@@ -15,7 +15,7 @@ import oracle_lib
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["replay_grey_absorb", "replay_grey_radeq", "replay_ia_lte", "replay_cart3d", "replay_ia_radio",
-         "replay_ia_radio_late"]
+         "replay_ia_radio_late", "replay_core_file", "replay_core_derived"]
 
 
 @pytest.mark.parametrize("name", CASES)
