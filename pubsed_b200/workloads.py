@@ -143,6 +143,9 @@ class Workload:
         L0 = P.function("core_luminosity", 0.0)
         if L0 != 0 and r_core != 0 and T_core == 0:
             T_core = (L0 / (4.0 * PI * r_core * r_core * SB_CGS)) ** 0.25
+        L = P.function("core_luminosity", self.zones.t_now)
+        if P.scalar("core_n_emit", int) <= 0:  # no emission spectrum is set up then (:481)
+            return T_core, (L if L != 0 else L0), None
         g = self.nu_grid()
         path = P.get("core_spectrum_file")
         weights, L_sum = None, 0.0
@@ -163,7 +166,6 @@ class Workload:
                 else:
                     bb = 2.0 * nu * nu * nu * H_CGS / C_CGS / C_CGS / (math.exp(H_CGS * nu / K_CGS / T_core) - 1)
                 L_sum += 4.0 * PI * r_core * r_core * PI * bb * dnu
-        L = P.function("core_luminosity", self.zones.t_now)
         if L == 0:
             L = L0 if L0 != 0 else L_sum
         return T_core, L, weights
