@@ -2316,7 +2316,7 @@ int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32
 {
   if (!o || !o->have_grid) return SED_ERR_STATE;
   if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
-  if (o->gtype != SED_GRID_1D_SPHERE || o->tp.radiative_eq || o->tp.fleck_alpha != 0 ||
+  if (!o->homologous || o->tp.radiative_eq || o->tp.fleck_alpha != 0 ||
       (o->tp.steady_state && o->tp.core_fix_luminosity))
     return fail(o, SED_ERR_ARG, "differentiable transport: unsupported configuration");
   if (n_bands < 1 || n_bands > o->nu.n) return fail(o, SED_ERR_ARG, "bad band count");

@@ -23,8 +23,8 @@ int diff_args_ok(sed_ctx* c)
 {
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "differentiable transport: no grid");
   if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "differentiable transport: opacity tables not set");
-  if (c->gtype != SED_GRID_1D_SPHERE || !c->homologous)
-    return set_err(c, SED_ERR_ARG, "differentiable transport: homologous 1D spherical grids only");
+  if (!c->homologous)
+    return set_err(c, SED_ERR_ARG, "differentiable transport: homologous velocity fields only");
   if (c->tp.radiative_eq)
     return set_err(c, SED_ERR_ARG, "differentiable transport: needs transport_radiative_equilibrium = 0 "
                                    "(absorbed energy leaves the packet)");

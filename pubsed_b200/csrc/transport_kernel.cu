@@ -1822,17 +1822,23 @@ int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_
   return n + 1;
 }
 
-int launch_propagate_diff(const StepArgs& a, const GridDev& g, int mode, int num_sms, cudaStream_t s)
+template <int GRID>
+int launch_diff_t(const StepArgs& b, const GridDev& g, int mode, int num_sms, cudaStream_t s)
 {
   constexpr int T = SED_PROP_THREADS, B = SED_PROP_MINB;
-  if (g.type != 0 || !g.homologous || (mode != 1 && mode != 2)) return -1;
+  if (b.precision == 0)
+    return mode == 1 ? launch_kernel_t<GRID, double2, double, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
+                     : launch_kernel_t<GRID, double2, double, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
+  return mode == 1 ? launch_kernel_t<GRID, float2, float, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
+                   : launch_kernel_t<GRID, float2, float, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
+}
+
+int launch_propagate_diff(const StepArgs& a, const GridDev& g, int mode, int num_sms, cudaStream_t s)
+{
+  if (!g.homologous || (mode != 1 && mode != 2)) return -1;
   StepArgs b = a;
   if (mode == 2) b.smem_zones = 0;  // the replay tallies nothing per zone
-  if (a.precision == 0)
-    return mode == 1 ? launch_kernel_t<0, double2, double, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
-                     : launch_kernel_t<0, double2, double, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
-  return mode == 1 ? launch_kernel_t<0, float2, float, 0, T, B, 1>(b, g, 0, num_sms, b.n_packets, s)
-                   : launch_kernel_t<0, float2, float, 0, T, B, 2>(b, g, 0, num_sms, b.n_packets, s);
+  return g.type == 0 ? launch_diff_t<0>(b, g, mode, num_sms, s) : launch_diff_t<1>(b, g, mode, num_sms, s);
 }
 
 int launch_gamma(const StepArgs& a, const StepArgs& ag, const RadioArgs& r, const GridDev& g, int num_sms,

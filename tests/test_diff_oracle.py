@@ -64,6 +64,40 @@ def test_oracle_jacobian_matches_central_differences():
     o.close()
 
 
+def small_absorbing_3d(n_packets=3000, seed=11):
+    return workloads.with_params("cart3d", {"transport_radiative_equilibrium": 0}, n_packets=n_packets, n_cells=8,
+                                 n_lines=3000, n_bins=256, spectrum_bins=64, n_mu=4, epsilon=0.05, seed=seed)
+
+
+def test_oracle_jacobian_matches_central_differences_3d():
+    """The same check on an 8^3 Cartesian grid (viewing-angle spectrum).
+    Columns below 1e-4 of the Jacobian's largest entry are left out: the
+    rounding error of a central difference is about 1e-16 x bin / h, which
+    for a column 1e-6 of the largest entry is already 1e-6 of that column
+    (some columns here are 1e-23 of the largest)."""
+    w = small_absorbing_3d()
+    nb = 8
+    o = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    o.set_opacity(1.0)
+    theta = np.ones(o.nz * nb)
+    oracle_lib.diff_forward(o, theta, nb, step=4)
+    jac = oracle_lib.diff_jacobian(o, nb)
+    cols = np.flatnonzero(np.abs(jac).max(axis=0) > 1e-4 * np.abs(jac).max())
+    assert cols.size >= 64
+    rng = np.random.default_rng(1)
+    for q in rng.choice(cols, 8, replace=False):
+        tp, tm = theta.copy(), theta.copy()
+        tp[q] += FD_STEP
+        tm[q] -= FD_STEP
+        oracle_lib.diff_forward(o, tp, nb, step=4)
+        fp, _ = o.spectrum()
+        oracle_lib.diff_forward(o, tm, nb, step=4)
+        fm, _ = o.spectrum()
+        fd = (fp - fm) / (2 * FD_STEP)
+        assert np.abs(fd - jac[:, q]).max() <= FD_RTOL * np.abs(jac[:, q]).max(), q
+    o.close()
+
+
 def test_weighted_spectrum_matches_reference_discrete_spectrum():
     ref = np.load(os.path.join(GOLDEN, "free_ia_absorb.npz"))
     kw = json.loads(str(ref["kwargs"]))

@@ -69,6 +69,41 @@ def test_weighted_forward_and_adjoint_match_oracle(sed_lib):
     g.close()
 
 
+def test_weighted_forward_and_adjoint_match_oracle_3d(sed_lib):
+    """The weighted forward and both replays on an 8^3 Cartesian grid
+    against the oracle on the same deviates."""
+    n, nb = 3000, 8
+    w = workloads.with_params("cart3d", {"transport_radiative_equilibrium": 0}, n_packets=n, n_cells=8,
+                              n_lines=3000, n_bins=256, spectrum_bins=64, n_mu=4, epsilon=0.05, seed=11)
+    o = oracle_lib.Engine(oracle_lib.oracle_lib(), "oracle_", w)
+    g = oracle_lib.Engine(sed_lib, "sed_", w)
+    theta = 1 + 0.2 * np.random.default_rng(3).standard_normal(o.nz * nb)
+    for e in (o, g):
+        e.set_opacity(1.0)
+        e.record(True)
+        oracle_lib.diff_forward(e, theta, nb, step=2)
+    ro, rg = o.records(n), g.records(n)
+    assert np.array_equal(ro["fate"], rg["fate"])
+    assert np.array_equal(ro["ind"], rg["ind"])
+    assert np.array_equal(ro["draws"], rg["draws"])
+    oracle_lib.check_states(rg["state"], ro["state"])
+    fo, co = o.spectrum()
+    fg, cg = g.spectrum()
+    assert np.array_equal(co, cg)
+    assert np.abs(fg - fo).max() <= oracle_lib.TALLY_RTOL * np.abs(fo).max()
+    Jo, Jg = oracle_lib.diff_jacobian(o, nb), oracle_lib.diff_jacobian(g, nb)
+    assert np.abs(Jo).max() > 0
+    assert np.abs(Jg - Jo).max() <= 1e-10 * np.abs(Jo).max()
+    gv = np.random.default_rng(4).standard_normal(o.nspec)
+    vg = oracle_lib.diff_vjp(g, gv, nb)
+    assert np.abs(vg - gv @ Jo).max() <= 1e-10 * np.abs(gv) @ np.abs(Jo).max(axis=1)
+    dg, do = oracle_lib.diff_vjp_density(g, gv), oracle_lib.diff_vjp_density(o, gv)
+    assert np.abs(do).max() > 0
+    assert np.abs(dg - do).max() <= 1e-9 * np.abs(do).max()
+    o.close()
+    g.close()
+
+
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
 def test_adjoint_matches_central_differences(sed_lib, precision):
     w = absorbing(100_000, n_zones=64, n_lines=20000, n_bins=1024, spectrum_bins=256, seed=41)
