@@ -334,8 +334,8 @@ int sed_set_rng_step(sed_ctx* ctx, uint32_t step);
  * the reference (it has no adjoint); the checks are central finite
  * differences of the weighted forward itself with common random numbers.
  *
- * The weighted forward is the same transport step (1D sphere, after
- * sed_set_opacity or sed_load_opacity) with one change of estimator:
+ * The weighted forward is the same transport step (homologous 1D sphere or
+ * 3D Cartesian grid, after sed_set_opacity or sed_load_opacity) with one change of estimator:
  * interactions are sampled from the scattering opacity alone and absorption
  * is a continuous weight exp(-a dshift l) on each segment.  Its expected
  * spectrum is the reference's (radiative_eq = 0, fleck_alpha = 0, no
