@@ -24,7 +24,7 @@ def gpu_available() -> bool:
 
 @pytest.fixture(scope="session")
 def sed_lib():
-    """The CUDA library; GPU tests fail (not skip) if it is missing on a GPU box."""
+    """The CUDA library; GPU tests fail (not skip) if it is missing on a machine with a GPU."""
     if not gpu_available():
         pytest.skip("no CUDA device")
     from pubsed_b200 import _lib
