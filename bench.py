@@ -54,6 +54,25 @@ METRIC = "MC packets/s at matched spectrum chi-squared (mixed/batched vs plain F
 UNIT = "packets/s"
 
 
+def captured_traffic(workload: str, n_segments: int):
+    """DRAM bytes (read + write) of one packet-kernel launch of `workload`
+    from the ncu captures in profiles/propagate_kernel_traffic.json: as
+    captured where the working set stays in L2 (scale "none"), else scaled
+    from the captured launch by segments.  None without a capture."""
+    tfile = os.path.join(ROOT, "profiles", "propagate_kernel_traffic.json")
+    if not os.path.exists(tfile):
+        return None
+    with open(tfile) as f:
+        entries = json.load(f)
+    for tr in entries if isinstance(entries, list) else [entries]:
+        if tr.get("workload") != workload:
+            continue
+        if tr.get("scale") == "segments":
+            return float(tr["dram_bytes"]) / float(tr["segments"]) * float(n_segments)
+        return float(tr["dram_bytes"])
+    return None
+
+
 def _env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -304,7 +323,8 @@ def main_batch(args, rank: int, world: int, local: int):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                       "traffic": None, "kernel": "propagate_kernel (batched)", "kernel_ms": kern_ms,
+                       "traffic": captured_traffic(bw.name, last["n_segments"]),
+                       "kernel": "propagate_kernel (batched)", "kernel_ms": kern_ms,
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
     out["clocks"] = clk.summary()
     if not args.no_cpu_baseline:
@@ -684,18 +704,7 @@ def main():
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "propagate_kernel_traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            tr = json.load(f)
-        # DRAM bytes of one launch of this workload's packet kernel captured
-        # with ncu (after the same L2 flush); the tables stay L2-resident, so
-        # the traffic is their first touch and does not grow with the packet
-        # count when the capture says so
-        same_n = int(tr.get("packets", -1)) == args.packets or tr.get("scales_with_packets") is False
-        if same_n and tr.get("workload") == w.name:
-            traffic = float(tr["dram_bytes"])
+    traffic = captured_traffic(w.name, last["n_segments"])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
