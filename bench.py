@@ -156,8 +156,8 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": w.name, "n_zones": w_full.zones.n_zones, "n_lines": w.notes.get("n_lines"),
-                       "n_bins": w.nu_grid().n, "packets_per_step": n_sample, "threads": cores,
-                       "sample_zones": w.zones.n_zones},
+                       "n_bins": w.nu_grid().n, "packets_per_step": n_full, "threads": cores,
+                       "sample_packets_per_step": n_sample_all, "sample_zones": w.zones.n_zones},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": "transport::step of the %s workload (%s sizes) with %d "
                                        "packets per step (%.2f s, of which set_opacity %.2f s); full-step time "
@@ -489,7 +489,8 @@ def main_ddmc(args, rank: int, world: int, local: int):
                           "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                           "data": "synthetic", "config": {"workload": "diffusing_pulse_1d_ddmc",
-                                                          "packets_per_step": n_ref, "threads": cores},
+                                                          "packets_per_step": n, "threads": cores,
+                                                          "sample_packets_per_step": n_ref},
                           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                                            "sample": note},
                           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
