@@ -1764,8 +1764,10 @@ int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int 
 }
 
 // Single-context shapes, measured on the Type Ia step (1e7 packets): the
-// mixed form runs best with 256 x 3 (80 registers, 976 ms vs 1019 ms at
-// 128 x 8), the FP64 form with 256 x 4 (64 registers, 1753 ms vs 1788 ms).
+// FP64 form runs best with 256 x 4 (64 registers, 1753 ms vs 1788 ms at
+// 128 x 8); the mixed form with 128 x 7 on 1D grids (72 registers, 28 warps
+// per SM: 928 ms vs 959 ms at 256 x 3 and 1019 ms at 128 x 8) while seven
+// blocks' zone tallies fit in shared memory, else 256 x 3 (80 registers).
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
@@ -1777,8 +1779,13 @@ int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStr
   // expressions (the division-free transforms assume v = x / t)
   if (sizeof(OT) == sizeof(float2) && !g.homologous)
     return launch_kernel_t<GRID, OT, CT, 0, 256, 4, 0, false>(a, g, 0, num_sms, a.n_packets, s);
-  if (sizeof(OT) == sizeof(float2))
+  if constexpr (sizeof(OT) == sizeof(float2)) {
+    if constexpr (GRID == 0) {
+      if (!a.smem_zones || (size_t)7 * 5 * g.nzones * sizeof(double) <= (size_t)200 * 1024)
+        return launch_kernel_t<0, OT, CT, 0, 128, 7>(a, g, 0, num_sms, a.n_packets, s);
+    }
     return launch_kernel_t<GRID, OT, CT, 0, 256, 3>(a, g, 0, num_sms, a.n_packets, s);
+  }
   return launch_kernel_t<GRID, OT, CT, 0, 256, 4>(a, g, 0, num_sms, a.n_packets, s);
 }
 
