@@ -36,6 +36,16 @@ enum sed_status {
   SED_ERR_NOMEM = 6      /* device allocation failed */
 };
 
+/* Warnings of a step (sed_step_stats.warnings): conditions the reference
+ * reports on stderr and carries on from. */
+enum sed_warning {
+  /* the core packets did not fit next to the census and the radioactive
+   * packets (particles_max_total): none were emitted this step and the step
+   * propagated the others, as emit_inner_source does after printing
+   * "# Not enough particle space" (src/transport/emission.cpp:391-392) */
+  SED_WARN_NO_PARTICLE_SPACE = 1
+};
+
 /* Bin-edge array with the semantics of locate_array
  * (src/utils/locate_array.h:15-217): n bins, `right[i]` is the right wall of
  * bin i, `min` the left wall of bin 0; bins are closed on the left. */
@@ -183,7 +193,7 @@ typedef struct sed_step_stats {
   int64_t n_scatters;            /* interaction events */
   int64_t n_limit;               /* packets stopped by the segment limit */
   int32_t kernel_launches;       /* kernels launched by the call */
-  int32_t reserved;
+  int32_t warnings;              /* sed_warning bits of the step */
   float ms_opacity;              /* device time of the opacity build */
   float ms_transport;            /* device time of emission + propagation */
   float ms_total;                /* device time of the whole call */
@@ -220,7 +230,10 @@ int sed_load_opacity(sed_ctx* ctx, const double* abs, const double* scat,
 /* Wipes tallies, emits the core packets, propagates every packet, tallies
  * escapes and normalises J/e_abs/e_rad.  Replaces transport.cpp:46-124
  * (wipe_radiation, emit_particles, the propagate loop, spectrum count,
- * clean_up_particle_vector, steady-state rescale, reduce_radiation). */
+ * clean_up_particle_vector, steady-state rescale, reduce_radiation).
+ * Core packets that would not fit next to the census and the radioactive
+ * packets are not emitted: the step runs without them and sets
+ * SED_WARN_NO_PARTICLE_SPACE in stats->warnings (emission.cpp:391-392). */
 int sed_transport(sed_ctx* ctx, double dt, sed_step_stats* stats);
 
 /* sed_set_opacity followed by sed_transport: transport::step
@@ -360,7 +373,11 @@ int sed_diff_vjp(sed_ctx* ctx, const double* grad_flux, double* grad_scale, sed_
  * (a likelihood-ratio estimator: unbiased, noisier than the pathwise one). */
 int sed_diff_vjp_density(sed_ctx* ctx, const double* grad_flux, double* grad_rho, sed_step_stats* stats);
 /* Full Jacobian of the last weighted forward: jac[(s * n_zones + z) * n_bands
- * + k] = d flux[s] / d abs_scale[z, k], s over the n_spec spectrum bins. */
+ * + k] = d flux[s] / d abs_scale[z, k], s over the n_spec spectrum bins.
+ * The three replays need the context as the forward left it: any call of
+ * sed_set_grid, sed_set_opacity, sed_load_opacity, sed_step, sed_transport,
+ * sed_set_time, sed_initialize_particles, sed_set_core_source or
+ * sed_set_emission in between makes them return SED_ERR_STATE. */
 int sed_diff_jacobian(sed_ctx* ctx, double* jac, sed_step_stats* stats);
 
 /* ------------------------------------------------------------------ batches

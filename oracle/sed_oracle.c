@@ -1916,7 +1916,11 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
   int64_t n_census = o->n_census;
   int64_t n_radio = o->tp.n_emit_radioactive > 0 ? o->tp.n_emit_radioactive : 0;
   if (n_census + n_radio > o->tp.max_particles) n_radio = 0;
-  if (n_census + n_radio + n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
+  /* emit_inner_source: "# Not enough particle space", nothing emitted, and
+   * the step goes on with the census and radioactive packets
+   * (emission.cpp:391-392) */
+  int32_t warnings = 0;
+  if (n_census + n_radio + n_emit > o->tp.max_particles) { n_emit = 0; warnings |= SED_WARN_NO_PARTICLE_SPACE; }
   int64_t n_q = n_census + n_radio, n_all = n_emit + n_q;
   int census_gammas = 0;
   for (int64_t k = 0; k < n_census; ++k) census_gammas += (o->c_type[k] == T_GAMMA);
@@ -2036,7 +2040,7 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
   if (st) {
     memset(st, 0, sizeof *st);
     st->n_packets = n_all; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
-    st->n_segments = nseg; st->n_scatters = nscat;
+    st->n_segments = nseg; st->n_scatters = nscat; st->warnings = warnings;
   }
   if (o->n_reject_cap > 0) return fail(o, SED_ERR_LIMIT, "Compton scatters hit the rejection-sampling bound");
   return SED_OK;
@@ -2174,7 +2178,8 @@ int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
   if (!o) return SED_ERR_ARG;
   if (o->tp.use_ddmc != 0 && (o->tp.use_ddmc != 2 || o->gtype != SED_GRID_1D_SPHERE))
     return fail(o, SED_ERR_ARG, "discrete diffusion is built for method 2 on 1D spheres");
-  if (o->tp.n_emit_radioactive > 0 || o->n_census > 0 || !o->tp.steady_state) {
+  if (o->tp.n_emit_radioactive > 0 || o->n_census > 0 || !o->tp.steady_state ||
+      (int64_t)(o->tp.core_n_emit / 1.0) > o->tp.max_particles) {
     if (!o->have_grid) return SED_ERR_STATE;
     if (!o->have_opacity) return fail(o, SED_ERR_STATE, "opacity tables not set");
     return transport_general(o, dt, st);

@@ -16,6 +16,7 @@ SED_OK = 0
 SED_ERR_ARG = 1
 SED_ERR_CUDA = 2
 SED_ERR_CAPACITY = 3
+SED_WARN_NO_PARTICLE_SPACE = 1
 SED_ERR_STATE = 4
 SED_ERR_LIMIT = 5
 SED_ERR_NOMEM = 6
@@ -94,13 +95,13 @@ class StepStats(C.Structure):
     _fields_ = [
         ("n_packets", C.c_int64), ("n_escaped", C.c_int64), ("n_absorbed", C.c_int64),
         ("n_stopped", C.c_int64), ("n_segments", C.c_int64), ("n_scatters", C.c_int64),
-        ("n_limit", C.c_int64), ("kernel_launches", C.c_int32), ("reserved", C.c_int32),
+        ("n_limit", C.c_int64), ("kernel_launches", C.c_int32), ("warnings", C.c_int32),
         ("ms_opacity", C.c_float), ("ms_transport", C.c_float), ("ms_total", C.c_float),
         ("ms_propagate_kernel", C.c_float),
     ]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class BatchModel(C.Structure):

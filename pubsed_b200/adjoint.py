@@ -43,16 +43,33 @@ class DiffEngine(Engine):
         self.n_bands = int(n_bands)
         self.forward_id = 0          # increments with every forward
         self._have_tables = False
+        self._base = None            # tables of the last opacity build, kept while density-scaled ones are loaded
+        self._scaled = False         # the context holds density-scaled tables
 
     def tables(self, dt: float = 1.0):
         """Opacity build (sed_set_opacity); the forward runs on these tables."""
         self.set_opacity(dt)
         self._have_tables = True
+        self._base = None
+        self._scaled = False
+
+    def _load(self, abs_, scat):
+        b = self._base
+        k = abi.Keep()
+        self._check(self.L.sed_load_opacity(self.ctx, k.d(abs_), k.d(scat), k.d(b["emis_cdf"]), k.d(b["eps_imc"])),
+                    "sed_load_opacity")
 
     def forward(self, theta: Optional[np.ndarray] = None, step: Optional[int] = None, dt: float = 1.0):
-        """Weighted forward; returns (flux, click, stats)."""
+        """Weighted forward on the tables of the last opacity build; returns
+        (flux, click, stats)."""
         if not self._have_tables:
             self.tables(dt)
+        if self._scaled:  # a density forward left scaled tables: put the built ones back
+            self._load(self._base["abs"], self._base["scat"])
+            self._scaled = False
+        return self._forward(theta, step, dt)
+
+    def _forward(self, theta, step, dt):
         if step is not None:
             self._check(self.L.sed_set_rng_step(self.ctx, int(step) & 0xFFFFFFFF), "sed_set_rng_step")
         k = abi.Keep()
@@ -97,18 +114,16 @@ class DiffEngine(Engine):
         scattering); returns (flux, click, stats)."""
         if not self._have_tables:
             self.tables(dt)
-        if not hasattr(self, "_base"):
+        if self._base is None:
             self._base = self.opacity()
         r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
         if r.size != self.nz:
             raise ValueError("r has %d entries, expected %d" % (r.size, self.nz))
         b = self._base
-        ab = (b["abs"].reshape(self.nz, -1) * r[:, None]).ravel()
-        sc = (b["scat"].reshape(self.nz, -1) * r[:, None]).ravel()
-        k = abi.Keep()
-        self._check(self.L.sed_load_opacity(self.ctx, k.d(ab), k.d(sc), k.d(b["emis_cdf"]), k.d(b["eps_imc"])),
-                    "sed_load_opacity")
-        return self.forward(None, step=step, dt=dt)
+        self._load((b["abs"].reshape(self.nz, -1) * r[:, None]).ravel(),
+                   (b["scat"].reshape(self.nz, -1) * r[:, None]).ravel())
+        self._scaled = True
+        return self._forward(None, step, dt)
 
     def jacobian(self) -> np.ndarray:
         out = np.zeros(self.nspec * self.nz * self.n_bands)

@@ -802,8 +802,11 @@ extern "C" int sed_lte_electron_density_noalloc(int32_t n_zones, const double* r
     return SED_ERR_ARG;
   const size_t nz = (size_t)n_zones, na = (size_t)n_elems;
   const size_t ni = (size_t)n_ions_total, nl = (size_t)n_levels_total;
-  const size_t need = nz * (2 * na + 2 + 2 * ni + 2 * nl);
-  if (need > NOALLOC_SCRATCH_DOUBLES) return SED_ERR_CAPACITY;  // limit stated in include/sedona_gpu.h
+  // doubles per zone, then zones: the limit is checked as a quotient so that
+  // no product of the caller's counts can wrap around
+  const size_t per_zone = 2 * na + 2 + 2 * ni + 2 * nl;
+  if (per_zone > NOALLOC_SCRATCH_DOUBLES || nz > NOALLOC_SCRATCH_DOUBLES / per_zone)
+    return SED_ERR_CAPACITY;  // limit stated in include/sedona_gpu.h
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return SED_ERR_CUDA;

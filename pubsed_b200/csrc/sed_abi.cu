@@ -256,6 +256,7 @@ int sed_ctx_create(const sed_transport_params* p, int device, sed_ctx** out)
 int sed_set_grid(sed_ctx* c, const sed_grid* g)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!g || g->n_zones <= 0 || !g->vol || !g->rho || !g->T_gas) return set_err(c, SED_ERR_ARG, "sed_set_grid: missing zone arrays");
   if (g->n_elems < 0 || (g->n_elems > 0 && (!g->X || !g->elem_A || !g->elem_Z)))
     return set_err(c, SED_ERR_ARG, "sed_set_grid: missing composition");
@@ -463,6 +464,7 @@ int sed_set_atomic_data(sed_ctx* c, const sed_atomic_data* a)
 int sed::enqueue_opacity(sed_ctx* c, double dt)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_set_opacity: no grid");
   if (c->tp.steady_state) dt = 1;
   OpacityArgs A{};
@@ -550,6 +552,7 @@ int sed_set_opacity(sed_ctx* c, double dt)
 int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const double* emis_cdf, const double* eps_imc)
 {
   if (!c || !abs || !emis_cdf || !eps_imc) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_load_opacity: no grid");
   const size_t n = (size_t)c->nz * c->nu.n();
   // guide tables of the stored rows (value(i) = stored CDF entry i as a double)
@@ -640,23 +643,29 @@ static int build_census(sed_ctx* c, CensusArgs& C, int64_t n_all, int64_t* n_ali
 static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms_opacity)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_transport: no grid");
   if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "sed_transport: opacity tables not set");
   if (c->tp.steady_state) dt = 1;
   const bool timedep = !c->tp.steady_state;
   // emit_inner_source packet count and energy (src/transport/emission.cpp:383-392)
-  const int64_t n_emit = (int64_t)(c->tp.core_n_emit / 1.0);
+  int64_t n_emit = (int64_t)(c->tp.core_n_emit / 1.0);
   // The packet list of the step (transport.cpp:46-54): the census the last
   // step left, then emit_radioactive (emission.cpp:163-243: it adds nothing
   // when its packets would not fit next to the census), then the core
-  // packets, which must fit next to both.  Census and radioactive packets
-  // are the queue; their Philox streams come first, the core packets' after.
+  // packets.  When those would not fit next to both, emit_inner_source
+  // prints "# Not enough particle space" and emits nothing
+  // (emission.cpp:391-392), and the step goes on with the others: so here,
+  // flagged in the step's warnings.  Census and radioactive packets are the
+  // queue; their Philox streams come first, the core packets' after.
   const int64_t n_census = c->n_census;
   int64_t n_radio = c->tp.n_emit_radioactive > 0 ? c->tp.n_emit_radioactive : 0;
   if (n_census + n_radio > c->tp.max_particles) n_radio = 0;
-  if (n_census + n_radio + n_emit > c->tp.max_particles)
-    return set_err(c, SED_ERR_CAPACITY, "Not enough particle space: %lld packets > particles_max_total %lld",
-                   (long long)(n_census + n_radio + n_emit), (long long)c->tp.max_particles);
+  int32_t warnings = 0;
+  if (n_census + n_radio + n_emit > c->tp.max_particles) {
+    n_emit = 0;
+    warnings |= SED_WARN_NO_PARTICLE_SPACE;
+  }
   if (c->tp.use_ddmc != 0 && (c->tp.use_ddmc != 2 || c->gtype != SED_GRID_1D_SPHERE))
     return set_err(c, SED_ERR_ARG, "transport_use_ddmc %d: discrete diffusion is built for method 2 on 1D spheres",
                    (int)c->tp.use_ddmc);
@@ -799,6 +808,7 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     stats->n_scatters = (int64_t)cnt[C_SCATTERS];
     stats->n_limit = (int64_t)cnt[C_LIMIT];
     stats->kernel_launches = launches;
+    stats->warnings = warnings;
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
     stats->ms_propagate_kernel = ms;
@@ -820,6 +830,7 @@ int sed_transport(sed_ctx* c, double dt, sed_step_stats* stats) { return transpo
 int sed_set_emission(sed_ctx* c, double core_n_emit, int64_t n_emit_radioactive)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!(core_n_emit >= 0) || n_emit_radioactive < 0)
     return set_err(c, SED_ERR_ARG, "sed_set_emission: negative packet count");
   c->tp.core_n_emit = core_n_emit;
@@ -973,6 +984,7 @@ int64_t sed_n_particles(sed_ctx* c) { return c ? c->n_census : 0; }
 int sed_set_core_source(sed_ctx* c, double luminosity, const double* weights)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!(luminosity >= 0)) return set_err(c, SED_ERR_ARG, "sed_set_core_source: luminosity %g", luminosity);
   c->tp.core_luminosity = luminosity;
   if (weights) {
@@ -1006,6 +1018,7 @@ int sed_wipe_spectra(sed_ctx* c)
 int sed_set_time(sed_ctx* c, double t_now)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   c->t_now = t_now;
   c->have_t_now = true;
   return SED_OK;
@@ -1029,6 +1042,7 @@ int sed_get_particles(sed_ctx* c, int64_t n, int32_t* ind, int32_t* type, double
 int sed_initialize_particles(sed_ctx* c, int64_t n, const double* e_rad)
 {
   if (!c) return SED_ERR_ARG;
+  c->have_diff = false;  // the last weighted forward no longer matches the context
   if (!c->have_grid) return set_err(c, SED_ERR_STATE, "sed_initialize_particles: no grid");
   if (n < 0 || (n > 0 && !e_rad)) return set_err(c, SED_ERR_ARG, "sed_initialize_particles: bad arguments");
   if (n == 0) return SED_OK;

@@ -344,12 +344,12 @@ def time_dependent(base: str, n_initialize: int = 0, dt_days: float = 0.1, param
     carried to the next, the grid expands homologously between steps
     (`homologous_step`), and particles_n_initialize packets of the initial
     radiation field (e_rad = a T^4) start in the census; `params` are set
-    over the base's parameters.  notes["dt"] is the step (dt_days)."""
+    last, over the base's parameters and these.  notes["dt"] is the step (dt_days)."""
     w = globals()[base](**kw)
-    w.params.update(params or {})
     w.params["transport_steady_iterate"] = 0
     w.params["particles_n_initialize"] = int(n_initialize)
     w.params["particles_max_total"] = max(int(w.params.get("particles_max_total", 1e7)), 4 * int(n_initialize) + 1)
+    w.params.update(params or {})
     w.name = w.name + "_td"
     w.notes["dt"] = dt_days * 86400.0
     return w

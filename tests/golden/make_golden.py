@@ -88,6 +88,12 @@ TD_CASES = {
                                                    params={"transport_use_ddmc": 2,
                                                            "transport_ddmc_tau_threshold": 0.1},
                                                    n_packets=0, n_zones=32, n_bins=64, radiative_eq=1, seed=7), 3),
+    # particles_max_total below census + core packets on every other step:
+    # those steps emit no core packets ("# Not enough particle space") and
+    # propagate the census alone
+    "replay_td_full": ("time_dependent", dict(base="lightbulb_grey", n_initialize=300, dt_days=0.1, n_packets=200,
+                                              n_zones=32, n_bins=128, radiative_eq=0, seed=37,
+                                              params={"particles_max_total": 450}), 4),
 }
 TD_KEYS = ["pkt_fate", "pkt_ind", "pkt_draws", "pkt_state", "pkt_type", "census_ind", "census_type", "census_state",
            "J_nu", "e_abs", "e_rad", "fr_rad", "spec_flux", "spec_click", "T_gas"]

@@ -241,3 +241,29 @@ def test_density_autograd_function(sed_lib):
     ref = e.vjp_density(g.numpy()) / 1.1
     assert np.allclose(r.grad.numpy(), ref, rtol=1e-12, atol=0)
     e.close()
+
+
+def test_density_forward_leaves_the_built_tables(sed_lib):
+    """Forwards on the built tables, on density-scaled tables and after a
+    rebuild at another temperature interleave: a plain forward always runs on
+    the last build, a density forward scales the last build (not an earlier
+    one), and a replay after a call that changed the context is refused."""
+    w = workloads.type_ia(n_packets=20_000, n_zones=16, n_lines=2000, n_bins=128, spectrum_bins=32, epsilon=1e-4,
+                          radiative_eq=0, seed=33)
+    e = DiffEngine(w, n_bands=1)
+    f0, _, _ = e.forward(step=3)
+    f1, _, _ = e.forward_density(np.full(e.nz, 1.3), step=3)
+    assert not np.array_equal(f0, f1)
+    f2, _, _ = e.forward(step=3)
+    assert np.array_equal(f0, f2)  # the built tables are back
+    w.zones.T = w.zones.T * 1.1
+    e.upload_grid()
+    e.tables()
+    g0, _, _ = e.forward(step=3)
+    g1, _, _ = e.forward_density(np.ones(e.nz), step=3)
+    assert np.array_equal(g0, g1)  # density factor 1 on the new build, not the old one
+    assert not np.array_equal(g0, f0)
+    e.tables()  # a rebuild after the forward: nothing left to replay
+    with pytest.raises(RuntimeError, match="replay"):
+        e.vjp(np.ones(e.nspec))
+    e.close()

@@ -153,17 +153,23 @@ def test_no_radioactive_material_emits_nothing(sed_lib):
 
 
 def test_capacity_rules(sed_lib):
-    """Core and radioactive packets must fit in particles_max_total together
-    (an error, as the reference's emit_inner_source); radioactive packets
-    that alone exceed it are not emitted (emission.cpp:215-218)."""
+    """Core packets that do not fit next to the radioactive ones are not
+    emitted and the step runs with the decay packets alone, flagged in its
+    warnings (emit_inner_source, emission.cpp:391-392); radioactive packets
+    that alone exceed particles_max_total are not emitted
+    (emission.cpp:215-218)."""
     w = workloads.type_ia(n_packets=500, n_zones=16, n_lines=2000, n_bins=128, n_levels_per_ion=6, v_core=1e8,
                           n_radioactive=300, seed=43)
     w.params["particles_max_total"] = 700
-    g = oracle_lib.Engine(sed_lib, "sed_", w)
-    g.set_opacity(1.0)
-    with pytest.raises(RuntimeError, match=r"\(3\)"):
-        g.transport(1.0)
-    g.close()
+    out = []
+    for lib in (sed_lib, oracle_lib.oracle_lib()):
+        e, st = _step(lib, w)
+        assert st["n_packets"] == 300
+        assert st["warnings"] & abi.SED_WARN_NO_PARTICLE_SPACE
+        out.append(e.records(300))
+        e.close()
+    assert np.array_equal(out[0]["fate"], out[1]["fate"])
+    assert np.array_equal(out[0]["draws"], out[1]["draws"])
     w.params["particles_max_total"] = 200
     w.params["core_n_emit"] = 100
     for lib in (sed_lib, oracle_lib.oracle_lib()):

@@ -33,7 +33,8 @@ def _load(name):
     return d, kw
 
 
-@pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio", "replay_td_ddmc_ia", "replay_td_ddmc_grey"])
+@pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio", "replay_td_ddmc_ia", "replay_td_ddmc_grey",
+                                  "replay_td_full"])
 def test_time_dependent_steps_match_reference_replay(sed_lib, name):
     ref, kw = _load(name)
     w = workloads.time_dependent(**kw)
@@ -43,6 +44,8 @@ def test_time_dependent_steps_match_reference_replay(sed_lib, name):
     for s, r in enumerate(res):
         sf = "_s%d" % s
         rec = r["records"]
+        if name == "replay_td_full":  # every other step has no room for its core packets
+            assert bool(r["stats"]["warnings"] & abi.SED_WARN_NO_PARTICLE_SPACE) == (s % 2 == 0), s
         for k in ("fate", "ind", "draws"):
             assert np.array_equal(rec[k], ref["pkt_" + k + sf]), (s, k)
         oracle_lib.check_states(rec["state"], ref["pkt_state" + sf].reshape(-1, 9))

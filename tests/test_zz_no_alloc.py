@@ -111,3 +111,10 @@ def test_noalloc_rejects_oversized_request(sed_lib):
     # the size check runs before any device access
     rc = f(100000, 1, 1, 1, 1, 1, C.byref(ad), 2, 2, 1e3, 1e8, 1, 1, None)
     assert rc == abi.SED_ERR_CAPACITY
+    # counts whose 64-bit product zones x doubles-per-zone wraps around to
+    # 458740, below the array size: still refused
+    nz, na, ni, nl = 2147450882, 1431677610, 1431677609, 1431677609
+    assert (nz * (2 * na + 2 + 2 * ni + 2 * nl)) % 2**64 < 524288
+    ad.n_atoms = na
+    rc = f(nz, 1, 1, 1, na, 1, C.byref(ad), ni, nl, 1e3, 1e8, 1, 1, None)
+    assert rc == abi.SED_ERR_CAPACITY
