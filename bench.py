@@ -152,11 +152,17 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
     grid_note = "" if zone_scale == 1 else (
         " on a reduced %d-zone grid of the same model: set_opacity scaled by the zone count (x%g), "
         "propagation per packet measured on the reduced grid" % (w.zones.n_zones, zone_scale))
+    # what ran is a step of n_sample_all packets (ms_per_step); the value is
+    # the throughput of a full step projected from it (projected_ms_per_step)
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_sample * 1e3,
+            "projected_ms_per_step": t * 1e3,
+            "value_basis": "projected: %d packets / (set_opacity + propagation per packet x %d packets), "
+                           "from steps of %d packets" % (n_full, n_full, n_sample_all),
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": w.name, "n_zones": w_full.zones.n_zones, "n_lines": w.notes.get("n_lines"),
-                       "n_bins": w.nu_grid().n, "packets_per_step": n_full, "threads": cores,
+                       "n_bins": w.nu_grid().n, "projected_packets_per_step": n_full, "threads": cores,
                        "sample_packets_per_step": n_sample_all, "sample_zones": w.zones.n_zones},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": "transport::step of the %s workload (%s sizes) with %d "
@@ -169,15 +175,93 @@ def run_reference(args, workload_fn, rank: int, sample_fn=None) -> dict:
 
 
 # ------------------------------------------------------------------ batches
-def _chi2_per_dof(fa, ca, fb, cb, min_clicks=10):
-    """chi^2 / dof between two binned spectra, sigma^2 = F^2 / clicks per run,
-    over bins with at least `min_clicks` packets in both."""
+def _timed_batch(bw, local, flush, precision, steps, warmup, tune=True, clock=False):
+    """The batch stepped as one (CUDA graphs, autotuned launch shape): the
+    engine, per-step stats, the tuning and the clock sampler."""
+    import torch
+    from pubsed_b200.batch import BatchEngine
+    be = BatchEngine(bw, precision=precision, device=local, graph=True)
+    tuning = be.autotune(0.02) if tune else None
+    for _ in range(warmup):
+        flush.fill_(1.0)
+        be.step(1.0)
+    stats = []
+    clk = ClockSampler(local)
+    with (clk if clock else _Null()):
+        for i in range(steps):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            stats.append(be.step(1.0))
+    return be, stats, tuning, clk
+
+
+def _separate(bw, local, flush, precision):
+    """The batch's models as separate contexts, one after another (a warm-up
+    step each, then one timed step): total device ms and the spectra."""
+    import torch
+    from pubsed_b200 import engine
+    tot_ms, specs = 0.0, []
+    for w in bw.models:
+        e = engine.Engine(w, precision=precision, device=local)
+        flush.fill_(1.0)
+        e.step(1.0)
+        flush.fill_(2.0)
+        torch.cuda.synchronize()
+        tot_ms += e.step(1.0)["ms_total"]
+        specs.append(e.spectrum())
+        e.close()
+    return tot_ms, specs
+
+
+def batch_leg(local, flush, packet_scale: float, steps: int = 2, warmup: int = 2) -> dict:
+    """The batching configuration at `packet_scale` of its packets: batched
+    mixed-precision packets/s against the same models as separate plain-FP64
+    contexts, and the per-model chi^2 / dof between the two forms' spectra."""
+    from pubsed_b200 import abi, workloads
+    bw = workloads.batch64(packet_scale=packet_scale)
+    n = bw.n_packets
+    be, stats, tuning, _ = _timed_batch(bw, local, flush, abi.PREC_MIXED, steps, warmup)
+    ms = sum(st["ms_total"] for st in stats) / len(stats)
+    spec_b = [be.spectrum(m) for m in range(len(bw.models))]
+    be.close()
+    ms64, spec64 = _separate(bw, local, flush, abi.PREC_FP64)
+    chi2 = [_chi2_per_dof(fb, cb, f6, c6) for (fb, cb), (f6, c6) in zip(spec_b, spec64)]
+    chi2 = [c for c in chi2 if c is not None]
+    return {"packet_scale": packet_scale, "packets_per_step": n, "n_models": len(bw.models),
+            "mixed_batched": {"value": n / (ms * 1e-3), "ms_per_step": ms, "steps": steps, "tuning": tuning},
+            "plain_fp64": {"value": n / (ms64 * 1e-3), "ms_per_step": ms64,
+                           "form": "separate contexts, FP64 tables, one after another"},
+            "ratio": ms64 / ms,
+            "chi2_per_dof_vs_plain_fp64": {"median": float(np.median(chi2)) if chi2 else None,
+                                           "max": float(np.max(chi2)) if chi2 else None, "models": len(chi2)}}
+
+
+def _chi2(fa, ca, fb, cb, min_clicks=10):
+    """chi^2 between two binned spectra of independent runs, sigma^2 =
+    F^2 / clicks per run (equal-energy packets), over the bins with at least
+    `min_clicks` packets in both: (chi^2, dof) or None."""
     use = (ca >= min_clicks) & (cb >= min_clicks)
     if not use.any():
         return None
     va = fa[use] ** 2 / ca[use]
     vb = fb[use] ** 2 / cb[use]
-    return float(np.sum((fa[use] - fb[use]) ** 2 / (va + vb)) / use.sum())
+    return float(np.sum((fa[use] - fb[use]) ** 2 / (va + vb))), int(use.sum())
+
+
+def _chi2_per_dof(fa, ca, fb, cb, min_clicks=10):
+    r = _chi2(fa, ca, fb, cb, min_clicks)
+    return None if r is None else r[0] / r[1]
+
+
+def chi2_summary(fa, ca, fb, cb) -> dict:
+    """chi^2 / dof, dof and the p-value of chi^2 for that many degrees of
+    freedom (the survival function of the chi^2 distribution)."""
+    from scipy import stats as sst
+    r = _chi2(fa, ca, fb, cb)
+    if r is None:
+        return {"chi2_per_dof": None, "dof": 0, "p_value": None}
+    c, dof = r
+    return {"chi2_per_dof": c / dof, "dof": dof, "p_value": float(sst.chi2.sf(c, dof))}
 
 
 def reference_batch(bw, n_sample: int, cores: int) -> dict:
@@ -219,9 +303,15 @@ def main_batch(args, rank: int, world: int, local: int):
             print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}), flush=True)
             return
         v = n_total / r["seconds"]
+        rcfg = {k: val for k, val in cfg.items() if k != "packets_per_step"}
+        rcfg.update(projected_packets_per_step=n_total, sample_packets_per_model=n_ref)
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
-                          "steps": 1, "warmup": 0, "ms_per_step": r["seconds"] * 1e3, "higher_is_better": True,
-                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "steps": 1, "warmup": 0, "ms_per_step": r["sample_seconds"] * 1e3,
+                          "projected_ms_per_step": r["seconds"] * 1e3,
+                          "value_basis": "projected: per model set_opacity + propagation per packet x the "
+                                         "model's packets, from steps of %d packets per model" % n_ref,
+                          "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": rcfg,
                           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                                            "sample": ref_sample},
                           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
@@ -229,25 +319,12 @@ def main_batch(args, rank: int, world: int, local: int):
         return
 
     import torch
-    from pubsed_b200 import abi, engine
-    from pubsed_b200.batch import BatchEngine
+    from pubsed_b200 import abi
     torch.cuda.set_device(local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def timed_batch(precision, steps, warmup, tune=True, clock=False):
-        be = BatchEngine(bw, precision=precision, device=local, graph=True)
-        tuning = be.autotune(0.02) if tune else None
-        for _ in range(warmup):
-            flush.fill_(1.0)
-            be.step(1.0)
-        stats = []
-        clk = ClockSampler(local)
-        with (clk if clock else _Null()):
-            for i in range(steps):
-                flush.fill_(float(i))
-                torch.cuda.synchronize()
-                stats.append(be.step(1.0))
-        return be, stats, tuning, clk
+        return _timed_batch(bw, local, flush, precision, steps, warmup, tune, clock)
 
     be, stats, tuning, clk = timed_batch(abi.PREC_MIXED, args.steps, args.warmup, clock=True)
     ms = sum(s["ms_total"] for s in stats) / len(stats)
@@ -275,20 +352,8 @@ def main_batch(args, rank: int, world: int, local: int):
     e2e = sum(e2e_t) / len(e2e_t)
     be.close()
 
-    # the same models as separate contexts, one after another: plain FP64
-    # (the denominator of the mixed/batched target) and mixed precision
     def separate(precision):
-        tot_ms, specs = 0.0, []
-        for w in bw.models:
-            e = engine.Engine(w, precision=precision, device=local)
-            flush.fill_(1.0)
-            e.step(1.0)
-            flush.fill_(2.0)
-            torch.cuda.synchronize()
-            tot_ms += e.step(1.0)["ms_total"]
-            specs.append(e.spectrum())
-            e.close()
-        return tot_ms, specs
+        return _separate(bw, local, flush, precision)
 
     ms64, spec64 = separate(abi.PREC_FP64)
     chi2 = [_chi2_per_dof(fb, cb, f6, c6) for (fb, cb), (f6, c6) in zip(spec_b, spec64)]
@@ -363,7 +428,10 @@ def main_adjoint(args, rank: int, world: int, local: int):
         if args.impl == "reference":
             if world > 1 and rank != 0:
                 return
-            ref["config"] = dict(cfg, note="reference forward only: it has no adjoint")
+            ref["config"] = dict({k: v for k, v in cfg.items() if k != "packets_per_step"},
+                                 projected_packets_per_step=n,
+                                 sample_packets_per_step=ref["config"]["sample_packets_per_step"],
+                                 note="reference forward only: it has no adjoint")
             print(json.dumps(ref), flush=True)
             return
     import torch
@@ -486,10 +554,12 @@ def main_ddmc(args, rank: int, world: int, local: int):
             print(json.dumps({"impl": "reference", "unavailable": note}), flush=True)
             return
         print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
-                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": n_ref / v * 1e3,
+                          "projected_ms_per_step": n / v * 1e3,
+                          "value_basis": "carried packets per second of steps of %d packets" % n_ref,
                           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                           "data": "synthetic", "config": {"workload": "diffusing_pulse_1d_ddmc",
-                                                          "packets_per_step": n, "threads": cores,
+                                                          "projected_packets_per_step": n, "threads": cores,
                                                           "sample_packets_per_step": n_ref},
                           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                                            "sample": note},
@@ -566,6 +636,8 @@ def main():
     ap.add_argument("--ref-packets", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--batch-leg-scale", type=float, default=0.25,
+                    help="type_ia: packet scale of the batching leg added to the line (0: no batching leg)")
     args = ap.parse_args()
     rank, world, local = _env_rank()
     if args.workload == "batch64":
@@ -656,6 +728,7 @@ def main():
         e64.close()
 
     eng, stats, wall, clk = run_mode(abi.PREC_MIXED, args.steps, args.warmup, record_clock=True)
+    spec32 = eng.spectrum()  # the last timed step's spectrum
     ms = [s["ms_total"] for s in stats]
     ms_step = sum(ms) / len(ms)
     # max over ranks
@@ -718,6 +791,9 @@ def main():
                    "parallelism": "replicas" if world > 1 else "single"},
         "ms_opacity": last["ms_opacity"], "ms_transport": last["ms_transport"],
         "plain_fp64": fp64,
+        # the matched-chi^2 half of the metric: the mixed step's spectrum
+        # against the plain-FP64 step's, both at the full packet count
+        "chi2_vs_plain_fp64": chi2_summary(spec32[0], spec32[1], spec64[0], spec64[1]) if fp64 else None,
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_t * 1e3},
@@ -726,6 +802,13 @@ def main():
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clk.summary(),
     }
+    if fp64:
+        fp64["ratio_mixed_over_fp64"] = fp64["ms_per_step"] / ms_max
+    eng.close()
+    if args.workload == "type_ia" and args.batch_leg_scale > 0 and world == 1:
+        # the batched half of the metric, at a reduced packet count so the
+        # default run stays within a few minutes
+        line["batch64"] = batch_leg(local, flush, args.batch_leg_scale)
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         try:
             ref = run_reference(argparse.Namespace(ref_packets=args.ref_packets, warmup=1, steps=1,
@@ -740,7 +823,6 @@ def main():
                                     "sample": "failed: %s" % str(ex)[:200]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.destroy_process_group()
 

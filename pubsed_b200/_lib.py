@@ -12,8 +12,7 @@ import subprocess
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# SED_LIB_PATH selects another build of the same library (e.g. a tuning variant)
-LIB_PATH = os.environ.get("SED_LIB_PATH") or os.path.join(HERE, "libsedona_gpu.so")
+LIB_PATH = os.path.join(HERE, "libsedona_gpu.so")
 CSRC = os.path.join(HERE, "csrc")
 _lib = None
 

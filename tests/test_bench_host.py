@@ -25,3 +25,20 @@ def test_every_bench_workload_with_a_capture_reports_traffic():
         else:
             assert bench.captured_traffic(e["workload"], 123) == e["dram_bytes"]
     assert bench.captured_traffic("no_such_workload", 1) is None
+
+
+def test_chi2_summary_of_two_spectra():
+    """The matched-chi^2 figure bench.py reports: two independent spectra of
+    the same equal-energy packet process give chi^2 / dof near 1 and a p-value
+    that is not small; a 5% distortion of one of them is rejected."""
+    import numpy as np
+    rng = np.random.default_rng(7)
+    lam = 2000.0 * np.exp(-np.linspace(0, 3, 400))
+    ca, cb = rng.poisson(lam).astype(float), rng.poisson(lam).astype(float)
+    fa, fb = 3.0 * ca, 3.0 * cb
+    same = bench.chi2_summary(fa, ca, fb, cb)
+    assert same["dof"] == int(((ca >= 10) & (cb >= 10)).sum())
+    assert 0.8 < same["chi2_per_dof"] < 1.2 and same["p_value"] > 0.01
+    bent = bench.chi2_summary(fa * (1 + 0.05 * np.sin(np.arange(400))), ca, fb, cb)
+    assert bent["p_value"] < 1e-6
+    assert bench.chi2_summary(fa, 0 * ca, fb, cb) == {"chi2_per_dof": None, "dof": 0, "p_value": None}
