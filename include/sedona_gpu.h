@@ -101,8 +101,10 @@ typedef struct sed_transport_params {
                                     The reference passes spectrum_nu_grid here
                                     (transport_init.cpp:170-173), not gamma_nu_grid */
   /* discrete diffusion in optically thick zones (1D spheres):
-   * transport_use_ddmc (0 off, 2 DDMC, Densmore et al. 2007,
-   * src/transport/discrete_diffusion.cpp:114-404) and
+   * transport_use_ddmc (0 off; 1 IMD, Gentile 2001, discrete_diffuse_IMD
+   * with the per-step hop probabilities of compute_diffusion_probabilities,
+   * src/transport/discrete_diffusion.cpp:18-110, 687-756; 2 DDMC, Densmore
+   * et al. 2007, src/transport/discrete_diffusion.cpp:114-404) and
    * transport_ddmc_tau_threshold: a zone is diffusive for a photon when its
    * total opacity at the photon's comoving frequency times the zone width
    * exceeds it */

@@ -93,6 +93,11 @@ struct oracle_ctx {
   int64_t nspec_g;
   double *gflux, *gclick;
   int64_t n_reject_cap;  /* Compton scatters that hit the rejection bound */
+  int64_t n_limit;       /* packets of the step stopped by the segment limit */
+  /* IMD (transport_use_ddmc = 1): per-zone hop / stay / absorption
+   * probabilities of the step (compute_diffusion_probabilities) */
+  double *imd_up, *imd_dn, *imd_stay, *imd_abs;
+  int64_t n_imd_cap;     /* IMD calls that hit the hop bound */
   /* transport clock (transport::t_now_) and the packets carried to the next
    * step, in the reference's vector order */
   double t_now;
@@ -244,6 +249,8 @@ static void free_grid(oracle_ctx* o)
   free(o->eZ); free(o->eA);
   free(o->J); free(o->e_abs); free(o->e_rad); free(o->fx); free(o->fy); free(o->fz); free(o->fr);
   free(o->abs); free(o->scat); free(o->cdf); free(o->eps_imc); free(o->n_elec); free(o->planck); free(o->ross); free(o->L_th);
+  free(o->imd_up); free(o->imd_dn); free(o->imd_stay); free(o->imd_abs);
+  o->imd_up = o->imd_dn = o->imd_stay = o->imd_abs = NULL;
   o->v_r = o->vol = o->rho = o->T = o->e_gas = o->grey = o->X = NULL;
   o->eZ = o->eA = NULL;
 }
@@ -1188,6 +1195,110 @@ static int move_across(const oracle_ctx* o, packet* p, int new_ind, double sigma
   return 0;
 }
 
+/* ---------------------------------------------------------------- IMD
+ * transport_use_ddmc = 1: Implicit Monte Carlo Diffusion (Gentile 2001) as
+ * the reference has it, 1D spheres.  The Monte Carlo side (the diffusive-
+ * zone test of every pass, the interface into a diffusive zone) is the
+ * DDMC one; inside a diffusive zone a photon makes one IMD call. */
+
+/* transport::compute_diffusion_probabilities (discrete_diffusion.cpp:
+ * 687-756): hop up / down probabilities from the Planck-mean diffusion
+ * coefficients of the zone and its neighbours, normalised together with the
+ * (zero) advection and absorption probabilities; the rest is "stay" */
+static void imd_probabilities(oracle_ctx* o, double dt)
+{
+  int nz = o->nzones;
+  double* arr[4] = {o->imd_up, o->imd_dn, o->imd_stay, o->imd_abs};
+  for (int k = 0; k < 4; k++) free(arr[k]);
+  o->imd_up = (double*)calloc((size_t)nz, sizeof(double));
+  o->imd_dn = (double*)calloc((size_t)nz, sizeof(double));
+  o->imd_stay = (double*)calloc((size_t)nz, sizeof(double));
+  o->imd_abs = (double*)calloc((size_t)nz, sizeof(double));
+  for (int i = 0; i < nz; i++) {
+    double dx = zone_size(o, i);
+    int ip = i + 1;
+    if (ip == nz) ip = i;
+    int im = i - 1;
+    if (im < 0) im = 0;
+    double Dj0 = PC_C / (3.0 * o->planck[i]);
+    double Djp = PC_C / (3.0 * o->planck[ip]);
+    double Djm = PC_C / (3.0 * o->planck[im]);
+    double Dh_up = 2 * dx * (Dj0 * Djp) / (Dj0 * dx + Djp * dx);
+    double Dh_dn = 2 * dx * (Dj0 * Djm) / (Dj0 * dx + Djm * dx);
+    double r_p = o->r_out.x[i];     /* grid_1D_sphere::coordinates: r_out[i] */
+    double r_m = o->r_out.x[im];
+    if (i == 0) r_m = 0;
+    double r_0 = 0.5 * (r_p + r_m);
+    double up = (dt / dx) * (Dh_up / dx) * r_p * r_p / r_0 / r_0;
+    double dn = (dt / dx) * (Dh_dn / dx) * r_m * r_m / r_0 / r_0;
+    if (i == 0) dn = 0;
+    double adv = 0.0, ab = 0.0;
+    double norm = 1 + adv + ab;
+    norm += up + dn;
+    ab /= norm;
+    up /= norm;
+    dn /= norm;
+    o->imd_up[i] = up; o->imd_dn[i] = dn; o->imd_abs[i] = ab; o->imd_stay[i] = 1.0 / norm;
+  }
+}
+
+#define IMD_HOPS (1 << 24)
+/* transport::discrete_diffuse_IMD (discrete_diffusion.cpp:18-110), called
+ * with the end time of the step where the function means the step
+ * (transport.cpp:237): the photon's time advances by tstop, the J tally and
+ * the advection take tstop as the interval.  Hops one zone up or down (a
+ * radial move by the starting zone's width) until it stays, then is
+ * advected, loses energy adiabatically and stops.  The hop loop, unbounded
+ * in the reference, gives up after 2^24 hops (counted). */
+static int imd_event(oracle_ctx* o, packet* p, double dt)
+{
+  int nn = o->nu.n, nj = o->tp.store_Jnu ? nn : 1;
+  double dx = zone_size(o, p->ind);
+  p->t += dt;
+  for (int hops = 0;; hops++) {
+    if (hops >= IMD_HOPS) { o->n_imd_cap++; break; }
+    p->ind = get_zone(o, p->x);
+    if (p->ind == -1) return F_ABSORBED;
+    if (p->ind == -2) return F_ESCAPED;
+    o->e_abs[p->ind] += p->e * o->imd_abs[p->ind];
+    o->J[(size_t)p->ind * nj] += p->e * o->imd_stay[p->ind] * dt * PC_C;
+    double P_diff = o->imd_up[p->ind] + o->imd_dn[p->ind];
+    double P_stay = o->imd_abs[p->ind] + o->imd_stay[p->ind];
+    double r1 = draw(o, p);
+    if (r1 < P_diff) {
+      double r2 = draw(o, p);
+      if (r2 < o->imd_up[p->ind] / P_diff) {
+        p->ind++;
+        double rr = pr(p);
+        p->x[0] += p->x[0] / rr * dx;
+        p->x[1] += p->x[1] / rr * dx;
+        p->x[2] += p->x[2] / rr * dx;
+      } else {
+        p->ind--;
+        double rr = pr(p);
+        p->x[0] -= p->x[0] / rr * dx;
+        p->x[1] -= p->x[1] / rr * dx;
+        p->x[2] -= p->x[2] / rr * dx;
+      }
+    } else {
+      double r2 = draw(o, p);
+      double f_abs = o->imd_abs[p->ind] / P_stay;
+      if (r2 < f_abs) return F_ABSORBED;
+      double v[3], dvds;
+      get_velocity(o, p->ind, p->x, p->D, v, &dvds);
+      p->x[0] += v[0] * dt;
+      p->x[1] += v[1] * dt;
+      p->x[2] += v[2] * dt;
+      p->e *= (1 - dvds * dt);
+      break;
+    }
+  }
+  p->ind = get_zone(o, p->x);
+  if (p->ind == -1) return F_ABSORBED;
+  if (p->ind == -2) return F_ESCAPED;
+  return F_STOPPED;
+}
+
 #define DDMC_SCATTER_TRIES (1 << 16)
 /* one pass of the event loop of transport::discrete_diffuse_DDMC
  * (discrete_diffusion.cpp:136-404); *dt_remaining carries over the passes of
@@ -1349,11 +1460,15 @@ static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int
   int64_t seg = 0;
   /* discrete diffusion: the zone test before every pass (transport.cpp:
    * 216-246, 272-286); the remaining time of one diffusion call */
-  int dd = (o->tp.use_ddmc == 2) && (o->gtype == SED_GRID_1D_SPHERE);
+  int dd = (o->tp.use_ddmc == 2 || o->tp.use_ddmc == 1) && (o->gtype == SED_GRID_1D_SPHERE);
   int in_call = 0;
   double dt_remaining = 0;
   while (fate == F_MOVING) {
-    if (seg++ >= limit) { fate = F_STOPPED; break; }
+    if (seg++ >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    if (dd && o->tp.use_ddmc == 1 && in_ddmc_zone(o, p)) {
+      fate = imd_event(o, p, tstop);
+      continue;
+    }
     if (dd && in_ddmc_zone(o, p)) {
       if (!in_call) { dt_remaining = tstop - p->t; in_call = 1; }
       fate = ddmc_event(o, p, &dt_remaining, nscat);
@@ -1503,6 +1618,8 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
   int64_t n_emit = (int64_t)(o->tp.core_n_emit / 1.0);
   if (n_emit > o->tp.max_particles) return fail(o, SED_ERR_CAPACITY, "Not enough particle space");
   if (first == 0) {
+    if (o->tp.use_ddmc == 1) imd_probabilities(o, dt);  /* transport.cpp:44 */
+    o->n_imd_cap = 0;
     wipe_tallies(o);
     memset(o->flux, 0, (size_t)o->nspec * sizeof(double));
     memset(o->click, 0, (size_t)o->nspec * sizeof(double));
@@ -1510,6 +1627,7 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
     o->n_active_acc = 0;
   }
   if (first < 0 || first + count > n_emit) return fail(o, SED_ERR_ARG, "packet range outside the emission");
+  o->n_limit = 0;
   double Ep = o->tp.core_luminosity * dt / n_emit;
   uint32_t K = draws_per_emission(o);
   if (o->record) {
@@ -1552,8 +1670,10 @@ int oracle_transport_range(oracle_ctx* o, double dt, int64_t first, int64_t coun
   if (st) {
     memset(st, 0, sizeof *st);
     st->n_packets = count; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
-    st->n_segments = nseg; st->n_scatters = nscat;
+    st->n_segments = nseg; st->n_scatters = nscat; st->n_limit = o->n_limit;
   }
+  if (o->n_limit > 0) return fail(o, SED_ERR_LIMIT, "packets hit the segment limit");
+  if (o->n_imd_cap > 0) return fail(o, SED_ERR_LIMIT, "IMD calls hit the hop bound");
   return SED_OK;
 }
 
@@ -1770,7 +1890,7 @@ static int propagate_gamma(oracle_ctx* o, packet* p, double t_now, double dt, in
   int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
   int64_t seg = 0;
   while (fate == F_MOVING && !*photon) {
-    if (seg++ >= limit) { fate = F_STOPPED; break; }
+    if (seg++ >= limit) { fate = F_STOPPED; o->n_limit++; break; }
     int iz = p->ind;
     double d_bn = 0;
     int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);
@@ -1926,6 +2046,8 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
   for (int64_t k = 0; k < n_census; ++k) census_gammas += (o->c_type[k] == T_GAMMA);
   int gamma_phase = n_radio > 0 || census_gammas > 0;
   int nz = o->nzones;
+  if (o->tp.use_ddmc == 1) imd_probabilities(o, dt);  /* transport.cpp:44 */
+  o->n_imd_cap = 0;
   wipe_tallies(o);
   /* spectra accumulate over time-dependent steps; a steady-state iteration
    * starts from empty ones (SedonaClass.cpp:349) */
@@ -1940,6 +2062,7 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
     if (n_radio == 0) memset(o->L_emit, 0, (size_t)nz * sizeof(double));
   }
   o->n_reject_cap = 0;
+  o->n_limit = 0;
   double Ep_r = L_tot * dt / (1.0 * n_radio);
   if (o->record || timedep) {
     free(o->r_fate); free(o->r_ind); free(o->r_draws); free(o->r_state); free(o->r_type);
@@ -2040,8 +2163,10 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
   if (st) {
     memset(st, 0, sizeof *st);
     st->n_packets = n_all; st->n_escaped = nesc; st->n_absorbed = nabs; st->n_stopped = nstop;
-    st->n_segments = nseg; st->n_scatters = nscat; st->warnings = warnings;
+    st->n_segments = nseg; st->n_scatters = nscat; st->warnings = warnings; st->n_limit = o->n_limit;
   }
+  if (o->n_limit > 0) return fail(o, SED_ERR_LIMIT, "packets hit the segment limit");
+  if (o->n_imd_cap > 0) return fail(o, SED_ERR_LIMIT, "IMD calls hit the hop bound");
   if (o->n_reject_cap > 0) return fail(o, SED_ERR_LIMIT, "Compton scatters hit the rejection-sampling bound");
   return SED_OK;
 }
@@ -2176,8 +2301,8 @@ int oracle_get_radioactive_tallies(oracle_ctx* o, double* L_emit, double* L_dep)
 int oracle_transport(oracle_ctx* o, double dt, sed_step_stats* st)
 {
   if (!o) return SED_ERR_ARG;
-  if (o->tp.use_ddmc != 0 && (o->tp.use_ddmc != 2 || o->gtype != SED_GRID_1D_SPHERE))
-    return fail(o, SED_ERR_ARG, "discrete diffusion is built for method 2 on 1D spheres");
+  if (o->tp.use_ddmc != 0 && ((o->tp.use_ddmc != 1 && o->tp.use_ddmc != 2) || o->gtype != SED_GRID_1D_SPHERE))
+    return fail(o, SED_ERR_ARG, "discrete diffusion is built for methods 1 and 2 on 1D spheres");
   if (o->tp.n_emit_radioactive > 0 || o->n_census > 0 || !o->tp.steady_state ||
       (int64_t)(o->tp.core_n_emit / 1.0) > o->tp.max_particles) {
     if (!o->have_grid) return SED_ERR_STATE;
@@ -2219,7 +2344,7 @@ static int propagate_weighted(oracle_ctx* o, packet* p, double t_now, double dt,
   int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
   int64_t seg = 0;
   while (fate == F_MOVING) {
-    if (seg++ >= limit) { fate = F_STOPPED; break; }
+    if (seg++ >= limit) { fate = F_STOPPED; o->n_limit++; break; }
     int iz = p->ind;
     double d_bn = 0;
     int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);

@@ -63,6 +63,10 @@ DEFAULTS: dict[str, Any] = {
     "spectrum_nu_grid": [1, 1, 1], "spectrum_n_mu": 1, "spectrum_n_phi": 1,
     "spectrum_suppress_txt": 0, "gamma_name": "", "gamma_nu_grid": [1, 1, 1],
     "spectrum_particle_list_name": "", "spectrum_particle_list_maxn": 1e9,
+    # knobs of this implementation (no reference counterpart): the per-packet
+    # segment limit (0: 10^7), after which a packet stops and the step
+    # returns SED_ERR_LIMIT
+    "gpu_max_segments": 0,
 }
 
 

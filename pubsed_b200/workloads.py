@@ -109,7 +109,7 @@ class Workload:
         tp.core_temperature = T_core
         tp.core_photon_frequency = P.scalar("core_photon_frequency")
         tp.fleck_alpha = P.scalar("transport_fleck_alpha")
-        tp.max_segments = 0
+        tp.max_segments = P.scalar("gpu_max_segments", int)
         tp.nu_grid = abi.locate_grid(keep, self.nu_grid())
         tp.spec_time = abi.locate_grid(keep, tg)
         tp.spec_nu = abi.locate_grid(keep, ng)

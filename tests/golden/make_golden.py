@@ -88,6 +88,18 @@ TD_CASES = {
                                                    params={"transport_use_ddmc": 2,
                                                            "transport_ddmc_tau_threshold": 0.1},
                                                    n_packets=0, n_zones=32, n_bins=64, radiative_eq=1, seed=7), 3),
+    # IMD (transport_use_ddmc = 1) on the same two configurations as DDMC:
+    # every zone diffusive, and line opacity with diffusive and Monte Carlo
+    # zones and frequencies
+    "replay_td_imd_grey": ("time_dependent", dict(base="lightbulb_grey", n_initialize=400, dt_days=0.1,
+                                                  params={"transport_use_ddmc": 1,
+                                                          "transport_ddmc_tau_threshold": 0.1},
+                                                  n_packets=0, n_zones=32, n_bins=64, radiative_eq=1, seed=41), 3),
+    "replay_td_imd_ia": ("time_dependent", dict(base="type_ia", n_initialize=200, dt_days=0.5,
+                                                params={"transport_use_ddmc": 1,
+                                                        "transport_ddmc_tau_threshold": 3.0},
+                                                n_packets=100, n_zones=16, n_lines=5000, n_bins=256,
+                                                n_levels_per_ion=6, v_core=1e8, t_days=40.0, seed=43), 3),
     # particles_max_total below census + core packets on every other step:
     # those steps emit no core packets ("# Not enough particle space") and
     # propagate the census alone

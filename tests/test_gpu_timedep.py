@@ -34,7 +34,7 @@ def _load(name):
 
 
 @pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio", "replay_td_ddmc_ia", "replay_td_ddmc_grey",
-                                  "replay_td_full"])
+                                  "replay_td_full", "replay_td_imd_grey", "replay_td_imd_ia"])
 def test_time_dependent_steps_match_reference_replay(sed_lib, name):
     ref, kw = _load(name)
     w = workloads.time_dependent(**kw)

@@ -32,7 +32,7 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("name", ["replay_td_grey", "replay_td_ia_radio", "replay_td_ddmc_ia", "replay_td_ddmc_grey",
-                                  "replay_td_full"])
+                                  "replay_td_full", "replay_td_imd_grey", "replay_td_imd_ia"])
 def test_oracle_matches_reference_time_dependent_replay(name):
     ref, w, kw = load_td(name)
     steps = int(ref["steps"])
@@ -78,9 +78,10 @@ def test_oracle_matches_reference_time_dependent_replay(name):
         if "T_gas" in r:
             assert _rel(r["T_gas"], ref["T_gas" + sf]) <= 1e-10
     # the carried packets end the last step at its end time, which is also
-    # the grid's time after the last hydro step
+    # the grid's time after the last hydro step (not after an IMD call: it
+    # advances the photon's time by the step's end time, as the reference does)
     last = res[-1]["census"]["state"]
-    if last.size:
+    if last.size and kw.get("params", {}).get("transport_use_ddmc") != 1:
         ww = e2.w if kw.get("n_initialize") else w
         assert np.allclose(last[:, 6], ww.zones.t_now, rtol=1e-12)
 
