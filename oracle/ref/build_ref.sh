@@ -82,3 +82,22 @@ $CXX "${FLAGS[@]}" -o "$OUT/sedona_ref" "$OBJ"/*.o "$OUT/liblua.a" -ldl -lm
 $CXX "${FLAGS[@]}" "${INC[@]}" -o "$OUT/locate_array_test" "$REF/src/utils/locate_array_test.cpp" \
   "$OBJ/utils_locate_array.cpp.o" "$OBJ/utils_h5utils.cpp.o" "$OBJ/shims.o" -lm
 echo "built $OUT/sedona_ref"
+
+# --- the compiled C++ binding of the B200 library -----------------------------
+# sedona_ref_gpu: the same harness with its "gpu" mode, linking the binding
+# (pubsed_b200/binding/transport_gpu.cpp, compiled here against the
+# reference's own headers) and pubsed_b200/libsedona_gpu.so, found at run time
+# next to the repository's oracle/_ref through $ORIGIN
+ROOT=$(cd "$HERE/../.." && pwd)
+if [ -f "$ROOT/pubsed_b200/libsedona_gpu.so" ]; then
+  OBJG="$OUT/obj_gpu"
+  mkdir -p "$OBJG"
+  GINC=("${INC[@]}" -I"$ROOT/include" -I"$ROOT/pubsed_b200/binding")
+  $CXX "${FLAGS[@]}" "${GINC[@]}" -c "$ROOT/pubsed_b200/binding/transport_gpu.cpp" -o "$OBJG/transport_gpu.o"
+  $CXX "${FLAGS[@]}" "${GINC[@]}" -DSED_GPU_BINDING -c "$HERE/ref_harness.cpp" -o "$OBJG/ref_harness_gpu.o"
+  REFOBJ=()
+  for o in "$OBJ"/*.o; do [ "$(basename "$o")" = "ref_harness.o" ] || REFOBJ+=("$o"); done
+  $CXX "${FLAGS[@]}" -o "$OUT/sedona_ref_gpu" "${REFOBJ[@]}" "$OBJG/ref_harness_gpu.o" "$OBJG/transport_gpu.o" \
+    "$OUT/liblua.a" -L"$ROOT/pubsed_b200" -lsedona_gpu -Wl,-rpath,'$ORIGIN/../../pubsed_b200' -ldl -lm
+  echo "built $OUT/sedona_ref_gpu"
+fi

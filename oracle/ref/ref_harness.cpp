@@ -14,6 +14,12 @@
 //   free     transport::step itself, OpenMP threads, free-running streams;
 //            prints the wall time of each step (the timed CPU baseline).
 //   opacity  transport::init + set_opacity only; dumps the opacity tables.
+//   gpu      (sedona_ref_gpu only, built with SED_GPU_BINDING) transport::init,
+//            then the steps run by the compiled C++ binding of the B200
+//            library (pubsed_b200/binding/transport_gpu.cpp): the binding
+//            fills the C ABI's structs from the live transport, steps on the
+//            device and copies the results back into the transport, whose
+//            tables and tallies are then dumped as in the other modes.
 //
 // Inputs: a Lua parameter file (read by the reference's ParameterReader),
 // the model file it names, and optionally a "store" file whose datasets and
@@ -53,6 +59,9 @@
 #include "physical_constants.h"
 #undef private
 #undef protected
+#ifdef SED_GPU_BINDING
+#include "transport_gpu.h"
+#endif
 
 namespace pc = physical_constants;
 
@@ -332,8 +341,8 @@ int replay_step(transport& t, double dt, uint32_t seed, uint32_t step, Out& o, i
 void usage()
 {
   std::fprintf(stderr,
-               "usage: sedona_ref <replay|free|opacity> <param.lua> <out_prefix> [--store FILE] [--seed S]\n"
-               "                  [--step N] [--steps N] [--threads T] [--dt DT]\n");
+               "usage: sedona_ref <replay|free|opacity|gpu> <param.lua> <out_prefix> [--store FILE] [--seed S]\n"
+               "                  [--step N] [--steps N] [--threads T] [--dt DT] [--precision P]\n");
   std::exit(1);
 }
 }  // namespace
@@ -345,7 +354,7 @@ int main(int argc, char** argv)
   Out o;
   o.prefix = argv[3];
   uint32_t seed = 0, step = 0;
-  int steps = 1, threads = omp_get_max_threads();
+  int steps = 1, threads = omp_get_max_threads(), precision = 0;
   double dt = 1.0;
   for (int a = 4; a < argc; ++a) {
     std::string k = argv[a];
@@ -357,6 +366,7 @@ int main(int argc, char** argv)
     else if (k == "--steps") steps = std::stoi(v);
     else if (k == "--threads") threads = std::stoi(v);
     else if (k == "--dt") dt = std::stod(v);
+    else if (k == "--precision") precision = std::stoi(v);
     else usage();
   }
   omp_set_num_threads(threads);
@@ -446,6 +456,29 @@ int main(int argc, char** argv)
     o.f64("step_seconds", times);
     o.f64("set_opacity_seconds", opac_times);
     dump_tables(t, o);
+  } else if (mode == "gpu") {
+#ifdef SED_GPU_BINDING
+    hydro_homologous hydro;
+    const bool use_hydro = !t.steady_state && params.getScalar<std::string>("hydro_module") == "homologous";
+    if (use_hydro) hydro.init(&params, grid);
+    sed_binding::GpuTransport* b = sed_binding::attach(t, &params, precision, 0);
+    if (!b) { std::fprintf(stderr, "gpu: %s\n", sed_binding::last_error(nullptr)); return 5; }
+    std::vector<double> esc;
+    for (int s = 0; s < steps; ++s) {
+      if (use_hydro) hydro.step(dt);
+      sed_step_stats st{};
+      const int rc = sed_binding::step(t, b, dt, &st);
+      if (rc) { std::fprintf(stderr, "gpu: step %d: %s\n", s, sed_binding::last_error(b)); return 6; }
+      esc.push_back((double)st.n_escaped);
+    }
+    o.f64("n_escaped_steps", esc);
+    dump_tables(t, o);
+    sed_binding::detach(b);
+#else
+    (void)precision;
+    std::fprintf(stderr, "gpu mode needs the sedona_ref_gpu build\n");
+    return 4;
+#endif
   } else {
     usage();
   }

@@ -20,6 +20,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(os.path.dirname(HERE), "_ref", "sedona_ref")
+# the same harness with its "gpu" mode: the compiled C++ binding of the B200
+# library stepping the reference's transport
+REF_GPU_BIN = os.path.join(os.path.dirname(HERE), "_ref", "sedona_ref_gpu")
 
 
 def available() -> bool:
@@ -168,15 +171,19 @@ def load_outputs(prefix: str) -> dict:
 
 def run(workload, mode: str, n_packets: Optional[int] = None, threads: Optional[int] = None,
         seed: Optional[int] = None, steps: int = 1, timeout: float = 3600, keep_dir: Optional[str] = None,
-        dt: Optional[float] = None) -> dict:
-    """mode: replay | free | opacity.  dt: the step of a time-dependent run.
-    Returns the harness outputs."""
-    if not available():
-        raise FileNotFoundError("reference harness not built: " + REF_BIN)
+        dt: Optional[float] = None, precision: Optional[int] = None) -> dict:
+    """mode: replay | free | opacity, or gpu (sedona_ref_gpu: the binding's
+    steps; precision: enum sed_precision).  dt: the step of a time-dependent
+    run.  Returns the harness outputs."""
+    binary = REF_GPU_BIN if mode == "gpu" else REF_BIN
+    if not (os.path.exists(binary) and os.access(binary, os.X_OK)):
+        raise FileNotFoundError("reference harness not built: " + binary)
     d = keep_dir or tempfile.mkdtemp(prefix="sedref_")
     ppath, spath = render(workload, d, n_packets)
     prefix = os.path.join(d, "out")
-    cmd = [REF_BIN, mode, ppath, prefix, "--store", spath, "--steps", str(steps)]
+    cmd = [binary, mode, ppath, prefix, "--store", spath, "--steps", str(steps)]
+    if precision is not None:
+        cmd += ["--precision", str(int(precision))]
     if dt is not None:
         cmd += ["--dt", repr(float(dt))]
     if seed is not None:
