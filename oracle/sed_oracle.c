@@ -1464,7 +1464,8 @@ static int propagate_from(oracle_ctx* o, packet* p, double t_now, double dt, int
   int in_call = 0;
   double dt_remaining = 0;
   while (fate == F_MOVING) {
-    if (seg++ >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    if (seg >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    seg++;
     if (dd && o->tp.use_ddmc == 1 && in_ddmc_zone(o, p)) {
       fate = imd_event(o, p, tstop);
       continue;
@@ -1890,7 +1891,8 @@ static int propagate_gamma(oracle_ctx* o, packet* p, double t_now, double dt, in
   int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
   int64_t seg = 0;
   while (fate == F_MOVING && !*photon) {
-    if (seg++ >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    if (seg >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    seg++;
     int iz = p->ind;
     double d_bn = 0;
     int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);
@@ -2344,7 +2346,8 @@ static int propagate_weighted(oracle_ctx* o, packet* p, double t_now, double dt,
   int64_t limit = o->tp.max_segments > 0 ? o->tp.max_segments : 10000000;
   int64_t seg = 0;
   while (fate == F_MOVING) {
-    if (seg++ >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    if (seg >= limit) { fate = F_STOPPED; o->n_limit++; break; }
+    seg++;
     int iz = p->ind;
     double d_bn = 0;
     int new_ind = get_next_zone(o, p->x, p->D, iz, o->tp.core_radius, &d_bn);

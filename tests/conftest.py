@@ -37,3 +37,16 @@ def sed_lib():
 def oracle():
     import oracle_lib
     return oracle_lib.oracle_lib()
+
+
+def pytest_sessionfinish(session, exitstatus):
+    """With SED_STATE_LOG set, the per-call outcomes of
+    oracle_lib.check_states (packets compared, packets over 1e-12, largest
+    difference) are written there as JSON."""
+    path = os.environ.get("SED_STATE_LOG")
+    if not path:
+        return
+    import json
+    import oracle_lib
+    with open(path, "w") as f:
+        json.dump([{"test": t, "n": n, "n_over": k, "max": m} for t, n, k, m in oracle_lib.STATE_LOG], f, indent=0)

@@ -210,10 +210,17 @@ def zone_tally_close(a: np.ndarray, b: np.ndarray, rtol: float = ZONE_TALLY_RTOL
     return d / max(scale, 1e-300)
 
 
+# every check_states call of the session: (test, packets, packets over
+# STATE_RTOL, largest difference); tests/conftest.py writes them out when
+# SED_STATE_LOG names a file
+STATE_LOG: list = []
+
+
 def check_states(Sg: np.ndarray, So: np.ndarray) -> dict:
     r = state_rel_per_packet(Sg, So)
     q = float(np.quantile(r, STATE_QUANTILE)) if r.size else 0.0
-    out = {"max": float(r.max()) if r.size else 0.0, "q": q, "n_over": int((r > STATE_RTOL).sum())}
+    out = {"max": float(r.max()) if r.size else 0.0, "q": q, "n_over": int((r > STATE_RTOL).sum()), "n": int(r.size)}
+    STATE_LOG.append((os.environ.get("PYTEST_CURRENT_TEST", ""), out["n"], out["n_over"], out["max"]))
     assert q <= STATE_RTOL, out
     assert out["max"] <= STATE_RTOL_MAX, out
     return out
