@@ -1,0 +1,458 @@
+// mixed_kernel.cuh -- the mixed-precision packet kernel for homologous 1D
+// spheres (FP32 {abs, scat} tables and emissivity CDF, FP64 packet state).
+// Included by transport_kernel.cu inside its anonymous namespace, after the
+// shared helpers (emit_core, spectrum_count, cdf_row_sample, the batch zone
+// tables).
+//
+// It runs the steps of propagate_monte_carlo (src/transport/transport.cpp:
+// 260-484), do_scatter and isotropic_scatter (src/transport/scatter.cpp:
+// 12-70, 303-351) and is held, like the mixed form of propagate_kernel, to
+// the reference's spectra within Monte Carlo noise, not to its bits.  What
+// differs is how much a segment costs:
+//
+//  * The optical depth to the next interaction is drawn once per flight
+//    (after emission and after each interaction) and the depth a segment
+//    crosses is subtracted when the segment ends at a zone wall, a
+//    frequency-bin step or the end of the step.  The reference draws a new
+//    depth every segment; for an exponential depth both give the same
+//    distribution of interaction points (the remaining depth of an
+//    exponential is again exponential), and segments that end at a wall or
+//    a bin step then cost no deviate and no logarithm.
+//  * One Philox4x32-10 block per interaction: word 0 is the next flight's
+//    optical depth, word 1 the absorption test, word 2 the emissivity-CDF
+//    deviate, word 3 the comoving direction cosine.  The deviates the
+//    interaction needs beyond those are recycled (Devroye, Non-Uniform
+//    Random Variate Generation, 1986, on reusing a uniform after a
+//    comparison): given the outcome of "u <= eps", u / eps (or
+//    (u - eps) / (1 - eps)) is again uniform on [0, 1) and independent of the
+//    outcome, so it gives the effective-scattering test and then the
+//    azimuth; given the CDF bin k that u >= cdf[k-1] selected,
+//    (u - cdf[k-1]) / (cdf[k] - cdf[k-1]) is uniform and gives the position
+//    within the bin.  A recycled deviate keeps 2^32 p distinct values when
+//    its branch has probability p.
+//  * FP64 square roots, reciprocal square roots and reciprocals from the
+//    FP32 hardware estimate refined by one Newton-Raphson step with its
+//    second-order term (Markstein, IA-64 and Elementary Functions, 2000):
+//    the estimate's ~2^-22 relative error cubed is below FP64 rounding.
+//    They are not correctly rounded, which the mixed form does not need;
+//    position, time, frequency and the Lorentz transforms stay FP64.
+//  * -ln(u) in FP32 (hardware log2, or an atanh series where u > 1/2), the
+//    interaction and bin-step distances as FP32 quotients (they set where a
+//    segment ends, not the state it carries).
+//  * The zone's walls are loaded once per zone visit, |x|^2 and x.D once
+//    per move.
+namespace mixed {
+
+// 1/sqrt(a), a in (1e-36, 1e37)
+__device__ __forceinline__ double rsqrt_nr(double a)
+{
+  const double y = (double)rsqrtf((float)a);
+  const double h = fma(-a * y, y, 1.0);        // 1 - a y^2
+  return fma(y * h, fma(0.375, h, 0.5), y);    // y (1 + h/2 + 3 h^2/8)
+}
+
+// sqrt(a), a >= 0
+__device__ __forceinline__ double sqrt_nr(double a)
+{
+  if (!(a > 1e-36 && a < 1e37)) return sqrt(a);
+  return a * rsqrt_nr(a);
+}
+
+// 1/a, |a| in (1e-36, 1e37)
+__device__ __forceinline__ double rcp_nr(double a)
+{
+  const double y = (double)__fdividef(1.0f, (float)a);
+  const double e = fma(-a, y, 1.0);            // 1 - a y
+  return fma(y, fma(e, e, e), y);              // y (1 + e + e^2)
+}
+
+constexpr float W32 = 2.3283064365386963e-10f;  // 2^-32
+
+// -ln(u), u = (w + 1/2) 2^-32 in (0, 1), relative error ~1e-7: the hardware
+// logarithm where |ln u| > ln 2; above u = 1/2, with x = 1 - u (formed from
+// the integer, so exact) and y = x / (2 - x) <= 1/3, the odd series of
+// 2 atanh(y) = -ln(1 - x) to y^11
+__device__ __forceinline__ float neg_log_u(uint32_t w)
+{
+  if (w < 0x80000000u) return -__logf(((float)w + 0.5f) * W32);
+  const float x = ((float)(0xFFFFFFFFu - w) + 0.5f) * W32;
+  const float y = __fdividef(x, 2.0f - x);
+  const float y2 = y * y;
+  float s = fmaf(y2, 1.0f / 11.0f, 1.0f / 9.0f);
+  s = fmaf(y2, s, 1.0f / 7.0f);
+  s = fmaf(y2, s, 1.0f / 5.0f);
+  s = fmaf(y2, s, 1.0f / 3.0f);
+  s = fmaf(y2, s, 1.0f);
+  return 2.0f * y * s;
+}
+
+// the zone's walls, as get_next_zone (grid_1D_sphere.cpp:510-590) derives
+// them: outer wall, inner wall after the core substitution, inner and outer
+// neighbour, and whether the inner wall is r = 0 of zone 0 (no inner wall)
+struct Walls {
+  double r_o, r_i;
+  int in_nbr, out_nbr;
+  bool no_inner;
+};
+
+template <int BATCH>
+__device__ __forceinline__ Walls zone_walls(const StepArgs& A, const GridDev& G, int i)
+{
+  Walls w;
+  w.r_o = __ldg(G.r_out.right + i);
+  if constexpr (BATCH) {
+    const int4 nb = __ldg(A.zone_nbr + i);
+    w.r_i = __ldg(A.zone_rin + i);
+    w.in_nbr = nb.x;
+    w.out_nbr = nb.y;
+    w.no_inner = nb.z != 0;
+  } else {
+    if (i != 0) { w.r_i = __ldg(G.r_out.right + i - 1); w.in_nbr = i - 1; }
+    else { w.r_i = G.r_out.min; w.in_nbr = -1; }
+    if (A.core_radius >= w.r_i) { w.r_i = A.core_radius; w.in_nbr = -1; }
+    w.no_inner = (i == 0) && (w.r_i == 0);
+    w.out_nbr = (i + 1 == G.nzones) ? -2 : i + 1;
+  }
+  return w;
+}
+
+// distance to the zone's boundary along D and the zone entered there, with
+// the reference's tiny_offset push across the wall
+__device__ __forceinline__ int next_zone(const Walls& w, double rsq, double xd, double* l)
+{
+  const double l_out = sqrt_nr(fma(xd, xd, fma(w.r_o, w.r_o, -rsq))) - xd;
+  double l_in = -1;
+  if (!w.no_inner && xd < 0) {
+    const double rad = fma(xd, xd, fma(w.r_i, w.r_i, -rsq));
+    if (rad >= 0) l_in = -xd - sqrt_nr(rad);
+  }
+  constexpr double tiny_offset = 1 + 1e-6;
+  constexpr double inv_tiny_offset = 1 / tiny_offset;
+  if ((l_out < l_in) || (l_in < 0)) {
+    *l = (w.out_nbr == -2) ? l_out * inv_tiny_offset : l_out * tiny_offset;
+    return w.out_nbr;
+  }
+  *l = (w.in_nbr == -1) ? l_in * inv_tiny_offset : l_in * tiny_offset;
+  return w.in_nbr;
+}
+
+// isotropic_scatter (scatter.cpp:303-351) on a homologous flow, with the
+// comoving direction from mu and the azimuth deviate vphi, and (redist) the
+// comoving frequency from the zone's emissivity CDF with deviate word w_cdf
+template <typename CT>
+__device__ __forceinline__ void scatter(const StepArgs& A, Pkt& p, double rsq, double xd, double mu, float vphi,
+                                        uint32_t w_cdf, bool redist)
+{
+  const double gamma = rsqrt_nr(fma(-rsq, A.inv_ct2, 1.0));
+  const double dshift_in = gamma * fma(-xd, A.inv_ct, 1.0);
+  p.e = p.e * dshift_in;
+  p.nu = p.nu * dshift_in;
+  float sf, cf;
+  __sincosf(fmaf((float)(2.0 * PI), vphi, -(float)PI), &sf, &cf);
+  const double smu = sqrt_nr(fma(-mu, mu, 1.0));
+  const double Dn0 = smu * (double)cf, Dn1 = smu * (double)sf, Dn2 = mu;
+  if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
+    const int nn = A.nu.n;
+    if (nn == 1) p.nu = loc_sample(A.nu, 0, 0.5);
+    else {
+      const double u = (double)w_cdf * (1.0 / 4294967296.0);
+      int k = cdf_row_sample<CT>(A, p.ind, u);
+      if (k > nn - 1) k = nn - 1;
+      const CT* row = reinterpret_cast<const CT*>(A.cdf) + (size_t)p.ind * nn;
+      const double lo = (k == 0) ? 0.0 : (double)__ldg(row + k - 1);
+      const double hi = (double)__ldg(row + k);
+      float f = __fdividef((float)(u - lo), (float)(hi - lo));
+      f = fminf(fmaxf(f, 0.0f), 0.99999994f);
+      p.nu = loc_sample(A.nu, k, (double)f);
+    }
+  }
+  // comoving -> lab with the velocity reversed, beta = x / (c t)
+  const double b0 = p.x[0] * A.inv_ct, b1 = p.x[1] * A.inv_ct, b2 = p.x[2] * A.inv_ct;
+  const double bdp = -fma(b0, Dn0, fma(b1, Dn1, b2 * Dn2));
+  const double vd_out = gamma * (1 - bdp);
+  const double gf = gamma * fma(-gamma * bdp, rcp_nr(gamma + 1), 1.0);
+  const double inv_vd = rcp_nr(vd_out);
+  const double D0 = inv_vd * fma(gf, b0, Dn0);
+  const double D1 = inv_vd * fma(gf, b1, Dn1);
+  const double D2 = inv_vd * fma(gf, b2, Dn2);
+  const double inv_norm = rsqrt_nr(fma(D0, D0, fma(D1, D1, D2 * D2)));
+  p.D[0] = D0 * inv_norm;
+  p.D[1] = D1 * inv_norm;
+  p.D[2] = D2 * inv_norm;
+  p.e = p.e * vd_out;
+  p.nu = p.nu * vd_out;
+}
+
+}  // namespace mixed
+
+// BATCH = 0: one model (core packets, then the queue of census and
+// radioactive photons); BATCH = 1: the batched 1D models of sed_batch_*.
+template <int BATCH, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const StepArgs A, const GridDev G)
+{
+  using namespace mixed;
+  using CT = float;
+  extern __shared__ double s_tal[];  // [5][nz] when A.smem_zones
+  // the block's event counters, added to once per packet (escaped, absorbed,
+  // stopped, segments, interactions, segment-limit stops)
+  __shared__ unsigned long long s_cnt[6];
+  if (threadIdx.x < 6) s_cnt[threadIdx.x] = 0;
+  const int nz = G.nzones;
+  const int nn = A.nu.n;
+  const int nj = A.store_Jnu ? nn : 1;
+  if (A.smem_zones)
+    for (int i = threadIdx.x; i < 5 * nz; i += blockDim.x) s_tal[i] = 0.0;
+  __syncthreads();
+  double* t_eabs = A.smem_zones ? s_tal : A.e_abs;
+  double* t_fx = A.smem_zones ? s_tal + nz : A.fx;
+  double* t_fy = A.smem_zones ? s_tal + 2 * nz : A.fy;
+  double* t_fz = A.smem_zones ? s_tal + 3 * nz : A.fz;
+  double* t_fr = A.smem_zones ? s_tal + 4 * nz : A.fr;
+  if (!A.smem_zones && A.n_rep > 0) {
+    double* base = A.zone_rep + (size_t)(blockIdx.x % A.n_rep) * 5 * nz;
+    t_eabs = base; t_fx = base + nz; t_fy = base + 2 * nz; t_fz = base + 3 * nz; t_fr = base + 4 * nz;
+  }
+  const float2* __restrict__ opac = reinterpret_cast<const float2*>(A.opac);
+  const int32_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
+  uint32_t K = ((A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u + 3u) / 4u;
+  uint32_t step = A.step;
+  if constexpr (BATCH) step = *A.step_dev;
+  int64_t q_next = 0, q_end = 0;
+  int m = 0, esc_model = -1;
+  unsigned long long esc_count = 0;
+  uint32_t n_scat = 0;  // interactions of the current packet
+  Pkt p;
+  PacketRng rng;
+  int fate = ABSORBED;  // no packet yet
+  bool have = false;
+  unsigned long long pid = 0;
+  int32_t seg = 0;
+  int acc_zone = -1;
+  double acc_eabs = 0, acc_fx = 0, acc_fy = 0, acc_fz = 0, acc_fr = 0;
+  Walls wl{};
+  double rsq = 0, xd = 0;
+  float tau_rem = 0;  // optical depth left to the next interaction
+  for (;;) {
+    if (fate != MOVING) {
+      if (have) {
+        if (acc_zone >= 0) {
+          atomicAdd(t_eabs + acc_zone, acc_eabs);
+          if (A.tally_forces) {
+            atomicAdd(t_fx + acc_zone, acc_fx);
+            atomicAdd(t_fy + acc_zone, acc_fy);
+            atomicAdd(t_fz + acc_zone, acc_fz);
+            atomicAdd(t_fr + acc_zone, acc_fr);
+          }
+        }
+        atomicAdd(s_cnt + 3, (unsigned long long)seg);
+        atomicAdd(s_cnt + 4, (unsigned long long)n_scat);
+        n_scat = 0;
+        if (fate == ESCAPED) {
+          const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
+          if constexpr (BATCH) {
+            const int64_t so = A.models[m].spec_off;
+            spectrum_count(A, A.flux + so, A.click + so, t_obs, p.nu, p.e, p.D);
+            if (m != esc_model) {
+              if (esc_model >= 0) atomicAdd(A.model_escaped + esc_model, esc_count);
+              esc_model = m;
+              esc_count = 0;
+            }
+            ++esc_count;
+          } else {
+            spectrum_count(A, A.flux, A.click, t_obs, p.nu, p.e, p.D);
+          }
+          p.t = t_obs;
+          atomicAdd(s_cnt + 0, 1ULL);
+        } else if (fate == ABSORBED) {
+          atomicAdd(s_cnt + 1, 1ULL);
+        } else {
+          atomicAdd(s_cnt + 2, 1ULL);
+        }
+        if (A.rec_fate) {
+          A.rec_fate[pid] = fate;
+          A.rec_ind[pid] = p.ind;
+          A.rec_draws[pid] = (int32_t)(rng.n - K);
+          if (A.rec_type) A.rec_type[pid] = TYPE_PHOTON;
+          double* s = A.rec_state + pid * 9;
+          s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
+          s[3] = p.D[0]; s[4] = p.D[1]; s[5] = p.D[2];
+          s[6] = p.t; s[7] = p.e; s[8] = p.nu;
+        }
+        have = false;
+      }
+      if constexpr (BATCH) {
+        if (q_next >= q_end) {
+          q_next = (int64_t)atomicAdd(A.counters + C_QUEUE, (unsigned long long)A.queue_chunk);
+          q_end = q_next + A.queue_chunk;
+          if (q_end > A.n_packets) q_end = A.n_packets;
+        }
+        if (q_next >= A.n_packets) break;
+        pid = (unsigned long long)q_next++;
+        m = find_model(A.models, A.n_models, (int64_t)pid);
+        const BatchModel& M = A.models[m];
+        K = (M.emit_draws + 3u) / 4u;
+        rng.init(M.seed, (uint64_t)(M.first_pid + ((int64_t)pid - M.pkt_off)), step, 0);
+        BatchZoneOf zf;
+        zf.slice = G.r_out;
+        zf.slice.n = M.n_zones;
+        zf.slice.min = M.r_min;
+        zf.slice.right = G.r_out.right + M.zone_off;
+        zf.zone_off = M.zone_off;
+        DrawWords d{rng};
+        emit_core<0>(A, G, p, d, M.core_radius, M.Ep, M.core_cdf, zf);
+        tau_rem = neg_log_u(d.word());  // the first flight's depth: the emission's spare word
+      } else {
+        pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
+        if (pid >= (unsigned long long)A.n_packets) break;
+        if (A.q_n != nullptr && (int64_t)pid >= A.n_core) {
+          // a queued photon: census (stream position 0) or an optical
+          // photon the gamma-ray kernel handed over at its stream position
+          const int64_t k = (int64_t)pid - A.n_core;
+          const uint32_t qn = A.q_n[k];
+          if (qn == RADIO_NO_PHOTON) continue;
+          const double* q = A.q_state + (size_t)k * 9;
+          p.x[0] = q[0]; p.x[1] = q[1]; p.x[2] = q[2];
+          p.D[0] = q[3]; p.D[1] = q[4]; p.D[2] = q[5];
+          p.t = q[6]; p.e = q[7]; p.nu = q[8];
+          p.ind = A.q_ind[k];
+          rng.init(A.seed, (uint64_t)(A.radio_first_pid + k), step, qn);
+          K = 0;
+          tau_rem = neg_log_u(rng.block().x);
+        } else {
+          rng.init(A.seed, (uint64_t)A.first_pid + pid, step, 0);
+          DrawWords d{rng};
+          emit_core<0>(A, G, p, d, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<0>{G});
+          tau_rem = neg_log_u(d.word());  // the first flight's depth: the emission's spare word
+        }
+      }
+      fate = MOVING;
+      if (p.ind == -1) fate = ABSORBED;
+      else if (p.ind == -2) fate = ESCAPED;
+      seg = 0;
+      acc_zone = -1;
+      acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
+      have = true;
+      if (fate != MOVING) continue;
+      rsq = fma(p.x[0], p.x[0], fma(p.x[1], p.x[1], p.x[2] * p.x[2]));
+      xd = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
+    }
+    // ------------------------------------------------------------- segment
+    if (seg >= limit) { fate = STOPPED; atomicAdd(s_cnt + 5, 1ULL); continue; }
+    ++seg;
+    const int iz = p.ind;
+    if (iz != acc_zone) {
+      if (acc_zone >= 0) {
+        atomicAdd(t_eabs + acc_zone, acc_eabs);
+        if (A.tally_forces) {
+          atomicAdd(t_fx + acc_zone, acc_fx);
+          atomicAdd(t_fy + acc_zone, acc_fy);
+          atomicAdd(t_fz + acc_zone, acc_fz);
+          atomicAdd(t_fr + acc_zone, acc_fr);
+        }
+      }
+      acc_zone = iz;
+      acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
+      wl = zone_walls<BATCH>(A, G, iz);
+    }
+    double d_bn;
+    int new_ind = next_zone(wl, rsq, xd, &d_bn);
+    // comoving frequency and the opacity of its bin (transport_opacity.cpp:268-299)
+    const double gamma = rsqrt_nr(fma(-rsq, A.inv_ct2, 1.0));
+    const double dshift = gamma * fma(-xd, A.inv_ct, 1.0);
+    const double nu_cmf = p.nu * dshift;
+    const int i_nu = loc_within_fast<true>(A.nu, nu_cmf);
+    const float2 ab = __ldg(opac + (size_t)iz * nn + i_nu);
+    const float a_f = ab.x;
+    const float s_f = A.omit_scat ? 0.0f : ab.y;
+    const float op_f = a_f + s_f;
+    // distance over which the comoving frequency drifts by the bin's width
+    const float d_nu_f = __fdividef((float)(loc_delta(A.nu, i_nu) * A.ct), (float)p.nu);
+    const double d_nu = (double)fabsf(d_nu_f);
+    if (d_nu < d_bn) { d_bn = d_nu; new_ind = iz; }
+    const float tot_f = (float)((double)op_f * dshift);
+    const double d_sc = (tot_f > 0.0f) ? (double)__fdividef(tau_rem, tot_f) : (double)INFINITY;
+    const double d_tm = A.steady ? (double)INFINITY : (A.tstop - p.t) * C_LIGHT;
+    int event;
+    double this_d;
+    if ((d_sc < d_bn) && (d_sc < d_tm)) { event = 0; this_d = d_sc; }
+    else if (d_bn < d_tm) { event = 1; this_d = d_bn; }
+    else { event = 2; this_d = d_tm; }
+    // tallies (transport.cpp:361-392)
+    const double this_E = p.e * this_d;
+    const double eps_imc = __ldg(A.eps_imc + iz);
+    const double ed = this_E * dshift;
+    acc_eabs = fma(ed * dshift * (double)a_f, eps_imc, acc_eabs);
+    atomicAdd(A.J + (size_t)iz * nj + (A.store_Jnu ? i_nu : 0), this_E);
+    if (A.tally_forces) {
+      const double wd = ed * (double)op_f * dshift;
+      acc_fx = fma(wd, p.D[0], acc_fx);
+      acc_fy = fma(wd, p.D[1], acc_fy);
+      acc_fz = fma(wd, p.D[2], acc_fz);
+      acc_fr = fma(wd * xd, rsqrt_nr(rsq), acc_fr);
+    }
+    // move
+    p.x[0] = fma(this_d, p.D[0], p.x[0]);
+    p.x[1] = fma(this_d, p.D[1], p.x[1]);
+    p.x[2] = fma(this_d, p.D[2], p.x[2]);
+    constexpr double INV_C = 1.0 / C_LIGHT;
+    p.t = fma(this_d, INV_C, p.t);
+    rsq = fma(p.x[0], p.x[0], fma(p.x[1], p.x[1], p.x[2] * p.x[2]));
+    xd = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
+    if (event != 0) tau_rem = fmaxf(0.0f, fmaf(-tot_f, (float)this_d, tau_rem));  // depth crossed
+    if (event == 1) {
+      if (new_ind == -1) {
+        if (A.bound_in_reflect) { p.D[0] = -p.D[0]; p.D[1] = -p.D[1]; p.D[2] = -p.D[2]; xd = -xd; }
+        else { p.ind = new_ind; fate = ABSORBED; }
+      } else if (new_ind == -2) {
+        if (A.bound_out_reflect) { p.D[0] = -p.D[0]; p.D[1] = -p.D[1]; p.D[2] = -p.D[2]; xd = -xd; }
+        else { p.ind = new_ind; fate = ESCAPED; }
+      } else {
+        p.ind = new_ind;
+      }
+    } else if (event == 0) {
+      // do_scatter (scatter.cpp:12-70): u <= eps is the absorption branch;
+      // the deviate left over from each test is recycled into the next
+      ++n_scat;
+      const uint4 blk = rng.block();
+      tau_rem = neg_log_u(blk.x);  // the next flight's depth
+      const float u1 = (float)blk.y * W32;
+      const float num = u1 * op_f;
+      bool redist = false;
+      float v;
+      if (num <= a_f && a_f > 0.0f) {
+        v = __fdividef(num, a_f);
+        redist = true;
+        if (!A.radiative_eq) {
+          const float ei = (float)eps_imc;
+          if (v > ei) v = __fdividef(v - ei, 1.0f - ei);  // effective scattering
+          else { fate = ABSORBED; redist = false; }
+        }
+      } else {
+        v = __fdividef(num - a_f, s_f);
+      }
+      if (fate == MOVING) {
+        const double mu = 1.0 - 2.0 * ((double)blk.w * (1.0 / 4294967296.0));
+        scatter<CT>(A, p, rsq, xd, mu, fminf(fmaxf(v, 0.0f), 1.0f), blk.z, redist);
+        xd = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
+      }
+    } else {
+      fate = STOPPED;
+    }
+  }
+  if constexpr (BATCH) {
+    if (esc_model >= 0 && esc_count) atomicAdd(A.model_escaped + esc_model, esc_count);
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    constexpr int slot[6] = {C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT};
+    const unsigned long long v = s_cnt[threadIdx.x];
+    if (v) atomicAdd(A.counters + slot[threadIdx.x], v);
+  }
+  if (A.smem_zones) {
+    double* g[5] = {A.e_abs, A.fx, A.fy, A.fz, A.fr};
+    for (int i = threadIdx.x; i < 5 * nz; i += blockDim.x) {
+      const double v = s_tal[i];
+      if (v != 0.0 || isnan(v)) atomicAdd(g[i / nz] + (i % nz), v);
+    }
+  }
+}

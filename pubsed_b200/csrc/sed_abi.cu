@@ -666,8 +666,9 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     n_emit = 0;
     warnings |= SED_WARN_NO_PARTICLE_SPACE;
   }
-  if (c->tp.use_ddmc != 0 && (c->tp.use_ddmc != 2 || c->gtype != SED_GRID_1D_SPHERE))
-    return set_err(c, SED_ERR_ARG, "transport_use_ddmc %d: discrete diffusion is built for method 2 on 1D spheres",
+  if (c->tp.use_ddmc != 0 && ((c->tp.use_ddmc != 1 && c->tp.use_ddmc != 2) || c->gtype != SED_GRID_1D_SPHERE))
+    return set_err(c, SED_ERR_ARG,
+                   "transport_use_ddmc %d: discrete diffusion is built for methods 1 (IMD) and 2 (DDMC) on 1D spheres",
                    (int)c->tp.use_ddmc);
   const int64_t n_q = n_census + n_radio;
   const int64_t n_all = n_emit + n_q;
@@ -771,6 +772,11 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     A.radio_first_pid = c->tp.first_packet_id;
     A.q_state = c->d_q_state.p; A.q_ind = c->d_q_ind.p; A.q_n = c->d_q_n.p;
   }
+  if (c->tp.use_ddmc == 1) {  // compute_diffusion_probabilities(dt) (transport.cpp:44)
+    CK(c->d_imd_p.resize(4 * nz));
+    launches += launch_imd_probabilities(G, c->d_planck.p, dt, c->d_imd_p.p, c->stream);
+    A.imd_p = c->d_imd_p.p;
+  }
   CK(cudaEventRecord(c->ev[3], c->stream));
   if (A.n_packets > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
   CK(cudaGetLastError());
@@ -820,6 +826,7 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
   if (cnt[C_LIMIT] > 0) return set_err(c, SED_ERR_LIMIT, "%llu packets hit the segment limit", cnt[C_LIMIT]);
   if (cnt[C_DDMC_CAP] > 0)
     return set_err(c, SED_ERR_LIMIT, "%llu diffusion scatters found no new frequency bin", cnt[C_DDMC_CAP]);
+  if (cnt[C_IMD_CAP] > 0) return set_err(c, SED_ERR_LIMIT, "%llu IMD calls hit the hop bound", cnt[C_IMD_CAP]);
   if (n_reject_cap > 0)
     return set_err(c, SED_ERR_LIMIT, "%d Compton scatters hit the rejection-sampling bound", (int)n_reject_cap);
   return SED_OK;

@@ -22,7 +22,8 @@ struct GridDev {
 struct BatchModel;
 
 // counters[] slots written by the packet kernel
-enum Counter { C_QUEUE = 0, C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT, C_DDMC_CAP, C_COUNT };
+enum Counter { C_QUEUE = 0, C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT, C_DDMC_CAP, C_IMD_CAP,
+               C_COUNT };
 
 struct StepArgs {
   int32_t steady, radiative_eq, bound_in_reflect, bound_out_reflect;
@@ -35,8 +36,9 @@ struct StepArgs {
   double core_radius, core_freq;
   const double* core_cdf;     // [n_nu] normalised core emission CDF
   int32_t max_segments;
-  int32_t use_ddmc;           // 2: discrete diffusion in diffusive zones (1D)
+  int32_t use_ddmc;           // 1: IMD, 2: DDMC in diffusive zones (1D)
   double ddmc_tau;            // transport_ddmc_tau_threshold
+  const double* imd_p;        // IMD: [4][nz] hop up, hop down, stay, absorb probabilities of the step
   int32_t smem_zones;         // 1: per-block shared-memory zone tallies
   int32_t n_rep;              // >0 (and smem_zones 0): zone-scalar tallies in n_rep global copies
   double* zone_rep;           // [n_rep][5][nz] e_abs, fx, fy, fz, fr copies, summed by the finish kernel
@@ -176,6 +178,9 @@ struct BatchModel {
 
 // launches the persistent packet kernel; returns the number of launches
 int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s);
+// IMD probabilities of the step (transport::compute_diffusion_probabilities)
+// from the zone Planck means into out[4][nz]
+int launch_imd_probabilities(const GridDev& g, const double* planck, double dt, double* out, cudaStream_t s);
 // zone-scalar tally normalisation (reduce_radiation) and steady-state rescale
 int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_t nspec, cudaStream_t s);
 

@@ -378,13 +378,14 @@ struct DrawWords {
   PacketRng& r;
   uint4 b;
   int used = 4;
-  __device__ double operator()()
+  __device__ uint32_t word()
   {
     if (used == 4) { b = r.block(); used = 0; }
     const uint32_t w = (used == 0) ? b.x : (used == 1) ? b.y : (used == 2) ? b.z : b.w;
     ++used;
-    return w01(w);
+    return w;
   }
+  __device__ double operator()() { return w01(word()); }
 };
 
 template <int GRID, class ZoneOf, class Draw>
@@ -472,6 +473,13 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 #ifndef SED_PROP_THREADS
 #define SED_PROP_THREADS 128
 #endif
+// launch shape of the mixed-form 1D kernel (propagate_mixed_kernel)
+#ifndef SED_MIXED_THREADS
+#define SED_MIXED_THREADS 128
+#endif
+#ifndef SED_MIXED_MINB
+#define SED_MIXED_MINB 6
+#endif
 #ifndef SED_PROP_MINB
 #define SED_PROP_MINB 8
 #endif
@@ -505,7 +513,10 @@ template <typename OT>
 __device__ __forceinline__ int ddmc_opacity(const StepArgs& A, const OT* __restrict__ opac, int iz, double nu_cmf,
                                             double* op, double* eps);
 
-// DD: discrete diffusion on (transport_use_ddmc = 2; 1D, FP64 expressions)
+template <typename OT>
+__device__ int imd_event(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng, double* t_eabs,
+                         unsigned long long& n_cap);
+// DD: discrete diffusion on (transport_use_ddmc = 1 IMD or 2 DDMC; 1D, FP64 expressions)
 template <int GRID, typename OT, typename CT, int BATCH, int MODE, bool FAST, int THREADS, int MINB, bool DD = false>
 __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs A, const GridDev G)
 {
@@ -568,7 +579,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   // call of discrete_diffuse_DDMC) and the time that call has left
   bool dd_call = false;
   double dd_rem = 0;
-  unsigned long long n_ddcap = 0;
+  unsigned long long n_ddcap = 0, n_imdcap = 0;
   for (;;) {
     if (fate != MOVING) {
       if (have && MODE == 2) {
@@ -733,6 +744,10 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         // transport::propagate's zone test (transport.cpp:216-246): a photon
         // in a diffusive zone takes a diffusion event instead of a segment
         if (ddmc_zone<OT>(A, G, opac, p)) {
+          if (A.use_ddmc == 1) {  // one IMD call (transport.cpp:236-237)
+            fate = imd_event<OT>(A, G, p, rng, t_eabs, n_imdcap);
+            continue;
+          }
           if (!dd_call) { dd_rem = A.tstop - p.t; dd_call = true; }
           fate = ddmc_event<OT, CT>(A, G, opac, p, rng, dd_rem, acc_eabs, n_scat, n_ddcap);
           continue;
@@ -918,7 +933,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
   // counters: warp reduction, one atomic per warp
   n_esc = warp_sum(n_esc); n_abs = warp_sum(n_abs); n_stop = warp_sum(n_stop);
   n_seg = warp_sum(n_seg); n_scat = warp_sum(n_scat); n_lim = warp_sum(n_lim);
-  if constexpr (DD) n_ddcap = warp_sum(n_ddcap);
+  if constexpr (DD) { n_ddcap = warp_sum(n_ddcap); n_imdcap = warp_sum(n_imdcap); }
   if ((threadIdx.x & 31) == 0) {
     if (n_esc) atomicAdd(A.counters + C_ESCAPED, n_esc);
     if (n_abs) atomicAdd(A.counters + C_ABSORBED, n_abs);
@@ -927,6 +942,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
     if (n_scat) atomicAdd(A.counters + C_SCATTERS, n_scat);
     if (n_lim) atomicAdd(A.counters + C_LIMIT, n_lim);
     if (n_ddcap) atomicAdd(A.counters + C_DDMC_CAP, n_ddcap);
+    if (n_imdcap) atomicAdd(A.counters + C_IMD_CAP, n_imdcap);
   }
   if (MODE != 2 && A.smem_zones) {
     __syncthreads();
@@ -1226,6 +1242,113 @@ __device__ void ddmc_move_across(const StepArgs& A, const GridDev& G, Pkt& p, Pa
     p.D[0] = -p.D[0]; p.D[1] = -p.D[1]; p.D[2] = -p.D[2];
   }
   lorentz_transform<0>(G, p, 1);
+}
+
+// ------------------------------------------------------------ IMD
+// transport::discrete_diffuse_IMD (discrete_diffusion.cpp:18-110), IMD
+// (Gentile 2001) as the reference has it: propagate calls it with the end
+// time of the step where the function means the step (transport.cpp:237), so
+// the photon's time advances by tstop and the J tally and the advection take
+// tstop as the interval.  The photon hops one zone up or down (a radial move
+// by its starting zone's width) until it stays, is then advected, loses
+// energy adiabatically and stops.  J goes to bin 0 of the zone, as in the
+// reference; the hop loop, unbounded there, gives up after 2^24 hops
+// (counted, SED_ERR_LIMIT).
+template <typename OT>
+__device__ int imd_event(const StepArgs& A, const GridDev& G, Pkt& p, PacketRng& rng, double* t_eabs,
+                         unsigned long long& n_cap)
+{
+  const int nz = G.nzones, nn = A.nu.n;
+  const int nj = A.store_Jnu ? nn : 1;
+  const double* P_up = A.imd_p;
+  const double* P_dn = A.imd_p + nz;
+  const double* P_st = A.imd_p + 2 * nz;
+  const double* P_ab = A.imd_p + 3 * nz;
+  const double dt = A.tstop;
+  const double dx = loc_delta(G.r_out, p.ind);
+  p.t += dt;
+  for (int hops = 0;; ++hops) {
+    if (hops >= (1 << 24)) { ++n_cap; break; }
+    p.ind = get_zone<0>(G, p.x);
+    if (p.ind == -1) return ABSORBED;
+    if (p.ind == -2) return ESCAPED;
+    const int i = p.ind;
+    atomicAdd(t_eabs + i, p.e * __ldg(P_ab + i));
+    atomicAdd(A.J + (size_t)i * nj, p.e * __ldg(P_st + i) * dt * C_LIGHT);
+    const double P_diff = __ldg(P_up + i) + __ldg(P_dn + i);
+    const double P_stay = __ldg(P_ab + i) + __ldg(P_st + i);
+    const double r1 = rng.next();
+    if (r1 < P_diff) {
+      const double r2 = rng.next();
+      if (r2 < __ldg(P_up + i) / P_diff) {
+        p.ind++;
+        const double rr = sqrt(p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+        p.x[0] += p.x[0] / rr * dx;
+        p.x[1] += p.x[1] / rr * dx;
+        p.x[2] += p.x[2] / rr * dx;
+      } else {
+        p.ind--;
+        const double rr = sqrt(p.x[0] * p.x[0] + p.x[1] * p.x[1] + p.x[2] * p.x[2]);
+        p.x[0] -= p.x[0] / rr * dx;
+        p.x[1] -= p.x[1] / rr * dx;
+        p.x[2] -= p.x[2] / rr * dx;
+      }
+    } else {
+      const double r2 = rng.next();
+      const double f_abs = __ldg(P_ab + i) / P_stay;
+      if (r2 < f_abs) return ABSORBED;
+      double v[3], dvds;
+      get_velocity<0>(G, p.ind, p.x, p.D, v, &dvds);
+      p.x[0] += v[0] * dt;
+      p.x[1] += v[1] * dt;
+      p.x[2] += v[2] * dt;
+      p.e *= (1 - dvds * dt);
+      break;
+    }
+  }
+  p.ind = get_zone<0>(G, p.x);
+  if (p.ind == -1) return ABSORBED;
+  if (p.ind == -2) return ESCAPED;
+  return STOPPED;
+}
+
+// transport::compute_diffusion_probabilities (discrete_diffusion.cpp:687-756)
+// for zone i: hop probabilities from the Planck-mean diffusion coefficients
+// of the zone and its neighbours, normalised with the (zero) advection and
+// absorption probabilities; the rest is "stay"
+__global__ void imd_probabilities_kernel(const GridDev G, const double* __restrict__ planck, double dt,
+                                         double* __restrict__ out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nz = G.nzones;
+  if (i >= nz) return;
+  const double dx = loc_delta(G.r_out, i);
+  int ip = i + 1;
+  if (ip == nz) ip = i;
+  int im = i - 1;
+  if (im < 0) im = 0;
+  const double Dj0 = C_LIGHT / (3.0 * planck[i]);
+  const double Djp = C_LIGHT / (3.0 * planck[ip]);
+  const double Djm = C_LIGHT / (3.0 * planck[im]);
+  const double Dh_up = 2 * dx * (Dj0 * Djp) / (Dj0 * dx + Djp * dx);
+  const double Dh_dn = 2 * dx * (Dj0 * Djm) / (Dj0 * dx + Djm * dx);
+  const double r_p = __ldg(G.r_out.right + i);  // grid_1D_sphere::coordinates: r_out[i]
+  double r_m = __ldg(G.r_out.right + im);
+  if (i == 0) r_m = 0;
+  const double r_0 = 0.5 * (r_p + r_m);
+  double up = (dt / dx) * (Dh_up / dx) * r_p * r_p / r_0 / r_0;
+  double dn = (dt / dx) * (Dh_dn / dx) * r_m * r_m / r_0 / r_0;
+  if (i == 0) dn = 0;
+  double adv = 0.0, ab = 0.0;
+  double norm = 1 + adv + ab;
+  norm += up + dn;
+  ab /= norm;
+  up /= norm;
+  dn /= norm;
+  out[i] = up;
+  out[nz + i] = dn;
+  out[2 * nz + i] = 1.0 / norm;
+  out[3 * nz + i] = ab;
 }
 
 // One pass of the event loop of transport::discrete_diffuse_DDMC
@@ -1743,6 +1866,32 @@ __global__ void init_particles_kernel(const InitArgs I, const GridDev G)
   }
 }
 
+#include "mixed_kernel.cuh"
+
+// the mixed-form 1D kernel (propagate_mixed_kernel) in one compiled shape
+// (zone-scalar tallies go straight to global memory when MINB blocks'
+// shared-memory copies would not fit on an SM)
+template <int BATCH, int THREADS, int MINB>
+int launch_mixed_t(const StepArgs& a0, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
+                   cudaStream_t s)
+{
+  StepArgs a = a0;
+  if (a.smem_zones && (size_t)MINB * 5 * g.nzones * sizeof(double) > (size_t)200 * 1024) a.smem_zones = 0;
+  const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
+  auto kern = propagate_mixed_kernel<BATCH, THREADS, MINB>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
+  if (per_sm < 1) per_sm = 1;
+  if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+  int64_t blocks = (int64_t)num_sms * per_sm;
+  const int64_t need = (total + THREADS - 1) / THREADS;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  kern<<<(unsigned)blocks, THREADS, smem, s>>>(a, g);
+  return 1;
+}
+
 template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB, int MODE = 0,
           bool FAST = (sizeof(OT) == sizeof(float2)), bool DD = false>
 int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
@@ -1773,20 +1922,19 @@ int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStr
 {
   // discrete diffusion (1D): the reference's expressions in both forms
   if constexpr (GRID == 0) {
-    if (a.use_ddmc == 2) return launch_kernel_t<0, OT, CT, 0, 256, 4, 0, false, true>(a, g, 0, num_sms, a.n_packets, s);
+    if (a.use_ddmc == 1 || a.use_ddmc == 2)
+      return launch_kernel_t<0, OT, CT, 0, 256, 4, 0, false, true>(a, g, 0, num_sms, a.n_packets, s);
   }
   // mixed tables on a grid with a tabulated velocity field: the reference's
   // expressions (the division-free transforms assume v = x / t)
   if (sizeof(OT) == sizeof(float2) && !g.homologous)
     return launch_kernel_t<GRID, OT, CT, 0, 256, 4, 0, false>(a, g, 0, num_sms, a.n_packets, s);
   if constexpr (sizeof(OT) == sizeof(float2)) {
-    if constexpr (GRID == 0) {
-      if (!a.smem_zones || (size_t)7 * 5 * g.nzones * sizeof(double) <= (size_t)200 * 1024)
-        return launch_kernel_t<0, OT, CT, 0, 128, 7>(a, g, 0, num_sms, a.n_packets, s);
-    }
-    return launch_kernel_t<GRID, OT, CT, 0, 256, 3>(a, g, 0, num_sms, a.n_packets, s);
+    if constexpr (GRID == 0) return launch_mixed_t<0, SED_MIXED_THREADS, SED_MIXED_MINB>(a, g, 0, num_sms, a.n_packets, s);
+    else return launch_kernel_t<GRID, OT, CT, 0, 256, 3>(a, g, 0, num_sms, a.n_packets, s);
+  } else {
+    return launch_kernel_t<GRID, OT, CT, 0, 256, 4>(a, g, 0, num_sms, a.n_packets, s);
   }
-  return launch_kernel_t<GRID, OT, CT, 0, 256, 4>(a, g, 0, num_sms, a.n_packets, s);
 }
 
 // batched kernel shapes {threads, min blocks per SM}: 32 or 24 warps per SM
@@ -1797,11 +1945,20 @@ template <typename OT, typename CT>
 int launch_batch_t(const StepArgs& a, const GridDev& g, int variant, int bps, int num_sms, int64_t total,
                    cudaStream_t s)
 {
-  switch (variant) {
-    case 1: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[1][0], BATCH_SHAPES[1][1]>(a, g, bps, num_sms, total, s);
-    case 2: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[2][0], BATCH_SHAPES[2][1]>(a, g, bps, num_sms, total, s);
-    case 3: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[3][0], BATCH_SHAPES[3][1]>(a, g, bps, num_sms, total, s);
-    default: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[0][0], BATCH_SHAPES[0][1]>(a, g, bps, num_sms, total, s);
+  if constexpr (sizeof(OT) == sizeof(float2)) {  // mixed form: propagate_mixed_kernel
+    switch (variant) {
+      case 1: return launch_mixed_t<1, BATCH_SHAPES[1][0], BATCH_SHAPES[1][1]>(a, g, bps, num_sms, total, s);
+      case 2: return launch_mixed_t<1, BATCH_SHAPES[2][0], BATCH_SHAPES[2][1]>(a, g, bps, num_sms, total, s);
+      case 3: return launch_mixed_t<1, BATCH_SHAPES[3][0], BATCH_SHAPES[3][1]>(a, g, bps, num_sms, total, s);
+      default: return launch_mixed_t<1, BATCH_SHAPES[0][0], BATCH_SHAPES[0][1]>(a, g, bps, num_sms, total, s);
+    }
+  } else {
+    switch (variant) {
+      case 1: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[1][0], BATCH_SHAPES[1][1]>(a, g, bps, num_sms, total, s);
+      case 2: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[2][0], BATCH_SHAPES[2][1]>(a, g, bps, num_sms, total, s);
+      case 3: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[3][0], BATCH_SHAPES[3][1]>(a, g, bps, num_sms, total, s);
+      default: return launch_kernel_t<0, OT, CT, 1, BATCH_SHAPES[0][0], BATCH_SHAPES[0][1]>(a, g, bps, num_sms, total, s);
+    }
   }
 }
 
@@ -1815,6 +1972,12 @@ int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStrea
   }
   if (a.precision == 0) return launch_propagate_t<1, double2, double>(a, g, num_sms, s);
   return launch_propagate_t<1, float2, float>(a, g, num_sms, s);
+}
+
+int launch_imd_probabilities(const GridDev& g, const double* planck, double dt, double* out, cudaStream_t s)
+{
+  imd_probabilities_kernel<<<(g.nzones + 127) / 128, 128, 0, s>>>(g, planck, dt, out);
+  return 1;
 }
 
 int launch_finish(const StepArgs& a, const GridDev& g, const double* vol, int64_t nspec, cudaStream_t s)
