@@ -8,16 +8,18 @@
 # 5.2.1 is built from the reference's vendored tarball in a temporary
 # directory and only its static library is kept (oracle/_ref/liblua.a).
 #
-# usage: oracle/ref/build_ref.sh [reference_root]   (default /root/reference)
+# usage: oracle/ref/build_ref.sh [reference_root]
+#   reference_root: the argument, else $SEDONA_REFERENCE, else /root/reference.
+#   Exits 3 (nothing built) when no reference sources are there.
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${SEDONA_REFERENCE:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$(cd "$HERE/.." && pwd)/_ref
-mkdir -p "$OUT"
 if [ ! -d "$REF/src" ]; then
-  echo "reference sources not found at $REF; nothing built" >&2
-  exit 1
+  echo "reference sources not found at $REF (pass the reference root or set SEDONA_REFERENCE); nothing built" >&2
+  exit 3
 fi
+mkdir -p "$OUT"
 JOBS=${JOBS:-8}
 # pick a C++ driver that can link OpenMP (the plain g++ wrapper on this image
 # cannot find libgomp.spec; the triplet-named driver can)
