@@ -382,6 +382,29 @@ int sed_diff_vjp_density(sed_ctx* ctx, const double* grad_flux, double* grad_rho
  * sed_set_emission in between makes them return SED_ERR_STATE. */
 int sed_diff_jacobian(sed_ctx* ctx, double* jac, sed_step_stats* stats);
 
+/* Device-pointer forms for callers whose data already lives on the GPU (a
+ * torch tensor, another library's buffer): the same computations with every
+ * array argument a device pointer of this context's device.  The caller's
+ * work that writes those arrays must be complete before the call (the
+ * library reads them on its own stream); the results are complete when the
+ * call returns.  sed_diff_forward_dev also copies the binned spectrum
+ * (n_spec doubles) into flux_dev when flux_dev is not NULL. */
+int sed_diff_forward_dev(sed_ctx* ctx, double dt, const double* abs_scale_dev, int32_t n_bands, double* flux_dev,
+                         sed_step_stats* stats);
+int sed_diff_vjp_dev(sed_ctx* ctx, const double* grad_flux_dev, double* grad_scale_dev, sed_step_stats* stats);
+int sed_diff_vjp_density_dev(sed_ctx* ctx, const double* grad_flux_dev, double* grad_rho_dev,
+                             sed_step_stats* stats);
+
+/* Per-zone density factors for the differentiable transport: both
+ * extinctions of zone z in the tables of the last opacity build (or load)
+ * are multiplied by rho_scale[z] (n_zones entries; the opacity per unit mass
+ * held), in place of the tables the packet kernels read, until the next call
+ * or build.  NULL puts the built tables back.  The built tables are kept on
+ * the device, so repeated calls scale the build, never an earlier scaling.
+ * The _dev form takes a device pointer.  No reference counterpart. */
+int sed_diff_scale_extinction(sed_ctx* ctx, const double* rho_scale);
+int sed_diff_scale_extinction_dev(sed_ctx* ctx, const double* rho_scale_dev);
+
 /* ------------------------------------------------------------------ batches
  * Many independent 1D spherical ejecta models (grid_1D_sphere, homologous)
  * stepped together: one opacity build over all their zones and ONE packet

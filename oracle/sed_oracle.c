@@ -94,6 +94,9 @@ struct oracle_ctx {
   double *gflux, *gclick;
   int64_t n_reject_cap;  /* Compton scatters that hit the rejection bound */
   int64_t n_limit;       /* packets of the step stopped by the segment limit */
+  /* the built {abs, scat} tables while density-scaled ones are in abs/scat */
+  double *abs_base, *scat_base;
+  int base_valid;
   /* IMD (transport_use_ddmc = 1): per-zone hop / stay / absorption
    * probabilities of the step (compute_diffusion_probabilities) */
   double *imd_up, *imd_dn, *imd_stay, *imd_abs;
@@ -251,6 +254,9 @@ static void free_grid(oracle_ctx* o)
   free(o->abs); free(o->scat); free(o->cdf); free(o->eps_imc); free(o->n_elec); free(o->planck); free(o->ross); free(o->L_th);
   free(o->imd_up); free(o->imd_dn); free(o->imd_stay); free(o->imd_abs);
   o->imd_up = o->imd_dn = o->imd_stay = o->imd_abs = NULL;
+  free(o->abs_base); free(o->scat_base);
+  o->abs_base = o->scat_base = NULL;
+  o->base_valid = 0;
   o->v_r = o->vol = o->rho = o->T = o->e_gas = o->grey = o->X = NULL;
   o->eZ = o->eA = NULL;
 }
@@ -807,6 +813,7 @@ int oracle_set_opacity(oracle_ctx* o, double dt)
   free(opac); free(aopac); free(emis); free(t1); free(t2);
   free(g.ion_part); free(g.ion_frac); free(g.lev_n); free(g.n_dens); free(g.mass_frac);
   o->have_opacity = 1;
+  o->base_valid = 0;
   return SED_OK;
 }
 
@@ -821,6 +828,29 @@ int oracle_load_opacity(oracle_ctx* o, const double* abs, const double* scat, co
   }
   for (int i = 0; i < o->nzones; ++i) o->eps_imc[i] = eps_imc[i];
   o->have_opacity = 1;
+  o->base_valid = 0;
+  return SED_OK;
+}
+
+/* sed_diff_scale_extinction: both extinctions of zone z of the built tables
+ * times r[z]; r NULL puts the built tables back (no reference counterpart) */
+int oracle_diff_scale_extinction(oracle_ctx* o, const double* r)
+{
+  if (!o || !o->have_opacity) return SED_ERR_STATE;
+  size_t nn = (size_t)o->nu.n, n = (size_t)o->nzones * nn;
+  if (!o->base_valid) {
+    free(o->abs_base); free(o->scat_base);
+    o->abs_base = (double*)malloc(n * sizeof(double));
+    o->scat_base = (double*)malloc(n * sizeof(double));
+    memcpy(o->abs_base, o->abs, n * sizeof(double));
+    memcpy(o->scat_base, o->scat, n * sizeof(double));
+    o->base_valid = 1;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    double f = r ? r[i / nn] : 1.0;
+    o->abs[i] = r ? o->abs_base[i] * f : o->abs_base[i];
+    o->scat[i] = r ? o->scat_base[i] * f : o->scat_base[i];
+  }
   return SED_OK;
 }
 

@@ -48,6 +48,7 @@ int oracle_diff_forward(oracle_ctx* o, double dt, const double* abs_scale, int32
 int oracle_diff_vjp(oracle_ctx* o, const double* grad_flux, double* grad_scale, sed_step_stats* stats);
 int oracle_diff_vjp_density(oracle_ctx* o, const double* grad_flux, double* grad_rho, sed_step_stats* st);
 int oracle_diff_jacobian(oracle_ctx* o, double* jac, sed_step_stats* stats);
+int oracle_diff_scale_extinction(oracle_ctx* o, const double* rho_scale);
 /* packets carried between time-dependent steps, the transport clock, and
  * the initial radiation field's packets */
 int64_t oracle_n_particles(oracle_ctx* o);

@@ -41,6 +41,8 @@ EXPORTED = [
     "sed_get_zone_tallies", "sed_get_opacity", "sed_record_packets", "sed_get_packet_records",
     "sed_n_particles", "sed_last_error", "sed_ctx_destroy", "sed_version",
     "sed_set_rng_step", "sed_diff_forward", "sed_diff_vjp", "sed_diff_vjp_density", "sed_diff_jacobian", "sed_solve_temperature",
+    "sed_diff_forward_dev", "sed_diff_vjp_dev", "sed_diff_vjp_density_dev", "sed_diff_scale_extinction",
+    "sed_diff_scale_extinction_dev",
     "sed_get_gamma_spectrum", "sed_get_radioactive_tallies", "sed_set_emission",
     "sed_get_particles", "sed_set_time", "sed_get_time", "sed_initialize_particles", "sed_wipe_spectra", "sed_set_core_source",
     "sed_batch_create", "sed_batch_set_opacity_params", "sed_batch_set_atomic_data", "sed_batch_autotune",

@@ -213,6 +213,12 @@ def declare(lib: C.CDLL, prefix: str) -> C.CDLL:
             "batch_get_packet_records": ([vp, C.c_int32, C.c_int64, _ip, _ip, _ip, _dp], C.c_int),
             "batch_last_error": ([vp], C.c_char_p),
             "batch_destroy": ([vp], None),
+            # device-pointer forms of the differentiable transport (pointers as integers)
+            "diff_forward_dev": ([vp, C.c_double, vp, C.c_int32, vp, C.POINTER(StepStats)], C.c_int),
+            "diff_vjp_dev": ([vp, vp, vp, C.POINTER(StepStats)], C.c_int),
+            "diff_vjp_density_dev": ([vp, vp, vp, C.POINTER(StepStats)], C.c_int),
+            "diff_scale_extinction": ([vp, _dp], C.c_int),
+            "diff_scale_extinction_dev": ([vp, vp], C.c_int),
         })
     for name, (args, res) in sig.items():
         fn = getattr(lib, prefix + name)

@@ -16,8 +16,12 @@ theta.
 `vjp_density(g)` is the gradient with respect to each zone's density (both
 extinctions of the zone scale with it; opacity per unit mass held), and
 `spectrum_from_density(r, engine, step)` the torch Function of the per-zone
-density factors r: its forward scales the tables of the last opacity build,
-its backward is that replay.  The scattering part of the density derivative
+density factors r: its forward scales the tables of the last opacity build
+on the device (sed_diff_scale_extinction), its backward is that replay.
+
+Both torch Functions keep CUDA tensors on the device: theta or r, the
+spectrum and the gradients go through the _dev entry points as device
+pointers (no host copy); CPU tensors take the host entry points.  The scattering part of the density derivative
 is a likelihood-ratio (score) term, since the scattering opacity decides
 where a path goes: unbiased, but not a smooth function of r for fixed
 deviates, so it is checked against finite differences of the expected
@@ -43,31 +47,71 @@ class DiffEngine(Engine):
         self.n_bands = int(n_bands)
         self.forward_id = 0          # increments with every forward
         self._have_tables = False
-        self._base = None            # tables of the last opacity build, kept while density-scaled ones are loaded
         self._scaled = False         # the context holds density-scaled tables
 
     def tables(self, dt: float = 1.0):
         """Opacity build (sed_set_opacity); the forward runs on these tables."""
         self.set_opacity(dt)
         self._have_tables = True
-        self._base = None
         self._scaled = False
 
-    def _load(self, abs_, scat):
-        b = self._base
-        k = abi.Keep()
-        self._check(self.L.sed_load_opacity(self.ctx, k.d(abs_), k.d(scat), k.d(b["emis_cdf"]), k.d(b["eps_imc"])),
-                    "sed_load_opacity")
+    def _unscale(self):
+        if self._scaled:  # a density forward left scaled tables: the built ones back
+            self._check(self.L.sed_diff_scale_extinction(self.ctx, None), "sed_diff_scale_extinction")
+            self._scaled = False
 
     def forward(self, theta: Optional[np.ndarray] = None, step: Optional[int] = None, dt: float = 1.0):
         """Weighted forward on the tables of the last opacity build; returns
         (flux, click, stats)."""
         if not self._have_tables:
             self.tables(dt)
-        if self._scaled:  # a density forward left scaled tables: put the built ones back
-            self._load(self._base["abs"], self._base["scat"])
-            self._scaled = False
+        self._unscale()
         return self._forward(theta, step, dt)
+
+    def forward_dev(self, theta, step: Optional[int] = None, dt: float = 1.0):
+        """forward() with theta a CUDA float64 tensor ([n_zones, n_bands] or
+        None); returns the spectrum as a CUDA float64 tensor, on the device
+        throughout (sed_diff_forward_dev)."""
+        import torch
+        if not self._have_tables:
+            self.tables(dt)
+        self._unscale()
+        if step is not None:
+            self._check(self.L.sed_set_rng_step(self.ctx, int(step) & 0xFFFFFFFF), "sed_set_rng_step")
+        th = None
+        if theta is not None:
+            theta = _dev_f64(theta, self.nz * self.n_bands, "theta")
+        flux = torch.empty(self.nspec, dtype=torch.float64, device=theta.device if theta is not None else "cuda")
+        torch.cuda.current_stream().synchronize()  # theta written before the library's stream reads it
+        st = abi.StepStats()
+        self._check(self.L.sed_diff_forward_dev(self.ctx, dt, theta.data_ptr() if theta is not None else None,
+                                                self.n_bands, flux.data_ptr(), C.byref(st)), "sed_diff_forward_dev")
+        self.forward_id += 1
+        return flux
+
+    def vjp_dev(self, grad_flux, density: bool = False):
+        """vjp() / vjp_density() with grad_flux a CUDA float64 tensor; the
+        gradient comes back as a CUDA tensor ([n_zones, n_bands] or [n_zones])."""
+        import torch
+        g = _dev_f64(grad_flux, self.nspec, "grad_flux")
+        out = torch.empty(self.nz if density else self.nz * self.n_bands, dtype=torch.float64, device=g.device)
+        torch.cuda.current_stream().synchronize()
+        st = abi.StepStats()
+        fn = self.L.sed_diff_vjp_density_dev if density else self.L.sed_diff_vjp_dev
+        self._check(fn(self.ctx, g.data_ptr(), out.data_ptr(), C.byref(st)), "sed_diff_vjp_dev")
+        self.last_replay = st.as_dict()
+        return out if density else out.reshape(self.nz, self.n_bands)
+
+    def scale_density_dev(self, r):
+        """Both extinctions of zone z of the built tables times r[z], r a CUDA
+        float64 tensor (sed_diff_scale_extinction_dev)."""
+        import torch
+        if not self._have_tables:
+            self.tables()
+        r = _dev_f64(r, self.nz, "r")
+        torch.cuda.current_stream().synchronize()
+        self._check(self.L.sed_diff_scale_extinction_dev(self.ctx, r.data_ptr()), "sed_diff_scale_extinction_dev")
+        self._scaled = True
 
     def _forward(self, theta, step, dt):
         if step is not None:
@@ -114,14 +158,10 @@ class DiffEngine(Engine):
         scattering); returns (flux, click, stats)."""
         if not self._have_tables:
             self.tables(dt)
-        if self._base is None:
-            self._base = self.opacity()
         r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
         if r.size != self.nz:
             raise ValueError("r has %d entries, expected %d" % (r.size, self.nz))
-        b = self._base
-        self._load((b["abs"].reshape(self.nz, -1) * r[:, None]).ravel(),
-                   (b["scat"].reshape(self.nz, -1) * r[:, None]).ravel())
+        self._check(self.L.sed_diff_scale_extinction(self.ctx, r.ctypes.data_as(abi._dp)), "sed_diff_scale_extinction")
         self._scaled = True
         return self._forward(None, step, dt)
 
@@ -139,6 +179,17 @@ def _torch():
     return torch
 
 
+def _dev_f64(t, n: int, what: str):
+    """t as a contiguous CUDA float64 tensor of n entries."""
+    torch = _torch()
+    if not (isinstance(t, torch.Tensor) and t.is_cuda):
+        raise TypeError("%s must be a CUDA tensor" % what)
+    t = t.detach().to(torch.float64).contiguous().reshape(-1)
+    if t.numel() != n:
+        raise ValueError("%s has %d entries, expected %d" % (what, t.numel(), n))
+    return t
+
+
 def _make_function():
     torch = _torch()
 
@@ -151,23 +202,30 @@ def _make_function():
 
         @staticmethod
         def forward(ctx, theta, engine: DiffEngine, step: int):
-            th = theta.detach().to("cpu", torch.float64).numpy()
-            flux, _, _ = engine.forward(th, step=step)
             ctx.engine = engine
             ctx.step = step
-            ctx.fid = engine.forward_id
             ctx.save_for_backward(theta)
-            return torch.from_numpy(flux).to(theta.device)
+            if theta.is_cuda:
+                flux = engine.forward_dev(theta, step=step)
+            else:
+                f, _, _ = engine.forward(theta.detach().to(torch.float64).numpy(), step=step)
+                flux = torch.from_numpy(f)
+            ctx.fid = engine.forward_id
+            return flux
 
         @staticmethod
         def backward(ctx, grad_flux):
             (theta,) = ctx.saved_tensors
             eng = ctx.engine
+            if theta.is_cuda:
+                if eng.forward_id != ctx.fid:
+                    eng.forward_dev(theta, step=ctx.step)
+                grad = eng.vjp_dev(grad_flux)
+                return grad.to(theta.dtype), None, None
             if eng.forward_id != ctx.fid:
-                eng.forward(theta.detach().to("cpu", torch.float64).numpy(), step=ctx.step)
-            g = grad_flux.detach().to("cpu", torch.float64).numpy()
-            grad = eng.vjp(g)
-            return torch.from_numpy(grad).to(theta.device, theta.dtype), None, None
+                eng.forward(theta.detach().to(torch.float64).numpy(), step=ctx.step)
+            grad = eng.vjp(grad_flux.detach().to("cpu", torch.float64).numpy())
+            return torch.from_numpy(grad).to(theta.dtype), None, None
 
     return SpectrumFromAbsorption
 
@@ -183,26 +241,47 @@ def _make_density_function():
 
         @staticmethod
         def forward(ctx, r, engine: DiffEngine, step: int):
-            rr = r.detach().to("cpu", torch.float64).numpy()
-            flux, _, _ = engine.forward_density(rr, step=step)
             ctx.engine = engine
             ctx.step = step
-            ctx.fid = engine.forward_id
             ctx.save_for_backward(r)
-            return torch.from_numpy(flux).to(r.device)
+            if r.is_cuda:
+                flux = _density_forward_dev(engine, r, step)
+            else:
+                f, _, _ = engine.forward_density(r.detach().to(torch.float64).numpy(), step=step)
+                flux = torch.from_numpy(f)
+            ctx.fid = engine.forward_id
+            return flux
 
         @staticmethod
         def backward(ctx, grad_flux):
             (r,) = ctx.saved_tensors
             eng = ctx.engine
-            rr = r.detach().to("cpu", torch.float64).numpy()
+            if r.is_cuda:
+                if eng.forward_id != ctx.fid:
+                    _density_forward_dev(eng, r, ctx.step)
+                grad = eng.vjp_dev(grad_flux, density=True) / r.detach().to(torch.float64)
+                return grad.to(r.dtype), None, None
+            rr = r.detach().to(torch.float64).numpy()
             if eng.forward_id != ctx.fid:
                 eng.forward_density(rr, step=ctx.step)
-            g = grad_flux.detach().to("cpu", torch.float64).numpy()
-            grad = eng.vjp_density(g) / rr
-            return torch.from_numpy(grad).to(r.device, r.dtype), None, None
+            grad = eng.vjp_density(grad_flux.detach().to("cpu", torch.float64).numpy()) / rr
+            return torch.from_numpy(grad).to(r.dtype), None, None
 
     return SpectrumFromDensity
+
+
+def _density_forward_dev(engine: DiffEngine, r, step: int):
+    """Weighted forward on the built tables scaled by r (a CUDA tensor), all on the device."""
+    engine.scale_density_dev(r)
+    if step is not None:
+        engine._check(engine.L.sed_set_rng_step(engine.ctx, int(step) & 0xFFFFFFFF), "sed_set_rng_step")
+    import torch
+    flux = torch.empty(engine.nspec, dtype=torch.float64, device=r.device)
+    st = abi.StepStats()
+    engine._check(engine.L.sed_diff_forward_dev(engine.ctx, 1.0, None, engine.n_bands, flux.data_ptr(), C.byref(st)),
+                  "sed_diff_forward_dev")
+    engine.forward_id += 1
+    return flux
 
 
 _FN = None

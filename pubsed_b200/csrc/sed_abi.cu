@@ -546,6 +546,8 @@ int sed_set_opacity(sed_ctx* c, double dt)
   CK(cudaEventRecord(c->ev[1], c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_opacity = true;
+  c->opac_base_valid = false;
+  c->opac_scaled = false;
   return SED_OK;
 }
 
@@ -604,6 +606,8 @@ int sed_load_opacity(sed_ctx* c, const double* abs, const double* scat, const do
   CK(cudaMemcpyAsync(c->d_eps_imc.p, eps_imc, (size_t)c->nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_opacity = true;
+  c->opac_base_valid = false;
+  c->opac_scaled = false;
   return SED_OK;
 }
 

@@ -120,6 +120,10 @@ struct sed_ctx {
   // tables
   bool have_opacity = false;
   DevBuf<unsigned char> d_opac, d_cdf, d_cdf_coarse;
+  DevBuf<double> d_rho_scale;         // per-zone extinction factors of the last scaling
+  DevBuf<unsigned char> d_opac_base;  // the built {abs, scat} tables while scaled ones are in d_opac
+  bool opac_base_valid = false;       // d_opac_base holds the tables of the last build or load
+  bool opac_scaled = false;           // d_opac holds density-scaled tables
   int n_coarse = 0;
   DevBuf<uint16_t> d_cdf_guide;  // CDF guide tables, guide_n + 1 entries per zone
   int guide_n = 0;

@@ -83,6 +83,25 @@ int replay(sed_ctx* c, bool jacobian, sed_step_stats* st, bool density = false)
   return SED_OK;
 }
 
+// out[z][j] = base[z][j] * r[z] for both members of the {abs, scat} pair;
+// in FP64, then rounded to the table's type (what scaling the widened tables
+// on the host and loading them again rounds to)
+template <typename P>
+__global__ void scale_rows_kernel(const P* __restrict__ base, P* __restrict__ out, const double* __restrict__ r,
+                                  size_t nz, size_t nn)
+{
+  using T = decltype(P::x);
+  const size_t n = nz * nn;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double f = r[i / nn];
+    const P b = base[i];
+    P o;
+    o.x = (T)((double)b.x * f);
+    o.y = (T)((double)b.y * f);
+    out[i] = o;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -94,7 +113,9 @@ int sed_set_rng_step(sed_ctx* c, uint32_t step)
   return SED_OK;
 }
 
-int sed_diff_forward(sed_ctx* c, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* st)
+// the weighted forward; abs_scale (or null) is read with copy kind `in`
+int diff_forward(sed_ctx* c, double dt, const double* abs_scale, cudaMemcpyKind in, int32_t n_bands,
+                 sed_step_stats* st)
 {
   if (!c) return SED_ERR_ARG;
   int rc = diff_args_ok(c);
@@ -108,7 +129,10 @@ int sed_diff_forward(sed_ctx* c, double dt, const double* abs_scale, int32_t n_b
   const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n(), nj = c->tp.store_Jnu ? nn : 1;
   CK(c->d_esc_bin.resize((size_t)std::max<int64_t>(n_emit, 1)));
   CK(c->d_esc_e.resize((size_t)std::max<int64_t>(n_emit, 1)));
-  if (abs_scale) CK(upload(c, c->d_abs_scale, abs_scale, nz * (size_t)n_bands));
+  if (abs_scale) {
+    CK(c->d_abs_scale.resize(nz * (size_t)n_bands));
+    CK(cudaMemcpyAsync(c->d_abs_scale.p, abs_scale, nz * (size_t)n_bands * sizeof(double), in, c->stream));
+  }
   if (c->record) {
     CK(c->d_rec_fate.resize(std::max<int64_t>(n_emit, 1)));
     CK(c->d_rec_ind.resize(std::max<int64_t>(n_emit, 1)));
@@ -162,32 +186,105 @@ int sed_diff_forward(sed_ctx* c, double dt, const double* abs_scale, int32_t n_b
   return SED_OK;
 }
 
-int sed_diff_vjp(sed_ctx* c, const double* grad_flux, double* grad_scale, sed_step_stats* st)
+int sed_diff_forward(sed_ctx* c, double dt, const double* abs_scale, int32_t n_bands, sed_step_stats* st)
 {
-  if (!c || !grad_flux || !grad_scale) return SED_ERR_ARG;
-  const size_t n_out = (size_t)c->nz * (size_t)std::max(c->diff_bands, 1);
-  CK(upload(c, c->d_adj_g, grad_flux, (size_t)c->nspec));
+  return diff_forward(c, dt, abs_scale, cudaMemcpyHostToDevice, n_bands, st);
+}
+
+int sed_diff_forward_dev(sed_ctx* c, double dt, const double* abs_scale_dev, int32_t n_bands, double* flux_dev,
+                         sed_step_stats* st)
+{
+  int rc = diff_forward(c, dt, abs_scale_dev, cudaMemcpyDeviceToDevice, n_bands, st);
+  if (rc) return rc;
+  if (flux_dev) {
+    CK(cudaMemcpyAsync(flux_dev, c->d_flux.p, c->nspec * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return SED_OK;
+}
+
+// vector-Jacobian product of the last forward (per (zone, band) or, with
+// density, per zone): grad_flux read and the result written with the given
+// copy kinds
+int diff_vjp(sed_ctx* c, const double* grad_flux, cudaMemcpyKind in, double* out, cudaMemcpyKind out_kind,
+             bool density, sed_step_stats* st)
+{
+  if (!c || !grad_flux || !out) return SED_ERR_ARG;
+  const size_t n_out = density ? (size_t)c->nz : (size_t)c->nz * (size_t)std::max(c->diff_bands, 1);
+  CK(c->d_adj_g.resize((size_t)c->nspec));
+  CK(cudaMemcpyAsync(c->d_adj_g.p, grad_flux, (size_t)c->nspec * sizeof(double), in, c->stream));
   CK(c->d_adj_out.resize(n_out));
   CK(cudaMemsetAsync(c->d_adj_out.p, 0, n_out * sizeof(double), c->stream));
-  int rc = replay(c, false, st);
+  int rc = replay(c, false, st, density);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(grad_scale, c->d_adj_out.p, n_out * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(out, c->d_adj_out.p, n_out * sizeof(double), out_kind, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return SED_OK;
 }
 
+int sed_diff_vjp(sed_ctx* c, const double* grad_flux, double* grad_scale, sed_step_stats* st)
+{
+  return diff_vjp(c, grad_flux, cudaMemcpyHostToDevice, grad_scale, cudaMemcpyDeviceToHost, false, st);
+}
+
+int sed_diff_vjp_dev(sed_ctx* c, const double* grad_flux_dev, double* grad_scale_dev, sed_step_stats* st)
+{
+  return diff_vjp(c, grad_flux_dev, cudaMemcpyDeviceToDevice, grad_scale_dev, cudaMemcpyDeviceToDevice, false, st);
+}
+
 int sed_diff_vjp_density(sed_ctx* c, const double* grad_flux, double* grad_rho, sed_step_stats* st)
 {
-  if (!c || !grad_flux || !grad_rho) return SED_ERR_ARG;
-  const size_t n_out = (size_t)c->nz;
-  CK(upload(c, c->d_adj_g, grad_flux, (size_t)c->nspec));
-  CK(c->d_adj_out.resize(n_out));
-  CK(cudaMemsetAsync(c->d_adj_out.p, 0, n_out * sizeof(double), c->stream));
-  int rc = replay(c, false, st, true);
-  if (rc) return rc;
-  CK(cudaMemcpyAsync(grad_rho, c->d_adj_out.p, n_out * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return diff_vjp(c, grad_flux, cudaMemcpyHostToDevice, grad_rho, cudaMemcpyDeviceToHost, true, st);
+}
+
+int sed_diff_vjp_density_dev(sed_ctx* c, const double* grad_flux_dev, double* grad_rho_dev, sed_step_stats* st)
+{
+  return diff_vjp(c, grad_flux_dev, cudaMemcpyDeviceToDevice, grad_rho_dev, cudaMemcpyDeviceToDevice, true, st);
+}
+
+// both extinctions of zone z of the built tables times r[z], in place of the
+// tables the packet kernels read; r null: the built tables back
+int scale_extinction(sed_ctx* c, const double* r, cudaMemcpyKind in)
+{
+  if (!c) return SED_ERR_ARG;
+  if (!c->have_opacity) return set_err(c, SED_ERR_STATE, "sed_diff_scale_extinction: opacity tables not set");
+  c->have_diff = false;  // the last weighted forward no longer matches the context
+  const size_t nz = (size_t)c->nz, nn = (size_t)c->nu.n();
+  const size_t bytes = c->d_opac.n;
+  if (!c->opac_base_valid) {
+    CK(c->d_opac_base.resize(bytes));
+    CK(cudaMemcpyAsync(c->d_opac_base.p, c->d_opac.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    c->opac_base_valid = true;
+  }
+  if (!r) {
+    if (c->opac_scaled) CK(cudaMemcpyAsync(c->d_opac.p, c->d_opac_base.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    c->opac_scaled = false;
+  } else {
+    CK(c->d_rho_scale.resize(nz));
+    CK(cudaMemcpyAsync(c->d_rho_scale.p, r, nz * sizeof(double), in, c->stream));
+    if (c->tp.precision)
+      scale_rows_kernel<float2><<<c->num_sms * 4, 256, 0, c->stream>>>(
+          reinterpret_cast<const float2*>(c->d_opac_base.p), reinterpret_cast<float2*>(c->d_opac.p),
+          c->d_rho_scale.p, nz, nn);
+    else
+      scale_rows_kernel<double2><<<c->num_sms * 4, 256, 0, c->stream>>>(
+          reinterpret_cast<const double2*>(c->d_opac_base.p), reinterpret_cast<double2*>(c->d_opac.p),
+          c->d_rho_scale.p, nz, nn);
+    CK(cudaGetLastError());
+    c->opac_scaled = true;
+  }
   CK(cudaStreamSynchronize(c->stream));
   return SED_OK;
+}
+
+int sed_diff_scale_extinction(sed_ctx* c, const double* rho_scale)
+{
+  return scale_extinction(c, rho_scale, cudaMemcpyHostToDevice);
+}
+
+int sed_diff_scale_extinction_dev(sed_ctx* c, const double* rho_scale_dev)
+{
+  return scale_extinction(c, rho_scale_dev, cudaMemcpyDeviceToDevice);
 }
 
 int sed_diff_jacobian(sed_ctx* c, double* jac, sed_step_stats* st)

@@ -267,3 +267,39 @@ def test_density_forward_leaves_the_built_tables(sed_lib):
     with pytest.raises(RuntimeError, match="replay"):
         e.vjp(np.ones(e.nspec))
     e.close()
+
+
+def test_autograd_functions_keep_cuda_tensors_on_the_device(sed_lib):
+    """theta and r as CUDA tensors: the forward returns a CUDA spectrum and
+    the backward a CUDA gradient through the device-pointer entry points,
+    equal to the host entry points' results (the same device computations,
+    only the copies differ)."""
+    import torch
+    from pubsed_b200.adjoint import spectrum_from_density
+    w = absorbing(5000, seed=53)
+    nb = 8
+    eng = DiffEngine(w, n_bands=nb)
+    th = 1 + 0.1 * torch.rand(eng.nz, nb, dtype=torch.float64, generator=torch.Generator().manual_seed(2))
+    theta = th.cuda().requires_grad_(True)
+    weights = torch.linspace(0.5, 1.5, eng.nspec, dtype=torch.float64, device="cuda")
+    flux = spectrum_from_absorption(theta, eng, 4)
+    assert flux.is_cuda
+    (flux * weights).sum().backward()
+    assert theta.grad.is_cuda
+    f_host, _, _ = eng.forward(th.numpy(), step=4)
+    assert np.array_equal(flux.detach().cpu().numpy(), f_host)
+    assert np.array_equal(theta.grad.cpu().numpy(), eng.vjp(weights.cpu().numpy()))
+    # density factors
+    r0 = torch.linspace(0.9, 1.1, eng.nz, dtype=torch.float64)
+    r = r0.cuda().requires_grad_(True)
+    fr = spectrum_from_density(r, eng, 6)
+    (fr * weights).sum().backward()
+    assert fr.is_cuda and r.grad.is_cuda
+    fr_host, _, _ = eng.forward_density(r0.numpy(), step=6)
+    assert np.array_equal(fr.detach().cpu().numpy(), fr_host)
+    g_host = eng.vjp_density(weights.cpu().numpy()) / r0.numpy()
+    assert np.array_equal(r.grad.cpu().numpy(), g_host)
+    # a plain forward afterwards runs on the built tables again
+    f_again, _, _ = eng.forward(th.numpy(), step=4)
+    assert np.array_equal(f_again, f_host)
+    eng.close()
