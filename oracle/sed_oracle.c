@@ -2199,7 +2199,8 @@ static int transport_general(oracle_ctx* o, double dt, sed_step_stats* st)
   }
   if (o->n_limit > 0) return fail(o, SED_ERR_LIMIT, "packets hit the segment limit");
   if (o->n_imd_cap > 0) return fail(o, SED_ERR_LIMIT, "IMD calls hit the hop bound");
-  if (o->n_reject_cap > 0) return fail(o, SED_ERR_LIMIT, "Compton scatters hit the rejection-sampling bound");
+  if (o->n_reject_cap > 0)
+    return fail(o, SED_ERR_LIMIT, "Compton rejection or diffusion effective-scattering loops hit their bound");
   return SED_OK;
 }
 

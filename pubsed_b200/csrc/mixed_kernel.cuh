@@ -183,10 +183,69 @@ __device__ __forceinline__ void scatter(const StepArgs& A, Pkt& p, double rsq, d
   p.nu = p.nu * vd_out;
 }
 
+// the state emit_mixed_kernel stored for core packet q
+__device__ __forceinline__ void load_emitted(const StepArgs& A, Pkt& p, int64_t q)
+{
+  const int64_t n = A.em_n;
+  const double* s = A.em_state + q;
+  p.x[0] = __ldg(s); p.x[1] = __ldg(s + n); p.x[2] = __ldg(s + 2 * n);
+  p.D[0] = __ldg(s + 3 * n); p.D[1] = __ldg(s + 4 * n); p.D[2] = __ldg(s + 5 * n);
+  p.t = __ldg(s + 6 * n); p.e = __ldg(s + 7 * n); p.nu = __ldg(s + 8 * n);
+  p.ind = __ldg(A.em_ind + q);
+}
+
 }  // namespace mixed
+
+// Emission of the core packets ahead of the packet kernel
+// (emit_inner_source, src/transport/emission.cpp:370-485): one thread per
+// packet, all lanes of a warp on the same code, the packet's state, zone and
+// first optical depth (the emission's spare deviate) stored for the packet
+// kernel.  Emission is the longest stretch of the packet kernel's loop
+// (double-precision sincos, searches of the core CDF and of the zone walls);
+// inside the persistent loop one lane emitting holds its whole warp.
+template <int BATCH>
+__global__ void __launch_bounds__(256) emit_mixed_kernel(const StepArgs A, const GridDev G)
+{
+  using namespace mixed;
+  const int64_t n = A.em_n;
+  uint32_t step = A.step;
+  if constexpr (BATCH) step = *A.step_dev;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    Pkt p;
+    PacketRng rng;
+    float tau;
+    if constexpr (BATCH) {
+      const int m = find_model(A.models, A.n_models, q);
+      const BatchModel& M = A.models[m];
+      rng.init(M.seed, (uint64_t)(M.first_pid + (q - M.pkt_off)), step, 0);
+      BatchZoneOf zf;
+      zf.slice = G.r_out;
+      zf.slice.n = M.n_zones;
+      zf.slice.min = M.r_min;
+      zf.slice.right = G.r_out.right + M.zone_off;
+      zf.zone_off = M.zone_off;
+      DrawWords d{rng};
+      emit_core<0>(A, G, p, d, M.core_radius, M.Ep, M.core_cdf, zf);
+      tau = neg_log_u(d.word());
+      A.em_model[q] = m;
+    } else {
+      rng.init(A.seed, (uint64_t)A.first_pid + q, step, 0);
+      DrawWords d{rng};
+      emit_core<0>(A, G, p, d, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<0>{G});
+      tau = neg_log_u(d.word());
+    }
+    double* s = A.em_state + q;
+    s[0] = p.x[0]; s[n] = p.x[1]; s[2 * n] = p.x[2];
+    s[3 * n] = p.D[0]; s[4 * n] = p.D[1]; s[5 * n] = p.D[2];
+    s[6 * n] = p.t; s[7 * n] = p.e; s[8 * n] = p.nu;
+    A.em_ind[q] = p.ind;
+    A.em_tau[q] = tau;
+  }
+}
 
 // BATCH = 0: one model (core packets, then the queue of census and
 // radioactive photons); BATCH = 1: the batched 1D models of sed_batch_*.
+// Core packets come from emit_mixed_kernel's buffers.
 template <int BATCH, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const StepArgs A, const GridDev G)
 {
@@ -288,19 +347,13 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
         }
         if (q_next >= A.n_packets) break;
         pid = (unsigned long long)q_next++;
-        m = find_model(A.models, A.n_models, (int64_t)pid);
+        m = __ldg(A.em_model + pid);
         const BatchModel& M = A.models[m];
         K = (M.emit_draws + 3u) / 4u;
-        rng.init(M.seed, (uint64_t)(M.first_pid + ((int64_t)pid - M.pkt_off)), step, 0);
-        BatchZoneOf zf;
-        zf.slice = G.r_out;
-        zf.slice.n = M.n_zones;
-        zf.slice.min = M.r_min;
-        zf.slice.right = G.r_out.right + M.zone_off;
-        zf.zone_off = M.zone_off;
-        DrawWords d{rng};
-        emit_core<0>(A, G, p, d, M.core_radius, M.Ep, M.core_cdf, zf);
-        tau_rem = neg_log_u(d.word());  // the first flight's depth: the emission's spare word
+        // the stream continues after the emission's blocks
+        rng.init(M.seed, (uint64_t)(M.first_pid + ((int64_t)pid - M.pkt_off)), step, K);
+        load_emitted(A, p, (int64_t)pid);
+        tau_rem = __ldg(A.em_tau + pid);
       } else {
         pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
         if (pid >= (unsigned long long)A.n_packets) break;
@@ -319,10 +372,9 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
           K = 0;
           tau_rem = neg_log_u(rng.block().x);
         } else {
-          rng.init(A.seed, (uint64_t)A.first_pid + pid, step, 0);
-          DrawWords d{rng};
-          emit_core<0>(A, G, p, d, A.core_radius, A.Ep, A.core_cdf, GridZoneOf<0>{G});
-          tau_rem = neg_log_u(d.word());  // the first flight's depth: the emission's spare word
+          rng.init(A.seed, (uint64_t)A.first_pid + pid, step, K);  // after the emission's blocks
+          load_emitted(A, p, (int64_t)pid);
+          tau_rem = __ldg(A.em_tau + pid);
         }
       }
       fate = MOVING;

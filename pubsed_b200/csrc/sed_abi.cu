@@ -781,6 +781,12 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     launches += launch_imd_probabilities(G, c->d_planck.p, dt, c->d_imd_p.p, c->stream);
     A.imd_p = c->d_imd_p.p;
   }
+  if (mixed_1d_path(A, G) && n_emit > 0) {  // core packets emitted ahead of the packet kernel
+    CK(c->d_em_state.resize((size_t)n_emit * 9));
+    CK(c->d_em_ind.resize((size_t)n_emit));
+    CK(c->d_em_tau.resize((size_t)n_emit));
+    A.em_state = c->d_em_state.p; A.em_ind = c->d_em_ind.p; A.em_tau = c->d_em_tau.p; A.em_n = n_emit;
+  }
   CK(cudaEventRecord(c->ev[3], c->stream));
   if (A.n_packets > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
   CK(cudaGetLastError());

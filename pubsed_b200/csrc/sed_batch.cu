@@ -50,6 +50,10 @@ struct sed_batch {
   int record = 0;
   DevBuf<int32_t> d_rec_fate, d_rec_ind, d_rec_draws;
   DevBuf<double> d_rec_state;
+  // packets emitted ahead of the mixed-form kernel (state [9][n], zone, first depth, model)
+  DevBuf<double> d_em_state;
+  DevBuf<int32_t> d_em_ind, d_em_model;
+  DevBuf<float> d_em_tau;
 };
 
 namespace {
@@ -151,6 +155,10 @@ StepArgs step_args(sed_batch* b, double dt, const BatchModel* models, int64_t to
   A.model_escaped = b->d_model_esc.p; A.step_dev = b->d_step.p;
   A.n_rep = A.smem_zones ? 0 : b->n_rep;
   A.zone_rep = b->d_zone_rep.p;
+  if (b->d_em_state.p) {  // the mixed form emits every queue entry ahead of the packet kernel
+    A.em_state = b->d_em_state.p; A.em_ind = b->d_em_ind.p; A.em_tau = b->d_em_tau.p;
+    A.em_model = b->d_em_model.p; A.em_n = total;
+  }
   return A;
 }
 
@@ -329,6 +337,12 @@ int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n
   if ((e = b->d_click.resize((size_t)n_models * nspec)) != cudaSuccess) return fail(e);
   if ((e = b->d_model_esc.resize(n_models)) != cudaSuccess) return fail(e);
   if ((e = b->d_step.resize(1)) != cudaSuccess) return fail(e);
+  if (c->tp.precision != 0 && pkt > 0) {  // the mixed form emits its packets ahead of the packet kernel
+    if ((e = b->d_em_state.resize((size_t)pkt * 9)) != cudaSuccess) return fail(e);
+    if ((e = b->d_em_ind.resize((size_t)pkt)) != cudaSuccess) return fail(e);
+    if ((e = b->d_em_tau.resize((size_t)pkt)) != cudaSuccess) return fail(e);
+    if ((e = b->d_em_model.resize((size_t)pkt)) != cudaSuccess) return fail(e);
+  }
   // zones beyond the per-block shared-memory tallies: 32 copies of the
   // zone-scalar tallies (fewer if that would pass 256 MiB)
   if ((size_t)5 * nz_tot * sizeof(double) > 64 * 1024) {
@@ -638,6 +652,7 @@ void sed_batch_destroy(sed_batch* b)
   for (auto& ev : b->ev) if (ev) cudaEventDestroy(ev);
   b->d_models.release(); b->d_sample_models.release(); b->d_nbr.release(); b->d_rin.release();
   b->d_core_cdf.release(); b->d_flux.release(); b->d_click.release(); b->d_model_esc.release(); b->d_step.release();
+  b->d_em_state.release(); b->d_em_ind.release(); b->d_em_tau.release(); b->d_em_model.release();
   b->d_zone_rep.release();
   b->d_rec_fate.release(); b->d_rec_ind.release(); b->d_rec_draws.release(); b->d_rec_state.release();
   if (b->inner) sed_ctx_destroy(b->inner);

@@ -130,6 +130,10 @@ struct sed_ctx {
   int chunk_zones = 0;  // zones per opacity-build pass (bounds the FP64/LTE scratch)
   int opacity_launches = 0;
   DevBuf<double> d_imd_p;  // IMD probabilities of the step [4][nz]
+  // core packets emitted ahead of the mixed-form 1D kernel: state [9][n], zone, first optical depth
+  DevBuf<double> d_em_state;
+  DevBuf<int32_t> d_em_ind;
+  DevBuf<float> d_em_tau;
   DevBuf<double> d_eps_imc, d_abs64, d_scat64, d_emis64, d_epsl64, d_epsf64, d_planck, d_ross, d_L, d_n_elec, d_n_dens, d_mass_frac,
       d_temp_c, d_ion_part, d_ion_frac, d_lev_n, d_boltz;
   DevBuf<int32_t> d_solve_err;

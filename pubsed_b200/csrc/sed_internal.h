@@ -75,6 +75,12 @@ struct StepArgs {
   const int32_t* q_ind;              // [n_q] their zone (or -1 / -2)
   const uint32_t* q_n;               // [n_q] next deviate index; RADIO_NO_PHOTON: none
   double *L_dep, *L_emit;            // [nz] radioactive tallies normalised by the finish kernel, or null
+  // ---- packets emitted ahead of the mixed-form 1D kernel (emit_mixed_kernel) ----
+  double* em_state;                  // [9][n] {x, D, t, e, nu} of core packet q at em_state[k * n + q]
+  int32_t* em_ind;                   // [n] its zone (or -1 / -2)
+  float* em_tau;                     // [n] optical depth of its first flight
+  int32_t* em_model;                 // [n] its model (batches)
+  int64_t em_n;                      // core packets emitted there (the stride of em_state)
   // ---- differentiable transport (weighted forward and adjoint replay kernels only) ----
   const double* abs_scale;           // [nz * n_bands] factor on the absorption opacity, or null
   int32_t n_bands;                   // band of bin i = i * n_bands / n_nu
@@ -178,6 +184,10 @@ struct BatchModel {
 
 // launches the persistent packet kernel; returns the number of launches
 int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s);
+// whether launch_propagate runs the mixed-form 1D kernel for these
+// arguments: its core packets are then emitted ahead into the em_* buffers
+// (A.em_n of them), which the caller provides
+bool mixed_1d_path(const StepArgs& a, const GridDev& g);
 // IMD probabilities of the step (transport::compute_diffusion_probabilities)
 // from the zone Planck means into out[4][nz]
 int launch_imd_probabilities(const GridDev& g, const double* planck, double dt, double* out, cudaStream_t s);

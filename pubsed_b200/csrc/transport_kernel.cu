@@ -1879,6 +1879,11 @@ int launch_mixed_t(const StepArgs& a0, const GridDev& g, int blocks_per_sm, int 
   if (a.smem_zones && (size_t)MINB * 5 * g.nzones * sizeof(double) > (size_t)200 * 1024) a.smem_zones = 0;
   const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
   auto kern = propagate_mixed_kernel<BATCH, THREADS, MINB>;
+  if (a.em_n > 0) {  // the core packets, emitted ahead
+    int64_t eb = (a.em_n + 255) / 256;
+    if (eb > (int64_t)num_sms * 16) eb = (int64_t)num_sms * 16;
+    emit_mixed_kernel<BATCH><<<(unsigned)eb, 256, 0, s>>>(a, g);
+  }
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
@@ -1889,7 +1894,7 @@ int launch_mixed_t(const StepArgs& a0, const GridDev& g, int blocks_per_sm, int 
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
   kern<<<(unsigned)blocks, THREADS, smem, s>>>(a, g);
-  return 1;
+  return a.em_n > 0 ? 2 : 1;
 }
 
 template <int GRID, typename OT, typename CT, int BATCH, int THREADS, int MINB, int MODE = 0,
@@ -1963,6 +1968,11 @@ int launch_batch_t(const StepArgs& a, const GridDev& g, int variant, int bps, in
 }
 
 }  // namespace
+
+bool mixed_1d_path(const StepArgs& a, const GridDev& g)
+{
+  return a.precision != 0 && g.type == 0 && g.homologous && a.use_ddmc == 0;
+}
 
 int launch_propagate(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {

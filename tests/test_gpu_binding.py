@@ -48,17 +48,19 @@ def test_binding_step_matches_the_abi_path(sed_lib, case, precision):
     f, c = g.spectrum()
     T = g.tallies()
     O = g.opacity()
-    assert int(out["n_escaped_steps"][0]) == st["n_escaped"]
-    assert np.array_equal(out["spec_click"], c)
-    assert np.array_equal(out["spec_flux"], f)
-    for k, rk in (("J_nu", "J_nu"), ("e_abs", "e_abs"), ("e_rad", "e_rad"), ("fr", "fr_rad")):
-        a, b = out[rk], T[k]
-        assert np.array_equal(np.isfinite(a), np.isfinite(b)), k
-        fin = np.isfinite(b)
-        assert np.array_equal(a[fin], b[fin]), k
+    # the tables are built deterministically: equal; packets take the same
+    # paths: equal counts; tallies are sums of FP64 atomics, whose order
+    # varies from run to run: oracle_lib's tally tolerances
     for k in ("abs", "scat", "emis_cdf", "eps_imc", "planck_mean", "rosseland_mean"):
         assert np.array_equal(out[k], O[k]), k
+    assert int(out["n_escaped_steps"][0]) == st["n_escaped"]
+    assert np.array_equal(out["spec_click"], c)
+    fin = c > 0
+    assert np.all(np.abs(out["spec_flux"][fin] - f[fin]) <= oracle_lib.TALLY_RTOL * np.abs(f[fin]))
+    for k, rk in (("J_nu", "J_nu"), ("e_abs", "e_abs"), ("e_rad", "e_rad"), ("fr", "fr_rad")):
+        oracle_lib.zone_tally_close(out[rk], T[k])
     if int(w.params.get("transport_radiative_equilibrium", 0)):
+        # Brent on tallies equal to ~1e-12 stops within its tolerance
         T_gpu, _ = oracle_lib.solve_temperature(g)
-        assert np.array_equal(out["T_gas"], T_gpu)
+        assert np.allclose(out["T_gas"], T_gpu, rtol=1e-6, atol=0)
     g.close()

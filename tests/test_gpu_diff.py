@@ -251,18 +251,23 @@ def test_density_forward_leaves_the_built_tables(sed_lib):
     w = workloads.type_ia(n_packets=20_000, n_zones=16, n_lines=2000, n_bins=128, spectrum_bins=32, epsilon=1e-4,
                           radiative_eq=0, seed=33)
     e = DiffEngine(w, n_bands=1)
-    f0, _, _ = e.forward(step=3)
-    f1, _, _ = e.forward_density(np.full(e.nz, 1.3), step=3)
-    assert not np.array_equal(f0, f1)
-    f2, _, _ = e.forward(step=3)
-    assert np.array_equal(f0, f2)  # the built tables are back
+    # the same deviates give the same packet histories: the same spectrum
+    # clicks, and fluxes equal up to the order of the FP64 atomic sums
+    def same(a, b):
+        return np.array_equal(a[1], b[1]) and np.allclose(a[0], b[0], rtol=oracle_lib.TALLY_RTOL, atol=0)
+
+    f0 = e.forward(step=3)
+    f1 = e.forward_density(np.full(e.nz, 1.3), step=3)
+    assert not same(f0, f1)
+    f2 = e.forward(step=3)
+    assert same(f0, f2)  # the built tables are back
     w.zones.T = w.zones.T * 1.1
     e.upload_grid()
     e.tables()
-    g0, _, _ = e.forward(step=3)
-    g1, _, _ = e.forward_density(np.ones(e.nz), step=3)
-    assert np.array_equal(g0, g1)  # density factor 1 on the new build, not the old one
-    assert not np.array_equal(g0, f0)
+    g0 = e.forward(step=3)
+    g1 = e.forward_density(np.ones(e.nz), step=3)
+    assert same(g0, g1)  # density factor 1 on the new build, not the old one
+    assert not same(g0, f0)
     e.tables()  # a rebuild after the forward: nothing left to replay
     with pytest.raises(RuntimeError, match="replay"):
         e.vjp(np.ones(e.nspec))
@@ -286,9 +291,12 @@ def test_autograd_functions_keep_cuda_tensors_on_the_device(sed_lib):
     assert flux.is_cuda
     (flux * weights).sum().backward()
     assert theta.grad.is_cuda
+    # equal up to the order of FP64 atomic sums, which varies from run to run
+    tol = dict(rtol=1e-10, atol=0)
     f_host, _, _ = eng.forward(th.numpy(), step=4)
-    assert np.array_equal(flux.detach().cpu().numpy(), f_host)
-    assert np.array_equal(theta.grad.cpu().numpy(), eng.vjp(weights.cpu().numpy()))
+    assert np.allclose(flux.detach().cpu().numpy(), f_host, **tol)
+    v = eng.vjp(weights.cpu().numpy())
+    assert np.allclose(theta.grad.cpu().numpy(), v, rtol=1e-10, atol=1e-10 * np.abs(v).max())
     # density factors
     r0 = torch.linspace(0.9, 1.1, eng.nz, dtype=torch.float64)
     r = r0.cuda().requires_grad_(True)
@@ -296,10 +304,10 @@ def test_autograd_functions_keep_cuda_tensors_on_the_device(sed_lib):
     (fr * weights).sum().backward()
     assert fr.is_cuda and r.grad.is_cuda
     fr_host, _, _ = eng.forward_density(r0.numpy(), step=6)
-    assert np.array_equal(fr.detach().cpu().numpy(), fr_host)
+    assert np.allclose(fr.detach().cpu().numpy(), fr_host, **tol)
     g_host = eng.vjp_density(weights.cpu().numpy()) / r0.numpy()
-    assert np.array_equal(r.grad.cpu().numpy(), g_host)
+    assert np.allclose(r.grad.cpu().numpy(), g_host, rtol=1e-10, atol=1e-10 * np.abs(g_host).max())
     # a plain forward afterwards runs on the built tables again
     f_again, _, _ = eng.forward(th.numpy(), step=4)
-    assert np.array_equal(f_again, f_host)
+    assert np.allclose(f_again, f_host, **tol)
     eng.close()

@@ -72,9 +72,11 @@ def test_segment_limit_stops_packets(sed_lib, precision):
 
 
 def test_diffusion_effective_scattering_bound(sed_lib):
-    """DDMC (method 2) on a grey sphere of one frequency bin with absorption
-    (epsilon 0.5), Fleck factor 1 and no radiative equilibrium: every
-    effective-scattering event absorbs on every pass and never changes bin,
+    """DDMC (method 2) on the diffusing pulse's grey sphere with four
+    frequency bins, absorption (epsilon 0.5), Fleck factor 1 (no Fleck
+    factor) and no radiative equilibrium: an effective-scattering event
+    (there are some: the zone's emission is spread over the bins, so the
+    inelastic fraction is not 0) absorbs on every pass and never changes bin,
     so each one ends at the 65 536-pass bound; the step returns
     SED_ERR_LIMIT and the oracle, bounded the same way, agrees packet for
     packet."""
@@ -83,6 +85,7 @@ def test_diffusion_effective_scattering_bound(sed_lib):
     w.params["opacity_epsilon"] = 0.5
     w.params["transport_radiative_equilibrium"] = 0
     w.params["transport_fleck_alpha"] = 0
+    w.params["transport_nu_grid"] = [1e14, 1e16, 10 ** 0.5 - 1, 1]  # four log bins
     dt = 5e-10
     out = []
     for lib, prefix in ((sed_lib, "sed_"), (oracle_lib.oracle_lib(), "oracle_")):

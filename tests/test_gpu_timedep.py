@@ -154,8 +154,8 @@ def test_ddmc_steps_match_oracle(sed_lib, tau):
 
 
 def test_ddmc_rejects_what_is_not_built(sed_lib):
-    """Methods 1 and 3 (IMD, random walk) and 3D grids return SED_ERR_ARG."""
-    w = workloads.time_dependent("lightbulb_grey", n_initialize=0, dt_days=0.1, params={"transport_use_ddmc": 1},
+    """Method 3 (random walk) returns SED_ERR_ARG."""
+    w = workloads.time_dependent("lightbulb_grey", n_initialize=0, dt_days=0.1, params={"transport_use_ddmc": 3},
                                  n_packets=100, n_zones=16, n_bins=64, seed=79)
     for lib, prefix in ((sed_lib, "sed_"), (oracle_lib.oracle_lib(), "oracle_")):
         e = oracle_lib.Engine(lib, prefix, w)
