@@ -245,12 +245,12 @@ struct LevView {
 // atom's number density, n_l n_atom, and their reciprocals (or the ion
 // populations for fuzz lines) are staged in shared memory level-major, ZT
 // zones contiguous; the ratio n_u g_l / (n_l g_u) is formed from them (the
-// atom density cancels).  Thread t takes the bins order[t], order[t + 256],
-// ... where `order` lists the bins by decreasing line count, so the lanes of
-// a warp walk lists of similar length; it walks each bin's lines (sorted by
-// bin, atom), loading each line record once and applying it to the ZT zones.
-// Sums accumulate in FP64 in the bin's list order.  In the mixed form the
-// per-line arithmetic is FP32.
+// atom density cancels).  A warp takes one bin at a time (warp w the bins
+// order[w], order[w + 8], ..., `order` listing the bins by decreasing line
+// count): its lanes are ZT zones x 32/ZT line slots, slot s summing the
+// bin's lines s, s + 32/ZT, ... (sorted by bin, atom) in FP64, and the slots
+// of a zone are then added in a fixed butterfly order, so the sums are the
+// same from run to run.  In the mixed form the per-line arithmetic is FP32.
 // Level populations come from the LTE solve, floored at 1e-30, so they are
 // normal FP32 numbers and the reference's n_l < DBL_MIN skip never applies
 // to them; a NaN term is skipped as in the reference.
@@ -296,91 +296,79 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
   const int32_t* seg = FUZZ ? A.fz_seg : A.ln_seg;
   const int32_t* order = FUZZ ? A.fz_order : A.ln_order;
   const double time = A.time;
-  for (int jj = tid; jj < nn; jj += bd) {
+  // a warp per bin: its 32 lanes are ZT zones x LS line slots; slot s takes
+  // the bin's lines s, s + LS, ..., so the lanes of a warp run the same
+  // number of lines (up to one) and read the same few line records
+  constexpr int LS = 32 / ZT;
+  const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
+  const int zi = lane % ZT, slot = lane / ZT;
+  for (int jj = warp; jj < nn; jj += nwarps) {
     const int j = __ldg(order + jj);
-    double acc[ZT], acce[ZT];
-#pragma unroll
-    for (int q = 0; q < ZT; ++q) { acc[q] = 0; acce[q] = 0; }
+    double acc = 0, acce = 0;
     const int k1 = seg[j + 1];
-    for (int k = seg[j]; k < k1; ++k) {
+    for (int k = seg[j] + slot; k < k1; k += LS) {
       int atom;
-      V term[ZT];
+      V term;
       if constexpr (!FUZZ) {
         // tau = n_l n_atom sigma_tot f lambda t (1 - n_u g_l / (n_l g_u)), 0 past the laser limit
         const int4 lv = __ldg(A.ln_lv + k);
         atom = lv.w;
-        const V* pl = pop + (size_t)lv.x * ZT;   // n_l n_atom
-        const V* il = ipop + (size_t)lv.x * ZT;  // 1 / (n_l n_atom)
-        const V* pu = pop + (size_t)lv.y * ZT;   // n_u n_atom
+        const V pl = pop[(size_t)lv.x * ZT + zi];   // n_l n_atom
+        const V il = ipop[(size_t)lv.x * ZT + zi];  // 1 / (n_l n_atom)
+        const V pu = pop[(size_t)lv.y * ZT + zi];   // n_u n_atom
         if constexpr (MIXED) {
           const float2 c = __ldg(A.ln_c32 + k);
-          const float ct = c.x * (float)time;
-#pragma unroll
-          for (int q = 0; q < ZT; ++q) {
-            const float r = pu[q] * il[q] * c.y;
-            const float tau = (r > 1.f) ? 0.f : pl[q] * ct * (1.f - r);
-            const float t = sobolev_term32(tau);
-            term[q] = (t == t) ? t : 0.f;
-          }
+          const float r = pu * il * c.y;
+          const float tau = (r > 1.f) ? 0.f : pl * (c.x * (float)time) * (1.f - r);
+          const float t = sobolev_term32(tau);
+          term = (t == t) ? t : 0.f;
         } else {
           const double2 c = __ldg(A.ln_c + k);
-#pragma unroll
-          for (int q = 0; q < ZT; ++q) {
-            const double nln = pl[q];
-            double t = 0;
-            if (!(nln < DBL_MIN)) {
-              const double r = pu[q] * il[q] * c.y;
-              const double tau = (r > 1) ? 0.0 : nln * c.x * time * (1 - r);
-              t = sobolev_term(tau);
-              if (isnan(t)) t = 0;
-            }
-            term[q] = t;
+          double t = 0;
+          if (!(pl < DBL_MIN)) {
+            const double r = pu * il * c.y;
+            const double tau = (r > 1) ? 0.0 : pl * c.x * time * (1 - r);
+            t = sobolev_term(tau);
+            if (isnan(t)) t = 0;
           }
+          term = t;
         }
       } else {
         // n_l = n_ion exp(-E_l/kT) / Z_ion, tau = sigma_tot lambda n_l gf (1 - exp(-h nu/kT)) t
         const int4 ia = __ldg(A.fz_ia + k);
         atom = ia.z;
-        const V* pi = pop + (size_t)ia.x * ZT;
+        const V pi = pop[(size_t)ia.x * ZT + zi];
         if constexpr (MIXED) {
           const float4 c = __ldg(A.fz_c32 + k);
-          const float ct = c.x * (float)time;
-#pragma unroll
-          for (int q = 0; q < ZT; ++q) {
-            const float stim = one_minus_exp32(c.z * invT[q]);
-            const float tau = ct * pi[q] * __expf(-c.y * invT[q]) * stim;
-            term[q] = sobolev_term32(tau);
-          }
+          const float stim = one_minus_exp32(c.z * invT[zi]);
+          const float tau = (c.x * (float)time) * pi * __expf(-c.y * invT[zi]) * stim;
+          term = sobolev_term32(tau);
         } else {
           const double2 c = __ldg(A.fz_c + k);
           const double h = __ldg(A.fz_h + k);
-#pragma unroll
-          for (int q = 0; q < ZT; ++q) {
-            if (q < nzt) {
-              const double temp = A.temp_c[z0 + q];
-              const double nl = pi[q] * exp(-c.y / temp);
-              const double stim_cor = (1 - exp(-h / temp));
-              const double tau = c.x * nl * stim_cor * time;
-              term[q] = sobolev_term(tau);
-            } else {
-              term[q] = 0;
-            }
+          if (zi < nzt) {
+            const double temp = A.temp_c[z0 + zi];
+            const double nl = pi * exp(-c.y / temp);
+            const double stim_cor = (1 - exp(-h / temp));
+            const double tau = c.x * nl * stim_cor * time;
+            term = sobolev_term(tau);
+          } else {
+            term = 0;
           }
         }
       }
-      const V e = epsv[atom];
-#pragma unroll
-      for (int q = 0; q < ZT; ++q) {
-        acc[q] += (double)term[q];
-        if (want_e) acce[q] += (double)(term[q] * e);
-      }
+      acc += (double)term;
+      if (want_e) acce += (double)(term * epsv[atom]);
     }
+    // the LS slots of each zone, summed in a fixed butterfly order
 #pragma unroll
-    for (int q = 0; q < ZT; ++q) {
-      if (q < nzt) {
-        S[(size_t)(z0 + q) * nn + j] = acc[q];
-        if (want_e) Se[(size_t)(z0 + q) * nn + j] = acce[q];
-      }
+    for (int off = ZT; off < 32; off <<= 1) {
+      acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      acce += __shfl_xor_sync(0xffffffffu, acce, off);
+    }
+    if (slot == 0 && zi < nzt) {
+      S[(size_t)(z0 + zi) * nn + j] = acc;
+      if (want_e) Se[(size_t)(z0 + zi) * nn + j] = acce;
     }
   }
 }
