@@ -180,15 +180,24 @@ def state_rel_per_packet(Sg: np.ndarray, So: np.ndarray) -> np.ndarray:
     return np.maximum(np.maximum(pos, dire), sc)
 
 
-# Final packet states after a whole history are compared per packet.  The
-# CPU libm and CUDA's log/sincos may differ in the last bit; near-tangent
-# shell crossings (sqrt of a discriminant close to zero) amplify such a
-# difference, so a few packets in a thousand exceed 1e-12.  The criterion:
-# 99% of packets within STATE_RTOL, every packet within STATE_RTOL_MAX,
-# and the integer history (fate, zone, deviates drawn) identical for all.
+# Final packet states after a whole history are compared per packet.  Every
+# packet whose state ends above 1e-12 that was traced to its first differing
+# segment (bisecting the segment limit on single-packet runs of the GPU and
+# the oracle) parts at an interaction or emission that sets a new direction,
+# with position, time, energy and frequency still equal and the direction
+# differing in its last bit: the azimuth's cos and sin, where the CPU libm
+# and CUDA's round differently (divisions and square roots are IEEE-rounded
+# in both).  The following hundreds of segments amplify it (near-tangent
+# shell crossings divide it by sqrt of a small discriminant).  The
+# criterion: 99% of packets within STATE_RTOL, at most STATE_OVER_FRAC of
+# them (at least 2) above it, every packet within STATE_RTOL_MAX, and the
+# integer history (fate, zone, deviates drawn) identical for all.  Measured
+# over the GPU suite: 61 of 1.3e6 compared packets above 1e-12, at most 8 of
+# 4000 (0.2%) in one comparison, the largest 1.8e-9 (gamma-rays at 120 d).
 STATE_RTOL = 1e-12
 STATE_QUANTILE = 0.99
-STATE_RTOL_MAX = 1e-8
+STATE_OVER_FRAC = 0.0025
+STATE_RTOL_MAX = 5e-9
 # Tallies are sums of the same terms in a different order (FP64 atomics);
 # the relative error of a reordered sum of n positive terms is below
 # n * 2^-53: 1e-10 covers up to ~1e6 contributions per bin.
@@ -222,6 +231,7 @@ def check_states(Sg: np.ndarray, So: np.ndarray) -> dict:
     out = {"max": float(r.max()) if r.size else 0.0, "q": q, "n_over": int((r > STATE_RTOL).sum()), "n": int(r.size)}
     STATE_LOG.append((os.environ.get("PYTEST_CURRENT_TEST", ""), out["n"], out["n_over"], out["max"]))
     assert q <= STATE_RTOL, out
+    assert out["n_over"] <= max(2, int(np.ceil(STATE_OVER_FRAC * out["n"]))), out
     assert out["max"] <= STATE_RTOL_MAX, out
     return out
 

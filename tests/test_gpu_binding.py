@@ -48,11 +48,15 @@ def test_binding_step_matches_the_abi_path(sed_lib, case, precision):
     f, c = g.spectrum()
     T = g.tallies()
     O = g.opacity()
-    # the tables are built deterministically: equal; packets take the same
-    # paths: equal counts; tallies are sums of FP64 atomics, whose order
-    # varies from run to run: oracle_lib's tally tolerances
+    # the tables: within the FP64 parity tolerance (the binding passes the
+    # atomic data the reference loaded, whose photoionisation tables its C++
+    # loader computed, where the ctypes path passes the Python restatement of
+    # that loader: the two round differently in the last bit); packets take
+    # the same paths: equal counts; tallies are sums of FP64 atomics, whose
+    # order varies from run to run: oracle_lib's tally tolerances
     for k in ("abs", "scat", "emis_cdf", "eps_imc", "planck_mean", "rosseland_mean"):
-        assert np.array_equal(out[k], O[k]), k
+        a, b = out[k], O[k]
+        assert np.all(np.abs(a - b) <= 1e-12 * np.maximum(np.abs(b), 1e-300)), k
     assert int(out["n_escaped_steps"][0]) == st["n_escaped"]
     assert np.array_equal(out["spec_click"], c)
     fin = c > 0
