@@ -36,9 +36,9 @@
 //    the estimate's ~2^-22 relative error cubed is below FP64 rounding.
 //    They are not correctly rounded, which the mixed form does not need;
 //    position, time, frequency and the Lorentz transforms stay FP64.
-//  * -ln(u) in FP32 (hardware log2, or an atanh series where u > 1/2), the
-//    interaction and bin-step distances as FP32 quotients (they set where a
-//    segment ends, not the state it carries).
+//  * -ln(u) in FP32 from the hardware logarithm, the interaction and
+//    bin-step distances as FP32 quotients (they set where a segment ends,
+//    not the state it carries).
 //  * The zone's walls are loaded once per zone visit, |x|^2 and x.D once
 //    per move.
 namespace mixed {
@@ -68,22 +68,14 @@ __device__ __forceinline__ double rcp_nr(double a)
 
 constexpr float W32 = 2.3283064365386963e-10f;  // 2^-32
 
-// -ln(u), u = (w + 1/2) 2^-32 in (0, 1), relative error ~1e-7: the hardware
-// logarithm where |ln u| > ln 2; above u = 1/2, with x = 1 - u (formed from
-// the integer, so exact) and y = x / (2 - x) <= 1/3, the odd series of
-// 2 atanh(y) = -ln(1 - x) to y^11
+// -ln(u), u = (w + 1/2) 2^-32 in (0, 1), from the hardware logarithm: a few
+// ulp relative where u < 1/2, an absolute error below 2^-21 in the optical
+// depth above (a short flight's depth off by what rounding the FP32 opacity
+// of a unit optical depth already moves it).  One code path for all lanes:
+// a branch to a series near u = 1 cost 2.6% of the Type Ia step.
 __device__ __forceinline__ float neg_log_u(uint32_t w)
 {
-  if (w < 0x80000000u) return -__logf(((float)w + 0.5f) * W32);
-  const float x = ((float)(0xFFFFFFFFu - w) + 0.5f) * W32;
-  const float y = __fdividef(x, 2.0f - x);
-  const float y2 = y * y;
-  float s = fmaf(y2, 1.0f / 11.0f, 1.0f / 9.0f);
-  s = fmaf(y2, s, 1.0f / 7.0f);
-  s = fmaf(y2, s, 1.0f / 5.0f);
-  s = fmaf(y2, s, 1.0f / 3.0f);
-  s = fmaf(y2, s, 1.0f);
-  return 2.0f * y * s;
+  return -__logf(((float)w + 0.5f) * W32);
 }
 
 // the zone's walls, as get_next_zone (grid_1D_sphere.cpp:510-590) derives
@@ -291,7 +283,16 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
   Walls wl{};
   double rsq = 0, xd = 0;
   float tau_rem = 0;  // optical depth left to the next interaction
+  bool live = true;   // the lane still takes packets from the queue
   for (;;) {
+    // The lanes of the warp meet here every iteration.  Without it, lanes
+    // whose packet ended, or that took a shorter branch, drift apart and the
+    // warp runs their iterations group after group with few lanes each;
+    // lanes that have run out of packets stay in the loop, idle, until the
+    // whole warp has.
+    __syncwarp();
+    if (!__any_sync(0xffffffffu, live)) break;
+    if (!live) continue;
     if (fate != MOVING) {
       if (have) {
         if (acc_zone >= 0) {
@@ -345,7 +346,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
           q_end = q_next + A.queue_chunk;
           if (q_end > A.n_packets) q_end = A.n_packets;
         }
-        if (q_next >= A.n_packets) break;
+        if (q_next >= A.n_packets) { live = false; continue; }
         pid = (unsigned long long)q_next++;
         m = __ldg(A.em_model + pid);
         const BatchModel& M = A.models[m];
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
         tau_rem = __ldg(A.em_tau + pid);
       } else {
         pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
-        if (pid >= (unsigned long long)A.n_packets) break;
+        if (pid >= (unsigned long long)A.n_packets) { live = false; continue; }
         if (A.q_n != nullptr && (int64_t)pid >= A.n_core) {
           // a queued photon: census (stream position 0) or an optical
           // photon the gamma-ray kernel handed over at its stream position
