@@ -473,7 +473,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 #ifndef SED_PROP_THREADS
 #define SED_PROP_THREADS 128
 #endif
-// launch shape of the mixed-form 1D kernel (propagate_mixed_kernel)
+// launch shape of the mixed-form 1D kernel (propagate_mixed_kernel):
+// 128 x 6 at 80 registers without spills (Type Ia step 835 ms; 128 x 8 at
+// 64 registers spills and ran 891 ms)
 #ifndef SED_MIXED_THREADS
 #define SED_MIXED_THREADS 128
 #endif
@@ -1917,11 +1919,11 @@ int launch_kernel_t(const StepArgs& a, const GridDev& g, int blocks_per_sm, int 
   return 1;
 }
 
-// Single-context shapes, measured on the Type Ia step (1e7 packets): the
-// FP64 form runs best with 256 x 4 (64 registers, 1753 ms vs 1788 ms at
-// 128 x 8); the mixed form with 128 x 7 on 1D grids (72 registers, 28 warps
-// per SM: 928 ms vs 959 ms at 256 x 3 and 1019 ms at 128 x 8) while seven
-// blocks' zone tallies fit in shared memory, else 256 x 3 (80 registers).
+// Single-context shapes: the FP64 form runs best with 256 x 4 (64
+// registers; Type Ia step 1753 ms vs 1788 ms at 128 x 8); the mixed form on
+// 1D grids is propagate_mixed_kernel (SED_MIXED_THREADS x SED_MIXED_MINB);
+// on 3D grids the mixed form runs 128 x 7 (64^3 cells, 2e7 packets: packet
+// kernel 572 ms vs 583 ms at 256 x 3).
 template <int GRID, typename OT, typename CT>
 int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStream_t s)
 {
@@ -1936,7 +1938,7 @@ int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStr
     return launch_kernel_t<GRID, OT, CT, 0, 256, 4, 0, false>(a, g, 0, num_sms, a.n_packets, s);
   if constexpr (sizeof(OT) == sizeof(float2)) {
     if constexpr (GRID == 0) return launch_mixed_t<0, SED_MIXED_THREADS, SED_MIXED_MINB>(a, g, 0, num_sms, a.n_packets, s);
-    else return launch_kernel_t<GRID, OT, CT, 0, 256, 3>(a, g, 0, num_sms, a.n_packets, s);
+    else return launch_kernel_t<GRID, OT, CT, 0, 128, 7>(a, g, 0, num_sms, a.n_packets, s);
   } else {
     return launch_kernel_t<GRID, OT, CT, 0, 256, 4>(a, g, 0, num_sms, a.n_packets, s);
   }
