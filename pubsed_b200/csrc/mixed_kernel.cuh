@@ -131,10 +131,13 @@ __device__ __forceinline__ int next_zone(const Walls& w, double rsq, double xd, 
 // isotropic_scatter (scatter.cpp:303-351) on a homologous flow, with the
 // comoving direction from mu and the azimuth deviate vphi, and (redist) the
 // comoving frequency from the zone's emissivity CDF with deviate word w_cdf
+// Returns the comoving frequency bin of a redistributed photon (-1 for a
+// coherent scatter) and its width times c t in *dnu_num.
 template <typename CT>
-__device__ __forceinline__ void scatter(const StepArgs& A, Pkt& p, double rsq, double xd, double mu, float vphi,
-                                        uint32_t w_cdf, bool redist)
+__device__ __forceinline__ int scatter(const StepArgs& A, Pkt& p, double rsq, double xd, double mu, float vphi,
+                                       uint32_t w_cdf, bool redist, float* dnu_num)
 {
+  int kbin = -1;
   const double gamma = rsqrt_nr(fma(-rsq, A.inv_ct2, 1.0));
   const double dshift_in = gamma * fma(-xd, A.inv_ct, 1.0);
   p.e = p.e * dshift_in;
@@ -155,7 +158,13 @@ __device__ __forceinline__ void scatter(const StepArgs& A, Pkt& p, double rsq, d
       const double hi = (double)__ldg(row + k);
       float f = __fdividef((float)(u - lo), (float)(hi - lo));
       f = fminf(fmaxf(f, 0.0f), 0.99999994f);
-      p.nu = loc_sample(A.nu, k, (double)f);
+      // locate_array::sample (locate_array.cpp:237-242) with the bin's walls
+      // kept for the next segment
+      const double wl = (k == 0) ? A.nu.min : __ldg(A.nu.right + k - 1);
+      const double wr = __ldg(A.nu.right + k);
+      p.nu = wl + (wr - wl) * (double)f;
+      kbin = k;
+      *dnu_num = (float)((wr - wl) * A.ct);
     }
   }
   // comoving -> lab with the velocity reversed, beta = x / (c t)
@@ -173,6 +182,7 @@ __device__ __forceinline__ void scatter(const StepArgs& A, Pkt& p, double rsq, d
   p.D[2] = D2 * inv_norm;
   p.e = p.e * vd_out;
   p.nu = p.nu * vd_out;
+  return kbin;
 }
 
 // the state emit_mixed_kernel stored for core packet q
@@ -284,6 +294,13 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
   double rsq = 0, xd = 0;
   float tau_rem = 0;  // optical depth left to the next interaction
   bool live = true;   // the lane still takes packets from the queue
+  // after a redistribution: the photon's comoving bin (its lab frequency
+  // transforms back into that bin at the next segment's start, which is the
+  // interaction point), the bin's {abs, scat} loaded ahead, and its width
+  // times c t; -1 when the next segment has to locate its bin
+  int nxt_bin = -1;
+  float2 nxt_ab = make_float2(0.f, 0.f);
+  float nxt_dnu = 0.f;
   for (;;) {
     // The lanes of the warp meet here every iteration.  Without it, lanes
     // whose packet ended, or that took a shorter branch, drift apart and the
@@ -382,6 +399,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       if (p.ind == -1) fate = ABSORBED;
       else if (p.ind == -2) fate = ESCAPED;
       seg = 0;
+      nxt_bin = -1;
       acc_zone = -1;
       acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
       have = true;
@@ -412,14 +430,24 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     // comoving frequency and the opacity of its bin (transport_opacity.cpp:268-299)
     const double gamma = rsqrt_nr(fma(-rsq, A.inv_ct2, 1.0));
     const double dshift = gamma * fma(-xd, A.inv_ct, 1.0);
-    const double nu_cmf = p.nu * dshift;
-    const int i_nu = loc_within_fast<true>(A.nu, nu_cmf);
-    const float2 ab = __ldg(opac + (size_t)iz * nn + i_nu);
+    int i_nu;
+    float2 ab;
+    float dnu_num;
+    if (nxt_bin >= 0) {  // the redistributed photon's bin, located and loaded at the interaction
+      i_nu = nxt_bin;
+      ab = nxt_ab;
+      dnu_num = nxt_dnu;
+      nxt_bin = -1;
+    } else {
+      i_nu = loc_within_fast<true>(A.nu, p.nu * dshift);
+      ab = __ldg(opac + (size_t)iz * nn + i_nu);
+      dnu_num = (float)(loc_delta(A.nu, i_nu) * A.ct);
+    }
     const float a_f = ab.x;
     const float s_f = A.omit_scat ? 0.0f : ab.y;
     const float op_f = a_f + s_f;
     // distance over which the comoving frequency drifts by the bin's width
-    const float d_nu_f = __fdividef((float)(loc_delta(A.nu, i_nu) * A.ct), (float)p.nu);
+    const float d_nu_f = __fdividef(dnu_num, (float)p.nu);
     const double d_nu = (double)fabsf(d_nu_f);
     if (d_nu < d_bn) { d_bn = d_nu; new_ind = iz; }
     const float tot_f = (float)((double)op_f * dshift);
@@ -485,7 +513,8 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       }
       if (fate == MOVING) {
         const double mu = 1.0 - 2.0 * ((double)blk.w * (1.0 / 4294967296.0));
-        scatter<CT>(A, p, rsq, xd, mu, fminf(fmaxf(v, 0.0f), 1.0f), blk.z, redist);
+        nxt_bin = scatter<CT>(A, p, rsq, xd, mu, fminf(fmaxf(v, 0.0f), 1.0f), blk.z, redist, &nxt_dnu);
+        if (nxt_bin >= 0) nxt_ab = __ldg(opac + (size_t)iz * nn + nxt_bin);  // ahead of its use
         xd = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
       }
     } else {
