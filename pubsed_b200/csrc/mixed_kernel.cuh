@@ -31,11 +31,12 @@
 //    within the bin.  A recycled deviate keeps 2^32 p distinct values when
 //    its branch has probability p.
 //  * FP64 square roots, reciprocal square roots and reciprocals from the
-//    FP32 hardware estimate refined by one Newton-Raphson step with its
-//    second-order term (Markstein, IA-64 and Elementary Functions, 2000):
-//    the estimate's ~2^-22 relative error cubed is below FP64 rounding.
-//    They are not correctly rounded, which the mixed form does not need;
-//    position, time, frequency and the Lorentz transforms stay FP64.
+//    hardware's FP64 approximations refined by one Newton-Raphson step with
+//    its second-order term (Markstein, IA-64 and Elementary Functions,
+//    2000): the approximation's ~2^-20 relative error cubed is below FP64
+//    rounding.  They are not correctly rounded, which the mixed form does
+//    not need; position, time, frequency and the Lorentz transforms stay
+//    FP64.
 //  * -ln(u) in FP32 from the hardware logarithm, the interaction and
 //    bin-step distances as FP32 quotients (they set where a segment ends,
 //    not the state it carries).
@@ -43,25 +44,37 @@
 //    per move.
 namespace mixed {
 
-// 1/sqrt(a), a in (1e-36, 1e37)
+// The FP64 square roots, reciprocal square roots and reciprocals start from
+// the hardware's FP64 approximations (PTX rsqrt.approx.ftz.f64 and
+// rcp.approx.ftz.f64, about 20 correct bits: measured on B200 over 2^20
+// log-uniform inputs in [1e-30, 2e30], largest relative error 2^-20.1 and
+// 2^-20.0) and take one Newton-Raphson step with its second-order term
+// (Markstein, IA-64 and Elementary Functions, 2000), which cubes the error:
+// measured largest relative error of the results 2^-52.7 and 2^-53.0.
+// The approximations take the FP64 operand whole (no FP32 conversion, so no
+// range limit short of subnormals, which they flush to zero).
+
+// 1/sqrt(a), a > 0 normal
 __device__ __forceinline__ double rsqrt_nr(double a)
 {
-  const double y = (double)rsqrtf((float)a);
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
   const double h = fma(-a * y, y, 1.0);        // 1 - a y^2
   return fma(y * h, fma(0.375, h, 0.5), y);    // y (1 + h/2 + 3 h^2/8)
 }
 
-// sqrt(a), a >= 0
+// sqrt(a), a >= 0 (0 for 0, NaN for a < 0)
 __device__ __forceinline__ double sqrt_nr(double a)
 {
-  if (!(a > 1e-36 && a < 1e37)) return sqrt(a);
-  return a * rsqrt_nr(a);
+  const double r = a * rsqrt_nr(a);
+  return (a == 0.0) ? a : r;
 }
 
-// 1/a, |a| in (1e-36, 1e37)
+// 1/a, a normal
 __device__ __forceinline__ double rcp_nr(double a)
 {
-  const double y = (double)__fdividef(1.0f, (float)a);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
   const double e = fma(-a, y, 1.0);            // 1 - a y
   return fma(y, fma(e, e, e), y);              // y (1 + e + e^2)
 }
@@ -185,6 +198,42 @@ __device__ __forceinline__ int scatter(const StepArgs& A, Pkt& p, double rsq, do
   return kbin;
 }
 
+// adds one zone visit's tallies: to the block's shared copy [5][nz] when
+// A.smem_zones, else to global copy rep_off / (5 nz) of the n_rep copies
+// (rep_off < 0: the arrays themselves).  The targets are formed here, from
+// the shared array and the kernel's arguments, rather than held as five
+// pointers across the packet loop.
+__device__ __forceinline__ void add_visit(const StepArgs& A, double* s_tal, int nz, int64_t rep_off, int z,
+                                          double e, double fx, double fy, double fz, double fr)
+{
+  if (A.smem_zones) {
+    atomicAdd(s_tal + z, e);
+    if (A.tally_forces) {
+      atomicAdd(s_tal + nz + z, fx);
+      atomicAdd(s_tal + 2 * nz + z, fy);
+      atomicAdd(s_tal + 3 * nz + z, fz);
+      atomicAdd(s_tal + 4 * nz + z, fr);
+    }
+  } else if (rep_off >= 0) {
+    double* b = A.zone_rep + rep_off + z;
+    atomicAdd(b, e);
+    if (A.tally_forces) {
+      atomicAdd(b + nz, fx);
+      atomicAdd(b + 2 * nz, fy);
+      atomicAdd(b + 3 * nz, fz);
+      atomicAdd(b + 4 * nz, fr);
+    }
+  } else {
+    atomicAdd(A.e_abs + z, e);
+    if (A.tally_forces) {
+      atomicAdd(A.fx + z, fx);
+      atomicAdd(A.fy + z, fy);
+      atomicAdd(A.fz + z, fz);
+      atomicAdd(A.fr + z, fr);
+    }
+  }
+}
+
 // the state emit_mixed_kernel stored for core packet q
 __device__ __forceinline__ void load_emitted(const StepArgs& A, Pkt& p, int64_t q)
 {
@@ -264,23 +313,14 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
   if (A.smem_zones)
     for (int i = threadIdx.x; i < 5 * nz; i += blockDim.x) s_tal[i] = 0.0;
   __syncthreads();
-  double* t_eabs = A.smem_zones ? s_tal : A.e_abs;
-  double* t_fx = A.smem_zones ? s_tal + nz : A.fx;
-  double* t_fy = A.smem_zones ? s_tal + 2 * nz : A.fy;
-  double* t_fz = A.smem_zones ? s_tal + 3 * nz : A.fz;
-  double* t_fr = A.smem_zones ? s_tal + 4 * nz : A.fr;
-  if (!A.smem_zones && A.n_rep > 0) {
-    double* base = A.zone_rep + (size_t)(blockIdx.x % A.n_rep) * 5 * nz;
-    t_eabs = base; t_fx = base + nz; t_fy = base + 2 * nz; t_fz = base + 3 * nz; t_fr = base + 4 * nz;
-  }
+  const int64_t rep_off = (!A.smem_zones && A.n_rep > 0) ? (int64_t)(blockIdx.x % A.n_rep) * 5 * nz : -1;
   const float2* __restrict__ opac = reinterpret_cast<const float2*>(A.opac);
   const int32_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
   uint32_t K = ((A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u + 3u) / 4u;
   uint32_t step = A.step;
   if constexpr (BATCH) step = *A.step_dev;
   int64_t q_next = 0, q_end = 0;
-  int m = 0, esc_model = -1;
-  unsigned long long esc_count = 0;
+  int m = 0;
   uint32_t n_scat = 0;  // interactions of the current packet
   Pkt p;
   PacketRng rng;
@@ -312,15 +352,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     if (!live) continue;
     if (fate != MOVING) {
       if (have) {
-        if (acc_zone >= 0) {
-          atomicAdd(t_eabs + acc_zone, acc_eabs);
-          if (A.tally_forces) {
-            atomicAdd(t_fx + acc_zone, acc_fx);
-            atomicAdd(t_fy + acc_zone, acc_fy);
-            atomicAdd(t_fz + acc_zone, acc_fz);
-            atomicAdd(t_fr + acc_zone, acc_fr);
-          }
-        }
+        if (acc_zone >= 0) add_visit(A, s_tal, nz, rep_off, acc_zone, acc_eabs, acc_fx, acc_fy, acc_fz, acc_fr);
         atomicAdd(s_cnt + 3, (unsigned long long)seg);
         atomicAdd(s_cnt + 4, (unsigned long long)n_scat);
         n_scat = 0;
@@ -329,12 +361,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
           if constexpr (BATCH) {
             const int64_t so = A.models[m].spec_off;
             spectrum_count(A, A.flux + so, A.click + so, t_obs, p.nu, p.e, p.D);
-            if (m != esc_model) {
-              if (esc_model >= 0) atomicAdd(A.model_escaped + esc_model, esc_count);
-              esc_model = m;
-              esc_count = 0;
-            }
-            ++esc_count;
+            atomicAdd(A.model_escaped + m, 1ULL);
           } else {
             spectrum_count(A, A.flux, A.click, t_obs, p.nu, p.e, p.D);
           }
@@ -412,15 +439,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     ++seg;
     const int iz = p.ind;
     if (iz != acc_zone) {
-      if (acc_zone >= 0) {
-        atomicAdd(t_eabs + acc_zone, acc_eabs);
-        if (A.tally_forces) {
-          atomicAdd(t_fx + acc_zone, acc_fx);
-          atomicAdd(t_fy + acc_zone, acc_fy);
-          atomicAdd(t_fz + acc_zone, acc_fz);
-          atomicAdd(t_fr + acc_zone, acc_fr);
-        }
-      }
+      if (acc_zone >= 0) add_visit(A, s_tal, nz, rep_off, acc_zone, acc_eabs, acc_fx, acc_fy, acc_fz, acc_fr);
       acc_zone = iz;
       acc_eabs = acc_fx = acc_fy = acc_fz = acc_fr = 0;
       wl = zone_walls<BATCH>(A, G, iz);
@@ -520,9 +539,6 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     } else {
       fate = STOPPED;
     }
-  }
-  if constexpr (BATCH) {
-    if (esc_model >= 0 && esc_count) atomicAdd(A.model_escaped + esc_model, esc_count);
   }
   __syncthreads();
   if (threadIdx.x < 6) {

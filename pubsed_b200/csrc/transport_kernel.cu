@@ -474,8 +474,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 #define SED_PROP_THREADS 128
 #endif
 // launch shape of the mixed-form 1D kernel (propagate_mixed_kernel):
-// 128 x 6 at 80 registers without spills (Type Ia step 835 ms; 128 x 8 at
-// 64 registers spills and ran 891 ms)
+// 128 x 6 at 80 registers without spills (Type Ia packet kernel 733 ms with
+// the FP32-estimate square roots; 128 x 7 at 72 registers spills 68 B and
+// ran 792 ms, 128 x 5 at 84 registers 875 ms)
 #ifndef SED_MIXED_THREADS
 #define SED_MIXED_THREADS 128
 #endif
