@@ -474,14 +474,14 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 #define SED_PROP_THREADS 128
 #endif
 // launch shape of the mixed-form 1D kernel (propagate_mixed_kernel):
-// 128 x 6 at 80 registers without spills (Type Ia packet kernel 733 ms with
-// the FP32-estimate square roots; 128 x 7 at 72 registers spills 68 B and
-// ran 792 ms, 128 x 5 at 84 registers 875 ms)
+// 128 x 7 at 72 registers without spills, 28 warps per SM (Type Ia packet
+// kernel 631 ms; 128 x 6 at 79 registers 678 ms, 128 x 8 at 64 registers
+// spills 52 B and ran 676 ms)
 #ifndef SED_MIXED_THREADS
 #define SED_MIXED_THREADS 128
 #endif
 #ifndef SED_MIXED_MINB
-#define SED_MIXED_MINB 6
+#define SED_MIXED_MINB 7
 #endif
 #ifndef SED_PROP_MINB
 #define SED_PROP_MINB 8
@@ -1872,14 +1872,16 @@ __global__ void init_particles_kernel(const InitArgs I, const GridDev G)
 #include "mixed_kernel.cuh"
 
 // the mixed-form 1D kernel (propagate_mixed_kernel) in one compiled shape
-// (zone-scalar tallies go straight to global memory when MINB blocks'
-// shared-memory copies would not fit on an SM)
+// (zone-scalar tallies go to global memory when MINB blocks' shared-memory
+// copies, next to their per-thread visit sums and the block's 1 KB, would not
+// fit in an SM's 228 KB)
 template <int BATCH, int THREADS, int MINB>
 int launch_mixed_t(const StepArgs& a0, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
                    cudaStream_t s)
 {
   StepArgs a = a0;
-  if (a.smem_zones && (size_t)MINB * 5 * g.nzones * sizeof(double) > (size_t)200 * 1024) a.smem_zones = 0;
+  const size_t per_block = (size_t)5 * g.nzones * sizeof(double) + (size_t)5 * THREADS * sizeof(double) + 1024 + 64;
+  if (a.smem_zones && (size_t)MINB * per_block > (size_t)228 * 1024) a.smem_zones = 0;
   const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
   auto kern = propagate_mixed_kernel<BATCH, THREADS, MINB>;
   if (a.em_n > 0) {  // the core packets, emitted ahead
@@ -1945,9 +1947,9 @@ int launch_propagate_t(const StepArgs& a, const GridDev& g, int num_sms, cudaStr
   }
 }
 
-// batched kernel shapes {threads, min blocks per SM}: 32 or 24 warps per SM
-// (64 or 80 registers per thread) in blocks of 4 or 8 warps
-constexpr int BATCH_SHAPES[BATCH_VARIANTS][2] = {{128, 8}, {256, 4}, {128, 6}, {256, 3}};
+// batched kernel shapes {threads, min blocks per SM}: 32, 28 or 24 warps per
+// SM (64, 72 or 80 registers per thread) in blocks of 4 or 8 warps
+constexpr int BATCH_SHAPES[BATCH_VARIANTS][2] = {{128, 8}, {256, 4}, {128, 7}, {256, 3}};
 
 template <typename OT, typename CT>
 int launch_batch_t(const StepArgs& a, const GridDev& g, int variant, int bps, int num_sms, int64_t total,
