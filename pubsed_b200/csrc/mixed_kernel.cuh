@@ -92,8 +92,10 @@ __device__ __forceinline__ float neg_log_u(uint32_t w)
 }
 
 // the zone's walls, as get_next_zone (grid_1D_sphere.cpp:510-590) derives
-// them: outer wall, inner wall after the core substitution, inner and outer
-// neighbour, and whether the inner wall is r = 0 of zone 0 (no inner wall)
+// them: outer wall, inner wall after the core substitution, and (batched
+// models, from their neighbour tables) inner and outer neighbour and whether
+// the inner wall is r = 0 of zone 0 (no inner wall).  One model's
+// neighbours follow from the zone index and the inner wall (next_zone).
 struct Walls {
   double r_o, r_i;
   int in_nbr, out_nbr;
@@ -112,33 +114,45 @@ __device__ __forceinline__ Walls zone_walls(const StepArgs& A, const GridDev& G,
     w.out_nbr = nb.y;
     w.no_inner = nb.z != 0;
   } else {
-    if (i != 0) { w.r_i = __ldg(G.r_out.right + i - 1); w.in_nbr = i - 1; }
-    else { w.r_i = G.r_out.min; w.in_nbr = -1; }
-    if (A.core_radius >= w.r_i) { w.r_i = A.core_radius; w.in_nbr = -1; }
-    w.no_inner = (i == 0) && (w.r_i == 0);
-    w.out_nbr = (i + 1 == G.nzones) ? -2 : i + 1;
+    w.r_i = (i != 0) ? __ldg(G.r_out.right + i - 1) : G.r_out.min;
+    if (A.core_radius >= w.r_i) w.r_i = A.core_radius;
+    w.in_nbr = w.out_nbr = 0;
+    w.no_inner = false;
   }
   return w;
 }
 
-// distance to the zone's boundary along D and the zone entered there, with
+// distance to zone iz's boundary along D and the zone entered there, with
 // the reference's tiny_offset push across the wall
-__device__ __forceinline__ int next_zone(const Walls& w, double rsq, double xd, double* l)
+template <int BATCH>
+__device__ __forceinline__ int next_zone(const StepArgs& A, const GridDev& G, const Walls& w, int iz, double rsq,
+                                         double xd, double* l)
 {
+  int in_nbr, out_nbr;
+  bool no_inner;
+  if constexpr (BATCH) {
+    in_nbr = w.in_nbr;
+    out_nbr = w.out_nbr;
+    no_inner = w.no_inner;
+  } else {  // the inner wall is the core's when the substitution moved it there
+    in_nbr = (iz == 0 || w.r_i == A.core_radius) ? -1 : iz - 1;
+    out_nbr = (iz + 1 == G.nzones) ? -2 : iz + 1;
+    no_inner = (iz == 0) && (w.r_i == 0);
+  }
   const double l_out = sqrt_nr(fma(xd, xd, fma(w.r_o, w.r_o, -rsq))) - xd;
   double l_in = -1;
-  if (!w.no_inner && xd < 0) {
+  if (!no_inner && xd < 0) {
     const double rad = fma(xd, xd, fma(w.r_i, w.r_i, -rsq));
     if (rad >= 0) l_in = -xd - sqrt_nr(rad);
   }
   constexpr double tiny_offset = 1 + 1e-6;
   constexpr double inv_tiny_offset = 1 / tiny_offset;
   if ((l_out < l_in) || (l_in < 0)) {
-    *l = (w.out_nbr == -2) ? l_out * inv_tiny_offset : l_out * tiny_offset;
-    return w.out_nbr;
+    *l = (out_nbr == -2) ? l_out * inv_tiny_offset : l_out * tiny_offset;
+    return out_nbr;
   }
-  *l = (w.in_nbr == -1) ? l_in * inv_tiny_offset : l_in * tiny_offset;
-  return w.in_nbr;
+  *l = (in_nbr == -1) ? l_in * inv_tiny_offset : l_in * tiny_offset;
+  return in_nbr;
 }
 
 // isotropic_scatter (scatter.cpp:303-351) on a homologous flow, with the
@@ -234,6 +248,16 @@ __device__ __forceinline__ void add_visit(const StepArgs& A, double* s_tal, int 
   }
 }
 
+// 8 bytes from global memory to a shared-memory slot without a register
+// holding them in between (cp.async, cached in L1); cp_async_wait completes
+// the thread's copies before the slot is read
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // the state emit_mixed_kernel stored for core packet q
 __device__ __forceinline__ void load_emitted(const StepArgs& A, Pkt& p, int64_t q)
 {
@@ -316,25 +340,35 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
   const int64_t rep_off = (!A.smem_zones && A.n_rep > 0) ? (int64_t)(blockIdx.x % A.n_rep) * 5 * nz : -1;
   const float2* __restrict__ opac = reinterpret_cast<const float2*>(A.opac);
   const int32_t limit = A.max_segments > 0 ? A.max_segments : 10000000;
-  uint32_t K = ((A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u + 3u) / 4u;
+  const uint32_t K_core = ((A.core_radius == 0 ? 2u : 4u) + (A.core_freq > 0 ? 0u : 2u) + 1u + 3u) / 4u;
   uint32_t step = A.step;
   if constexpr (BATCH) step = *A.step_dev;
-  int64_t q_next = 0, q_end = 0;
-  int m = 0;
-  uint32_t n_scat = 0;  // interactions of the current packet
   Pkt p;
   PacketRng rng;
   int fate = ABSORBED;  // no packet yet
   bool have = false;
-  unsigned long long pid = 0;
   int32_t seg = 0;
+  const int tid = threadIdx.x;
+  // What the loop reads only when a packet starts or ends, or one segment
+  // after forming it, sits in the thread's own slots of shared memory
+  // rather than in registers: the packet's queue index, the Philox counter
+  // where its records count draws from and where its interactions start
+  // (one block per interaction), the {abs, scat} and bin width of a
+  // redistributed photon's new bin, and for a batch the model and the
+  // claimed queue range.
+  __shared__ unsigned long long s_pid[THREADS];
+  __shared__ uint32_t s_k0[THREADS], s_n0[THREADS];
+  __shared__ float2 s_nab[BATCH ? THREADS : 1];
+  __shared__ float s_ndnu[BATCH ? THREADS : 1];
+  __shared__ int s_m[BATCH ? THREADS : 1];
+  __shared__ long long s_qn[BATCH ? THREADS : 1], s_qe[BATCH ? THREADS : 1];
+  if constexpr (BATCH) { s_qn[tid] = 0; s_qe[tid] = 0; }
   // the current zone visit's tallies (e_abs, fx, fy, fz, fr), summed in the
   // thread's own column of shared memory: held in registers they cost the
   // ten that take the kernel from 28 to 24 warps per SM (Type Ia packet
   // kernel 631 ms against 661 ms)
   int acc_zone = -1;
   __shared__ double s_acc[5][THREADS];
-  const int tid = threadIdx.x;
   auto clear_visit = [&]() {
     s_acc[0][tid] = 0.0; s_acc[1][tid] = 0.0; s_acc[2][tid] = 0.0; s_acc[3][tid] = 0.0; s_acc[4][tid] = 0.0;
   };
@@ -350,8 +384,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
   bool live = true;   // the lane still takes packets from the queue
   // after a redistribution: the photon's comoving bin (its lab frequency
   // transforms back into that bin at the next segment's start, which is the
-  // interaction point), the bin's {abs, scat} loaded ahead, and its width
-  // times c t; -1 when the next segment has to locate its bin
+  // interaction point), its {abs, scat}, loaded ahead, and its width times
+  // c t; -1 when the next segment has to locate its bin.  One model's kernel
+  // holds the last two in registers (its segment loop ran 4% slower with
+  // them in shared memory at the same occupancy); the batched kernel keeps
+  // them in s_nab, s_ndnu, which it needs to fit 72 registers.
   int nxt_bin = -1;
   float2 nxt_ab = make_float2(0.f, 0.f);
   float nxt_dnu = 0.f;
@@ -368,11 +405,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       if (have) {
         flush_visit();
         atomicAdd(s_cnt + 3, (unsigned long long)seg);
-        atomicAdd(s_cnt + 4, (unsigned long long)n_scat);
-        n_scat = 0;
+        atomicAdd(s_cnt + 4, (unsigned long long)(rng.n - s_n0[tid]));
         if (fate == ESCAPED) {
           const double t_obs = p.t - (p.x[0] * p.D[0] + p.x[1] * p.D[1] + p.x[2] * p.D[2]) / C_LIGHT;
           if constexpr (BATCH) {
+            const int m = s_m[tid];
             const int64_t so = A.models[m].spec_off;
             spectrum_count(A, A.flux + so, A.click + so, t_obs, p.nu, p.e, p.D);
             atomicAdd(A.model_escaped + m, 1ULL);
@@ -387,9 +424,10 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
           atomicAdd(s_cnt + 2, 1ULL);
         }
         if (A.rec_fate) {
+          const unsigned long long pid = s_pid[tid];
           A.rec_fate[pid] = fate;
           A.rec_ind[pid] = p.ind;
-          A.rec_draws[pid] = (int32_t)(rng.n - K);
+          A.rec_draws[pid] = (int32_t)(rng.n - s_k0[tid]);
           if (A.rec_type) A.rec_type[pid] = TYPE_PHOTON;
           double* s = A.rec_state + pid * 9;
           s[0] = p.x[0]; s[1] = p.x[1]; s[2] = p.x[2];
@@ -399,23 +437,30 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
         have = false;
       }
       if constexpr (BATCH) {
+        long long q_next = s_qn[tid], q_end = s_qe[tid];
         if (q_next >= q_end) {
-          q_next = (int64_t)atomicAdd(A.counters + C_QUEUE, (unsigned long long)A.queue_chunk);
+          q_next = (long long)atomicAdd(A.counters + C_QUEUE, (unsigned long long)A.queue_chunk);
           q_end = q_next + A.queue_chunk;
           if (q_end > A.n_packets) q_end = A.n_packets;
+          s_qe[tid] = q_end;
         }
         if (q_next >= A.n_packets) { live = false; continue; }
-        pid = (unsigned long long)q_next++;
-        m = __ldg(A.em_model + pid);
+        const unsigned long long pid = (unsigned long long)q_next;
+        s_qn[tid] = q_next + 1;
+        s_pid[tid] = pid;
+        const int m = __ldg(A.em_model + pid);
+        s_m[tid] = m;
         const BatchModel& M = A.models[m];
-        K = (M.emit_draws + 3u) / 4u;
+        const uint32_t K = (M.emit_draws + 3u) / 4u;
         // the stream continues after the emission's blocks
         rng.init(M.seed, (uint64_t)(M.first_pid + ((int64_t)pid - M.pkt_off)), step, K);
+        s_k0[tid] = K;
         load_emitted(A, p, (int64_t)pid);
         tau_rem = __ldg(A.em_tau + pid);
       } else {
-        pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
+        const unsigned long long pid = atomicAdd(A.counters + C_QUEUE, 1ULL);
         if (pid >= (unsigned long long)A.n_packets) { live = false; continue; }
+        s_pid[tid] = pid;
         if (A.q_n != nullptr && (int64_t)pid >= A.n_core) {
           // a queued photon: census (stream position 0) or an optical
           // photon the gamma-ray kernel handed over at its stream position
@@ -428,10 +473,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
           p.t = q[6]; p.e = q[7]; p.nu = q[8];
           p.ind = A.q_ind[k];
           rng.init(A.seed, (uint64_t)(A.radio_first_pid + k), step, qn);
-          K = 0;
+          s_k0[tid] = 0;
           tau_rem = neg_log_u(rng.block().x);
         } else {
-          rng.init(A.seed, (uint64_t)A.first_pid + pid, step, K);  // after the emission's blocks
+          rng.init(A.seed, (uint64_t)A.first_pid + pid, step, K_core);  // after the emission's blocks
+          s_k0[tid] = K_core;
           load_emitted(A, p, (int64_t)pid);
           tau_rem = __ldg(A.em_tau + pid);
         }
@@ -444,6 +490,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       acc_zone = -1;
       clear_visit();
       have = true;
+      s_n0[tid] = rng.n;
       if (fate != MOVING) continue;
       rsq = fma(p.x[0], p.x[0], fma(p.x[1], p.x[1], p.x[2] * p.x[2]));
       xd = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
@@ -459,7 +506,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       wl = zone_walls<BATCH>(A, G, iz);
     }
     double d_bn;
-    int new_ind = next_zone(wl, rsq, xd, &d_bn);
+    int new_ind = next_zone<BATCH>(A, G, wl, iz, rsq, xd, &d_bn);
     // comoving frequency and the opacity of its bin (transport_opacity.cpp:268-299)
     const double gamma = rsqrt_nr(fma(-rsq, A.inv_ct2, 1.0));
     const double dshift = gamma * fma(-xd, A.inv_ct, 1.0);
@@ -468,8 +515,14 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     float dnu_num;
     if (nxt_bin >= 0) {  // the redistributed photon's bin, located and loaded at the interaction
       i_nu = nxt_bin;
-      ab = nxt_ab;
-      dnu_num = nxt_dnu;
+      if constexpr (BATCH) {
+        cp_async_wait();
+        ab = s_nab[tid];
+        dnu_num = s_ndnu[tid];
+      } else {
+        ab = nxt_ab;
+        dnu_num = nxt_dnu;
+      }
       nxt_bin = -1;
     } else {
       i_nu = loc_within_fast<true>(A.nu, p.nu * dshift);
@@ -528,7 +581,6 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     } else if (event == 0) {
       // do_scatter (scatter.cpp:12-70): u <= eps is the absorption branch;
       // the deviate left over from each test is recycled into the next
-      ++n_scat;
       const uint4 blk = rng.block();
       tau_rem = neg_log_u(blk.x);  // the next flight's depth
       const float u1 = (float)blk.y * W32;
@@ -548,14 +600,24 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       }
       if (fate == MOVING) {
         const double mu = 1.0 - 2.0 * ((double)blk.w * (1.0 / 4294967296.0));
-        nxt_bin = scatter<CT>(A, p, rsq, xd, mu, fminf(fmaxf(v, 0.0f), 1.0f), blk.z, redist, &nxt_dnu);
-        if (nxt_bin >= 0) nxt_ab = __ldg(opac + (size_t)iz * nn + nxt_bin);  // ahead of its use
+        float dnu_new = 0.f;
+        nxt_bin = scatter<CT>(A, p, rsq, xd, mu, fminf(fmaxf(v, 0.0f), 1.0f), blk.z, redist, &dnu_new);
+        if (nxt_bin >= 0) {  // the new bin's {abs, scat}, loaded ahead of its use
+          if constexpr (BATCH) {
+            cp_async8(s_nab + tid, opac + (size_t)iz * nn + nxt_bin);
+            s_ndnu[tid] = dnu_new;
+          } else {
+            nxt_ab = __ldg(opac + (size_t)iz * nn + nxt_bin);
+            nxt_dnu = dnu_new;
+          }
+        }
         xd = fma(p.D[0], p.x[0], fma(p.D[1], p.x[1], p.D[2] * p.x[2]));
       }
     } else {
       fate = STOPPED;
     }
   }
+  cp_async_wait();
   __syncthreads();
   if (threadIdx.x < 6) {
     constexpr int slot[6] = {C_ESCAPED, C_ABSORBED, C_STOPPED, C_SEGMENTS, C_SCATTERS, C_LIMIT};

@@ -474,14 +474,14 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v)
 #define SED_PROP_THREADS 128
 #endif
 // launch shape of the mixed-form 1D kernel (propagate_mixed_kernel):
-// 128 x 7 at 72 registers without spills, 28 warps per SM (Type Ia packet
-// kernel 631 ms; 128 x 6 at 79 registers 678 ms, 128 x 8 at 64 registers
-// spills 52 B and ran 676 ms)
+// 128 x 8 at 64 registers without spills, 32 warps per SM (Type Ia packet
+// kernel 623 ms; 128 x 7 at 70 registers 638 ms; 128 x 9 at 56 registers
+// spills 40 B and ran 676 ms)
 #ifndef SED_MIXED_THREADS
 #define SED_MIXED_THREADS 128
 #endif
 #ifndef SED_MIXED_MINB
-#define SED_MIXED_MINB 7
+#define SED_MIXED_MINB 8
 #endif
 #ifndef SED_PROP_MINB
 #define SED_PROP_MINB 8
@@ -1873,17 +1873,19 @@ __global__ void init_particles_kernel(const InitArgs I, const GridDev G)
 
 // the mixed-form 1D kernel (propagate_mixed_kernel) in one compiled shape
 // (zone-scalar tallies go to global memory when MINB blocks' shared-memory
-// copies, next to their per-thread visit sums and the block's 1 KB, would not
-// fit in an SM's 228 KB)
+// copies, next to the kernel's static per-thread slots and the block's 1 KB,
+// would not fit in an SM's 228 KB)
 template <int BATCH, int THREADS, int MINB>
 int launch_mixed_t(const StepArgs& a0, const GridDev& g, int blocks_per_sm, int num_sms, int64_t total,
                    cudaStream_t s)
 {
   StepArgs a = a0;
-  const size_t per_block = (size_t)5 * g.nzones * sizeof(double) + (size_t)5 * THREADS * sizeof(double) + 1024 + 64;
+  auto kern = propagate_mixed_kernel<BATCH, THREADS, MINB>;
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, kern);
+  const size_t per_block = (size_t)5 * g.nzones * sizeof(double) + fa.sharedSizeBytes + 1024;
   if (a.smem_zones && (size_t)MINB * per_block > (size_t)228 * 1024) a.smem_zones = 0;
   const size_t smem = a.smem_zones ? (size_t)5 * g.nzones * sizeof(double) : 0;
-  auto kern = propagate_mixed_kernel<BATCH, THREADS, MINB>;
   if (a.em_n > 0) {  // the core packets, emitted ahead
     int64_t eb = (a.em_n + 255) / 256;
     if (eb > (int64_t)num_sms * 16) eb = (int64_t)num_sms * 16;
