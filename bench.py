@@ -54,11 +54,13 @@ METRIC = "MC packets/s at matched spectrum chi-squared (mixed/batched vs plain F
 UNIT = "packets/s"
 
 
-def captured_traffic(workload: str, n_segments: int):
+def captured_traffic(workload: str, n_segments: int, n_packets: int = 0):
     """DRAM bytes (read + write) of one packet-kernel launch of `workload`
     from the ncu captures in profiles/propagate_kernel_traffic.json: as
-    captured where the working set stays in L2 (scale "none"), else scaled
-    from the captured launch by segments.  None without a capture."""
+    captured where the working set stays in L2 (scale "none"), scaled from
+    the captured launch by segments (scale "segments"), or a fixed part plus
+    a part per packet (scale "packets": the pre-emitted state each packet
+    reads).  None without a capture."""
     tfile = os.path.join(ROOT, "profiles", "propagate_kernel_traffic.json")
     if not os.path.exists(tfile):
         return None
@@ -69,6 +71,9 @@ def captured_traffic(workload: str, n_segments: int):
             continue
         if tr.get("scale") == "segments":
             return float(tr["dram_bytes"]) / float(tr["segments"]) * float(n_segments)
+        if tr.get("scale") == "packets":
+            fixed = float(tr["fixed_bytes"])
+            return fixed + (float(tr["dram_bytes"]) - fixed) / float(tr["packets"]) * float(n_packets)
         return float(tr["dram_bytes"])
     return None
 
@@ -389,7 +394,7 @@ def main_batch(args, rank: int, world: int, local: int):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "traffic": captured_traffic(bw.name, last["n_segments"]),
-                       "kernel": "propagate_kernel (batched)", "kernel_ms": kern_ms,
+                       "kernel": "propagate_mixed_kernel (batched)", "kernel_ms": kern_ms,
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
     out["clocks"] = clk.summary()
     if not args.no_cpu_baseline:
@@ -636,7 +641,7 @@ def main():
     ap.add_argument("--ref-packets", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
-    ap.add_argument("--batch-leg-scale", type=float, default=0.25,
+    ap.add_argument("--batch-leg-scale", type=float, default=1.0,
                     help="type_ia: packet scale of the batching leg added to the line (0: no batching leg)")
     args = ap.parse_args()
     rank, world, local = _env_rank()
@@ -778,7 +783,7 @@ def main():
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = captured_traffic(w.name, last["n_segments"])
+    traffic = captured_traffic(w.name, last["n_segments"], n_step)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -798,7 +803,9 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": e2e_t * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "propagate_kernel", "kernel_ms": kern_ms,
+                     "traffic": traffic,
+                     "kernel": "propagate_mixed_kernel" if w.zones.type != abi.GRID_3D_CART else "propagate_kernel",
+                     "kernel_ms": kern_ms,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clk.summary(),
     }
@@ -806,8 +813,8 @@ def main():
         fp64["ratio_mixed_over_fp64"] = fp64["ms_per_step"] / ms_max
     eng.close()
     if args.workload == "type_ia" and args.batch_leg_scale > 0 and world == 1:
-        # the batched half of the metric, at a reduced packet count so the
-        # default run stays within a few minutes
+        # the batched half of the metric (64 models, by default at their full
+        # packet counts)
         line["batch64"] = batch_leg(local, flush, args.batch_leg_scale)
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         try:

@@ -53,8 +53,9 @@ __device__ __forceinline__ int get_zone(const GridDev& G, const double* x)
 
 // grid_1D_sphere::get_next_zone (grid_1D_sphere.cpp:510-590) and
 // grid_3D_cart::get_next_zone (grid_3D_cart.cpp:396-469)
-// (1D: rsq = x.x and xdotD = D.x come from the caller)
-template <int GRID>
+// (1D: rsq = x.x and xdotD = D.x come from the caller; FAST, the mixed
+// form: the 3D wall distances from the FP64 reciprocal approximation)
+template <int GRID, bool FAST = false>
 __device__ __forceinline__ int get_next_zone(const GridDev& G, const double* x, const double* D, int i,
                                              double r_core, double rsq, double xdotD, double* l)
 {
@@ -95,7 +96,8 @@ __device__ __forceinline__ int get_next_zone(const GridDev& G, const double* x, 
     for (int a = 0; a < 3; ++a) {
       const double dd = loc_delta(G.ax[a], idx3[a]);
       const double bn = (D[a] > 0) ? __ldg(G.ax[a].right + idx3[a]) + dd * tiny : loc_left(G.ax[a], idx3[a]) - dd * tiny;
-      len[a] = (bn - x[a]) / D[a];
+      if constexpr (FAST) len[a] = (D[a] != 0.0) ? (bn - x[a]) * rcp_nr(D[a]) : (double)INFINITY;
+      else len[a] = (bn - x[a]) / D[a];
     }
     int d[3] = {0, 0, 0};
     if ((len[0] < len[1]) && (len[0] < len[2])) { d[0] = (D[0] < 0) ? -1 : 1; *l = len[0]; }
@@ -318,8 +320,8 @@ __device__ __forceinline__ void isotropic_scatter(const StepArgs& A, const GridD
 // transport::do_dshift, lab -> comoving, from rsq = x.x and xdotD = D.x
 __device__ __forceinline__ double dshift_fast(const StepArgs& A, double rsq, double xdotD)
 {
-  const double gamma = rsqrt(1 - rsq * A.inv_ct2);
-  return gamma * (1 - xdotD * A.inv_ct);
+  const double gamma = rsqrt_nr(fma(-rsq, A.inv_ct2, 1.0));
+  return gamma * fma(-xdotD, A.inv_ct, 1.0);
 }
 
 // transport::isotropic_scatter (scatter.cpp:303-351), homologous flow
@@ -330,17 +332,21 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
 {
   const double b0 = p.x[0] * A.inv_ct, b1 = p.x[1] * A.inv_ct, b2 = p.x[2] * A.inv_ct;  // v / c
   const double bdotD = fma(b0, p.D[0], fma(b1, p.D[1], b2 * p.D[2]));
-  const double gamma = rsqrt(1 - fma(b0, b0, fma(b1, b1, b2 * b2)));
+  const double gamma = rsqrt_nr(1 - fma(b0, b0, fma(b1, b1, b2 * b2)));
   const double dshift_in = gamma * (1 - bdotD);
   p.e = p.e * dshift_in;
   p.nu = p.nu * dshift_in;
   const double mu = 1 - 2.0 * w01(w.x);
-  // the azimuth's sine and cosine in FP32 (a direction sample, not a frame
-  // transform; the transforms below and the normalisation are FP64)
+  // the azimuth's sine and cosine in FP32 from the hardware's sincos on
+  // [-pi, pi): phi - pi has sine -sin(phi) and cosine -cos(phi) (a direction
+  // sample, not a frame transform; the transforms below and the
+  // normalisation are FP64)
   const float phi = (float)(2.0 * PI * w01(w.y));
-  const double smu = sqrt(1 - mu * mu);
+  const double smu = sqrt_nr(fma(-mu, mu, 1.0));
   float sf, cf;
-  sincosf(phi, &sf, &cf);
+  __sincosf(phi - (float)PI, &sf, &cf);
+  sf = -sf;
+  cf = -cf;
   const double Dn[3] = {smu * (double)cf, smu * (double)sf, mu};
   if (redist) {  // transport::sample_photon_frequency (emission.cpp:27-46)
     const int nn = A.nu.n;
@@ -351,13 +357,13 @@ __device__ __forceinline__ void isotropic_scatter_fast(const StepArgs& A, Pkt& p
   // comoving -> lab with the velocity reversed: beta' = -beta
   const double bdp = -fma(b0, Dn[0], fma(b1, Dn[1], b2 * Dn[2]));
   const double vd_out = gamma * (1 - bdp);
-  const double f = 1 - gamma * bdp / (gamma + 1);
+  const double f = fma(-gamma * bdp, rcp_nr(gamma + 1), 1.0);
   const double gf = gamma * f;
-  const double inv_vd = 1.0 / vd_out;
+  const double inv_vd = rcp_nr(vd_out);
   p.D[0] = inv_vd * fma(gf, b0, Dn[0]);
   p.D[1] = inv_vd * fma(gf, b1, Dn[1]);
   p.D[2] = inv_vd * fma(gf, b2, Dn[2]);
-  const double inv_norm = rsqrt(fma(p.D[0], p.D[0], fma(p.D[1], p.D[1], p.D[2] * p.D[2])));
+  const double inv_norm = rsqrt_nr(fma(p.D[0], p.D[0], fma(p.D[1], p.D[1], p.D[2] * p.D[2])));
   p.D[0] *= inv_norm;
   p.D[1] *= inv_norm;
   p.D[2] *= inv_norm;
@@ -768,7 +774,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       }
       int new_ind;
       if constexpr (BATCH) new_ind = get_next_zone_batch(A, G, iz, rsq, xdotD, &d_bn);
-      else new_ind = get_next_zone<GRID>(G, p.x, p.D, iz, A.core_radius, rsq, xdotD, &d_bn);
+      else new_ind = get_next_zone<GRID, FAST>(G, p.x, p.D, iz, A.core_radius, rsq, xdotD, &d_bn);
       double dshift;
       if (fast) {
         dshift = dshift_fast(A, rsq, xdotD);
@@ -804,7 +810,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
       double d_nu;
       // distance to the bin's edge: only where the segment stops to look up
       // the next bin, so FP32 in the mixed form
-      if (fast) d_nu = (double)((float)(loc_delta(A.nu, i_nu) * A.ct) / (float)p.nu);
+      if (fast) d_nu = (double)__fdividef((float)(loc_delta(A.nu, i_nu) * A.ct), (float)p.nu);
       else {
         d_nu = loc_delta(A.nu, i_nu) / p.nu * C_LIGHT / p.dvds;
         if (p.dvds == 0) d_nu = INFINITY;
@@ -826,9 +832,10 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_kernel(const StepArgs
         tau_r = -1.0 * log(1 - rng.next());
       }
       // mixed form: tau is an FP32 deviate, so its distance is formed in FP32
-      // (an IEEE division, off the FP64 pipe); position and time stay FP64
+      // (the hardware's FP32 division, off the FP64 pipe); position and time
+      // stay FP64
       double d_sc;
-      if constexpr (FAST) d_sc = (double)((float)tau_r / (float)tot_lab);
+      if constexpr (FAST) d_sc = (double)__fdividef((float)tau_r, (float)tot_lab);
       else d_sc = tau_r / tot_lab;
       if (tot_lab == 0) d_sc = INFINITY;
       double d_tm = (A.tstop - p.t) * C_LIGHT;

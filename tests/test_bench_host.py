@@ -22,6 +22,14 @@ def test_every_bench_workload_with_a_capture_reports_traffic():
             # the captured launch itself is reproduced, and twice the segments twice the bytes
             assert abs(bench.captured_traffic(e["workload"], e["segments"]) - e["dram_bytes"]) < 1
             assert abs(bench.captured_traffic(e["workload"], 2 * e["segments"]) - 2 * e["dram_bytes"]) < 2
+        elif e["scale"] == "packets":
+            # the captured launch is reproduced; the part beyond the fixed
+            # first touch grows with the packets
+            assert abs(bench.captured_traffic(e["workload"], 123, e["packets"]) - e["dram_bytes"]) < 1
+            per = (e["dram_bytes"] - e["fixed_bytes"]) / e["packets"]
+            assert 0 < per < 1000
+            twice = bench.captured_traffic(e["workload"], 123, 2 * e["packets"])
+            assert abs(twice - (2 * e["dram_bytes"] - e["fixed_bytes"])) < 2
         else:
             assert bench.captured_traffic(e["workload"], 123) == e["dram_bytes"]
     assert bench.captured_traffic("no_such_workload", 1) is None
