@@ -57,14 +57,13 @@ __device__ __forceinline__ float neg_log_u(uint32_t w)
 }
 
 // the zone's walls, as get_next_zone (grid_1D_sphere.cpp:510-590) derives
-// them: outer wall, inner wall after the core substitution, and (batched
-// models, from their neighbour tables) inner and outer neighbour and whether
-// the inner wall is r = 0 of zone 0 (no inner wall).  One model's
-// neighbours follow from the zone index and the inner wall (next_zone).
+// them: outer wall and inner wall after the core substitution, held for the
+// zone visit.  The neighbours are formed where next_zone needs them: from
+// the zone index and the inner wall for one model, from the batch's
+// neighbour table (inner and outer neighbour, whether the inner wall is
+// r = 0 of zone 0) for a batch.
 struct Walls {
   double r_o, r_i;
-  int in_nbr, out_nbr;
-  bool no_inner;
 };
 
 template <int BATCH>
@@ -73,16 +72,10 @@ __device__ __forceinline__ Walls zone_walls(const StepArgs& A, const GridDev& G,
   Walls w;
   w.r_o = __ldg(G.r_out.right + i);
   if constexpr (BATCH) {
-    const int4 nb = __ldg(A.zone_nbr + i);
     w.r_i = __ldg(A.zone_rin + i);
-    w.in_nbr = nb.x;
-    w.out_nbr = nb.y;
-    w.no_inner = nb.z != 0;
   } else {
     w.r_i = (i != 0) ? __ldg(G.r_out.right + i - 1) : G.r_out.min;
     if (A.core_radius >= w.r_i) w.r_i = A.core_radius;
-    w.in_nbr = w.out_nbr = 0;
-    w.no_inner = false;
   }
   return w;
 }
@@ -96,9 +89,10 @@ __device__ __forceinline__ int next_zone(const StepArgs& A, const GridDev& G, co
   int in_nbr, out_nbr;
   bool no_inner;
   if constexpr (BATCH) {
-    in_nbr = w.in_nbr;
-    out_nbr = w.out_nbr;
-    no_inner = w.no_inner;
+    const int4 nb = __ldg(A.zone_nbr + iz);
+    in_nbr = nb.x;
+    out_nbr = nb.y;
+    no_inner = nb.z != 0;
   } else {  // the inner wall is the core's when the substitution moved it there
     in_nbr = (iz == 0 || w.r_i == A.core_radius) ? -1 : iz - 1;
     out_nbr = (iz + 1 == G.nzones) ? -2 : iz + 1;
