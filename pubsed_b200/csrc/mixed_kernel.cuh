@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       }
       nxt_bin = -1;
     } else {
-      i_nu = loc_within_fast<true>(A.nu, p.nu * dshift);
+      i_nu = loc_within_mixed(A.nu, p.nu * dshift);
       ab = __ldg(opac + (size_t)iz * nn + i_nu);
       dnu_num = (float)(loc_delta(A.nu, i_nu) * A.ct);
     }

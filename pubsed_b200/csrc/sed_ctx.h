@@ -238,6 +238,7 @@ inline DevLoc dev_loc(const HostLoc& h, const DevBuf<double>& d)
   if (h.type == LOC_LOG && h.del > 0) g.inv_step = (float)(1.0 / std::log2(1.0 + h.del));
   else if (h.type == LOC_LIN && h.del > 0) g.inv_step = (float)(1.0 / h.del);
   g.lmin_step = (h.type == LOC_LOG && h.min > 0) ? (float)(std::log2(h.min) * g.inv_step) : 0.f;
+  g.inv_min = (h.type == LOC_LOG && h.min > 0) ? (float)(1.0 / h.min) : 0.f;
   return g;
 }
 
