@@ -99,11 +99,12 @@ __device__ __forceinline__ int next_zone(const StepArgs& A, const GridDev& G, co
     no_inner = (iz == 0) && (w.r_i == 0);
   }
   const double l_out = sqrt_nr(fma(xd, xd, fma(w.r_o, w.r_o, -rsq))) - xd;
-  double l_in = -1;
-  if (!no_inner && xd < 0) {
-    const double rad = fma(xd, xd, fma(w.r_i, w.r_i, -rsq));
-    if (rad >= 0) l_in = -xd - sqrt_nr(rad);
-  }
+  // the inner wall's distance for every lane (a warp nearly always holds
+  // inward and outward photons), kept where the photon moves inward and
+  // meets it
+  const double rad = fma(xd, xd, fma(w.r_i, w.r_i, -rsq));
+  const double l_in_c = -xd - sqrt_nr(fmax(rad, 0.0));
+  const double l_in = (!no_inner && xd < 0 && rad >= 0) ? l_in_c : -1.0;
   constexpr double tiny_offset = 1 + 1e-6;
   constexpr double inv_tiny_offset = 1 / tiny_offset;
   if ((l_out < l_in) || (l_in < 0)) {
