@@ -787,6 +787,17 @@ static int transport_impl(sed_ctx* c, double dt, sed_step_stats* stats, float ms
     CK(c->d_em_tau.resize((size_t)n_emit));
     A.em_state = c->d_em_state.p; A.em_ind = c->d_em_ind.p; A.em_tau = c->d_em_tau.p; A.em_n = n_emit;
   }
+  if (mixed_1d_path(A, G)) {
+    // the 1D mixed kernel adds each zone visit's tallies to one of n_rep
+    // global copies (block b to copy b % n_rep, fire-and-forget reductions),
+    // which the finish kernel sums: against the per-block shared-memory
+    // copies, whose atomic adds hold the warp, the Type Ia packet kernel ran
+    // 563 ms against 587 ms
+    const int n_rep = (int)std::min<size_t>(32, std::max<size_t>(1, (size_t(256) << 20) / (5 * sizeof(double) * nz)));
+    CK(c->d_zone_rep.resize((size_t)n_rep * 5 * nz));
+    CK(cudaMemsetAsync(c->d_zone_rep.p, 0, (size_t)n_rep * 5 * nz * sizeof(double), c->stream));
+    A.smem_zones = 0; A.n_rep = n_rep; A.zone_rep = c->d_zone_rep.p;
+  }
   CK(cudaEventRecord(c->ev[3], c->stream));
   if (A.n_packets > 0) launches += launch_propagate(A, G, c->num_sms, c->stream);
   CK(cudaGetLastError());
@@ -1130,6 +1141,8 @@ void sed_ctx_destroy(sed_ctx* c)
   c->d_q_ind.release(); c->d_reject.release(); c->d_q_n.release();
   c->d_rec_type.release(); c->d_census_state.release(); c->d_census_ind.release(); c->d_census_type.release();
   c->d_q_type.release(); c->d_cmp.release(); c->d_scan_tmp.release(); c->d_cmp_count.release();
+  c->d_rho_scale.release(); c->d_opac_base.release(); c->d_imd_p.release(); c->d_zone_rep.release();
+  c->d_em_state.release(); c->d_em_ind.release(); c->d_em_tau.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -120,6 +120,7 @@ struct sed_ctx {
   // tables
   bool have_opacity = false;
   DevBuf<unsigned char> d_opac, d_cdf, d_cdf_coarse;
+  DevBuf<double> d_zone_rep;          // [n_rep][5][nz] zone-scalar tally copies of the 1D mixed kernel
   DevBuf<double> d_rho_scale;         // per-zone extinction factors of the last scaling
   DevBuf<unsigned char> d_opac_base;  // the built {abs, scat} tables while scaled ones are in d_opac
   bool opac_base_valid = false;       // d_opac_base holds the tables of the last build or load

@@ -1022,6 +1022,15 @@ __global__ void finish_zones_kernel(const StepArgs A, const double* __restrict__
 {
   const int iz = blockIdx.x;
   if (iz >= nz) return;
+  if (!A.smem_zones && A.n_rep > 0) {  // add the zone-scalar tally copies
+    if (threadIdx.x < 5) {
+      double sum = 0;
+      for (int r = 0; r < A.n_rep; ++r) sum += A.zone_rep[((size_t)r * 5 + threadIdx.x) * nz + iz];
+      double* dst[5] = {A.e_abs, A.fx, A.fy, A.fz, A.fr};
+      dst[threadIdx.x][iz] += sum;
+    }
+    __syncthreads();
+  }
   const double fac = do_rescale ? rescale_factor(A.counters[C_ESCAPED], n_active) : 1.0;
   finish_zone(A, vol, iz, fac, do_rescale);
 }
