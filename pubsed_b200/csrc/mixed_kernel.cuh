@@ -42,6 +42,13 @@
 //    not the state it carries).
 //  * The zone's walls are loaded once per zone visit, |x|^2 and x.D once
 //    per move.
+//  * The frequency bin comes from the FP32 index estimate where it lies
+//    clear of a wall (loc_within_mixed), and after a redistribution from the
+//    interaction itself, with its opacity loaded there.
+//  * 64 registers, 32 warps per SM: the zone-visit tally sums and the state
+//    a packet reads only at its start or end sit in each thread's slots of
+//    shared memory, and a visit's sums go to one of 32 global tally copies
+//    by fire-and-forget reductions.
 namespace mixed {
 
 constexpr float W32 = 2.3283064365386963e-10f;  // 2^-32
