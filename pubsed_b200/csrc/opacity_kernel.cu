@@ -258,8 +258,10 @@ struct LevView {
 // Level populations come from the LTE solve, floored at 1e-30, so they are
 // normal FP32 numbers and the reference's n_l < DBL_MIN skip never applies
 // to them; a NaN term is skipped as in the reference.
+constexpr int LINE_SUM_WARPS = 8;  // line_sum_kernel runs 256 threads per CTA
+
 template <bool MIXED, bool FUZZ, int ZT>
-__global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, double* S, double* Se)
+__global__ void __launch_bounds__(32 * LINE_SUM_WARPS) line_sum_kernel(const OpacityArgs A, double* S, double* Se)
 {
   using V = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ double lsm[];
@@ -302,78 +304,107 @@ __global__ void __launch_bounds__(256) line_sum_kernel(const OpacityArgs A, doub
   const double time = A.time;
   // a warp per bin: its 32 lanes are ZT zones x LS line slots; slot s takes
   // the bin's lines s, s + LS, ..., so the lanes of a warp run the same
-  // number of lines (up to one) and read the same few line records
+  // number of lines (up to one) and read the same few line records.  The
+  // warp stages the bin's records 32 at a time in its shared-memory buffer,
+  // one coalesced load per lane, and the slots read them from there: one
+  // memory round trip per 32 records instead of one per LS (48^3 level-line
+  // build 61.2 -> 48.5 ms, Type Ia fuzz-line build 5.2 -> 5.0 ms).  The
+  // line loop is unrolled by two (Type Ia 6.9 -> 5.4 ms before the staging).
   constexpr int LS = 32 / ZT;
+  static_assert(32 % LS == 0, "a slot keeps its lines across the 32-record chunks");
   const int lane = tid & 31, warp = tid >> 5, nwarps = bd >> 5;
   const int zi = lane % ZT, slot = lane / ZT;
-  // the line loop unrolled by two keeps two records' loads in flight (Type Ia
-  // fuzz-line build 6.9 -> 5.4 ms, 48^3 level-line build 63.8 -> 61.3 ms;
-  // by four: 5.4 and 62.4 ms)
+  using CRec = typename std::conditional<MIXED, typename std::conditional<FUZZ, float4, float2>::type, double2>::type;
+  __shared__ int4 s_ix[LINE_SUM_WARPS][32];
+  __shared__ CRec s_cr[LINE_SUM_WARPS][32];
+  __shared__ double s_h[(FUZZ && !MIXED) ? LINE_SUM_WARPS : 1][32];
+  const int4* __restrict__ ix_g = FUZZ ? A.fz_ia : A.ln_lv;
+  const CRec* __restrict__ cr_g;
+  if constexpr (MIXED) {
+    if constexpr (FUZZ) cr_g = A.fz_c32; else cr_g = A.ln_c32;
+  } else {
+    cr_g = FUZZ ? A.fz_c : A.ln_c;
+  }
   for (int jj = warp; jj < nn; jj += nwarps) {
     const int j = __ldg(order + jj);
     double acc = 0, acce = 0;
     float ks = 0.f, kc = 0.f, kse = 0.f, kce = 0.f;  // the mixed form's FP32 Kahan sums
-    const int k1 = seg[j + 1];
-#pragma unroll 2
-    for (int k = seg[j] + slot; k < k1; k += LS) {
-      int atom;
-      V term;
-      if constexpr (!FUZZ) {
-        // tau = n_l n_atom sigma_tot f lambda t (1 - n_u g_l / (n_l g_u)), 0 past the laser limit
-        const int4 lv = __ldg(A.ln_lv + k);
-        atom = lv.w;
-        const V pl = pop[(size_t)lv.x * ZT + zi];   // n_l n_atom
-        const V il = ipop[(size_t)lv.x * ZT + zi];  // 1 / (n_l n_atom)
-        const V pu = pop[(size_t)lv.y * ZT + zi];   // n_u n_atom
-        if constexpr (MIXED) {
-          const float2 c = __ldg(A.ln_c32 + k);
-          const float r = pu * il * c.y;
-          const float tau = (r > 1.f) ? 0.f : pl * (c.x * (float)time) * (1.f - r);
-          const float t = sobolev_term32(tau);
-          term = (t == t) ? t : 0.f;
-        } else {
-          const double2 c = __ldg(A.ln_c + k);
-          double t = 0;
-          if (!(pl < DBL_MIN)) {
-            const double r = pu * il * c.y;
-            const double tau = (r > 1) ? 0.0 : pl * c.x * time * (1 - r);
-            t = sobolev_term(tau);
-            if (isnan(t)) t = 0;
-          }
-          term = t;
-        }
-      } else {
-        // n_l = n_ion exp(-E_l/kT) / Z_ion, tau = sigma_tot lambda n_l gf (1 - exp(-h nu/kT)) t
-        const int4 ia = __ldg(A.fz_ia + k);
-        atom = ia.z;
-        const V pi = pop[(size_t)ia.x * ZT + zi];
-        if constexpr (MIXED) {
-          const float4 c = __ldg(A.fz_c32 + k);
-          const float stim = one_minus_exp32(c.z * invT[zi]);
-          const float tau = (c.x * (float)time) * pi * __expf(-c.y * invT[zi]) * stim;
-          term = sobolev_term32(tau);
-        } else {
-          const double2 c = __ldg(A.fz_c + k);
-          const double h = __ldg(A.fz_h + k);
-          if (zi < nzt) {
-            const double temp = A.temp_c[z0 + zi];
-            const double nl = pi * exp(-c.y / temp);
-            const double stim_cor = (1 - exp(-h / temp));
-            const double tau = c.x * nl * stim_cor * time;
-            term = sobolev_term(tau);
-          } else {
-            term = 0;
-          }
-        }
+    const int k0 = seg[j], k1 = seg[j + 1];
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int nk = min(32, k1 - kb);
+      __syncwarp();
+      if (lane < nk) {
+        s_ix[warp][lane] = __ldg(ix_g + kb + lane);
+        s_cr[warp][lane] = __ldg(cr_g + kb + lane);
+        if constexpr (FUZZ && !MIXED) s_h[warp][lane] = __ldg(A.fz_h + kb + lane);
       }
-      if constexpr (MIXED) {
-        // Kahan (compensated) summation in FP32: the rounding error of each
-        // addition is carried into the next term
-        { const float y = term - kc; const float t = ks + y; kc = (t - ks) - y; ks = t; }
-        if (want_e) { const float y = term * epsv[atom] - kce; const float t = kse + y; kce = (t - kse) - y; kse = t; }
-      } else {
-        acc += (double)term;
-        if (want_e) acce += (double)(term * epsv[atom]);
+      __syncwarp();
+#pragma unroll 2
+      for (int kk = slot; kk < nk; kk += LS) {
+        int atom;
+        V term;
+        if constexpr (!FUZZ) {
+          // tau = n_l n_atom sigma_tot f lambda t (1 - n_u g_l / (n_l g_u)), 0 past the laser limit
+          const int4 lv = s_ix[warp][kk];
+          atom = lv.w;
+          const V pl = pop[(size_t)lv.x * ZT + zi];   // n_l n_atom
+          const V il = ipop[(size_t)lv.x * ZT + zi];  // 1 / (n_l n_atom)
+          const V pu = pop[(size_t)lv.y * ZT + zi];   // n_u n_atom
+          if constexpr (MIXED) {
+            const float2 c = s_cr[warp][kk];
+            const float r = pu * il * c.y;
+            const float tau = (r > 1.f) ? 0.f : pl * (c.x * (float)time) * (1.f - r);
+            const float t = sobolev_term32(tau);
+            term = (t == t) ? t : 0.f;
+          } else {
+            const double2 c = s_cr[warp][kk];
+            double t = 0;
+            if (!(pl < DBL_MIN)) {
+              const double r = pu * il * c.y;
+              const double tau = (r > 1) ? 0.0 : pl * c.x * time * (1 - r);
+              t = sobolev_term(tau);
+              if (isnan(t)) t = 0;
+            }
+            term = t;
+          }
+        } else {
+          // n_l = n_ion exp(-E_l/kT) / Z_ion, tau = sigma_tot lambda n_l gf (1 - exp(-h nu/kT)) t
+          const int4 ia = s_ix[warp][kk];
+          atom = ia.z;
+          const V pi = pop[(size_t)ia.x * ZT + zi];
+          if constexpr (MIXED) {
+            const float4 c = s_cr[warp][kk];
+            const float stim = one_minus_exp32(c.z * invT[zi]);
+            const float tau = (c.x * (float)time) * pi * __expf(-c.y * invT[zi]) * stim;
+            term = sobolev_term32(tau);
+          } else {
+            const double2 c = s_cr[warp][kk];
+            const double h = s_h[warp][kk];
+            if (zi < nzt) {
+              const double temp = A.temp_c[z0 + zi];
+              const double nl = pi * exp(-c.y / temp);
+              const double stim_cor = (1 - exp(-h / temp));
+              const double tau = c.x * nl * stim_cor * time;
+              term = sobolev_term(tau);
+            } else {
+              term = 0;
+            }
+          }
+        }
+        if constexpr (MIXED) {
+          // Kahan (compensated) summation in FP32: the rounding error of each
+          // addition is carried into the next term
+          { const float y = term - kc; const float t = ks + y; kc = (t - ks) - y; ks = t; }
+          if (want_e) {
+            const float y = term * epsv[atom] - kce;
+            const float t = kse + y;
+            kce = (t - kse) - y;
+            kse = t;
+          }
+        } else {
+          acc += (double)term;
+          if (want_e) acce += (double)(term * epsv[atom]);
+        }
       }
     }
     if constexpr (MIXED) { acc = (double)ks; acce = (double)kse; }
