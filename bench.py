@@ -78,6 +78,30 @@ def captured_traffic(workload: str, n_segments: int, n_packets: int = 0):
     return None
 
 
+def captured_issue(workload: str, n_segments: int, kernel_ms: float, sm_mhz, n_sms: int):
+    """Issue rate of the packet kernel: warp instructions per segment from
+    the ncu capture in profiles/propagate_kernel_traffic.json
+    (`warp_inst_per_segment`, `smsp__inst_executed.sum` / segments) times
+    this run's segments over its kernel time, against the issue ceiling of
+    one warp instruction per cycle per scheduler (4 per SM) at the SM clock
+    sampled during the timed steps.  None without a capture or a clock."""
+    tfile = os.path.join(ROOT, "profiles", "propagate_kernel_traffic.json")
+    if not os.path.exists(tfile) or not sm_mhz or not kernel_ms:
+        return None
+    with open(tfile) as f:
+        entries = json.load(f)
+    for tr in entries if isinstance(entries, list) else [entries]:
+        if tr.get("workload") != workload or "warp_inst_per_segment" not in tr:
+            continue
+        wps = float(tr["warp_inst_per_segment"])
+        achieved = wps * float(n_segments) / (kernel_ms * 1e-3)
+        peak = 4.0 * n_sms * float(sm_mhz) * 1e6
+        return {"achieved": achieved, "peak": peak, "unit": "warp inst/s", "frac": achieved / peak,
+                "warp_inst_per_segment": wps, "peak_basis": "4 schedulers x %d SMs x %.0f MHz (sampled)" % (n_sms, sm_mhz),
+                "source": tr.get("inst_source", "profiles/propagate_kernel_traffic.json")}
+    return None
+
+
 def _env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -400,6 +424,8 @@ def main_batch(args, rank: int, world: int, local: int):
                        "kernel": "propagate_mixed_kernel (batched)", "kernel_ms": kern_ms,
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
     out["clocks"] = clk.summary()
+    out["roofline"]["issue"] = captured_issue(bw.name, last["n_segments"], kern_ms, out["clocks"].get("sm_mhz"),
+                                              torch.cuda.get_device_properties(local).multi_processor_count)
     if not args.no_cpu_baseline:
         try:
             r = reference_batch(bw, n_ref, cores)
@@ -812,6 +838,11 @@ def main():
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "clocks": clk.summary(),
     }
+    # what bounds the kernel: its tables stay in L2, so the HBM fraction
+    # above is nominal; the issue rate against the scheduler ceiling is the
+    # figure that moves with it
+    line["roofline"]["issue"] = captured_issue(w.name, last["n_segments"], kern_ms, line["clocks"].get("sm_mhz"),
+                                               torch.cuda.get_device_properties(local).multi_processor_count)
     if fp64:
         fp64["ratio_mixed_over_fp64"] = fp64["ms_per_step"] / ms_max
     eng.close()

@@ -66,9 +66,11 @@ __device__ __forceinline__ float neg_log_u(uint32_t w)
 // the zone's walls, as get_next_zone (grid_1D_sphere.cpp:510-590) derives
 // them: outer wall and inner wall after the core substitution, held for the
 // zone visit.  The neighbours are formed where next_zone needs them: from
-// the zone index and the inner wall for one model, from the batch's
-// neighbour table (inner and outer neighbour, whether the inner wall is
-// r = 0 of zone 0) for a batch.
+// the zone index and the inner wall for one model, from the signs of the
+// batch's wall table for a batch (outer wall negative past the model's last
+// zone, inner wall negative where there is no inner neighbour, -0.0 for the
+// r = 0 centre of a model's zone 0), which spares the batch a neighbour-table
+// load per segment.
 struct Walls {
   double r_o, r_i;
 };
@@ -77,10 +79,12 @@ template <int BATCH>
 __device__ __forceinline__ Walls zone_walls(const StepArgs& A, const GridDev& G, int i)
 {
   Walls w;
-  w.r_o = __ldg(G.r_out.right + i);
-  if constexpr (BATCH) {
-    w.r_i = __ldg(A.zone_rin + i);
+  if constexpr (BATCH) {  // one 16-byte load; the neighbours ride in the signs
+    const double2 rw = __ldg(A.zone_wall + i);
+    w.r_o = rw.x;
+    w.r_i = rw.y;
   } else {
+    w.r_o = __ldg(G.r_out.right + i);
     w.r_i = (i != 0) ? __ldg(G.r_out.right + i - 1) : G.r_out.min;
     if (A.core_radius >= w.r_i) w.r_i = A.core_radius;
   }
@@ -95,11 +99,11 @@ __device__ __forceinline__ int next_zone(const StepArgs& A, const GridDev& G, co
 {
   int in_nbr, out_nbr;
   bool no_inner;
-  if constexpr (BATCH) {
-    const int4 nb = __ldg(A.zone_nbr + iz);
-    in_nbr = nb.x;
-    out_nbr = nb.y;
-    no_inner = nb.z != 0;
+  if constexpr (BATCH) {  // a model's zones are consecutive; the signs mark its edges and the core
+    const bool in_edge = __double_as_longlong(w.r_i) < 0;  // the sign bit, -0.0 included
+    in_nbr = in_edge ? -1 : iz - 1;
+    out_nbr = (w.r_o < 0) ? -2 : iz + 1;
+    no_inner = in_edge && (w.r_i == 0);
   } else {  // the inner wall is the core's when the substitution moved it there
     in_nbr = (iz == 0 || w.r_i == A.core_radius) ? -1 : iz - 1;
     out_nbr = (iz + 1 == G.nzones) ? -2 : iz + 1;

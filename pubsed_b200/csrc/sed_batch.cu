@@ -33,6 +33,7 @@ struct sed_batch {
   DevBuf<BatchModel> d_models, d_sample_models;
   DevBuf<int4> d_nbr;
   DevBuf<double> d_rin, d_core_cdf, d_flux, d_click;
+  DevBuf<double2> d_wall;
   DevBuf<unsigned long long> d_model_esc;
   DevBuf<uint32_t> d_step;
   DevBuf<double> d_zone_rep;            // copies of the zone-scalar tallies (many zones)
@@ -151,7 +152,7 @@ StepArgs step_args(sed_batch* b, double dt, const BatchModel* models, int64_t to
   A.fx = c->d_fx.p; A.fy = c->d_fy.p; A.fz = c->d_fz.p; A.fr = c->d_fr.p;
   A.flux = b->d_flux.p; A.click = b->d_click.p; A.counters = c->d_counters.p;
   A.models = models; A.n_models = b->n_models; A.queue_chunk = std::max(1, b->queue_chunk);
-  A.zone_nbr = b->d_nbr.p; A.zone_rin = b->d_rin.p;
+  A.zone_nbr = b->d_nbr.p; A.zone_rin = b->d_rin.p; A.zone_wall = b->d_wall.p;
   A.model_escaped = b->d_model_esc.p; A.step_dev = b->d_step.p;
   A.n_rep = A.smem_zones ? 0 : b->n_rep;
   A.zone_rep = b->d_zone_rep.p;
@@ -249,10 +250,11 @@ int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n
   std::vector<double> r_out, vol, rho, T, eg, grey, X;
   std::vector<int4> nbr;
   std::vector<double> rin;
+  std::vector<double2> wall;
   int64_t nz_tot = 0;
   for (int m = 0; m < n_models; ++m) nz_tot += models[m].n_zones;
   if (nz_tot > INT32_MAX / 2) { sed_ctx_destroy(b->inner); delete b; return SED_ERR_ARG; }
-  r_out.reserve(nz_tot); nbr.reserve(nz_tot); rin.reserve(nz_tot);
+  r_out.reserve(nz_tot); nbr.reserve(nz_tot); rin.reserve(nz_tot); wall.reserve(nz_tot);
   b->models.resize(n_models);
   b->L_core.resize(n_models);
   const int nn = c->nu.n();
@@ -289,6 +291,7 @@ int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n
       const int outer = (i + 1 == nz) ? -2 : g + 1;
       nbr.push_back(make_int4(ind_in, outer, no_inner, m));
       rin.push_back(r_in);
+      wall.push_back(make_double2(outer == -2 ? -M.r_out[i] : M.r_out[i], ind_in == -1 ? -r_in : r_in));
     }
     BatchModel& D = b->models[m];
     D.pkt_off = pkt;
@@ -330,6 +333,7 @@ int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n
   cudaError_t e;
   if ((e = upload(c, b->d_nbr, nbr.data(), nbr.size())) != cudaSuccess) return fail(e);
   if ((e = upload(c, b->d_rin, rin.data(), rin.size())) != cudaSuccess) return fail(e);
+  if ((e = upload(c, b->d_wall, wall.data(), wall.size())) != cudaSuccess) return fail(e);
   if ((e = upload(c, b->d_core_cdf, core_cdf.data(), core_cdf.size())) != cudaSuccess) return fail(e);
   for (int m = 0; m < n_models; ++m) b->models[m].core_cdf = b->d_core_cdf.p + (size_t)m * nn;
   if ((e = b->d_models.resize(n_models)) != cudaSuccess) return fail(e);
@@ -343,10 +347,15 @@ int sed_batch_create(const sed_transport_params* common, double t_now, int32_t n
     if ((e = b->d_em_tau.resize((size_t)pkt)) != cudaSuccess) return fail(e);
     if ((e = b->d_em_model.resize((size_t)pkt)) != cudaSuccess) return fail(e);
   }
-  // zones beyond the per-block shared-memory tallies: 32 copies of the
-  // zone-scalar tallies (fewer if that would pass 256 MiB)
+  // zones beyond the per-block shared-memory tallies: 128 copies of the
+  // zone-scalar tallies (fewer if that would pass 256 MiB).  A batch's
+  // packets are drawn model by model, so the lanes in flight crowd onto the
+  // few hundred zones of one or two models and visit each for ~1.2 segments;
+  // with 32 copies their reductions queued on the same addresses (64-model
+  // batch at half its packets: packet kernel 723 ms with 32 copies, 640 ms
+  // with 128, 640 ms with 256 or 512)
   if ((size_t)5 * nz_tot * sizeof(double) > 64 * 1024) {
-    b->n_rep = (int)std::min<size_t>(32, std::max<size_t>(1, (size_t(256) << 20) / (5 * sizeof(double) * nz_tot)));
+    b->n_rep = (int)std::min<size_t>(128, std::max<size_t>(1, (size_t(256) << 20) / (5 * sizeof(double) * nz_tot)));
     if ((e = b->d_zone_rep.resize((size_t)b->n_rep * 5 * nz_tot)) != cudaSuccess) return fail(e);
   }
   if ((e = cudaMemsetAsync(b->d_step.p, 0, sizeof(uint32_t), c->stream)) != cudaSuccess) return fail(e);
@@ -650,7 +659,7 @@ void sed_batch_destroy(sed_batch* b)
   }
   drop_graph(b);
   for (auto& ev : b->ev) if (ev) cudaEventDestroy(ev);
-  b->d_models.release(); b->d_sample_models.release(); b->d_nbr.release(); b->d_rin.release();
+  b->d_models.release(); b->d_sample_models.release(); b->d_nbr.release(); b->d_rin.release(); b->d_wall.release();
   b->d_core_cdf.release(); b->d_flux.release(); b->d_click.release(); b->d_model_esc.release(); b->d_step.release();
   b->d_em_state.release(); b->d_em_ind.release(); b->d_em_tau.release(); b->d_em_model.release();
   b->d_zone_rep.release();

@@ -66,6 +66,11 @@ struct StepArgs {
   int32_t queue_chunk;               // packets a thread claims per queue pop
   const int4* zone_nbr;              // [zones] {inner neighbour or -1, outer or -2, no-inner flag, model}
   const double* zone_rin;            // [zones] inner wall after the core substitution
+  // [zones] {outer wall, inner wall after the core substitution} with the
+  // neighbours in the signs: the outer wall negative where the outer
+  // neighbour is the model's edge (-2), the inner wall negative (-0.0 for a
+  // wall at r = 0) where the inner neighbour is -1
+  const double2* zone_wall;
   unsigned long long* model_escaped; // [n_models] escaped packets per model
   uint32_t* step_dev;                // step counter on the device (advanced by the finish kernel)
   // ---- queued packets: the census, then the radioactive packets (single-context kernels) ----

@@ -1,5 +1,6 @@
-"""Host-side pieces of bench.py that need no GPU: the DRAM traffic the
-roofline line reports, read from the ncu captures under profiles/."""
+"""Host-side pieces of bench.py that need no GPU: the DRAM traffic and the
+issue rate the roofline line reports, read from the ncu captures under
+profiles/."""
 import json
 import os
 import sys
@@ -33,6 +34,22 @@ def test_every_bench_workload_with_a_capture_reports_traffic():
         else:
             assert bench.captured_traffic(e["workload"], 123) == e["dram_bytes"]
     assert bench.captured_traffic("no_such_workload", 1) is None
+
+
+def test_issue_rate_from_the_captured_instruction_count():
+    """The issue figure beside the roofline: warp instructions per segment
+    from the capture x segments / kernel time, against 4 warp instructions
+    per cycle per SM at the sampled clock."""
+    with open(os.path.join(ROOT, "profiles", "propagate_kernel_traffic.json")) as f:
+        entries = json.load(f)
+    e = next(t for t in entries if "warp_inst_per_segment" in t)
+    wps = e["warp_inst_per_segment"]
+    r = bench.captured_issue(e["workload"], 1e10, 1000.0, 2000.0, 100)
+    assert abs(r["achieved"] - wps * 1e10) < 1e-3 * wps * 1e10
+    assert r["peak"] == 4 * 100 * 2000e6
+    assert abs(r["frac"] - wps * 1e10 / 8e11) < 1e-12
+    assert bench.captured_issue(e["workload"], 1e10, 1000.0, None, 100) is None
+    assert bench.captured_issue("no_such_workload", 1e10, 1000.0, 2000.0, 100) is None
 
 
 def test_chi2_summary_of_two_spectra():
