@@ -334,21 +334,32 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
   __shared__ int s_m[BATCH ? THREADS : 1];
   __shared__ long long s_qn[BATCH ? THREADS : 1], s_qe[BATCH ? THREADS : 1];
   if constexpr (BATCH) { s_qn[tid] = 0; s_qe[tid] = 0; }
-  // the current zone visit's tallies (e_abs, fx, fy, fz, fr), summed in the
-  // thread's own column of shared memory: held in registers they cost the
-  // ten that take the kernel from 28 to 24 warps per SM (Type Ia packet
-  // kernel 631 ms against 661 ms)
-  int acc_zone = -1;
-  __shared__ double s_acc[5][THREADS];
-  auto clear_visit = [&]() {
-    s_acc[0][tid] = 0.0; s_acc[1][tid] = 0.0; s_acc[2][tid] = 0.0; s_acc[3][tid] = 0.0; s_acc[4][tid] = 0.0;
+  // zone-visit tallies (e_abs, fx, fy, fz, fr), summed in the thread's own
+  // columns of shared memory (held in registers they cost the ten that take
+  // the kernel from 28 to 24 warps per SM: Type Ia packet kernel 631 ms
+  // against 661 ms).  One model's kernel keeps two slots: the zone being
+  // visited and the zone the packet came from.  A photon that steps back
+  // over the wall it just crossed carries on with that zone's sums; only a
+  // move to a third zone sends the older slot's sums to the tally copies
+  // (Type Ia packet kernel 562 -> 551 ms).  The batched kernel keeps one
+  // slot: with two its 64-register shapes spill and its step ran 1-4 %
+  // slower.  acc holds the current zone and its slot as (zone << 1) | slot
+  // (-1 before the packet's first segment), s_oz the zone whose sums sit in
+  // the other slot (-1: none); a slot that holds no zone holds zeros.  With
+  // one slot acc is the zone itself and the slot is zeroed when a visit
+  // starts.
+  constexpr int SLOTS = BATCH ? 1 : 2;
+  int acc = -1;
+  __shared__ double s_acc[SLOTS][5][THREADS];
+  __shared__ int s_oz[SLOTS == 2 ? THREADS : 1];
+  auto flush_slot = [&](int z, int k) {  // send slot k's sums for zone z and zero the slot
+    double* a = &s_acc[k][0][tid];
+    add_visit(A, s_tal, nz, rep_off, z, a[0], a[THREADS], a[2 * THREADS], a[3 * THREADS], a[4 * THREADS]);
+    a[0] = 0.0; a[THREADS] = 0.0; a[2 * THREADS] = 0.0; a[3 * THREADS] = 0.0; a[4 * THREADS] = 0.0;
   };
-  auto flush_visit = [&]() {
-    if (acc_zone >= 0)
-      add_visit(A, s_tal, nz, rep_off, acc_zone, s_acc[0][tid], s_acc[1][tid], s_acc[2][tid], s_acc[3][tid],
-                s_acc[4][tid]);
-  };
-  clear_visit();
+  for (int k = 0; k < SLOTS; ++k)
+    for (int q = 0; q < 5; ++q) s_acc[k][q][tid] = 0.0;
+  if constexpr (SLOTS == 2) s_oz[tid] = -1;
   Walls wl{};
   double rsq = 0, xd = 0;
   float tau_rem = 0;  // optical depth left to the next interaction
@@ -374,7 +385,18 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     if (!live) continue;
     if (fate != MOVING) {
       if (have) {
-        flush_visit();
+        if constexpr (SLOTS == 2) {
+          if (acc >= 0) {
+            const int oz = s_oz[tid];
+            flush_slot(acc >> 1, acc & 1);
+            if (oz >= 0) flush_slot(oz, (acc & 1) ^ 1);
+            s_oz[tid] = -1;
+            acc = -1;
+          }
+        } else if (acc >= 0) {
+          add_visit(A, s_tal, nz, rep_off, acc, s_acc[0][0][tid], s_acc[0][1][tid], s_acc[0][2][tid],
+                    s_acc[0][3][tid], s_acc[0][4][tid]);
+        }
         atomicAdd(s_cnt + 3, (unsigned long long)seg);
         atomicAdd(s_cnt + 4, (unsigned long long)(rng.n - s_n0[tid]));
         if (fate == ESCAPED) {
@@ -458,8 +480,11 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
       else if (p.ind == -2) fate = ESCAPED;
       seg = 0;
       nxt_bin = -1;
-      acc_zone = -1;
-      clear_visit();
+      if constexpr (SLOTS == 1) {
+        acc = -1;
+        s_acc[0][0][tid] = 0.0; s_acc[0][1][tid] = 0.0; s_acc[0][2][tid] = 0.0; s_acc[0][3][tid] = 0.0;
+        s_acc[0][4][tid] = 0.0;
+      }
       have = true;
       s_n0[tid] = rng.n;
       if (fate != MOVING) continue;
@@ -470,10 +495,21 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     if (seg >= limit) { fate = STOPPED; atomicAdd(s_cnt + 5, 1ULL); continue; }
     ++seg;
     const int iz = p.ind;
-    if (iz != acc_zone) {
-      flush_visit();
-      acc_zone = iz;
-      clear_visit();
+    if (iz != (SLOTS == 2 ? (acc >> 1) : acc)) {  // a zone change (or the packet's first segment)
+      if constexpr (SLOTS == 2) {
+        const int k = (acc < 0) ? 0 : ((acc & 1) ^ 1);  // the other slot takes zone iz
+        const int oz = s_oz[tid];
+        if (oz >= 0 && oz != iz) flush_slot(oz, k);  // a third zone: the older visit's sums go out
+        s_oz[tid] = acc >> 1;                        // the zone just left keeps its slot
+        acc = (iz << 1) | k;
+      } else {
+        if (acc >= 0)
+          add_visit(A, s_tal, nz, rep_off, acc, s_acc[0][0][tid], s_acc[0][1][tid], s_acc[0][2][tid],
+                    s_acc[0][3][tid], s_acc[0][4][tid]);
+        acc = iz;
+        s_acc[0][0][tid] = 0.0; s_acc[0][1][tid] = 0.0; s_acc[0][2][tid] = 0.0; s_acc[0][3][tid] = 0.0;
+        s_acc[0][4][tid] = 0.0;
+      }
       wl = zone_walls<BATCH>(A, G, iz);
     }
     double d_bn;
@@ -521,14 +557,15 @@ __global__ void __launch_bounds__(THREADS, MINB) propagate_mixed_kernel(const St
     const double this_E = p.e * this_d;
     const double eps_imc = __ldg(A.eps_imc + iz);
     const double ed = this_E * dshift;
-    s_acc[0][tid] = fma(ed * dshift * (double)a_f, eps_imc, s_acc[0][tid]);
+    double* sa = &s_acc[SLOTS == 2 ? (acc & 1) : 0][0][tid];
+    sa[0] = fma(ed * dshift * (double)a_f, eps_imc, sa[0]);
     atomicAdd(A.J + (size_t)iz * nj + (A.store_Jnu ? i_nu : 0), this_E);
     if (A.tally_forces) {
       const double wd = ed * (double)op_f * dshift;
-      s_acc[1][tid] = fma(wd, p.D[0], s_acc[1][tid]);
-      s_acc[2][tid] = fma(wd, p.D[1], s_acc[2][tid]);
-      s_acc[3][tid] = fma(wd, p.D[2], s_acc[3][tid]);
-      s_acc[4][tid] = fma(wd * xd, rsqrt_nr(rsq), s_acc[4][tid]);
+      sa[THREADS] = fma(wd, p.D[0], sa[THREADS]);
+      sa[2 * THREADS] = fma(wd, p.D[1], sa[2 * THREADS]);
+      sa[3 * THREADS] = fma(wd, p.D[2], sa[3 * THREADS]);
+      sa[4 * THREADS] = fma(wd * xd, rsqrt_nr(rsq), sa[4 * THREADS]);
     }
     // move
     p.x[0] = fma(this_d, p.D[0], p.x[0]);
