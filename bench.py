@@ -843,6 +843,10 @@ def main():
     # figure that moves with it
     line["roofline"]["issue"] = captured_issue(w.name, last["n_segments"], kern_ms, line["clocks"].get("sm_mhz"),
                                                torch.cuda.get_device_properties(local).multi_processor_count)
+    if radio_frac > 0:
+        # the captures are of the Type Ia step without decay packets: the
+        # same kernel and tables, per-segment and per-packet figures carried over
+        line["roofline"]["captured_on"] = "type_ia_1d without decay packets"
     if fp64:
         fp64["ratio_mixed_over_fp64"] = fp64["ms_per_step"] / ms_max
     eng.close()
